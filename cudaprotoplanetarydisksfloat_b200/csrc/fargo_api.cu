@@ -1,0 +1,860 @@
+// fargo_api.cu -- the C ABI (include/fargo_b200.h): contexts, batches,
+// device memory, the per-DT CUDA graph and the host-visible operations.
+//
+// One DT (the body of AlgoGas, SourceEuler.cu:208-301) is
+//   k_dt_begin [+ adiabatic sound speed refresh]  -> stream launches
+//   WHILE(any disk inside its DT) { one substep }  -> one CUDA graph launch
+// The WHILE node's condition is written by the last kernel of the substep
+// (cudaGraphSetConditional), so the host never waits inside a DT.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fargo_internal.h"
+#include "host_internal.h"
+#include "sg.h"
+
+namespace {
+
+constexpr int kSegMax = 2048;  // rings up to this many sectors are one azimuthal segment
+constexpr int kSeg = 1024;     // segment length for wider rings
+
+struct DiskHost {
+  fargo_params p;
+  fargo_planets planets0;
+  HostTables t;
+  DiskDev dev{};  // device pointers + parameters
+  std::vector<void*> allocs;
+  SelfGravity* sg = nullptr;
+};
+
+}  // namespace
+
+struct fargo_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<DiskHost> disks;
+  BatchDev bd{};
+  DiskDev* d_disks = nullptr;
+  DiskCtl* d_ctl = nullptr;
+  long long* d_cell_off = nullptr;
+  int* d_ring_off = nullptr;
+  int4* d_theta = nullptr;
+  int* d_flags = nullptr;
+  double* d_red = nullptr;  // reduction scratch for force/diagnostic kernels
+  int red_blocks = 0;
+  int max_nsec = 0;
+  int any_adiabatic = 0;
+  int n_sg = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphConditionalHandle handle = 0;
+  bool use_graph = true;
+  long long launches = 0;
+  long long ncell_ghost = 0;
+  std::string err;
+};
+
+struct fargo_ctx {
+  fargo_batch b;
+};
+
+namespace {
+
+fargo_status set_err(fargo_batch* b, fargo_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (b) b->err = buf;
+  return st;
+}
+
+#define CK(call)                                                                               \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) {                                                                   \
+      fargo_status st_ = (e_ == cudaErrorMemoryAllocation) ? FARGO_EOOM : FARGO_ECUDA;         \
+      return set_err(b, st_, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    }                                                                                          \
+  } while (0)
+
+template <class T>
+fargo_status dalloc(fargo_batch* b, DiskHost& h, T** ptr, size_t count) {
+  void* p = nullptr;
+  CK(cudaMalloc(&p, sizeof(T) * (count ? count : 1)));
+  CK(cudaMemsetAsync(p, 0, sizeof(T) * (count ? count : 1), b->stream));
+  h.allocs.push_back(p);
+  *ptr = (T*)p;
+  return FARGO_OK;
+}
+
+template <class T>
+fargo_status dupload(fargo_batch* b, DiskHost& h, const T** ptr, const std::vector<T>& v) {
+  T* p = nullptr;
+  fargo_status st = dalloc(b, h, &p, v.size());
+  if (st) return st;
+  CK(cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, b->stream));
+  *ptr = p;
+  return FARGO_OK;
+}
+
+fargo_status check_params(fargo_batch* b, const fargo_params* p, const fargo_planets* pl) {
+  if (p->NRAD < 4 || p->NSEC < 4) return set_err(b, FARGO_EINVAL, "NRAD and NSEC must be >= 4");
+  if (p->NSEC > 16384) return set_err(b, FARGO_EINVAL, "NSEC > 16384 is not supported");
+  if (p->OpenInner || p->NonReflecting || p->Evanescent)
+    return set_err(b, FARGO_EINVAL, "InnerBoundary %s: only RIGID/WALL boundaries are implemented", p->INNERBOUNDARY);
+  if (p->SelfGravity && !p->LogGrid)
+    return set_err(b, FARGO_EINVAL, "self-gravity needs RadialSpacing LOGARITHM (Main.cu:302-306)");
+  if (p->SelfGravity && p->SGZeroMode) return set_err(b, FARGO_EINVAL, "SelfGravity Z is not implemented");
+  if (pl->nb < 0 || pl->nb > FARGO_MAXPLANETS) return set_err(b, FARGO_EINVAL, "bad planet count %d", pl->nb);
+  int nfeel = 0;
+  for (int k = 0; k < pl->nb; k++) nfeel += pl->feeldisk[k] ? 1 : 0;
+  if (nfeel > FARGO_MAXBODY - 1)
+    return set_err(b, FARGO_EINVAL, "at most %d planets may feel the disk", FARGO_MAXBODY - 1);
+  if (p->Corotating && pl->nb < 1) return set_err(b, FARGO_EINVAL, "a corotating frame needs a planet");
+  return FARGO_OK;
+}
+
+// Device memory and constant tables of one disk.
+fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
+  const fargo_params* p = &h.p;
+  host_build_tables(p, radii, &h.t);
+  DiskDev& D = h.dev;
+  std::memset(&D, 0, sizeof(D));
+  D.nrad = p->NRAD;
+  D.nsec = p->NSEC;
+  D.DT = p->DT;
+  D.ADIABATICINDEX = p->ADIABATICINDEX;
+  D.ASPECTRATIO = p->ASPECTRATIO;
+  D.FLARINGINDEX = p->FLARINGINDEX;
+  D.SIGMASLOPE = p->SIGMASLOPE;
+  D.SIGMA0 = p->SIGMA0;
+  D.TRANSITIONRADIUS = p->TRANSITIONRADIUS;
+  D.TRANSITIONRATIO = p->TRANSITIONRATIO;
+  D.TRANSITIONWIDTH = p->TRANSITIONWIDTH;
+  D.LAMBDADOUBLING = p->LAMBDADOUBLING;
+  D.VISCOSITY = p->VISCOSITY;
+  D.ALPHAVISCOSITY = p->ALPHAVISCOSITY;
+  D.CAVITYRADIUS = p->CAVITYRADIUS;
+  D.CAVITYRATIO = p->CAVITYRATIO;
+  D.CAVITYWIDTH = p->CAVITYWIDTH;
+  D.MASSTAPER = p->MASSTAPER;
+  D.RELEASEDATE = p->RELEASEDATE;
+  D.RELEASERADIUS = p->RELEASERADIUS;
+  D.THICKNESSSMOOTHING = p->THICKNESSSMOOTHING;
+  D.ROCHESMOOTHING = p->ROCHESMOOTHING;
+  D.IMPOSEDDISKDRIFT = p->IMPOSEDDISKDRIFT;
+  D.Adiabatic = p->Adiabatic;
+  D.Cooling = p->Cooling;
+  D.ViscosityAlpha = p->ViscosityAlpha;
+  D.FastTransport = p->FastTransport;
+  D.Indirect_Term = p->Indirect_Term;
+  D.ExcludeHill = p->ExcludeHill;
+  D.ForcedCircular = p->ForcedCircular;
+  D.Corotating = p->Corotating;
+  D.GuidingCenter = p->GuidingCenter;
+  D.RocheSmoothing = p->RocheSmoothing;
+  D.SelfGravity = p->SelfGravity;
+  D.Evanescent = p->Evanescent;
+  D.OpenInner = p->OpenInner;
+  D.SloppyCFL = p->SloppyCFL;
+  D.IsDisk = p->IsDisk;
+  D.invdphi = h.t.invdphi;
+  D.onethird = h.t.onethird;
+  size_t ng = (size_t)(p->NRAD + 1) * p->NSEC;
+  size_t n1 = (size_t)p->NRAD + 1;
+  fargo_status st;
+#define A(ptr, n)                          \
+  if ((st = dalloc(b, h, &(ptr), (n)))) \
+    return st;
+  A(D.dens, ng) A(D.vrad, ng) A(D.vtheta, ng) A(D.energy, ng) A(D.vri, ng) A(D.vti, ng) A(D.trr, ng)
+  A(D.tpp, ng) A(D.trp, ng) A(D.qplus, ng) A(D.a0, ng) A(D.a1, ng) A(D.a2, ng) A(D.a3, ng) A(D.a4, ng)
+  if (p->Adiabatic) {
+    A(D.cs, ng) A(D.a5, ng)
+  } else {
+    D.cs = nullptr;
+    D.a5 = D.a4;  // never written in isothermal runs
+  }
+  A(D.pres, ng)
+  A(D.visc, n1) A(D.cs_ring, n1) A(D.csmean, n1) A(D.vmoy, n1) A(D.ringmin, n1) A(D.nshift, n1)
+  A(D.log_nshift, (size_t)FARGO_MAXLOG * p->NRAD) A(D.partials, n1 * 4 * FARGO_MAXBODY)
+  float *cp, *sp, *cc, *sc;
+  A(cp, (size_t)p->NSEC) A(sp, (size_t)p->NSEC) A(cc, (size_t)p->NSEC) A(sc, (size_t)p->NSEC)
+#undef A
+  D.cos_pot = cp;
+  D.sin_pot = sp;
+  D.cos_cell = cc;
+  D.sin_cell = sc;
+#define U(ptr, vec)                            \
+  if ((st = dupload(b, h, &(ptr), (vec)))) \
+    return st;
+  U(D.Rinf, h.t.Rinf) U(D.Rsup, h.t.Rsup) U(D.Rmed, h.t.Rmed) U(D.Surf, h.t.Surf) U(D.invRinf, h.t.invRinf)
+  U(D.invSurf, h.t.invSurf) U(D.invRmed, h.t.invRmed) U(D.invdiffRsup, h.t.invdiffRsup)
+  U(D.invdiffRmed, h.t.invdiffRmed) U(D.dxtheta, h.t.dxtheta) U(D.supp_torque, h.t.supp_torque)
+  U(D.SigmaMed, h.t.SigmaMed) U(D.SigmaInf, h.t.SigmaInf) U(D.EnergyMed, h.t.EnergyMed)
+  U(D.CoolingTimeMed, h.t.CoolingTimeMed) U(D.pow15, h.t.pow15)
+#undef U
+  // QplusMed is filled at initialisation (it needs the viscosity)
+  float* qpm;
+  if ((st = dalloc(b, h, &qpm, n1))) return st;
+  D.QplusMed = qpm;
+  if (p->SelfGravity) {
+    st = sg_create(&h.sg, p, h.t, b->stream, &D, b->err);
+    if (st) return st;
+  }
+  return FARGO_OK;
+}
+
+DiskCtl ctl_header(const fargo_batch* b, int d, cudaError_t* e) {
+  DiskCtl c;
+  *e = cudaMemcpy(&c, b->d_ctl + d, offsetof(DiskCtl, log_dt), cudaMemcpyDeviceToHost);
+  return c;
+}
+
+fargo_status put_ctl_header(fargo_batch* b, int d, const DiskCtl& c) {
+  CK(cudaMemcpyAsync(b->d_ctl + d, &c, offsetof(DiskCtl, log_dt), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return FARGO_OK;
+}
+
+void planets_to_ctl(const fargo_planets* pl, DiskCtl* c) {
+  c->nb = pl->nb;
+  for (int k = 0; k < pl->nb; k++) {
+    c->mass[k] = pl->mass[k];
+    c->x[k] = pl->x[k];
+    c->y[k] = pl->y[k];
+    c->vx[k] = pl->vx[k];
+    c->vy[k] = pl->vy[k];
+    c->feeldisk[k] = pl->feeldisk[k];
+    c->feelothers[k] = pl->feelothers[k];
+  }
+}
+
+void ctl_to_planets(const DiskCtl& c, const fargo_planets& names, fargo_planets* out) {
+  *out = names;
+  out->nb = c.nb;
+  for (int k = 0; k < c.nb; k++) {
+    out->mass[k] = c.mass[k];
+    out->x[k] = c.x[k];
+    out->y[k] = c.y[k];
+    out->vx[k] = c.vx[k];
+    out->vy[k] = c.vy[k];
+    out->feeldisk[k] = c.feeldisk[k];
+    out->feelothers[k] = c.feelothers[k];
+  }
+}
+
+// The initialisation part of main() between InitGasDensity and the DT loop
+// (Main.cu:292-344): self-gravity start-up, OmegaFrame, InitEuler's sound
+// speed, viscosity and velocities.  dens/energy: NULL = the reference's
+// axisymmetric profiles (InitGasDensity / InitGasEnergy, Pframeforce.cu:173-192).
+fargo_status init_disk_state(fargo_batch* b, int d, const float* dens, const float* energy) {
+  DiskHost& h = b->disks[d];
+  DiskDev& D = h.dev;
+  const fargo_params* p = &h.p;
+  const int nrad = p->NRAD, nsec = p->NSEC;
+  const size_t ng = (size_t)(nrad + 1) * nsec;
+  std::vector<float> S(ng, 0.0f), E(ng, 0.0f);
+  for (int i = 0; i < nrad; i++)
+    for (int j = 0; j < nsec; j++) {
+      S[(size_t)i * nsec + j] = h.t.SigmaMed[i];
+      if (p->Adiabatic) E[(size_t)i * nsec + j] = h.t.EnergyMed[i];
+    }
+  if (dens) std::memcpy(S.data(), dens, sizeof(float) * ng);
+  if (energy) std::memcpy(E.data(), energy, sizeof(float) * ng);
+  CK(cudaMemcpyAsync(D.dens, S.data(), sizeof(float) * ng, cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(D.energy, E.data(), sizeof(float) * ng, cudaMemcpyHostToDevice, b->stream));
+  float* scratch[] = {D.vrad, D.vtheta, D.vri, D.vti, D.trr, D.tpp, D.trp, D.qplus, D.a0, D.a1, D.a2, D.a3, D.a4};
+  for (float* f : scratch) CK(cudaMemsetAsync(f, 0, sizeof(float) * ng, b->stream));
+  // scalars and planets
+  DiskCtl c;
+  std::memset(&c, 0, offsetof(DiskCtl, log_dt));
+  fargo_planets pl = h.planets0;
+  c.PhysicalTime = 0.0f;
+  c.PhysicalTimeInitial = 0.0f;
+  planets_to_ctl(&pl, &c);
+  D.HillRadius = pl.nb > 0 ? (float)(pl.x[0] * std::pow(pl.mass[0] / 3., 1. / 3.)) : 0.0f;  // Psys.cu:206
+  fargo_status st;
+  if ((st = put_ctl_header(b, d, c))) return st;
+  CK(cudaMemcpy(b->d_disks + d, &D, sizeof(DiskDev), cudaMemcpyHostToDevice));
+  if (p->SelfGravity) {
+    // compute_selfgravity(init) + Init_planetarysys_withSG (Main.cu:302-329)
+    st = sg_accelerations(h.sg, b->bd, d, &D, b->stream, b->err);
+    if (st) return st;
+    std::vector<float> axi(nrad);
+    st = sg_axisymmetric(h.sg, &D, axi.data(), b->stream, b->err);
+    if (st) return st;
+    for (int k = 0; k < pl.nb; k++) {
+      float r, dist, ri, rip1, dr, sgacc;
+      int ipl;
+      r = pl.x[k];
+      dist = (float)(r / (1. + p->ECCENTRICITY));
+      ipl = 0;
+      while (h.t.Rmed[ipl] <= dist) ipl++;
+      ri = h.t.Rmed[ipl];
+      rip1 = h.t.Rmed[ipl + 1];
+      dr = rip1 - ri;
+      sgacc = (dist - ri) * axi[ipl + 1] + (rip1 - dist) * axi[ipl];
+      sgacc /= dr;
+      pl.vy[k] *= (float)sqrtf(1. - dist * dist * sgacc);
+    }
+    planets_to_ctl(&pl, &c);
+    // Init_azimutalvelocity_withSG (SourceEuler.cu:428-437)
+    st = sg_init_vtheta(h.sg, &D, axi.data(), b->stream, b->err);
+    if (st) return st;
+  }
+  // OmegaFrame (Main.cu:332-333)
+  c.OmegaFrame = p->OMEGAFRAME;
+  if (p->Corotating) c.OmegaFrame = host_get_psys_frequency(&pl);
+  if ((st = put_ctl_header(b, d, c))) return st;
+  // InitEuler's ComputeSoundSpeed, then Make1Dprofile(1) (SourceEuler.cu:199, Pframeforce.cu:242-245)
+  fargo_launch_cs_isothermal(b->bd, d, b->stream);
+  fargo_launch_cs_refresh(b->bd, d, b->stream);
+  CK(cudaGetLastError());
+  std::vector<float> csmean(nrad + 1, 0.0f);
+  CK(cudaMemcpyAsync(csmean.data(), D.csmean, sizeof(float) * (nrad + 1), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  // InitVelocities' viscosity table (Pframeforce.cu:262-265) and FillQplus (Theo.cu:299-311)
+  std::vector<float> visc(nrad + 1, 0.0f), qpm(nrad + 1, 0.0f);
+  for (int i = 0; i < nrad; i++) visc[i] = host_fviscosity(p, h.t, csmean.data(), h.t.Rmed[i], 0.0f, 0.0f);
+  visc[nrad] = host_fviscosity(p, h.t, csmean.data(), h.t.Rmed[nrad - 1], 0.0f, 0.0f);
+  if (p->Cooling)
+    for (int i = 0; i < nrad; i++) {
+      float r = h.t.Rmed[i];
+      float vis = host_fviscosity(p, h.t, csmean.data(), r, 0.0f, 0.0f);
+      qpm[i] = 2.25 * vis * p->SIGMA0 * std::pow(r, -p->SIGMASLOPE - 3.0);
+    }
+  CK(cudaMemcpyAsync(D.visc, visc.data(), sizeof(float) * (nrad + 1), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync((void*)D.QplusMed, qpm.data(), sizeof(float) * (nrad + 1), cudaMemcpyHostToDevice, b->stream));
+  // constant sub-Keplerian speeds
+  D.vkep_const = (!p->SelfGravity && p->LAMBDADOUBLING == 0.0f) ? 1 : 0;
+  if (D.vkep_const) {
+    double vin, vout;
+    host_vkep(p, h.t, 0.0f, 0.0f, &vin, &vout);
+    D.VKepIn = (float)vin;
+    D.VKepOut = (float)vout;
+  }
+  CK(cudaMemcpyAsync(b->d_disks + d, &D, sizeof(DiskDev), cudaMemcpyHostToDevice, b->stream));
+  // InitGasVelocitiesKernel
+  fargo_launch_init_velocities(b->bd, d, (long long)(nrad + 1) * nsec, b->stream);
+  CK(cudaGetLastError());
+  // pressure of the initial state for the isothermal temperature output
+  CK(cudaStreamSynchronize(b->stream));
+  return FARGO_OK;
+}
+
+fargo_status build_graph(fargo_batch* b) {
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if (!b->use_graph) return FARGO_OK;
+  CK(cudaGraphCreate(&b->graph, 0));
+  CK(cudaGraphConditionalHandleCreate(&b->handle, b->graph, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = b->handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, b->graph, nullptr, 0, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  CK(cudaStreamBeginCaptureToGraph(b->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  for (int d = 0; d < (int)b->disks.size(); d++)
+    if (b->disks[d].sg) sg_capture_substep(b->disks[d].sg, b->bd, d, &b->disks[d].dev, b->stream);
+  fargo_launch_substep(b->bd, b->handle, 1, b->stream, b->max_nsec, nullptr);
+  cudaError_t ec = cudaStreamEndCapture(b->stream, &body);
+  if (ec != cudaSuccess) return set_err(b, FARGO_ECUDA, "graph capture: %s", cudaGetErrorString(ec));
+  CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  return FARGO_OK;
+}
+
+fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, const fargo_planets* planets,
+                          const double* const* radii, int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_err(b, FARGO_ENODEV, "no CUDA device available");
+  if (device < 0) CK(cudaGetDevice(&device));
+  CK(cudaSetDevice(device));
+  b->device = device;
+  CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  b->disks.resize(n);
+  std::vector<long long> cell_off(n + 1, 0);
+  std::vector<int> ring_off(n + 1, 0);
+  std::vector<int4> theta;
+  int seg_max = 0;
+  for (int d = 0; d < n; d++) {
+    fargo_status st = check_params(b, &params[d], &planets[d]);
+    if (st) return st;
+    DiskHost& h = b->disks[d];
+    h.p = params[d];
+    h.planets0 = planets[d];
+    st = alloc_disk(b, h, radii ? radii[d] : nullptr);
+    if (st) return st;
+    int nrad = h.p.NRAD, nsec = h.p.NSEC;
+    h.dev.cell0 = cell_off[d];
+    h.dev.ring0 = ring_off[d];
+    cell_off[d + 1] = cell_off[d] + (long long)nrad * nsec;
+    ring_off[d + 1] = ring_off[d] + nrad;
+    b->ncell_ghost += (long long)(nrad + 1) * nsec;
+    b->max_nsec = std::max(b->max_nsec, nsec);
+    b->any_adiabatic |= h.p.Adiabatic;
+    b->n_sg += h.p.SelfGravity ? 1 : 0;
+    for (int i = 0; i < nrad; i++) {
+      if (nsec <= kSegMax) {
+        theta.push_back(make_int4(d, i, 0, nsec));
+        seg_max = std::max(seg_max, nsec);
+      } else {
+        for (int j0 = 0; j0 < nsec; j0 += kSeg) {
+          int S = std::min(kSeg, nsec - j0);
+          theta.push_back(make_int4(d, i, j0, S));
+          seg_max = std::max(seg_max, S);
+        }
+      }
+    }
+  }
+  CK(cudaMalloc(&b->d_disks, sizeof(DiskDev) * n));
+  CK(cudaMalloc(&b->d_ctl, sizeof(DiskCtl) * n));
+  CK(cudaMemsetAsync(b->d_ctl, 0, sizeof(DiskCtl) * n, b->stream));
+  CK(cudaMalloc(&b->d_cell_off, sizeof(long long) * (n + 1)));
+  CK(cudaMalloc(&b->d_ring_off, sizeof(int) * (n + 1)));
+  CK(cudaMalloc(&b->d_theta, sizeof(int4) * theta.size()));
+  CK(cudaMalloc(&b->d_flags, sizeof(int) * 4));
+  b->red_blocks = 296;
+  CK(cudaMalloc(&b->d_red, sizeof(double) * b->red_blocks * 4 * FARGO_DIMFXY));
+  CK(cudaMemcpyAsync(b->d_cell_off, cell_off.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_ring_off, ring_off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_theta, theta.data(), sizeof(int4) * theta.size(), cudaMemcpyHostToDevice, b->stream));
+  for (int d = 0; d < n; d++) b->disks[d].dev.ctl = b->d_ctl + d;
+  for (int d = 0; d < n; d++)
+    CK(cudaMemcpyAsync(b->d_disks + d, &b->disks[d].dev, sizeof(DiskDev), cudaMemcpyHostToDevice, b->stream));
+  BatchDev& bd = b->bd;
+  bd.ndisk = n;
+  bd.ncell = cell_off[n];
+  bd.nring = ring_off[n];
+  bd.cell_off = b->d_cell_off;
+  bd.ring_off = b->d_ring_off;
+  bd.disks = b->d_disks;
+  bd.theta_items = b->d_theta;
+  bd.ntheta_items = (int)theta.size();
+  bd.theta_seg = seg_max;
+  bd.flags = b->d_flags;
+  CK(fargo_kernel_attributes(b->max_nsec, seg_max));
+  fargo_launch_sector_tables(bd, b->max_nsec, b->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(b->stream));
+  for (int d = 0; d < n; d++) {
+    fargo_status st = init_disk_state(b, d, nullptr, nullptr);
+    if (st) return st;
+  }
+  return build_graph(b);
+}
+
+void batch_free(fargo_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto& h : b->disks) {
+    if (h.sg) sg_destroy(h.sg);
+    for (void* p : h.allocs) cudaFree(p);
+  }
+  void* ps[] = {b->d_disks, b->d_ctl, b->d_cell_off, b->d_ring_off, b->d_theta, b->d_flags, b->d_red};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+fargo_status advance_dt_async(fargo_batch* b) {
+  CK(cudaSetDevice(b->device));
+  fargo_launch_dt_begin(b->bd, b->stream);
+  b->launches += 1;
+  if (b->any_adiabatic) {
+    fargo_launch_cs_refresh(b->bd, -1, b->stream);
+    b->launches += 2;
+  }
+  CK(cudaGetLastError());
+  if (b->use_graph) {
+    CK(cudaGraphLaunch(b->exec, b->stream));
+  } else {
+    int more = 1;
+    int* hflag = nullptr;
+    CK(cudaMallocHost(&hflag, sizeof(int)));
+    while (more) {
+      for (int d = 0; d < (int)b->disks.size(); d++)
+        if (b->disks[d].sg) sg_capture_substep(b->disks[d].sg, b->bd, d, &b->disks[d].dev, b->stream);
+      fargo_launch_substep(b->bd, 0, 0, b->stream, b->max_nsec, nullptr);
+      CK(cudaMemcpyAsync(hflag, b->d_flags, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+      CK(cudaStreamSynchronize(b->stream));
+      more = *hflag;
+    }
+    cudaFreeHost(hflag);
+  }
+  return FARGO_OK;
+}
+
+fargo_status finish_dts(fargo_batch* b) {
+  CK(cudaStreamSynchronize(b->stream));
+  CK(cudaGetLastError());
+  int per = fargo_kernels_per_substep(b->any_adiabatic);
+  for (int d = 0; d < (int)b->disks.size(); d++) {
+    cudaError_t e;
+    DiskCtl c = ctl_header(b, d, &e);
+    if (e != cudaSuccess) return set_err(b, FARGO_ECUDA, "ctl read: %s", cudaGetErrorString(e));
+    if (c.error == 1) return set_err(b, FARGO_ENONFINITE, "disk %d: non-finite or non-positive CFL time step", d);
+    if (c.error == 2) return set_err(b, FARGO_ETIMEOUT, "disk %d: more than 1e5 substeps in one DT", d);
+    (void)per;
+  }
+  return FARGO_OK;
+}
+
+}  // namespace
+
+// =============================================================== C ABI
+
+extern "C" {
+
+int fargo_abi_version(void) { return FARGO_ABI_VERSION; }
+
+fargo_status fargo_create(const fargo_params* p, const fargo_planets* planets, const double* radii, int device,
+                          fargo_ctx** out) {
+  if (!p || !planets || !out) return FARGO_EINVAL;
+  *out = nullptr;
+  fargo_ctx* ctx = new fargo_ctx();
+  const double* r[1] = {radii};
+  fargo_status st = batch_create(&ctx->b, 1, p, planets, r, device);
+  *out = ctx;  // returned even on failure so that fargo_last_error can explain
+  return st;
+}
+
+void fargo_destroy(fargo_ctx* ctx) {
+  if (!ctx) return;
+  batch_free(&ctx->b);
+  delete ctx;
+}
+
+const char* fargo_last_error(const fargo_ctx* ctx) { return ctx ? ctx->b.err.c_str() : "null context"; }
+
+fargo_status fargo_init_state(fargo_ctx* ctx, const float* dens, const float* energy) {
+  if (!ctx) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  CK(cudaSetDevice(b->device));
+  return init_disk_state(b, 0, dens, energy);
+}
+
+fargo_status fargo_batch_init_state(fargo_batch* b, int disk, const float* dens, const float* energy) {
+  if (!b || disk < 0 || disk >= (int)b->disks.size()) return FARGO_EINVAL;
+  CK(cudaSetDevice(b->device));
+  return init_disk_state(b, disk, dens, energy);
+}
+
+static fargo_status upload_impl(fargo_batch* b, int d, const float* dens, const float* vrad, const float* vtheta,
+                                const float* energy) {
+  if (!b || d < 0 || d >= (int)b->disks.size()) return FARGO_EINVAL;
+  CK(cudaSetDevice(b->device));
+  const DiskDev& D = b->disks[d].dev;
+  size_t bytes = sizeof(float) * (size_t)(D.nrad + 1) * D.nsec;
+  if (dens) CK(cudaMemcpyAsync(D.dens, dens, bytes, cudaMemcpyHostToDevice, b->stream));
+  if (vrad) CK(cudaMemcpyAsync(D.vrad, vrad, bytes, cudaMemcpyHostToDevice, b->stream));
+  if (vtheta) CK(cudaMemcpyAsync(D.vtheta, vtheta, bytes, cudaMemcpyHostToDevice, b->stream));
+  if (energy) CK(cudaMemcpyAsync(D.energy, energy, bytes, cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return FARGO_OK;
+}
+
+// ComputeTemperatureFieldKernel (Kernels.cu:211-223) on the host copy.
+static void temperature_host(const fargo_params* p, const float* dens, const float* pres, const float* energy,
+                             float* T, size_t n, size_t nact) {
+  for (size_t l = 0; l < n; l++) {
+    if (l >= nact) {
+      T[l] = 0.0f;
+      continue;
+    }
+    if (!p->Adiabatic)
+      T[l] = 1.0 / 1.0 * pres[l] / dens[l];
+    else
+      T[l] = 1.0 / 1.0 * (p->ADIABATICINDEX - 1.0) * energy[l] / dens[l];
+  }
+}
+
+static fargo_status download_impl(fargo_batch* b, int d, float* dens, float* vrad, float* vtheta, float* energy,
+                                  float* temperature, float* qplus) {
+  if (!b || d < 0 || d >= (int)b->disks.size()) return FARGO_EINVAL;
+  CK(cudaSetDevice(b->device));
+  const DiskHost& h = b->disks[d];
+  const DiskDev& D = h.dev;
+  size_t n = (size_t)(D.nrad + 1) * D.nsec;
+  size_t bytes = sizeof(float) * n;
+  std::vector<float> S, P, E;
+  if (dens) CK(cudaMemcpyAsync(dens, D.dens, bytes, cudaMemcpyDeviceToHost, b->stream));
+  if (vrad) CK(cudaMemcpyAsync(vrad, D.vrad, bytes, cudaMemcpyDeviceToHost, b->stream));
+  if (vtheta) CK(cudaMemcpyAsync(vtheta, D.vtheta, bytes, cudaMemcpyDeviceToHost, b->stream));
+  if (energy) CK(cudaMemcpyAsync(energy, D.energy, bytes, cudaMemcpyDeviceToHost, b->stream));
+  if (qplus) {
+    if (h.p.Adiabatic)
+      CK(cudaMemcpyAsync(qplus, D.qplus, bytes, cudaMemcpyDeviceToHost, b->stream));
+    else
+      std::memset(qplus, 0, bytes);
+  }
+  if (temperature) {
+    S.resize(n);
+    P.resize(n);
+    E.resize(n);
+    CK(cudaMemcpyAsync(S.data(), D.dens, bytes, cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaMemcpyAsync(P.data(), D.pres, bytes, cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaMemcpyAsync(E.data(), D.energy, bytes, cudaMemcpyDeviceToHost, b->stream));
+  }
+  CK(cudaStreamSynchronize(b->stream));
+  if (temperature) temperature_host(&h.p, S.data(), P.data(), E.data(), temperature, n, (size_t)D.nrad * D.nsec);
+  return FARGO_OK;
+}
+
+fargo_status fargo_upload(fargo_ctx* ctx, const float* dens, const float* vrad, const float* vtheta,
+                          const float* energy) {
+  if (!ctx) return FARGO_EINVAL;
+  return upload_impl(&ctx->b, 0, dens, vrad, vtheta, energy);
+}
+
+fargo_status fargo_download(fargo_ctx* ctx, float* dens, float* vrad, float* vtheta, float* energy,
+                            float* temperature, float* qplus) {
+  if (!ctx) return FARGO_EINVAL;
+  return download_impl(&ctx->b, 0, dens, vrad, vtheta, energy, temperature, qplus);
+}
+
+static fargo_status get_planets_impl(fargo_batch* b, int d, fargo_planets* out) {
+  if (!b || !out || d < 0 || d >= (int)b->disks.size()) return FARGO_EINVAL;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  cudaError_t e;
+  DiskCtl c = ctl_header(b, d, &e);
+  if (e != cudaSuccess) return set_err(b, FARGO_ECUDA, "%s", cudaGetErrorString(e));
+  ctl_to_planets(c, b->disks[d].planets0, out);
+  return FARGO_OK;
+}
+
+fargo_status fargo_get_planets(fargo_ctx* ctx, fargo_planets* out) {
+  if (!ctx) return FARGO_EINVAL;
+  return get_planets_impl(&ctx->b, 0, out);
+}
+
+fargo_status fargo_set_planets(fargo_ctx* ctx, const fargo_planets* in) {
+  if (!ctx || !in || in->nb != ctx->b.disks[0].planets0.nb) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  cudaError_t e;
+  DiskCtl c = ctl_header(b, 0, &e);
+  if (e != cudaSuccess) return set_err(b, FARGO_ECUDA, "%s", cudaGetErrorString(e));
+  planets_to_ctl(in, &c);
+  return put_ctl_header(b, 0, c);
+}
+
+fargo_status fargo_advance_dt(fargo_ctx* ctx, int* nsub_out) {
+  if (!ctx) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  fargo_status st = advance_dt_async(b);
+  if (st) return st;
+  st = finish_dts(b);
+  if (st) return st;
+  if (nsub_out) {
+    cudaError_t e;
+    DiskCtl c = ctl_header(b, 0, &e);
+    *nsub_out = c.nsub;
+  }
+  return FARGO_OK;
+}
+
+fargo_status fargo_advance(fargo_ctx* ctx, int ndt) {
+  if (!ctx) return FARGO_EINVAL;
+  return fargo_batch_advance(&ctx->b, ndt);
+}
+
+fargo_status fargo_sync(fargo_ctx* ctx) {
+  if (!ctx) return FARGO_EINVAL;
+  return finish_dts(&ctx->b);
+}
+
+fargo_status fargo_advance_async(fargo_ctx* ctx, int ndt) {
+  if (!ctx) return FARGO_EINVAL;
+  for (int k = 0; k < ndt; k++) {
+    fargo_status st = advance_dt_async(&ctx->b);
+    if (st) return st;
+  }
+  return FARGO_OK;
+}
+
+static fargo_status disk_force_impl(fargo_batch* b, int d, double x, double y, double rsmoothing, double mass,
+                                    int dimfxy, double* gf) {
+  if (!b || !gf || dimfxy != FARGO_DIMFXY) return set_err(b, FARGO_EINVAL, "dimfxy must be %d", FARGO_DIMFXY);
+  CK(cudaSetDevice(b->device));
+  // ComputeForce (Force.cu:311-312): a and rh in double, kernel arguments float
+  double a = std::sqrt(x * x + y * y);
+  double rh = std::pow(mass / 3., 1. / 3.) * a + 1e-15;
+  fargo_launch_disk_force(b->bd, d, (float)x, (float)y, (float)rsmoothing, (float)rh, (float)a, b->d_red,
+                          b->red_blocks, b->stream);
+  CK(cudaGetLastError());
+  std::vector<double> part((size_t)b->red_blocks * 4 * FARGO_DIMFXY);
+  CK(cudaMemcpyAsync(part.data(), b->d_red, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  b->launches += 1;
+  for (int q = 0; q < 4 * FARGO_DIMFXY; q++) {
+    double s = 0;
+    for (int k = 0; k < b->red_blocks; k++) s += part[(size_t)k * 4 * FARGO_DIMFXY + q];
+    gf[q] = s;
+  }
+  return FARGO_OK;
+}
+
+fargo_status fargo_disk_force(fargo_ctx* ctx, double x, double y, double rsmoothing, double mass, int dimfxy,
+                              double* globalforce) {
+  if (!ctx) return FARGO_EINVAL;
+  return disk_force_impl(&ctx->b, 0, x, y, rsmoothing, mass, dimfxy, globalforce);
+}
+
+static fargo_status scalars_impl(fargo_batch* b, int d, fargo_scalars* out) {
+  if (!b || !out || d < 0 || d >= (int)b->disks.size()) return FARGO_EINVAL;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  cudaError_t e;
+  DiskCtl c = ctl_header(b, d, &e);
+  if (e != cudaSuccess) return set_err(b, FARGO_ECUDA, "%s", cudaGetErrorString(e));
+  fargo_launch_diagnostics(b->bd, d, b->d_red, b->red_blocks, b->stream);
+  CK(cudaGetLastError());
+  std::vector<double> part((size_t)b->red_blocks * 3);
+  CK(cudaMemcpyAsync(part.data(), b->d_red, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  b->launches += 1;
+  double m = 0, am = 0, hill = 0;
+  for (int k = 0; k < b->red_blocks; k++) {
+    m += part[3 * k];
+    am += part[3 * k + 1];
+    hill += part[3 * k + 2];
+  }
+  std::memset(out, 0, sizeof(*out));
+  out->physical_time = c.PhysicalTime;
+  out->omega_frame = c.OmegaFrame;
+  out->mdcp1 = (float)hill;
+  out->lost_mass = c.LostMass;
+  out->nsub_last_dt = c.nsub;
+  out->nsub_total = c.nsub_total;
+  out->mass = m;
+  out->angular_momentum = am;
+  out->last_dt = c.dt;
+  return FARGO_OK;
+}
+
+fargo_status fargo_get_scalars(fargo_ctx* ctx, fargo_scalars* out) {
+  if (!ctx) return FARGO_EINVAL;
+  return scalars_impl(&ctx->b, 0, out);
+}
+
+fargo_status fargo_get_substep_log(fargo_ctx* ctx, int cap, int* nshift, double* dt, int* nsub) {
+  if (!ctx) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  cudaError_t e;
+  DiskCtl c = ctl_header(b, 0, &e);
+  if (e != cudaSuccess) return set_err(b, FARGO_ECUDA, "%s", cudaGetErrorString(e));
+  int n = std::min(c.nsub, std::min(cap, FARGO_MAXLOG));
+  const DiskDev& D = b->disks[0].dev;
+  if (nshift && n > 0)
+    CK(cudaMemcpy(nshift, D.log_nshift, sizeof(int) * (size_t)n * D.nrad, cudaMemcpyDeviceToHost));
+  if (dt && n > 0)
+    CK(cudaMemcpy(dt, (const char*)(b->d_ctl) + offsetof(DiskCtl, log_dt), sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (nsub) *nsub = c.nsub;
+  return FARGO_OK;
+}
+
+long long fargo_kernel_launches(const fargo_ctx* ctx) { return ctx ? ctx->b.launches : 0; }
+
+// ---------------------------------------------------------------- batches
+
+fargo_status fargo_batch_create(int n, const fargo_params* params, const fargo_planets* planets, int device,
+                                fargo_batch** out) {
+  if (n < 1 || !params || !planets || !out) return FARGO_EINVAL;
+  fargo_batch* b = new fargo_batch();
+  fargo_status st = batch_create(b, n, params, planets, nullptr, device);
+  *out = b;
+  return st;
+}
+
+void fargo_batch_destroy(fargo_batch* b) {
+  if (!b) return;
+  batch_free(b);
+  delete b;
+}
+
+const char* fargo_batch_last_error(const fargo_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+fargo_status fargo_batch_upload(fargo_batch* b, int disk, const float* dens, const float* vrad, const float* vtheta,
+                                const float* energy) {
+  return upload_impl(b, disk, dens, vrad, vtheta, energy);
+}
+
+fargo_status fargo_batch_download(fargo_batch* b, int disk, float* dens, float* vrad, float* vtheta, float* energy) {
+  return download_impl(b, disk, dens, vrad, vtheta, energy, nullptr, nullptr);
+}
+
+fargo_status fargo_batch_advance(fargo_batch* b, int ndt) {
+  if (!b || ndt < 0) return FARGO_EINVAL;
+  for (int k = 0; k < ndt; k++) {
+    fargo_status st = advance_dt_async(b);
+    if (st) return st;
+  }
+  return finish_dts(b);
+}
+
+fargo_status fargo_batch_advance_async(fargo_batch* b, int ndt) {
+  if (!b || ndt < 0) return FARGO_EINVAL;
+  for (int k = 0; k < ndt; k++) {
+    fargo_status st = advance_dt_async(b);
+    if (st) return st;
+  }
+  return FARGO_OK;
+}
+
+fargo_status fargo_batch_sync(fargo_batch* b) {
+  if (!b) return FARGO_EINVAL;
+  return finish_dts(b);
+}
+
+fargo_status fargo_batch_get_scalars(fargo_batch* b, int disk, fargo_scalars* out) {
+  return scalars_impl(b, disk, out);
+}
+
+fargo_status fargo_batch_get_planets(fargo_batch* b, int disk, fargo_planets* out) {
+  return get_planets_impl(b, disk, out);
+}
+
+long long fargo_batch_kernel_launches(const fargo_batch* b) { return b ? b->launches : 0; }
+
+// Launch counting needs the substep counts: total launches of the batch's
+// own kernels so far (pre-DT launches + substeps x kernels per substep).
+long long fargo_batch_count_launches(fargo_batch* b) {
+  if (!b) return 0;
+  cudaStreamSynchronize(b->stream);
+  long long subs = 0;
+  for (int d = 0; d < (int)b->disks.size(); d++) {
+    cudaError_t e;
+    DiskCtl c = ctl_header(b, d, &e);
+    subs = std::max<long long>(subs, c.nsub_total);
+  }
+  return b->launches + subs * fargo_kernels_per_substep(b->any_adiabatic);
+}
+
+fargo_status fargo_set_graph_mode(fargo_ctx* ctx, int use_graph) {
+  if (!ctx) return FARGO_EINVAL;
+  ctx->b.use_graph = use_graph != 0;
+  return build_graph(&ctx->b);
+}
+
+}  // extern "C"

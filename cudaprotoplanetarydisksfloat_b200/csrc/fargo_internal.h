@@ -1,0 +1,148 @@
+// fargo_internal.h -- device-side data layout of the B200 FARGO step.
+//
+// A "batch" is a list of independent disks (a single disk is a batch of
+// one).  Every kernel takes the batch descriptor and walks a flat work list,
+// so one launch advances every disk that is still inside its DT.
+//
+// Per disk, in HBM:
+//   grid fields   float32, ring-major, (nrad+1)*nsec, element [i*nsec+j]
+//   ring tables   float32, nrad+1 entries (host-built in double, rounded
+//                 to float exactly as FillPolar1DArrays does)
+//   sector tables float32, nsec entries (cosf/sinf of the two angle
+//                 formulas the reference uses)
+//   DiskCtl       mutable scalars: DT bookkeeping, planets (FP64),
+//                 potential parameters, force sums, logs.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define FARGO_PI 3.14159265358979323844
+#define FARGO_CFLSECURITY 0.5
+#define FARGO_CVNR 1.41
+#define FARGO_MAXLOG 2048  // substeps logged per DT (Nshift + dt)
+
+#include "../../include/fargo_b200.h"
+
+// planets integrated on the device (the reference's limit, RungeKutta.cu:4)
+#define FARGO_MAXPLANETS_DEV FARGO_MAXPLANETS
+// bodies whose disk force is summed every substep: the star and up to 7
+// FeelDisk planets (each carries 2 double accumulators per thread)
+#define FARGO_MAXBODY 8
+
+struct DiskCtl {
+  // DT bookkeeping (SourceEuler.cu:211-241)
+  double dtemp;        // time advanced inside the current DT
+  double dt;           // current substep dt (double, as in AlgoGas)
+  float dtf;           // (float)dt, the value every kernel receives
+  int active;          // 1 while this disk is inside a substep of the current DT
+  int more;            // set by the CFL finalize: another substep follows
+  int nsub;            // substeps taken in the current DT
+  int nsub_total;
+  int error;           // nonzero: 1 non-finite CFL, 2 too many substeps
+  unsigned int counter;        // last-block ticket of the CFL/force kernel
+  float PhysicalTime;          // advanced at the end of each substep
+  float time_start;            // PhysicalTime at the start of this substep
+  float PhysicalTimeInitial;
+  float OmegaFrame;
+  float MassTaper;
+  float domega;                // CorrectVtheta amount of this substep (0 if not corotating)
+  float LostMass;
+  // potential parameters of this substep (FillForcesArraysKernel arguments, floats)
+  float itx, ity;              // IndirectTerm
+  float pxp[FARGO_MAXPLANETS_DEV], pyp[FARGO_MAXPLANETS_DEV], psmooth[FARGO_MAXPLANETS_DEV];
+  float pmass[FARGO_MAXPLANETS_DEV], pipd3[FARGO_MAXPLANETS_DEV];
+  // planets, FP64 (Types.cuh:2-15)
+  int nb;
+  double mass[FARGO_MAXPLANETS_DEV], x[FARGO_MAXPLANETS_DEV], y[FARGO_MAXPLANETS_DEV];
+  double vx[FARGO_MAXPLANETS_DEV], vy[FARGO_MAXPLANETS_DEV];
+  int feeldisk[FARGO_MAXPLANETS_DEV], feelothers[FARGO_MAXPLANETS_DEV];
+  float Xplanet_mark, Yplanet_mark;  // Psys.cu:79 static floats of GetPsysInfo
+  // bodies whose disk force the CFL/force kernel sums this substep:
+  // body 0 = star, then FeelDisk planets; coordinates as ComputeAccel floats
+  int nbody;
+  int body_planet[FARGO_MAXBODY];
+  float bx[FARGO_MAXBODY], by[FARGO_MAXBODY], brs[FARGO_MAXBODY];
+  float brh[FARGO_MAXBODY], ba[FARGO_MAXBODY];
+  // self-gravity axisymmetric accelerations at rings 0 and NRAD-1
+  float axisg_in, axisg_out;
+  // logs of the current DT
+  double log_dt[FARGO_MAXLOG];
+  // scratch of the device RK5 (q0, q1, k1..k6), used by one thread
+  double rk_work[14 * 4 * FARGO_MAXPLANETS_DEV];
+};
+
+struct DiskDev {
+  int nrad, nsec;
+  long long cell0;  // first active cell of this disk in the batch's flat index
+  int ring0;        // first ring of this disk in the batch's flat ring index
+  // parameters (floats, as the reference's globals)
+  float DT, ADIABATICINDEX, ASPECTRATIO, FLARINGINDEX, SIGMASLOPE, SIGMA0;
+  float TRANSITIONRADIUS, TRANSITIONRATIO, TRANSITIONWIDTH, LAMBDADOUBLING;
+  float VISCOSITY, ALPHAVISCOSITY, CAVITYRADIUS, CAVITYRATIO, CAVITYWIDTH;
+  float MASSTAPER, RELEASEDATE, RELEASERADIUS, THICKNESSSMOOTHING, ROCHESMOOTHING;
+  float IMPOSEDDISKDRIFT;
+  int Adiabatic, Cooling, ViscosityAlpha, FastTransport, Indirect_Term, ExcludeHill;
+  int ForcedCircular, Corotating, GuidingCenter, RocheSmoothing, SelfGravity, Evanescent;
+  int OpenInner, SloppyCFL, IsDisk;
+  float invdphi, onethird;
+  float HillRadius;
+  // constant sub-Keplerian boundary speeds (host double -> float) when they
+  // do not depend on time or self-gravity; otherwise computed on device
+  int vkep_const;
+  float VKepIn, VKepOut;
+  // state
+  float *dens, *vrad, *vtheta, *energy;
+  float *cs;  // per cell (adiabatic); isothermal uses cs_ring
+  float *pres;  // isothermal: pressure at the start of the DT's last substep (temperature output)
+  // scratch
+  float *vri, *vti, *trr, *tpp, *trp, *qplus;
+  float *a0, *a1, *a2, *a3, *a4, *a5;  // radial-transport outputs
+  // self-gravity accelerations (NRAD*NSEC), may be null
+  float *sg_accr, *sg_acct;
+  // ring tables
+  const float *Rinf, *Rsup, *Rmed, *Surf, *invRinf, *invSurf, *invRmed, *invdiffRsup, *invdiffRmed;
+  const float *dxtheta, *supp_torque, *SigmaMed, *SigmaInf, *EnergyMed, *CoolingTimeMed, *QplusMed;
+  const double* pow15;   // pow(Rmed[i], 1.5) from the host (FViscosity)
+  float* visc;           // viscosity_array of this substep
+  float* cs_ring;        // isothermal sound speed per ring
+  float* csmean;         // GLOBAL_bufarray: ring-mean sound speed
+  float* vmoy;           // ConditionCFLKernel1D ring mean
+  float* ringmin;        // newDT per ring
+  int* nshift;           // Nshift per ring of the current substep
+  int* log_nshift;       // [FARGO_MAXLOG][nrad]
+  double* partials;      // [nrad][4*FARGO_MAXBODY] force partial sums per ring
+  // sector tables
+  const float *cos_pot, *sin_pot;    // cosf/sinf of (float)j/(float)nsec*2.0*PI
+  const float *cos_cell, *sin_cell;  // cosf/sinf of 2.0*PI*(float)j/(float)nsec
+  DiskCtl* ctl;
+};
+
+struct BatchDev {
+  int ndisk;
+  long long ncell;       // total active cells
+  int nring;             // total rings
+  const long long* cell_off;  // [ndisk+1]
+  const int* ring_off;        // [ndisk+1]
+  DiskDev* disks;
+  // azimuthal transport work items: (disk, ring, first sector) per CTA
+  const int4* theta_items;
+  int ntheta_items;
+  int theta_seg;          // largest azimuthal segment (sectors)
+  int* flags;             // [0] OR of the disks' "more" flags after a substep
+};
+
+// kernel entry points (kernels_step.cu), launched by fargo_api.cu
+size_t fargo_theta_smem_bytes(int seg);
+cudaError_t fargo_kernel_attributes(int max_nsec, int seg);
+void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s);
+// only_disk >= 0: that disk; -1: every disk still inside its DT
+void fargo_launch_cs_refresh(const BatchDev& b, int only_disk, cudaStream_t s);
+void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s);
+void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int use_handle, cudaStream_t s,
+                          int max_nsec, long long* launches);
+void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s);
+void fargo_launch_init_velocities(const BatchDev& b, int disk, long long ncell_ghost, cudaStream_t s);
+void fargo_launch_disk_force(const BatchDev& b, int disk, float x, float y, float rs, float rh, float a,
+                             double* out44, int nblocks, cudaStream_t s);
+void fargo_launch_diagnostics(const BatchDev& b, int disk, double* out3, int nblocks, cudaStream_t s);
+int fargo_kernels_per_substep(int adiabatic);

@@ -1,0 +1,1459 @@
+// kernels_step.cu -- sm_100a kernels of one FARGO hydro substep, batched over disks.
+//
+// The reference runs ~120 single-purpose kernels, ~50 host-side reductions
+// (each with cudaMalloc/cudaFree) and ~15 full-grid device copies per
+// substep, with a device synchronisation after every launch
+// (SourceEuler.cu:230-299).  Here one substep is 8-9 launches that read and
+// write only the disk state and a few scratch fields, with the CFL count,
+// the disk forces and the planet integrator kept on the device:
+//
+//   k_cfl_force      ring means, CFL minimum, disk-on-body forces; the last
+//                    block of each disk finishes the substep's scalar work
+//                    (dt, mass taper, potential parameters, planet kicks,
+//                    FP64 RK5, frame rotation, per-ring viscosity)
+//   k_source1        Substep1 (pressure + potential + centrifugal kick),
+//                    potential evaluated on the fly, + self-gravity kick
+//   k_visc_tau       viscous stress tensor
+//   k_visc_update    viscous velocity update + sub-Keplerian boundary
+//   k_source2        artificial viscosity (Substep2) + energy predictor
+//   k_energy         viscous heating and implicit energy update (Substep3)
+//   k_transport_rad  momenta + radial van Leer for every transported quantity
+//   k_transport_theta  FARGO: ring mean, integer shift, residual and constant
+//                    azimuthal van Leer sweeps, shift fused into the store
+//   k_velocities     velocities from the transported momenta
+//   k_substep_end    disks still inside their DT -> graph loop condition
+//
+// Arithmetic per cell follows the reference kernels expression by expression
+// (a float meeting a double literal is promoted and rounded back on
+// assignment); where the reference computes one IEEE operation in double on
+// two float operands and rounds to float, the float operation is used, which
+// gives the same bits.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+
+#include "fargo_internal.h"
+
+#define PI_D FARGO_PI
+#define CVNR FARGO_CVNR
+#define CFLSEC FARGO_CFLSECURITY
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ int disk_of_cell(const BatchDev& B, long long c) {
+  int lo = 0, hi = B.ndisk - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (B.cell_off[mid] <= c)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int disk_of_ring(const BatchDev& B, int r) {
+  int lo = 0, hi = B.ndisk - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (B.ring_off[mid] <= r)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int jwrap_m(int j, int nsec) { return j == 0 ? nsec - 1 : j - 1; }
+__device__ __forceinline__ int jwrap_p(int j, int nsec) { return j + 1 == nsec ? 0 : j + 1; }
+
+// max2 / min2, Kernels.cu:1459-1470
+__device__ __forceinline__ float max2(float a, float b) { return (b > a) ? b : a; }
+__device__ __forceinline__ float min2(float a, float b) { return (b < a) ? b : a; }
+
+// AspectRatioDevice, Kernels.cu:1473-1488
+__device__ float aspect_ratio_dev(const DiskDev& D, float r, float PT, float PTI) {
+  float aspectratio, rmin, rmax, scale;
+  aspectratio = D.ASPECTRATIO;
+  rmin = D.TRANSITIONRADIUS - D.TRANSITIONWIDTH * D.ASPECTRATIO;
+  rmax = D.TRANSITIONRADIUS + D.TRANSITIONWIDTH * D.ASPECTRATIO;
+  scale = 1.0 + (PT - PTI) * D.LAMBDADOUBLING;
+  rmin *= scale;
+  rmax *= scale;
+  if (r < rmin) aspectratio *= D.TRANSITIONRATIO;
+  if ((r >= rmin) && (r <= rmax)) aspectratio *= expf((rmax - r) / (rmax - rmin) * logf(D.TRANSITIONRATIO));
+  return aspectratio;
+}
+
+// AspectRatioHost, Viscosity.cu:39-52 (double math)
+__device__ float aspect_ratio_host(const DiskDev& D, float r, float PT, float PTI) {
+  float aspectratio, rmin, rmax, scale;
+  aspectratio = D.ASPECTRATIO;
+  rmin = D.TRANSITIONRADIUS - D.TRANSITIONWIDTH * D.ASPECTRATIO;
+  rmax = D.TRANSITIONRADIUS + D.TRANSITIONWIDTH * D.ASPECTRATIO;
+  scale = 1.0 + (PT - PTI) * D.LAMBDADOUBLING;
+  rmin *= scale;
+  rmax *= scale;
+  if (r < rmin) aspectratio *= D.TRANSITIONRATIO;
+  if ((r >= rmin) && (r <= rmax))
+    aspectratio *= exp((rmax - r) / (rmax - rmin) * log((double)D.TRANSITIONRATIO));
+  return aspectratio;
+}
+
+// FViscosity, Viscosity.cu:19-37.  The ring search `while (Rmed[k] < r) k++`
+// ends at k = i for r = Rmed[i] on a strictly increasing grid.
+__device__ float fviscosity_ring(const DiskDev& D, int i, float PT, float PTI) {
+  float r = D.Rmed[i];
+  float viscosity, rmin, rmax, scale;
+  viscosity = D.VISCOSITY;
+  if (D.ViscosityAlpha) {
+    float g = D.csmean[i];
+    viscosity = D.ALPHAVISCOSITY * g * g * D.pow15[i];
+  }
+  rmin = D.CAVITYRADIUS - D.CAVITYWIDTH * D.ASPECTRATIO;
+  rmax = D.CAVITYRADIUS + D.CAVITYWIDTH * D.ASPECTRATIO;
+  scale = 1.0 + (PT - PTI) * D.LAMBDADOUBLING;
+  rmin *= scale;
+  rmax *= scale;
+  if (r < rmin) viscosity *= D.CAVITYRATIO;
+  if ((r >= rmin) && (r <= rmax)) viscosity *= exp((rmax - r) / (rmax - rmin) * log((double)D.CAVITYRATIO));
+  return viscosity;
+}
+
+// Compute_smoothing, Force.cu:69-74 (AspectRatioHost takes a float radius)
+__device__ double compute_smoothing(const DiskDev& D, double r, float PT, float PTI) {
+  return D.THICKNESSSMOOTHING * aspect_ratio_host(D, (float)r, PT, PTI) * pow(r, 1.0 + D.FLARINGINDEX);
+}
+
+// ---------------------------------------------------------------- planets (FP64)
+
+// DerivMotionRK5, RungeKutta.cu:9-46; the planet-planet term divides by the
+// cube of the perturber's distance to the star, as the reference does.
+__device__ void deriv_motion(const DiskDev& D, const DiskCtl* C, const double* q, double* deriv, int nb,
+                             float dt) {
+  const double *x = q, *y = q + nb, *vx = q + 2 * nb, *vy = q + 3 * nb;
+  double *dx = deriv, *dy = deriv + nb, *dvx = deriv + 2 * nb, *dvy = deriv + 3 * nb;
+  double Dist[FARGO_MAXPLANETS_DEV];
+  for (int i = 0; i < nb; i++) Dist[i] = sqrt(x[i] * x[i] + y[i] * y[i]);
+  for (int i = 0; i < nb; i++) {
+    dx[i] = vx[i];
+    dy[i] = vy[i];
+    dvx[i] = -1.0 * 1.0 / Dist[i] / Dist[i] / Dist[i] * x[i];
+    dvy[i] = -1.0 * 1.0 / Dist[i] / Dist[i] / Dist[i] * y[i];
+    for (int j = 0; j < nb; j++) {
+      if (D.Indirect_Term) {
+        dvx[i] -= 1.0 * C->mass[j] / Dist[j] / Dist[j] / Dist[j] * x[j];
+        dvy[i] -= 1.0 * C->mass[j] / Dist[j] / Dist[j] / Dist[j] * y[j];
+      }
+      if ((j != i) && C->feelothers[i]) {
+        dvx[i] += 1.0 * C->mass[j] / Dist[j] / Dist[j] / Dist[j] * (x[j] - x[i]);
+        dvy[i] += 1.0 * C->mass[j] / Dist[j] / Dist[j] / Dist[j] * (y[j] - y[i]);
+      }
+    }
+  }
+  for (int i = 0; i < 4 * nb; i++) deriv[i] *= dt;
+}
+
+// RungeKutta, RungeKutta.cu:55-74 (Cash-Karp coefficients of the reference)
+__device__ void runge_kutta(const DiskDev& D, const DiskCtl* C, const double* q0, float dt, double* q1,
+                            double* k, int nb) {
+  const double c[5][5] = {{0.2, 0.0, 0.0, 0.0, 0.0},
+                          {0.075, 0.225, 0.0, 0.0, 0.0},
+                          {0.3, -0.9, 1.2, 0.0, 0.0},
+                          {-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0.0},
+                          {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+  int n4 = 4 * nb;
+  for (int s = 0; s < 6 * n4; s++) k[s] = 0.0;
+  deriv_motion(D, C, q0, k, nb, dt);
+  for (int s = 0; s < 5; s++) {
+    for (int i = 0; i < n4; i++)
+      q1[i] = q0[i] + c[s][0] * k[i] + c[s][1] * k[n4 + i] + c[s][2] * k[2 * n4 + i] +
+              c[s][3] * k[3 * n4 + i] + c[s][4] * k[4 * n4 + i];
+    deriv_motion(D, C, q1, k + (s + 1) * n4, nb, dt);
+  }
+  for (int i = 0; i < n4; i++)
+    q1[i] = q0[i] + 37.0 / 378.0 * k[i] + 250.0 / 621.0 * k[2 * n4 + i] + 125.0 / 594.0 * k[3 * n4 + i] +
+            512.0 / 1771.0 * k[5 * n4 + i];
+}
+
+// AdvanceSystemRK5, Pframeforce.cu:94-157
+__device__ void advance_system_rk5(const DiskDev& D, DiskCtl* C, float dt, float PT, double* work) {
+  int nb = C->nb;
+  double dtheta, omega, rdot, x, y, r, new_r, vx, vy, theta, denom;
+  double* q0 = work;
+  double* q1 = work + 4 * FARGO_MAXPLANETS_DEV;
+  double* k = work + 8 * FARGO_MAXPLANETS_DEV;
+  if (!D.ForcedCircular && nb > 0) {
+    for (int i = 0; i < nb; i++) {
+      q0[i] = C->x[i];
+      q0[i + nb] = C->y[i];
+      q0[i + 2 * nb] = C->vx[i];
+      q0[i + 3 * nb] = C->vy[i];
+    }
+    runge_kutta(D, C, q0, dt, q1, k, nb);
+  }
+  for (int i = 1 - (PT >= D.RELEASEDATE); i < nb; i++) {
+    if (!D.ForcedCircular) {
+      C->x[i] = q1[i];
+      C->y[i] = q1[i + nb];
+      C->vx[i] = q1[i + 2 * nb];
+      C->vy[i] = q1[i + 3 * nb];
+    } else {
+      x = C->x[i];
+      y = C->y[i];
+      theta = atan2(y, x);
+      vx = C->vx[i];
+      vy = C->vy[i];
+      r = sqrt(x * x + y * y);
+      omega = (-y * vx + x * vy) / r / r;
+      dtheta = omega * dt;
+      C->x[i] = r * cos(theta + dtheta);
+      C->y[i] = r * sin(theta + dtheta);
+      C->vx[i] = vx * cos(dtheta + theta) - vy * sin(dtheta + theta);
+      C->vy[i] = vx * sin(dtheta + theta) + vy * cos(dtheta + theta);
+    }
+  }
+  if (PT < D.RELEASEDATE && nb > 0) {
+    x = C->x[0];
+    y = C->y[0];
+    r = sqrt(x * x + y * y);
+    theta = atan2(y, x);
+    rdot = (D.RELEASERADIUS - r) / (D.RELEASEDATE - PT);
+    omega = sqrt((1. + C->mass[0]) / r / r / r);
+    new_r = r + rdot * dt;
+    denom = r - new_r;
+    if (denom != 0.0)
+      dtheta = 2. * dt * r * omega / denom * (sqrt(r / new_r) - 1.);
+    else
+      dtheta = omega * dt;
+    vx = rdot;
+    vy = new_r * sqrt((1. + C->mass[0]) / new_r / new_r / new_r);
+    C->x[0] = new_r * cos(dtheta + theta);
+    C->y[0] = new_r * sin(dtheta + theta);
+    C->vx[0] = vx * cos(dtheta + theta) - vy * sin(dtheta + theta);
+    C->vy[0] = vx * sin(dtheta + theta) + vx * cos(dtheta + theta);  // Pframeforce.cu:154 uses vx twice
+  }
+}
+
+// GetPsysInfo, Psys.cu:236-306 (0 = GET, 1 = MARK, 2 = FREQUENCY)
+__device__ float get_psys_info(const DiskDev& D, DiskCtl* C, int action) {
+  double d1, d2, cross;
+  double x, y, vx, vy, m, h, d, Ax, Ay, e, a, E, M;
+  double xc, yc, omega;
+  double arg, PerihelionPA;
+  xc = x = C->x[0];
+  yc = y = C->y[0];
+  vx = C->vx[0];
+  vy = C->vy[0];
+  m = C->mass[0] + 1.;
+  h = x * vy - y * vx;
+  d = sqrt(x * x + y * y);
+  Ax = x * vy * vy - y * vx * vy - 1.0 * m * x / d;
+  Ay = y * vx * vx - x * vx * vy - 1.0 * m * y / d;
+  e = sqrt(Ax * Ax + Ay * Ay) / m;
+  a = h * h / 1.0 / m / (1. - e * e);
+  if (e == 0.0)
+    arg = 1.0;
+  else
+    arg = (1.0 - d / a) / e;
+  if (fabs(arg) >= 1.0)
+    E = PI_D * (1. - arg / fabs(arg)) / 2.;
+  else
+    E = acos((1.0 - d / a) / e);
+  if ((x * y * (vy * vy - vx * vx) + vx * vy * (x * x - y * y)) < 0) E = -E;
+  M = E - e * sin(E);
+  omega = sqrt(m / a / a / a);
+  PerihelionPA = atan2(Ay, Ax);
+  if (D.GuidingCenter) {
+    xc = a * cos(M + PerihelionPA);
+    yc = a * sin(M + PerihelionPA);
+  }
+  if (e < 1e-8) {
+    xc = x;
+    yc = y;
+  }
+  switch (action) {
+    case 1:
+      C->Xplanet_mark = xc;
+      C->Yplanet_mark = yc;
+      return 0.;
+    case 0:
+      x = xc;
+      y = yc;
+      d2 = sqrt(x * x + y * y);
+      d1 = sqrt((double)C->Xplanet_mark * C->Xplanet_mark + (double)C->Yplanet_mark * C->Yplanet_mark);
+      cross = C->Xplanet_mark * y - x * C->Yplanet_mark;
+      C->Xplanet_mark = x;
+      C->Yplanet_mark = y;
+      return asin(cross / (d1 * d2));
+    case 2:
+      return omega;
+  }
+  return 0.0;
+}
+
+// RotatePsys, Psys.cu:308-325
+__device__ void rotate_psys(DiskCtl* C, float angle) {
+  double sint = sin((double)angle), cost = cos((double)angle), xt, yt;
+  for (int i = 0; i < C->nb; i++) {
+    xt = C->x[i];
+    yt = C->y[i];
+    C->x[i] = xt * cost + yt * sint;
+    C->y[i] = -xt * sint + yt * cost;
+    xt = C->vx[i];
+    yt = C->vy[i];
+    C->vx[i] = xt * cost + yt * sint;
+    C->vy[i] = -xt * sint + yt * cost;
+  }
+}
+
+// Arguments of the force kernel for the star and every FeelDisk planet at
+// the planets' current positions (ComputeAccel takes floats, SideEuler.cu:151;
+// ComputeForce derives a and rh from them, Force.cu:311-312).
+__device__ void prepare_bodies(const DiskDev& D, DiskCtl* C) {
+  int nbody = 0;
+  C->bx[0] = 0.0f;
+  C->by[0] = 0.0f;
+  C->brs[0] = 0.0f;
+  C->ba[0] = 0.0f;
+  C->brh[0] = (float)(pow(0.0 / 3., 1. / 3.) * 0.0 + 1e-15);
+  C->body_planet[0] = -1;
+  nbody = 1;
+  for (int k = 0; k < C->nb && nbody < FARGO_MAXBODY; k++) {
+    if (!C->feeldisk[k]) continue;
+    double m = C->mass[k], x = C->x[k], y = C->y[k];
+    double r = sqrt(x * x + y * y), smoothing;
+    if (D.RocheSmoothing)
+      smoothing = r * pow(m / 3., 1. / 3.) * D.ROCHESMOOTHING;
+    else
+      smoothing = compute_smoothing(D, r, C->PhysicalTime, C->PhysicalTimeInitial);
+    float xf = (float)x, yf = (float)y, rsf = (float)smoothing, mf = (float)m;
+    double a = sqrt((double)xf * xf + (double)yf * yf);
+    double rh = pow((double)mf / 3., 1. / 3.) * a + 1e-15;
+    C->bx[nbody] = xf;
+    C->by[nbody] = yf;
+    C->brs[nbody] = rsf;
+    C->brh[nbody] = (float)rh;
+    C->ba[nbody] = (float)a;
+    C->body_planet[nbody] = k;
+    nbody++;
+  }
+  C->nbody = nbody;
+}
+
+// -------------------------------------------------------------- reductions
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ float warp_min_f(float v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    float w = __shfl_down_sync(0xffffffffu, v, o);
+    if (w < v) v = w;
+  }
+  return v;
+}
+
+// Minimum over the block with the reference's ordered comparison
+// (`if (x < m) m = x`, so NaNs are skipped).  All threads get the result.
+__device__ float block_min_f(float v, float* sh) {
+  v = warp_min_f(v);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < (int)(blockDim.x >> 5)) ? sh[l] : 1e30f;
+    v = warp_min_f(v);
+    if (l == 0) sh[0] = v;
+  }
+  __syncthreads();
+  float r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// -------------------------------------------------------------- CFL + forces
+
+// Last block of a disk: the scalar part of the substep (SourceEuler.cu:231-264).
+__device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* C, float* shf, double* shd) {
+  const int nrad = D.nrad, nsec = D.nsec, tid = threadIdx.x;
+  __shared__ double s_sum[4 * FARGO_MAXBODY];
+  // ConditionCFL host part (SourceEuler.cu:513-535): minimum over the ring
+  // minima, the shear limit DT1D (ConditionCFLKernel2D2, Kernels.cu:1425-1428)
+  // and DeltaT.
+  float m = 1e30f;
+  bool first = true;
+  for (int i = 1 + tid; i < nrad; i += blockDim.x) {
+    float v = D.ringmin[i];
+    if (first || v < m) m = v;
+    first = false;
+  }
+  for (int i = tid; i < nrad - 1; i += blockDim.x) {
+    float dt1 = 2.0 * PI_D * CFLSEC / (float)nsec / fabsf(D.vmoy[i] * D.invRmed[i] - D.vmoy[i + 1] * D.invRmed[i + 1]);
+    if (dt1 < m) m = dt1;
+  }
+  float newdt = block_min_f(m, shf);
+  // disk-force sums: fixed order, one warp per sum
+  int nbody = C->nbody, nsum = 4 * nbody;
+  int w = tid >> 5, l = tid & 31;
+  for (int s = w; s < nsum; s += blockDim.x >> 5) {
+    double acc = 0.0;
+    for (int r = l; r < nrad; r += 32) acc += D.partials[(size_t)r * 4 * FARGO_MAXBODY + s];
+    acc = warp_sum_d(acc);
+    if (l == 0) s_sum[s] = acc;
+  }
+  // FViscosity per ring for this substep (Viscosity.cu:84-85, SourceEuler.cu:350)
+  float PT = C->PhysicalTime;
+  for (int i = tid; i < nrad; i += blockDim.x) D.visc[i] = fviscosity_ring(D, i, PT, C->PhysicalTimeInitial);
+  __syncthreads();
+  if (tid != 0) return;
+
+  double DTd = (double)D.DT;
+  // MassTaper, SourceEuler.cu:231-232
+  float mt = PT / (D.MASSTAPER * 2.0 * M_PI);
+  mt = (mt > 1.0 ? 1.0 : pow(sin(mt * M_PI / 2.0), 2.0));
+  C->MassTaper = mt;
+  // substep count and dt (SourceEuler.cu:236-241, 535)
+  double dt = C->dt;
+  if (D.IsDisk && (!D.SloppyCFL || C->nsub == 0)) {
+    float DeltaT = DTd - C->dtemp;
+    if (DeltaT < newdt) newdt = DeltaT;
+    float q = DeltaT / newdt;
+    if (!(newdt > 0.0f) || !(q < 1.0e5f)) {
+      C->error = 1;
+      C->more = 0;
+      C->active = 0;
+      C->counter = 0;
+      return;
+    }
+    int n = (int)ceilf(q);
+    dt = (DTd - C->dtemp) / (double)n;
+  } else if (!D.IsDisk && C->nsub == 0) {
+    dt = DTd;
+  }
+  C->dt = dt;
+  C->dtf = (float)dt;
+  C->dtemp += dt;
+  if (C->nsub < FARGO_MAXLOG) C->log_dt[C->nsub] = dt;
+  float dtf = (float)dt;
+  if (D.Corotating) get_psys_info(D, C, 1);
+  // DiskOnPrimaryAcceleration (ComputeAccel for the star, SideEuler.cu:151-164):
+  // the Force fields are floats, their sum is a float.
+  float ax = 0.0f, ay = 0.0f;
+  if (D.IsDisk) {
+    ax = (float)s_sum[0] + (float)s_sum[1];
+    ay = (float)s_sum[2] + (float)s_sum[3];
+  }
+  // ComputeIndirectTerm, Pframeforce.cu:27-35
+  C->itx = -ax;
+  C->ity = -ay;
+  if (!D.Indirect_Term) {
+    C->itx = 0.0f;
+    C->ity = 0.0f;
+  }
+  // FillForcesArrays arguments (Pframeforce.cu:49-61)
+  for (int k = 0; k < C->nb; k++) {
+    double xplanet = C->x[k], yplanet = C->y[k], mplanet = C->mass[k] * mt;
+    double PlanetDistance = sqrt(xplanet * xplanet + yplanet * yplanet);
+    double InvPlanetDistance3 = 1.0 / PlanetDistance / PlanetDistance / PlanetDistance;
+    double RRoche = PlanetDistance * pow((1.0 / 3.0 * mplanet), 1.0 / 3.0);
+    double smoothing = D.RocheSmoothing ? RRoche * D.ROCHESMOOTHING
+                                        : compute_smoothing(D, PlanetDistance, PT, C->PhysicalTimeInitial);
+    double smooth = smoothing * smoothing;
+    C->pxp[k] = (float)xplanet;
+    C->pyp[k] = (float)yplanet;
+    C->psmooth[k] = (float)smooth;
+    C->pmass[k] = (float)mplanet;
+    C->pipd3[k] = (float)InvPlanetDistance3;
+  }
+  // AdvanceSystemFromDisk, Pframeforce.cu:68-92
+  if (D.IsDisk) {
+    for (int b = 1; b < nbody; b++) {
+      int k = C->body_planet[b];
+      float gx = (float)s_sum[4 * b] + (float)s_sum[4 * b + 1];
+      float gy = (float)s_sum[4 * b + 2] + (float)s_sum[4 * b + 3];
+      C->vx[k] += dtf * gx;
+      C->vy[k] += dtf * gy;
+      C->vx[k] += dtf * C->itx;
+      C->vy[k] += dtf * C->ity;
+    }
+  }
+  advance_system_rk5(D, C, dtf, PT, C->rk_work);
+  C->domega = 0.0f;
+  if (D.Corotating) {
+    double OmegaNew = get_psys_info(D, C, 0) / dt;
+    double domega = OmegaNew - C->OmegaFrame;
+    if (D.IsDisk) C->domega = (float)domega;
+    C->OmegaFrame = (float)OmegaNew;
+  }
+  rotate_psys(C, (float)(C->OmegaFrame * dt));
+  C->time_start = PT;
+  C->PhysicalTime = PT + dt;
+  C->nsub++;
+  C->nsub_total++;
+  C->more = (C->dtemp < 0.999999999 * DTd) ? 1 : 0;
+  if (C->nsub >= 100000) {
+    C->error = 2;
+    C->more = 0;
+  }
+  prepare_bodies(D, C);
+  C->counter = 0;
+  (void)shd;
+}
+
+// One block per ring: ConditionCFLKernel1D + ConditionCFLKernel2D1 + the ring
+// minimum of ConditionCFLKernel2D2 (Kernels.cu:1363-1422), and the disk force
+// of ComputeForceKernel (Kernels.cu:804-839) for the star and every FeelDisk
+// planet, accumulated in double.
+__global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
+  extern __shared__ float s_ring[];
+  __shared__ float s_min[32];
+  __shared__ double s_red[2 * FARGO_MAXBODY][kThreads / 32];
+  __shared__ float s_vm;
+  __shared__ unsigned s_ticket;
+  __shared__ float s_b[5][FARGO_MAXBODY];
+  const int gr = blockIdx.x;
+  const int d = disk_of_ring(B, gr);
+  const DiskDev& D = B.disks[d];
+  DiskCtl* C = D.ctl;
+  if (!C->active) return;
+  const int i = gr - D.ring0, nsec = D.nsec, nrad = D.nrad, tid = threadIdx.x;
+  const float* vt = D.vtheta + (size_t)i * nsec;
+  for (int j = tid; j < nsec; j += blockDim.x) s_ring[j] = vt[j];
+  const int nbody = C->nbody;
+  if (tid < nbody) {
+    s_b[0][tid] = C->bx[tid];
+    s_b[1][tid] = C->by[tid];
+    s_b[2][tid] = C->brs[tid];
+    s_b[3][tid] = C->brh[tid];
+    s_b[4][tid] = C->ba[tid];
+  }
+  __syncthreads();
+  if (tid == 0) {
+    float moy = 0.0f;
+    for (int j = 0; j < nsec; j++) moy += s_ring[j];
+    moy /= (float)nsec;
+    s_vm = moy;
+    D.vmoy[i] = moy;
+  }
+  __syncthreads();
+  const float vm = s_vm;
+  const float* vr = D.vrad + (size_t)i * nsec;
+  float lmin = 1e30f;
+  if (i > 0 && D.IsDisk) {
+    const float dxrad = D.Rsup[i] - D.Rinf[i];
+    const float dxt = D.dxtheta[i];
+    const float csr = D.Adiabatic ? 0.0f : D.cs_ring[i];
+    for (int j = tid; j < nsec; j += blockDim.x) {
+      float cs = D.Adiabatic ? D.cs[(size_t)i * nsec + j] : csr;
+      float vres = D.FastTransport ? s_ring[j] - vm : s_ring[j];
+      float invdt1 = cs / (min2(dxrad, dxt));
+      float invdt2 = fabsf(vr[j]) / dxrad;
+      float invdt3 = fabsf(vres) / dxt;
+      float dvr = vr[j + nsec] - vr[j];
+      float dvt = s_ring[jwrap_p(j, nsec)] - s_ring[j];
+      if (dvr >= 0.0)
+        dvr = 1e-10;
+      else
+        dvr = -dvr;
+      if (dvt >= 0.0)
+        dvt = 1e-10;
+      else
+        dvt = -dvt;
+      float invdt4 = max2(dvr / dxrad, dvt / dxt);
+      invdt4 *= 4.0 * CVNR * CVNR;
+      float dt2d = CFLSEC / sqrtf(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 + invdt4 * invdt4);
+      if (dt2d < lmin) lmin = dt2d;
+    }
+  }
+  float rmin = block_min_f(lmin, s_min);
+  if (tid == 0 && i > 0) D.ringmin[i] = rmin;
+
+  // disk forces of this ring
+  double sfx[FARGO_MAXBODY], sfy[FARGO_MAXBODY];
+#pragma unroll
+  for (int b = 0; b < FARGO_MAXBODY; b++) sfx[b] = sfy[b] = 0.0;
+  const int k = D.ExcludeHill ? FARGO_DIMFXY - 1 : 0;
+  const float hillcutfactor = (float)k / (float)(FARGO_DIMFXY - 1);
+  if (D.IsDisk) {
+    const float Rm = D.Rmed[i], Sf = D.Surf[i];
+    const float* dn = D.dens + (size_t)i * nsec;
+    for (int j = tid; j < nsec; j += blockDim.x) {
+      float cellmass = Sf * dn[j];
+      float cx = Rm * D.cos_cell[j];
+      float cy = Rm * D.sin_cell[j];
+#pragma unroll
+      for (int b = 0; b < FARGO_MAXBODY; b++) {
+        if (b < nbody) {
+          float dx = cx - s_b[0][b];
+          float dy = cy - s_b[1][b];
+          float rs = s_b[2][b];
+          float d2 = dx * dx + dy * dy;
+          float dist2 = d2 + rs * rs;
+          float distance = sqrtf(dist2);
+          // 1.0/dist2/distance: one division of the exact double product
+          float InvDist3 = 1.0 / ((double)dist2 * (double)distance);
+          float hill_cut;
+          if (k != 0) {
+            float rh = s_b[3][b] * hillcutfactor;
+            hill_cut = 1. - expf(-d2 / (rh * rh));
+          } else
+            hill_cut = 1.;
+          float fx = 1.0 * cellmass * dx * InvDist3 * hill_cut;
+          float fy = 1.0 * cellmass * dy * InvDist3 * hill_cut;
+          sfx[b] += fx;
+          sfy[b] += fy;
+        }
+      }
+    }
+  }
+  const int w = tid >> 5, l = tid & 31;
+#pragma unroll
+  for (int b = 0; b < FARGO_MAXBODY; b++) {
+    if (b < nbody) {
+      double a = warp_sum_d(sfx[b]);
+      double c = warp_sum_d(sfy[b]);
+      if (l == 0) {
+        s_red[2 * b][w] = a;
+        s_red[2 * b + 1][w] = c;
+      }
+    }
+  }
+  __syncthreads();
+  if (tid < 2 * nbody) {
+    double acc = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) acc += s_red[tid][q];
+    int b = tid >> 1, comp = tid & 1;  // comp 0: x, 1: y
+    bool inner = D.Rmed[i] < s_b[4][b];
+    double* P = D.partials + (size_t)i * 4 * FARGO_MAXBODY + 4 * b + 2 * comp;
+    P[0] = inner ? acc : 0.0;  // fx_inner / fy_inner
+    P[1] = inner ? 0.0 : acc;  // fx_outer / fy_outer
+  }
+  // last block of this disk finishes the substep's scalar work
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_ticket = atomicAdd(&C->counter, 1u);
+  __syncthreads();
+  if (s_ticket != (unsigned)(nrad - 1)) return;
+  __threadfence();
+  finish_cfl_and_planets(D, C, s_min, nullptr);
+}
+
+// ----------------------------------------------------------- source terms
+
+// Gravitational potential at cell (i, j): FillForcesArraysKernel
+// (Kernels.cu:1322-1349) summed over the planets in the reference's order.
+__device__ __forceinline__ float potential_at(const DiskDev& D, const DiskCtl* C, int i, int j) {
+  const float Rm = D.Rmed[i];
+  const float x = Rm * D.cos_pot[j];
+  const float y = Rm * D.sin_pot[j];
+  float P = 0.0f;
+  const int nb = C->nb;
+  for (int k = 0; k < nb; k++) {
+    const float xp = C->pxp[k], yp = C->pyp[k], mp = C->pmass[k];
+    float distance = (x - xp) * (x - xp) + (y - yp) * (y - yp);
+    float distancesmooth = sqrtf(distance + C->psmooth[k]);
+    float pot = __fdiv_rn(-mp, distancesmooth);  // -G*mplanet/distancesmooth
+    if (D.Indirect_Term) pot += 1.0 * mp * C->pipd3[k] * (x * xp + y * yp);
+    P += pot;
+    if (k == 0) {
+      float InvDistance = __fdiv_rn(1.0f, Rm);
+      pot = -InvDistance;
+      pot -= C->itx * x + C->ity * y;
+      P += pot;
+    }
+  }
+  return P;
+}
+
+__device__ __forceinline__ float pressure_at(const DiskDev& D, long long l, int i) {
+  if (!D.Adiabatic) {
+    float cs = D.cs_ring[i];
+    return D.dens[l] * cs * cs;
+  }
+  return (D.ADIABATICINDEX - 1.0) * D.energy[l];
+}
+
+#define CELL_PROLOGUE                                                   \
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;       \
+  if (c >= B.ncell) return;                                             \
+  const int d = disk_of_cell(B, c);                                     \
+  const DiskDev& D = B.disks[d];                                        \
+  const DiskCtl* C = D.ctl;                                             \
+  if (!C->active || !D.IsDisk) return;                                  \
+  const int nsec = D.nsec, nrad = D.nrad;                               \
+  const int loc = (int)(c - D.cell0);                                   \
+  const int i = loc / nsec, j = loc - i * nsec;                         \
+  const long long l = (long long)i * nsec + j;                          \
+  const int jm = jwrap_m(j, nsec), jp = jwrap_p(j, nsec);               \
+  (void)nrad;                                                           \
+  (void)jm;                                                             \
+  (void)jp;
+
+// Substep1KernelVrad / Substep1KernelVtheta (Kernels.cu:52-88), with
+// CorrectVthetaKernel (Kernels.cu:1352-1359) applied on the fly, and the
+// self-gravity kick of Update_sgvelocityKernel (Kernels.cu:1024-1041).
+__global__ void __launch_bounds__(kThreads) k_source1(BatchDev B) {
+  CELL_PROLOGUE
+  const float dt = C->dtf;
+  const float OmegaFrame = C->OmegaFrame;
+  const float dom = C->domega;
+  const float* Vt = D.vtheta;
+  const float* Dn = D.dens;
+  auto vth = [&](long long q, int r) -> float { return dom != 0.0f ? Vt[q] - dom * D.Rmed[r] : Vt[q]; };
+  const float P0 = pressure_at(D, l, i);
+  const float Phi0 = potential_at(D, C, i, j);
+  // ComputeTemperatureField divides the pressure of the substep start by the
+  // final density (SourceEuler.cu:280,293): keep the last substep's pressure
+  if (!D.Adiabatic && !C->more) D.pres[l] = P0;
+  if (i > 0) {
+    const long long lm = l - nsec;
+    const float Pm = pressure_at(D, lm, i - 1);
+    const float Phim = potential_at(D, C, i - 1, j);
+    float gradp = (P0 - Pm) * 2.0 / (Dn[l] + Dn[lm]) * D.invdiffRmed[i];
+    float gradphi = (Phi0 - Phim) * D.invdiffRmed[i];
+    const long long lp = (long long)i * nsec + jp;
+    float vt2 = vth(l, i) + vth(lp, i) + vth(lm, i - 1) + vth(lp - nsec, i - 1);
+    vt2 = vt2 / 4.0 + D.Rinf[i] * OmegaFrame;
+    vt2 = vt2 * vt2;
+    float vri = D.vrad[l] + dt * (-gradp - gradphi + vt2 * D.invRinf[i]);
+    if (D.SelfGravity)
+      vri += dt * ((D.Rinf[i] - D.Rmed[i - 1]) * D.sg_accr[l] + (D.Rmed[i] - D.Rinf[i]) * D.sg_accr[lm]) *
+             D.invdiffRmed[i];
+    D.vri[l] = vri;
+  } else {
+    D.vri[l] = 0.0f;  // VradInt's ring 0 is never written by the reference: zero
+  }
+  {
+    const long long la = (long long)i * nsec + jm;
+    float dxtheta = 2.0 * PI_D / (float)nsec * D.Rmed[i];
+    float invdxtheta = 1.0 / dxtheta;
+    const float Pa = pressure_at(D, la, i);
+    const float Phia = potential_at(D, C, i, jm);
+    float gradp = (P0 - Pa) * 2.0 / (Dn[l] + Dn[la]) * invdxtheta;
+    float gradphi = (Phi0 - Phia) * invdxtheta;
+    float vti = vth(l, i) - dt * (gradp + gradphi);
+    vti += dt * D.supp_torque[i];
+    if (D.SelfGravity) {
+      // the reference reads SG_Acct[i*nsec + (j-1)%nsec]: for j = 0 that is
+      // the last sector of ring i-1 (ring 0: taken from ring 0 itself)
+      long long lq = (j > 0) ? l - 1 : (i > 0 ? l - 1 : (long long)nsec - 1);
+      vti += 0.5 * dt * (D.sg_acct[l] + D.sg_acct[lq]);
+    }
+    D.vti[l] = vti;
+  }
+}
+
+// ViscousTermsKernelDRP + ViscousTermsKernelTAURP (Kernels.cu:843-880) on
+// (Vradial, Vazimutal); TAURP's third density sample is dens[i*nsec]
+// because the reference indexes ((j-1)*nsec)%nsec (Kernels.cu:876).
+struct Tau {
+  float rr, pp, rp, divv;
+};
+
+__device__ __forceinline__ Tau viscous_terms(const DiskDev& D, const float* Vr, const float* Va, int i, int j,
+                                             int nsec) {
+  const long long l = (long long)i * nsec + j;
+  const int jp = jwrap_p(j, nsec), jm = jwrap_m(j, nsec);
+  const long long lp = (long long)i * nsec + jp;
+  const float* Dn = D.dens;
+  const float nu = D.visc[i];
+  Tau t;
+  float DRR = (Vr[l + nsec] - Vr[l]) * D.invdiffRsup[i];
+  float DPP = (Va[lp] - Va[l]) * D.invdphi * D.invRmed[i] + 0.5 * (Vr[l + nsec] + Vr[l]) * D.invRmed[i];
+  float divV = (Vr[l + nsec] * D.Rsup[i] - Vr[l] * D.Rinf[i]) * D.invdiffRsup[i] * D.invRmed[i];
+  divV += (Va[lp] - Va[l]) * D.invdphi * D.invRmed[i];
+  t.divv = divV;
+  t.rr = 2.0 * Dn[l] * nu * (DRR - D.onethird * divV);
+  t.pp = 2.0 * Dn[l] * nu * (DPP - D.onethird * divV);
+  t.rp = 0.0f;
+  if (i > 0) {
+    const long long lm = (long long)i * nsec + jm;
+    float DRP = 0.5 * (D.Rinf[i] * (Va[l] * D.invRmed[i] - Va[l - nsec] * D.invRmed[i - 1]) * D.invdiffRmed[i] +
+                       (Vr[l] - Vr[lm]) * D.invdphi * D.invRinf[i]);
+    t.rp = 2.0 * 0.25 * (Dn[l] + Dn[l - nsec] + Dn[(long long)i * nsec] + Dn[lm - nsec]) * nu * DRP;
+  }
+  return t;
+}
+
+__global__ void __launch_bounds__(kThreads) k_visc_tau(BatchDev B) {
+  CELL_PROLOGUE
+  Tau t = viscous_terms(D, D.vri, D.vti, i, j, nsec);
+  D.trr[l] = t.rr;
+  D.tpp[l] = t.pp;
+  if (i > 0) D.trp[l] = t.rp;
+}
+
+// Sub-Keplerian boundary speeds (SideEuler.cu:250-268), device double math
+// when they change with time or self-gravity.
+__device__ void vkep_pair(const DiskDev& D, const DiskCtl* C, float* vin, float* vout) {
+  if (D.vkep_const) {
+    *vin = D.VKepIn;
+    *vout = D.VKepOut;
+    return;
+  }
+  const int nrad = D.nrad;
+  float PT = C->time_start, PTI = C->PhysicalTimeInitial;
+  float r0 = D.Rmed[0], r1 = D.Rmed[nrad - 1];
+  double f = (1.0 + D.SIGMASLOPE - 2.0 * D.FLARINGINDEX);
+  double a0 = 1.0 / r0 * (1.0 - f * pow((double)aspect_ratio_host(D, r0, PT, PTI), 2.0) * pow(r0, 2.0 * D.FLARINGINDEX));
+  double a1 = 1.0 / r1 * (1.0 - f * pow((double)aspect_ratio_host(D, r1, PT, PTI), 2.0) * pow(r1, 2.0 * D.FLARINGINDEX));
+  if (D.SelfGravity) {
+    a0 -= r0 * C->axisg_in;
+    a1 -= r1 * C->axisg_out;
+  }
+  *vin = sqrt(a0);
+  *vout = sqrt(a1);
+}
+
+// UpdateVelocitiesKernel (Kernels.cu:142-160) in place, then
+// ApplySubKeplerianBoundaryKernel (Kernels.cu:1490-1503).
+__global__ void __launch_bounds__(kThreads) k_visc_update(BatchDev B) {
+  CELL_PROLOGUE
+  const float DeltaT = C->dtf;
+  const float* Dn = D.dens;
+  const float *TRR = D.trr, *TRP = D.trp, *TPP = D.tpp;
+  const long long lmj = (long long)i * nsec + jm, lpj = (long long)i * nsec + jp;
+  if (i > 0 && i < nrad - 1) {
+    D.vti[l] += DeltaT * D.invRmed[i] *
+                ((D.Rsup[i] * TRP[l + nsec] - D.Rinf[i] * TRP[l]) * D.invdiffRsup[i] +
+                 (TPP[l] - TPP[lmj]) * D.invdphi + 0.5 * (TRP[l] + TRP[l + nsec])) /
+                (0.5 * (Dn[l] + Dn[lmj]));
+  }
+  if (i > 0) {
+    D.vri[l] += DeltaT * D.invRinf[i] *
+                ((D.Rmed[i] * TRR[l] - D.Rmed[i - 1] * TRR[l - nsec]) * D.invdiffRmed[i] +
+                 (TRP[lpj] - TRP[l]) * D.invdphi - 0.5 * (TPP[l] + TPP[l - nsec])) /
+                (0.5 * (Dn[l] + Dn[l - nsec]));
+  }
+  if (!D.Evanescent && (i == 0 || i == nrad - 1)) {
+    float vin, vout;
+    vkep_pair(D, C, &vin, &vout);
+    if (i == 0) D.vti[l] = vin - D.Rmed[0] * C->OmegaFrame;
+    if (i == nrad - 1) D.vti[l] = vout - D.Rmed[nrad - 1] * C->OmegaFrame;
+  }
+}
+
+// Substep2Kernel + Substep2Kernel2 (Kernels.cu:570-621), then the
+// ActualiseGasVrad/Vtheta copies become direct stores into the state.
+__device__ __forceinline__ float qvisc(float dv, float dens) {
+  if (dv < 0.0) return CVNR * CVNR * dens * dv * dv;
+  return 0.0f;
+}
+
+__global__ void __launch_bounds__(kThreads) k_source2(BatchDev B) {
+  CELL_PROLOGUE
+  const float dt = C->dtf;
+  const float* Dn = D.dens;
+  const float *VRI = D.vri, *VTI = D.vti;
+  const long long lmj = (long long)i * nsec + jm, lpj = (long long)i * nsec + jp;
+  float qr = qvisc(VRI[l + nsec] - VRI[l], Dn[l]);
+  float qt = qvisc(VTI[lpj] - VTI[l], Dn[l]);
+  float vr_new = 0.0f;
+  if (i > 0) {
+    float qrm = qvisc(VRI[l] - VRI[l - nsec], Dn[l - nsec]);
+    vr_new = VRI[l] - dt * 2.0 / (Dn[l] + Dn[l - nsec]) * (qr - qrm) * D.invdiffRmed[i];
+  }
+  float qtm = qvisc(VTI[l] - VTI[lmj], Dn[lmj]);
+  float dxtheta = 2.0 * PI_D / (float)nsec * D.Rmed[i];
+  float invdxtheta = 1.0 / dxtheta;
+  float vt_new = VTI[l] - dt * 2.0 / (Dn[l] + Dn[lmj]) * (qt - qtm) * invdxtheta;
+  if (D.Adiabatic) {
+    D.energy[l] = D.energy[l] - dt * qr * (VRI[l + nsec] - VRI[l]) * D.invdiffRsup[i] -
+                  dt * qt * (VTI[lpj] - VTI[l]) * invdxtheta;
+  }
+  D.vrad[l] = vr_new;
+  D.vtheta[l] = vt_new;
+  if (i == nrad - 1) D.vtheta[l + nsec] = 0.0f;  // VthetaNew's ghost row is zero
+}
+
+// Substep3Kernel + Substep3Kernel2 (Kernels.cu:91-139) with the viscous
+// terms of the new velocities (SourceEuler.cu:286-289) evaluated per cell.
+__device__ __forceinline__ float qplus_at(const DiskDev& D, int i, int j, int nsec, float* divv) {
+  Tau t = viscous_terms(D, D.vrad, D.vtheta, i, j, nsec);
+  *divv = t.divv;
+  const long long l = (long long)i * nsec + j;
+  const float nu = D.visc[i];
+  float q;
+  if (nu != 0.0) {
+    q = 0.5 / nu / D.dens[l] * (t.rr * t.rr + +t.rp * t.rp + t.pp * t.pp);
+    q += (2.0 / 9.0) * nu * D.dens[l] * t.divv * t.divv;
+  } else
+    q = 0.0;
+  return q;
+}
+
+__global__ void __launch_bounds__(kThreads) k_energy(BatchDev B) {
+  CELL_PROLOGUE
+  if (!D.Adiabatic) return;
+  const float dt = C->dtf;
+  float divv;
+  float q = 0.0f;
+  if (i > 0) {
+    q = qplus_at(D, i, j, nsec, &divv);
+  } else {
+    float dv1, dv2;
+    float q1 = qplus_at(D, 1, j, nsec, &dv1);
+    float q2 = qplus_at(D, 2, j, nsec, &dv2);
+    Tau t0 = viscous_terms(D, D.vrad, D.vtheta, 0, j, nsec);
+    divv = t0.divv;
+    if (D.visc[nrad - 1] != 0.0)
+      q = q1 * expf(logf(q1 / q2) * logf(D.Rmed[0] / D.Rmed[1]) / logf(D.Rmed[1] / D.Rmed[2]));
+    else
+      q = 0.0;
+  }
+  const float e_int = D.energy[l];
+  const float Dl = D.dens[l];
+  float num, den;
+  if (!D.Cooling) {
+    num = dt * q + e_int;
+    den = 1.0 + (D.ADIABATICINDEX - 1.0) * dt * divv;
+  } else {
+    num = D.EnergyMed[i] * dt * Dl / D.SigmaMed[i] + D.CoolingTimeMed[i] * e_int +
+          dt * D.CoolingTimeMed[i] * (q - D.QplusMed[i] * Dl / D.SigmaMed[i]);
+    den = dt + D.CoolingTimeMed[i] + (D.ADIABATICINDEX - 1.0) * dt * D.CoolingTimeMed[i] * divv;
+  }
+  D.qplus[l] = q;
+  D.energy[l] = num / den;
+  if (i == nrad - 1) D.energy[l + nsec] = 0.0f;  // EnergyNew's ghost row is zero
+}
+
+// ------------------------------------------------------------- transport
+
+// van Leer slope of StarRadKernel (Kernels.cu:917-927)
+__device__ __forceinline__ float vl_rad_slope(float qm, float q0, float qp, float invdm, float invdp) {
+  float dqm = (q0 - qm) * invdm;
+  float dqp = (qp - q0) * invdp;
+  if (dqp * dqm > 0.0) return 2.0 * dqp * dqm / (dqp + dqm);
+  return 0.0f;
+}
+
+// LRMomentaKernel (Kernels.cu:883-896) + the radial half of Transport:
+// StarRadKernel/StarRadKernel2/VanLeerRadialKernel (Kernels.cu:909-947,
+// 1137-1154) for RadMomP, RadMomM, ThetaMomP, ThetaMomM, energy and density,
+// with DivisePolarGridKernel's quotient (Kernels.cu:1127-1134) formed per row.
+__global__ void __launch_bounds__(kThreads) k_transport_rad(BatchDev B) {
+  CELL_PROLOGUE
+  const float dt = C->dtf;
+  const float Om = C->OmegaFrame;
+  const int adi = D.Adiabatic;
+  // rows i-2 .. i+2 (clamped; the clamped values are never used)
+  float S[5], M1[5], M2[5], M3[5], M4[5], E[5], Vr[6];
+  double den[5];
+  for (int q = 0; q < 5; q++) {
+    int r = i - 2 + q;
+    r = r < 0 ? 0 : (r > nrad - 1 ? nrad - 1 : r);
+    const long long lr = (long long)r * nsec + j;
+    const long long lrp = (long long)r * nsec + jp;
+    float s = D.dens[lr];
+    float rm = D.Rmed[r];
+    S[q] = s;
+    M1[q] = s * D.vrad[lr + nsec];
+    M2[q] = s * D.vrad[lr];
+    M3[q] = s * (D.vtheta[lrp] + rm * Om) * rm;
+    M4[q] = s * (D.vtheta[lr] + rm * Om) * rm;
+    E[q] = adi ? D.energy[lr] : 0.0f;
+    den[q] = (double)s + 1e-20;
+  }
+  Vr[0] = D.vrad[l];
+  Vr[1] = D.vrad[l + nsec];  // row i+1 (row nrad is the zero ghost row)
+  // slope rows: r = i-1, i, i+1 ; interface rows: i, i+1
+  const float idm_im1 = (i - 1 >= 1) ? D.invdiffRmed[i - 1] : 0.0f;
+  const float idm_i = D.invdiffRmed[i];
+  const float idm_ip1 = (i + 1 <= nrad - 1) ? D.invdiffRmed[i + 1] : 0.0f;
+  const float idm_ip2 = (i + 2 <= nrad - 1) ? D.invdiffRmed[i + 2] : 0.0f;
+  auto slope = [&](const float* Q, int q) -> float {
+    // slope at row r = i-2+q
+    int r = i - 2 + q;
+    if (r <= 0 || r >= nrad - 1) return 0.0f;
+    float invm = (q == 1) ? idm_im1 : (q == 2 ? idm_i : idm_ip1);
+    float invp = (q == 1) ? idm_i : (q == 2 ? idm_ip1 : idm_ip2);
+    return vl_rad_slope(Q[q - 1], Q[q], Q[q + 1], invm, invp);
+  };
+  auto qstar = [&](const float* Q, int rr, float v) -> float {
+    // upwind interface value at ring rr (rr = i or i+1)
+    if (rr == 0 || rr >= nrad) return 0.0f;
+    int q = rr - (i - 2);
+    if (v > 0.0 && rr > 0)
+      return Q[q - 1] + (D.Rmed[rr] - D.Rmed[rr - 1] - v * dt) * 0.5 * slope(Q, q - 1);
+    float rnext = (rr + 1 <= nrad - 1) ? D.Rmed[rr + 1] : 0.0f;  // Rmed[NRAD]: times a zero slope
+    return Q[q] - (rnext - D.Rmed[rr] + v * dt) * 0.5 * slope(Q, q);
+  };
+  const float dstar_i = qstar(S, i, Vr[0]);
+  const float dstar_ip = qstar(S, i + 1, Vr[1]);
+  float dtheta = 2.0 * PI_D / (float)nsec;
+  const float Ri = D.Rinf[i], Rs = D.Rsup[i], iS = D.invSurf[i];
+  auto advect = [&](const float* Q) -> float {
+    float W[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) W[q] = (double)Q[q] * (1.0 / den[q]);
+    float qi = qstar(W, i, Vr[0]);
+    float qip = qstar(W, i + 1, Vr[1]);
+    float varq = dt * dtheta * Ri * qi * dstar_i * Vr[0];
+    varq -= dt * dtheta * Rs * qip * dstar_ip * Vr[1];
+    return Q[2] + varq * iS;
+  };
+  D.a1[l] = advect(M1);
+  D.a2[l] = advect(M2);
+  D.a3[l] = advect(M3);
+  D.a4[l] = advect(M4);
+  if (adi) D.a5[l] = advect(E);
+  D.a0[l] = advect(S);
+}
+
+// Azimuthal half of Transport for one ring segment (OneWindTheta,
+// TransportEuler.cu:171-219): ring mean (serial, as
+// ComputeAverageThetaVelocitiesKernel), residual, Nshift and constant
+// residual (ComputeConstantResidualKernel, Kernels.cu:1201-1232), the
+// residual and the constant-residual van Leer sweeps (StarThetaKernel,
+// StarThetaKernel2, VanLeerThetaKernel, Kernels.cu:1157-1273) on the
+// quantities of k_transport_rad, and AdvectSHIFTKernel (Kernels.cu:1276-1289)
+// fused into the store.
+__global__ void __launch_bounds__(kThreads) k_transport_theta(BatchDev B) {
+  extern __shared__ float sm[];
+  __shared__ float s_vmed;
+  __shared__ int s_nshift;
+  __shared__ float s_vconst;
+  const int4 it = B.theta_items[blockIdx.x];
+  const DiskDev& D = B.disks[it.x];
+  const DiskCtl* C = D.ctl;
+  if (!C->active || !D.IsDisk) return;
+  const int i = it.y, j0 = it.z, S = it.w;  // S sectors of output
+  const int nsec = D.nsec, tid = threadIdx.x;
+  const int L = S + 8;
+  const int nq = D.Adiabatic ? 6 : 5;  // M1..M4, [E], Sigma last
+  float* Q = sm;                    // nq * L
+  float* Vres = Q + 6 * L;          // L
+  float* dstar = Vres + L;          // L
+  float* work = dstar + L;          // L
+  float* dqa = work + L;            // L
+  float* qrs = dqa + L;             // L
+  const float dt = C->dtf;
+  const float* vt = D.vtheta + (size_t)i * nsec;
+  if (tid == 0) {
+    float moy = 0.0f;
+    for (int j = 0; j < nsec; j++) moy += vt[j];
+    float VMed = moy / (float)nsec;
+    float invdt = 1.0 / dt;
+    float dpinvns = 2.0 * PI_D / (float)nsec;
+    float Ntilde = VMed * D.invRmed[i] * dt * (float)nsec / 2.0 / PI_D;
+    float Nround = floor(Ntilde + 0.5);
+    long nitemp = (long)Nround;
+    s_nshift = (int)nitemp;
+    s_vmed = VMed;
+    s_vconst = (Ntilde - Nround) * D.Rmed[i] * invdt * dpinvns;
+    if (j0 == 0) {
+      D.nshift[i] = (int)nitemp;
+      int sidx = C->nsub - 1;
+      if (sidx >= 0 && sidx < FARGO_MAXLOG) D.log_nshift[(size_t)sidx * D.nrad + i] = (int)nitemp;
+    }
+  }
+  __syncthreads();
+  const int ns = s_nshift;
+  const float VMed = s_vmed;
+  float vconst = s_vconst;
+  const bool fast = D.FastTransport;
+  // source window: sectors js-4 .. js+S+3, js = j0 - Nshift (mod nsec)
+  int js = (j0 - ns) % nsec;
+  if (js < 0) js += nsec;
+  const float* srcs[6] = {D.a1, D.a2, D.a3, D.a4, D.Adiabatic ? D.a5 : D.a0, D.a0};
+  for (int p = tid; p < L; p += blockDim.x) {
+    int g = (js - 4 + p) % nsec;
+    if (g < 0) g += nsec;
+    const long long lg = (long long)i * nsec + g;
+    for (int q = 0; q < nq; q++) Q[q * L + p] = srcs[q == nq - 1 ? 5 : q][lg];
+    float vres = vt[g] - VMed;
+    if (!fast) vres = vconst + vres;
+    Vres[p] = vres;
+  }
+  if (!fast) vconst = 0.0f;
+  __syncthreads();
+  const float Rm = D.Rmed[i];
+  float dxtheta = 2.0 * PI_D / (float)nsec * Rm;
+  float invdxtheta = 1.0 / dxtheta;
+  float invsurf = 1.0 / D.Surf[i];
+  float dxrad = (D.Rsup[i] - D.Rinf[i]) * dt;
+  const float* Sg = Q + (nq - 1) * L;  // density: updated last in each sweep
+  for (int sweep = 0; sweep < 2; sweep++) {
+    const bool uni = (sweep == 1);
+    // StarTheta of the density with this sweep's velocity -> DensStar
+    for (int p = tid; p < L; p += blockDim.x) {
+      float dqv = 0.0f;
+      if (p > 0 && p < L - 1) {
+        float dqm = (Sg[p] - Sg[p - 1]);
+        float dqp = (Sg[p + 1] - Sg[p]);
+        if (dqp * dqm > 0.0) dqv = dqp * dqm / (dqp + dqm) * invdxtheta;
+      }
+      dqa[p] = dqv;
+    }
+    __syncthreads();
+    for (int p = tid; p < L; p += blockDim.x) {
+      float v = uni ? vconst : Vres[p];
+      float ksi = v * dt;
+      float qsv;
+      if (ksi > 0.0)
+        qsv = (p > 0) ? Sg[p - 1] + (dxtheta - ksi) * dqa[p - 1] : 0.0f;
+      else
+        qsv = Sg[p] - (dxtheta + ksi) * dqa[p];
+      dstar[p] = qsv;
+    }
+    __syncthreads();
+    for (int q = 0; q < nq; q++) {
+      float* Qq = Q + q * L;
+      // DivisePolarGrid by the pre-sweep density (DensInt)
+      for (int p = tid; p < L; p += blockDim.x) work[p] = (double)Qq[p] / ((double)Sg[p] + 1e-20);
+      __syncthreads();
+      for (int p = tid; p < L; p += blockDim.x) {
+        float dqv = 0.0f;
+        if (p > 0 && p < L - 1) {
+          float dqm = (work[p] - work[p - 1]);
+          float dqp = (work[p + 1] - work[p]);
+          if (dqp * dqm > 0.0) dqv = dqp * dqm / (dqp + dqm) * invdxtheta;
+        }
+        dqa[p] = dqv;
+      }
+      __syncthreads();
+      for (int p = tid; p < L; p += blockDim.x) {
+        float v = uni ? vconst : Vres[p];
+        float ksi = v * dt;
+        float qsv;
+        if (ksi > 0.0)
+          qsv = (p > 0) ? work[p - 1] + (dxtheta - ksi) * dqa[p - 1] : 0.0f;
+        else
+          qsv = work[p] - (dxtheta + ksi) * dqa[p];
+        qrs[p] = qsv;
+      }
+      __syncthreads();
+      for (int p = tid; p < L - 1; p += blockDim.x) {
+        float v0 = uni ? vconst : Vres[p];
+        float v1 = uni ? vconst : Vres[p + 1];
+        float varq = dxrad * qrs[p] * dstar[p] * v0;
+        varq -= dxrad * qrs[p + 1] * dstar[p + 1] * v1;
+        Qq[p] += varq * invsurf;
+      }
+      __syncthreads();
+    }
+  }
+  // shifted store: out sector j0+t <- source window position t+4
+  float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.energy, D.dens};
+  for (int t = tid; t < S; t += blockDim.x) {
+    const long long lo = (long long)i * nsec + j0 + t;
+    for (int q = 0; q < nq; q++) dsts[q == nq - 1 ? 5 : q][lo] = Q[q * L + t + 4];
+  }
+}
+
+// ComputeVelocitiesKernel, Kernels.cu:1292-1306 (momenta after the shift
+// sit in vri, vti, trr, tpp).
+__global__ void __launch_bounds__(kThreads) k_velocities(BatchDev B) {
+  CELL_PROLOGUE
+  const float* Dn = D.dens;
+  const long long lmj = (long long)i * nsec + jm;
+  float vr;
+  if (i == 0)
+    vr = 0.0;
+  else
+    vr = (D.vri[l - nsec] + D.vti[l]) / (Dn[l] + Dn[l - nsec] + 1e-20);
+  float vt = (D.trr[lmj] + D.tpp[l]) / (Dn[l] + Dn[lmj] + 1e-15) / D.Rmed[i] - D.Rmed[i] * C->OmegaFrame;
+  D.vrad[l] = vr;
+  D.vtheta[l] = vt;
+}
+
+// End of a substep: which disks take another one; drives the graph's loop.
+__global__ void k_substep_end(BatchDev B, cudaGraphConditionalHandle h, int use_handle) {
+  int any = 0;
+  for (int d = threadIdx.x; d < B.ndisk; d += blockDim.x) {
+    DiskCtl* C = B.disks[d].ctl;
+    if (C->active) C->active = C->more;
+    any |= C->active;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    B.flags[0] = any;
+    if (use_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
+  }
+}
+
+// Start of a DT (AlgoGas entry, SourceEuler.cu:211-229).
+__global__ void k_dt_begin(BatchDev B) {
+  int d = blockIdx.x;
+  if (d >= B.ndisk || threadIdx.x != 0) return;
+  const DiskDev& D = B.disks[d];
+  DiskCtl* C = D.ctl;
+  C->dtemp = 0.0;
+  C->nsub = 0;
+  C->active = 1;
+  C->more = 1;
+  C->counter = 0;
+  prepare_bodies(D, C);
+}
+
+// ComputeSoundSpeedKernel, adiabatic branch (Kernels.cu:190-191)
+__global__ void __launch_bounds__(kThreads) k_cs_adiabatic(BatchDev B, int only_disk) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= B.ncell) return;
+  const int d = disk_of_cell(B, c);
+  const DiskDev& D = B.disks[d];
+  if (!D.Adiabatic) return;
+  if (only_disk >= 0 ? d != only_disk : !D.ctl->active) return;
+  const int loc = (int)(c - D.cell0);
+  const long long l = loc;
+  D.cs[l] = sqrtf(D.ADIABATICINDEX * (D.ADIABATICINDEX - 1.0) * D.energy[l] / D.dens[l]);
+}
+
+// ComputeSoundSpeedKernel, isothermal branch (Kernels.cu:185-188): one value per ring.
+__global__ void k_cs_isothermal(BatchDev B, int only_disk) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= B.nring) return;
+  const int d = disk_of_ring(B, r);
+  const DiskDev& D = B.disks[d];
+  if (D.Adiabatic) return;
+  if (only_disk >= 0 && d != only_disk) return;
+  const int i = r - D.ring0;
+  const DiskCtl* C = D.ctl;
+  float AspectRatio = aspect_ratio_dev(D, D.Rmed[i], C->PhysicalTime, C->PhysicalTimeInitial);
+  D.cs_ring[i] = AspectRatio * sqrtf(1.0 * 1.0 / D.Rmed[i]) * powf(D.Rmed[i], D.FLARINGINDEX);
+}
+
+// Make1DprofileKernel on the sound speed (Kernels.cu:726-738): GLOBAL_bufarray.
+// One warp per ring, lane 0 adds the sectors in order.
+__global__ void k_cs_ringmean(BatchDev B, int only_disk) {
+  int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (r >= B.nring) return;
+  const int d = disk_of_ring(B, r);
+  const DiskDev& D = B.disks[d];
+  if (only_disk >= 0 ? d != only_disk : !D.ctl->active) return;
+  if (lane != 0) return;
+  const int i = r - D.ring0, nsec = D.nsec;
+  float sum = 0.0f;
+  if (D.Adiabatic) {
+    const float* f = D.cs + (size_t)i * nsec;
+    for (int j = 0; j < nsec; j++) sum += f[j];
+  } else {
+    const float v = D.cs_ring[i];
+    for (int j = 0; j < nsec; j++) sum += v;
+  }
+  D.csmean[i] = sum / (float)nsec;
+}
+
+// Sector tables: the angle formulas of FillForcesArraysKernel
+// (Kernels.cu:1332) and InitComputeAccelKernel (Kernels.cu:170-171).
+__global__ void k_sector_tables(BatchDev B) {
+  int d = blockIdx.y;
+  if (d >= B.ndisk) return;
+  const DiskDev& D = B.disks[d];
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= D.nsec) return;
+  int nsec = D.nsec;
+  float angle = (float)j / (float)nsec * 2.0 * PI_D;
+  const_cast<float*>(D.cos_pot)[j] = cosf(angle);
+  const_cast<float*>(D.sin_pot)[j] = sinf(angle);
+  const_cast<float*>(D.cos_cell)[j] = cosf(2.0 * PI_D * (float)j / (float)nsec);
+  const_cast<float*>(D.sin_cell)[j] = sinf(2.0 * PI_D * (float)j / (float)nsec);
+}
+
+// InitGasVelocitiesKernel (Kernels.cu:759-800).  Its ViscosityAlpha argument
+// is always 0 in the reference (int global read as float, then converted
+// back, Pframeforce.cu:20,269), so the constant-viscosity drift is used.
+__global__ void __launch_bounds__(kThreads) k_init_velocities(BatchDev B, int disk) {
+  // cells of one disk including the ghost row
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int d = disk;
+  const DiskDev& D = B.disks[d];
+  if (c >= (long long)(D.nrad + 1) * D.nsec) return;
+  const long long base = 0;
+  const DiskCtl* C = D.ctl;
+  const int nsec = D.nsec, nrad = D.nrad;
+  const int loc = (int)(c - base), i = loc / nsec, j = loc - i * nsec;
+  const long long l = loc;
+  float omega, r, ri;
+  if (i == nrad) {
+    r = D.Rmed[nrad - 1];
+    ri = D.Rinf[nrad - 1];
+  } else {
+    r = D.Rmed[i];
+    ri = D.Rinf[i];
+  }
+  float vt = D.vtheta[l];
+  if (!D.SelfGravity) {
+    omega = sqrtf(1.0 * 1.0 / r / r / r);
+    vt = omega * r *
+         sqrtf(1.0 - powf(D.ASPECTRATIO, 2.0) * powf(r, 2.0 * D.FLARINGINDEX) *
+                         (1. + D.SIGMASLOPE - 2.0 * D.FLARINGINDEX));
+  }
+  vt -= C->OmegaFrame * r;
+  D.vtheta[l] = vt;
+  float vr;
+  if (i == nrad)
+    vr = 0.0;
+  else {
+    vr = D.IMPOSEDDISKDRIFT * D.SIGMA0 / D.SigmaInf[i] / ri;
+    vr -= 3.0 * D.visc[i] / r * (-D.SIGMASLOPE + .5);
+  }
+  if (i == 0) vr = 0.0;
+  D.vrad[l] = vr;
+  // initial pressure (ComputePressureField in InitEuler) for the temperature output
+  if (!D.Adiabatic && i < nrad) {
+    float cs = D.cs_ring[i];
+    D.pres[l] = D.dens[l] * cs * cs;
+  }
+}
+
+// ComputeForce for one body at every Hill-cut level (Force.cu:314-328), as
+// UpdateLog uses it: 44 double sums.
+__global__ void __launch_bounds__(kThreads) k_disk_force(BatchDev B, int disk, float x, float y, float rs,
+                                                         float rh0, float a, double* out) {
+  const DiskDev& D = B.disks[disk];
+  const int nsec = D.nsec, nrad = D.nrad;
+  long long n = (long long)nrad * nsec;
+  double s[4 * FARGO_DIMFXY];
+  for (int q = 0; q < 4 * FARGO_DIMFXY; q++) s[q] = 0.0;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(c / nsec), j = (int)(c - (long long)i * nsec);
+    float cellmass = D.Surf[i] * D.dens[c];
+    float dx = D.Rmed[i] * D.cos_cell[j] - x;
+    float dy = D.Rmed[i] * D.sin_cell[j] - y;
+    float d2 = dx * dx + dy * dy;
+    float dist2 = d2 + rs * rs;
+    float distance = sqrtf(dist2);
+    float InvDist3 = 1.0 / ((double)dist2 * (double)distance);
+    bool inner = D.Rmed[i] < a;
+    for (int k = 0; k < FARGO_DIMFXY; k++) {
+      float hillcutfactor = (float)k / (float)(FARGO_DIMFXY - 1);
+      float hill_cut;
+      if (k != 0) {
+        float rh = rh0 * hillcutfactor;
+        hill_cut = 1. - expf(-d2 / (rh * rh));
+      } else
+        hill_cut = 1.;
+      float fx = 1.0 * cellmass * dx * InvDist3 * hill_cut;
+      float fy = 1.0 * cellmass * dy * InvDist3 * hill_cut;
+      if (inner) {
+        s[k] += fx;
+        s[k + 2 * FARGO_DIMFXY] += fy;
+      } else {
+        s[k + FARGO_DIMFXY] += fx;
+        s[k + 3 * FARGO_DIMFXY] += fy;
+      }
+    }
+  }
+  __shared__ double red[kThreads / 32];
+  for (int q = 0; q < 4 * FARGO_DIMFXY; q++) {
+    double v = warp_sum_d(s[q]);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double acc = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) acc += red[w];
+      out[(size_t)blockIdx.x * 4 * FARGO_DIMFXY + q] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// FP64 diagnostics: mass, angular momentum, Hill-sphere mass of planet 0
+// (CircumPlanetaryMassKernel, Kernels.cu:245-261).
+__global__ void __launch_bounds__(kThreads) k_diagnostics(BatchDev B, int disk, double* out) {
+  const DiskDev& D = B.disks[disk];
+  const DiskCtl* C = D.ctl;
+  const int nsec = D.nsec, nrad = D.nrad;
+  long long n = (long long)nrad * nsec;
+  float xpl = C->nb > 0 ? (float)C->x[0] : 0.0f, ypl = C->nb > 0 ? (float)C->y[0] : 0.0f;
+  double m = 0, am = 0, hill = 0;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(c / nsec), j = (int)(c - (long long)i * nsec);
+    int jp = jwrap_p(j, nsec);
+    double cm = (double)D.Surf[i] * (double)D.dens[c];
+    m += cm;
+    am += cm * (double)D.Rmed[i] *
+          (0.5 * ((double)D.vtheta[c] + (double)D.vtheta[(long long)i * nsec + jp]) + (double)D.Rmed[i] * C->OmegaFrame);
+    float cx = D.Rmed[i] * D.cos_cell[j], cy = D.Rmed[i] * D.sin_cell[j];
+    float dist = sqrtf((cx - xpl) * (cx - xpl) + (cy - ypl) * (cy - ypl));
+    if (C->nb > 0 && dist < D.HillRadius) hill += (double)(float)(D.Surf[i] * D.dens[c]);
+  }
+  __shared__ double red[3][kThreads / 32];
+  m = warp_sum_d(m);
+  am = warp_sum_d(am);
+  hill = warp_sum_d(hill);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = m;
+    red[1][threadIdx.x >> 5] = am;
+    red[2][threadIdx.x >> 5] = hill;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double acc = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) acc += red[threadIdx.x][w];
+    out[(size_t)blockIdx.x * 3 + threadIdx.x] = acc;
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+
+static inline unsigned cell_blocks(long long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+size_t fargo_theta_smem_bytes(int seg) { return sizeof(float) * 11 * (size_t)(seg + 8); }
+
+void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s) { k_dt_begin<<<b.ndisk, 32, 0, s>>>(b); }
+
+void fargo_launch_cs_refresh(const BatchDev& b, int only_disk, cudaStream_t s) {
+  k_cs_adiabatic<<<cell_blocks(b.ncell), kThreads, 0, s>>>(b, only_disk);
+  k_cs_ringmean<<<(unsigned)((b.nring * 32 + kThreads - 1) / kThreads), kThreads, 0, s>>>(b, only_disk);
+}
+
+void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s) {
+  k_cs_isothermal<<<(unsigned)((b.nring + 127) / 128), 128, 0, s>>>(b, only_disk);
+}
+
+int fargo_kernels_per_substep(int adiabatic) { return adiabatic ? 10 : 9; }
+
+void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int use_handle, cudaStream_t s,
+                          int max_nsec, long long* launches) {
+  unsigned cb = cell_blocks(b.ncell);
+  size_t ring_smem = sizeof(float) * (size_t)max_nsec;
+  k_cfl_force<<<b.nring, kThreads, ring_smem, s>>>(b);
+  k_source1<<<cb, kThreads, 0, s>>>(b);
+  k_visc_tau<<<cb, kThreads, 0, s>>>(b);
+  k_visc_update<<<cb, kThreads, 0, s>>>(b);
+  k_source2<<<cb, kThreads, 0, s>>>(b);
+  k_energy<<<cb, kThreads, 0, s>>>(b);
+  k_transport_rad<<<cb, kThreads, 0, s>>>(b);
+  k_transport_theta<<<b.ntheta_items, kThreads, fargo_theta_smem_bytes(b.theta_seg), s>>>(b);
+  k_velocities<<<cb, kThreads, 0, s>>>(b);
+  k_substep_end<<<1, 128, 0, s>>>(b, h, use_handle);
+  if (launches) *launches += 10;
+}
+
+void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s) {
+  dim3 g((max_nsec + 255) / 256, b.ndisk);
+  k_sector_tables<<<g, 256, 0, s>>>(b);
+}
+
+void fargo_launch_init_velocities(const BatchDev& b, int disk, long long ncell_ghost, cudaStream_t s) {
+  k_init_velocities<<<cell_blocks(ncell_ghost), kThreads, 0, s>>>(b, disk);
+}
+
+void fargo_launch_disk_force(const BatchDev& b, int disk, float x, float y, float rs, float rh, float a,
+                             double* out44, int nblocks, cudaStream_t s) {
+  k_disk_force<<<nblocks, kThreads, 0, s>>>(b, disk, x, y, rs, rh, a, out44);
+}
+
+void fargo_launch_diagnostics(const BatchDev& b, int disk, double* out3, int nblocks, cudaStream_t s) {
+  k_diagnostics<<<nblocks, kThreads, 0, s>>>(b, disk, out3);
+}
+
+cudaError_t fargo_kernel_attributes(int max_nsec, int seg) {
+  cudaError_t e = cudaFuncSetAttribute(k_cfl_force, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(float) * max_nsec));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_transport_theta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)fargo_theta_smem_bytes(seg));
+}

@@ -1,0 +1,289 @@
+// sg.cu -- self-gravity (SgMain.cu:23-195) on B200: cuFFT as the FFT engine,
+// hand-written fused kernels for the pad, the kernel-spectrum multiply and
+// the unpad/normalise/acceleration step.
+//
+// Differences in method from the reference, all exact in arithmetic:
+//   - the kernel spectra K^r, K^t are transformed once, in FP64 (D2Z), at
+//     creation; the reference re-transforms the constant kernels in FP32
+//     every call (SgMain.cu:124,138);
+//   - the density transforms are real-to-complex and the inverse
+//     complex-to-real (the inputs are real, so the reference's C2C result
+//     is the same Hermitian spectrum), batched two at a time;
+//   - the velocity kick (Update_sgvelocityKernel) is fused into the
+//     Substep1 kernel, so the accelerations are stored once and read once.
+#include <cufft.h>
+
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "sg.h"
+
+#define PI_D FARGO_PI
+
+struct SelfGravity {
+  int nrad = 0, nsec = 0, nx = 0, nyh = 0;
+  cufftHandle fwd = 0, inv = 0;
+  float* real2 = nullptr;     // [2][2*nrad][nsec]: Sr, St, then Gr, Gphi
+  float2* spec2 = nullptr;    // [2][2*nrad][nsec/2+1]
+  float2* khat = nullptr;     // [2][2*nrad][nsec/2+1]: K^r, K^t spectra
+  float eps = 0, rstep = 0, tstep = 0;
+  bool plans = false;
+};
+
+namespace {
+
+// ComputeFFTKernel's density part (Kernels.cu:957-976) as real arrays.
+__global__ void k_sg_pad(DiskDev D, float* real2, float eps) {
+  const int nrad = D.nrad, nsec = D.nsec;
+  long long n = 2LL * nrad * nsec;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  if (!D.ctl->active) return;
+  int i = (int)(c / nsec);
+  float sr = 0.0f, st = 0.0f;
+  if (i < nrad) {
+    float var = D.dens[c] * sqrtf(D.Rmed[i] / D.Rmed[0]);
+    sr = var;
+    st = var * D.Rmed[i] / D.Rmed[0];
+  }
+  real2[c] = sr;
+  real2[n + c] = st;
+  (void)eps;
+}
+
+// ComputeConvolutionKernel, Kernels.cu:980-999 (half spectrum)
+__global__ void k_sg_mul(const DiskCtl* C, float2* spec2, const float2* khat, long long nh) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nh) return;
+  if (!C->active) return;
+  float2 sr = spec2[c], st = spec2[nh + c];
+  float2 kr = khat[c], kt = khat[nh + c];
+  float2 gr, gp;
+  gp.x = -1.0 * (kt.x * st.x - kt.y * st.y);
+  gp.y = -1.0 * (kt.x * st.y + kt.y * st.x);
+  gr.x = -1.0 * (kr.x * sr.x - kr.y * sr.y);
+  gr.y = -1.0 * (kr.x * sr.y + kr.y * sr.x);
+  spec2[c] = gr;
+  spec2[nh + c] = gp;
+}
+
+// ComputeSgAccKernel, Kernels.cu:1002-1021 (the C2R output is unnormalised,
+// as cufftExecC2C INVERSE is in the reference).
+__global__ void k_sg_acc(DiskDev D, const float* real2, float rstep, float tstep, float eps) {
+  const int nrad = D.nrad, nsec = D.nsec;
+  long long n = (long long)nrad * nsec;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  if (!D.ctl->active) return;
+  int i = (int)(c / nsec);
+  long long n2 = 2LL * nrad * nsec;
+  float normaccr, normacct, divRmed;
+  divRmed = D.Rmed[i] / D.Rmed[0];
+  normaccr = rstep * tstep / ((float)(2 * nrad) * (float)nsec);
+  normacct = normaccr;
+  normaccr /= sqrtf(divRmed);
+  normacct /= (divRmed * sqrtf(divRmed));
+  D.sg_acct[c] = real2[n2 + c] * normacct;
+  float a = real2[c] * normaccr;
+  a += 1.0 * D.dens[c] * rstep * tstep / eps;
+  D.sg_accr[c] = a;
+}
+
+// Make1Dprofile(2) at rings 0 and NRAD-1 (SideEuler.cu:261-267 needs only these)
+__global__ void k_sg_axi_edges(DiskDev D) {
+  if (!D.ctl->active) return;
+  int t = threadIdx.x;
+  if (t > 1) return;
+  int i = (t == 0) ? 0 : D.nrad - 1;
+  const float* f = D.sg_accr + (size_t)i * D.nsec;
+  float s = 0.0f;
+  for (int j = 0; j < D.nsec; j++) s += f[j];
+  s /= (float)D.nsec;
+  if (t == 0)
+    D.ctl->axisg_in = s;
+  else
+    D.ctl->axisg_out = s;
+}
+
+// Make1Dprofile(2), all rings (initialisation only)
+__global__ void k_sg_axi_all(DiskDev D, float* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.nrad) return;
+  const float* f = D.sg_accr + (size_t)i * D.nsec;
+  float s = 0.0f;
+  for (int j = 0; j < D.nsec; j++) s += f[j];
+  out[i] = s / (float)D.nsec;
+}
+
+// Azimutalvelocity_withSGKernel, Kernels.cu:1044-1059
+__global__ void k_sg_vtheta(DiskDev D, const float* axi) {
+  long long n = (long long)D.nrad * D.nsec;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  int i = (int)(c / D.nsec);
+  float omegakep, omega, invr;
+  invr = 1. / D.Rmed[i];
+  omegakep = sqrt(1.0 * 1.0 * invr * invr * invr);
+  omega = sqrt(omegakep * omegakep *
+                   (1.0 - (1. + D.SIGMASLOPE - 2.0 * D.FLARINGINDEX) * powf(D.ASPECTRATIO, 2.0) *
+                              powf(D.Rmed[i], 2.0 * D.FLARINGINDEX)) -
+               invr * axi[i]);
+  D.vtheta[c] = D.Rmed[i] * omega;
+}
+
+__global__ void k_to_complex_float(const double2* in, float2* out, long long n) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) out[c] = make_float2((float)in[c].x, (float)in[c].y);
+}
+
+inline unsigned blocks(long long n) { return (unsigned)((n + 255) / 256); }
+
+fargo_status fail(std::string& err, fargo_status st, const char* what, int code) {
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "self-gravity: %s failed (%d)", what, code);
+  err = buf;
+  return st;
+}
+
+}  // namespace
+
+fargo_status sg_create(SelfGravity** out, const fargo_params* p, const HostTables& t, cudaStream_t s, DiskDev* D,
+                       std::string& err) {
+  SelfGravity* sg = new SelfGravity();
+  *out = sg;
+  const int NRAD = p->NRAD, NSEC = p->NSEC;
+  sg->nrad = NRAD;
+  sg->nsec = NSEC;
+  sg->nx = 2 * NRAD;
+  sg->nyh = NSEC / 2 + 1;
+  // Main.cu:308-310
+  sg->eps = p->THICKNESSSMOOTHING * p->ASPECTRATIO;
+  sg->rstep = logf(t.Radii[NRAD] / t.Radii[0]) / (float)NRAD;
+  sg->tstep = 2.0 * PI_D / (float)NSEC;
+  long long nr = (long long)sg->nx * NSEC, nh = (long long)sg->nx * sg->nyh;
+  cudaError_t e;
+  if ((e = cudaMalloc(&sg->real2, sizeof(float) * 2 * nr))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  if ((e = cudaMalloc(&sg->spec2, sizeof(float2) * 2 * nh))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  if ((e = cudaMalloc(&sg->khat, sizeof(float2) * 2 * nh))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  if ((e = cudaMalloc(&D->sg_accr, sizeof(float) * (size_t)NRAD * NSEC))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  if ((e = cudaMalloc(&D->sg_acct, sizeof(float) * (size_t)NRAD * NSEC))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  cudaMemsetAsync(D->sg_accr, 0, sizeof(float) * (size_t)NRAD * NSEC, s);
+  cudaMemsetAsync(D->sg_acct, 0, sizeof(float) * (size_t)NRAD * NSEC, s);
+  int n[2] = {sg->nx, NSEC};
+  cufftResult r;
+  if ((r = cufftPlanMany(&sg->fwd, 2, n, nullptr, 1, (int)nr, nullptr, 1, (int)nh, CUFFT_R2C, 2)))
+    return fail(err, FARGO_ECUFFT, "cufftPlanMany R2C", r);
+  if ((r = cufftPlanMany(&sg->inv, 2, n, nullptr, 1, (int)nh, nullptr, 1, (int)nr, CUFFT_C2R, 2)))
+    return fail(err, FARGO_ECUFFT, "cufftPlanMany C2R", r);
+  sg->plans = true;
+  cufftSetStream(sg->fwd, s);
+  cufftSetStream(sg->inv, s);
+  // compute_kernel (SgMain.cu:49-81), host float math as in the reference
+  std::vector<double> K(2 * (size_t)nr);
+  float eps = sg->eps;
+  for (int i = 0; i < 2 * NRAD; i++) {
+    float u;
+    if (i < NRAD)
+      u = logf(t.Radii[i] / t.Radii[0]);
+    else
+      u = -logf(t.Radii[2 * NRAD - i] / t.Radii[0]);
+    for (int j = 0; j < NSEC; j++) {
+      float theta = 2.0 * PI_D * (float)j / (float)NSEC;
+      float Kr = 1.0 + eps * eps - cosf(theta) * expf(-u);
+      float base = eps * eps * expf(u) + 2.0 * (coshf(u) - cosf(theta));
+      Kr *= powf(base, -1.5);
+      float Kt = sinf(theta);
+      Kt *= powf(base, -1.5);
+      K[(size_t)i * NSEC + j] = Kr;
+      K[nr + (size_t)i * NSEC + j] = Kt;
+    }
+  }
+  // FP64 transform of the kernels, once
+  double* dK = nullptr;
+  double2* dKh = nullptr;
+  if ((e = cudaMalloc(&dK, sizeof(double) * 2 * nr))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  if ((e = cudaMalloc(&dKh, sizeof(double2) * 2 * nh))) {
+    cudaFree(dK);
+    return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  }
+  cudaMemcpyAsync(dK, K.data(), sizeof(double) * 2 * nr, cudaMemcpyHostToDevice, s);
+  cufftHandle pd;
+  if ((r = cufftPlanMany(&pd, 2, n, nullptr, 1, (int)nr, nullptr, 1, (int)nh, CUFFT_D2Z, 2))) {
+    cudaFree(dK);
+    cudaFree(dKh);
+    return fail(err, FARGO_ECUFFT, "cufftPlanMany D2Z", r);
+  }
+  cufftSetStream(pd, s);
+  r = cufftExecD2Z(pd, dK, dKh);
+  k_to_complex_float<<<blocks(2 * nh), 256, 0, s>>>(dKh, sg->khat, 2 * nh);
+  cudaStreamSynchronize(s);
+  cufftDestroy(pd);
+  cudaFree(dK);
+  cudaFree(dKh);
+  if (r) return fail(err, FARGO_ECUFFT, "cufftExecD2Z", r);
+  return FARGO_OK;
+}
+
+void sg_destroy(SelfGravity* sg) {
+  if (!sg) return;
+  if (sg->plans) {
+    cufftDestroy(sg->fwd);
+    cufftDestroy(sg->inv);
+  }
+  cudaFree(sg->real2);
+  cudaFree(sg->spec2);
+  cudaFree(sg->khat);
+  delete sg;
+}
+
+void sg_capture_substep(SelfGravity* sg, const BatchDev& b, int d, DiskDev* D, cudaStream_t s) {
+  (void)b;
+  (void)d;
+  long long nr = (long long)sg->nx * sg->nsec, nh = (long long)sg->nx * sg->nyh;
+  cufftSetStream(sg->fwd, s);
+  cufftSetStream(sg->inv, s);
+  k_sg_pad<<<blocks(nr), 256, 0, s>>>(*D, sg->real2, sg->eps);
+  cufftExecR2C(sg->fwd, sg->real2, (cufftComplex*)sg->spec2);
+  k_sg_mul<<<blocks(nh), 256, 0, s>>>(D->ctl, sg->spec2, sg->khat, nh);
+  cufftExecC2R(sg->inv, (cufftComplex*)sg->spec2, sg->real2);
+  k_sg_acc<<<blocks((long long)sg->nrad * sg->nsec), 256, 0, s>>>(*D, sg->real2, sg->rstep, sg->tstep, sg->eps);
+  k_sg_axi_edges<<<1, 32, 0, s>>>(*D);
+}
+
+fargo_status sg_accelerations(SelfGravity* sg, const BatchDev& b, int d, DiskDev* D, cudaStream_t s,
+                              std::string& err) {
+  // the per-substep kernels check ctl->active: mark the disk active for this call
+  int one = 1;
+  cudaMemcpyAsync(&D->ctl->active, &one, sizeof(int), cudaMemcpyHostToDevice, s);
+  sg_capture_substep(sg, b, d, D, s);
+  int zero = 0;
+  cudaMemcpyAsync(&D->ctl->active, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(err, FARGO_ECUDA, "accelerations", e);
+  return FARGO_OK;
+}
+
+fargo_status sg_axisymmetric(SelfGravity* sg, DiskDev* D, float* axi, cudaStream_t s, std::string& err) {
+  float* dax = nullptr;
+  cudaError_t e = cudaMalloc(&dax, sizeof(float) * sg->nrad);
+  if (e) return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  k_sg_axi_all<<<(sg->nrad + 127) / 128, 128, 0, s>>>(*D, dax);
+  cudaMemcpyAsync(axi, dax, sizeof(float) * sg->nrad, cudaMemcpyDeviceToHost, s);
+  e = cudaStreamSynchronize(s);
+  cudaFree(dax);
+  if (e) return fail(err, FARGO_ECUDA, "axisymmetric profile", e);
+  return FARGO_OK;
+}
+
+fargo_status sg_init_vtheta(SelfGravity* sg, DiskDev* D, const float* axi, cudaStream_t s, std::string& err) {
+  float* dax = nullptr;
+  cudaError_t e = cudaMalloc(&dax, sizeof(float) * sg->nrad);
+  if (e) return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  cudaMemcpyAsync(dax, axi, sizeof(float) * sg->nrad, cudaMemcpyHostToDevice, s);
+  k_sg_vtheta<<<blocks((long long)sg->nrad * sg->nsec), 256, 0, s>>>(*D, dax);
+  e = cudaStreamSynchronize(s);
+  cudaFree(dax);
+  if (e) return fail(err, FARGO_ECUDA, "vtheta init", e);
+  return FARGO_OK;
+}

@@ -1,0 +1,22 @@
+// sg.h -- self-gravity of one disk: the log-polar convolution of
+// compute_selfgravity (SgMain.cu:23-162) with cuFFT as the FFT engine.
+#pragma once
+#include <string>
+
+#include "fargo_internal.h"
+#include "host_internal.h"
+
+struct SelfGravity;
+
+fargo_status sg_create(SelfGravity** out, const fargo_params* p, const HostTables& t, cudaStream_t s, DiskDev* D,
+                       std::string& err);
+void sg_destroy(SelfGravity* sg);
+// pad -> R2C -> kernel-spectrum multiply -> C2R -> accelerations (SG_Accr/SG_Acct)
+fargo_status sg_accelerations(SelfGravity* sg, const BatchDev& b, int d, DiskDev* D, cudaStream_t s,
+                              std::string& err);
+// Make1Dprofile(2): ring means of SG_Accr, copied to the host (nrad values)
+fargo_status sg_axisymmetric(SelfGravity* sg, DiskDev* D, float* axi, cudaStream_t s, std::string& err);
+// Init_azimutalvelocity_withSG (SourceEuler.cu:428-437)
+fargo_status sg_init_vtheta(SelfGravity* sg, DiskDev* D, const float* axi, cudaStream_t s, std::string& err);
+// enqueue the per-substep pipeline (capturable)
+void sg_capture_substep(SelfGravity* sg, const BatchDev& b, int d, DiskDev* D, cudaStream_t s);

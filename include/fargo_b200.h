@@ -1,0 +1,233 @@
+/*
+ * fargo_b200.h -- C ABI of the B200-native FARGO / FARGO_ADSG disk-hydro timestep.
+ *
+ * The reference (MatiasFloresS/CudaProtoplanetaryDisksFloat) has no library
+ * interface: its hot path is the set of host functions that AlgoGas calls,
+ * acting on ~60 process-global device arrays.  This header replaces exactly
+ * that path.  Every entry point names the reference code it stands in for.
+ *
+ * Conventions
+ *   - Plain C types, caller-owned host buffers (copied in/out), no torch types.
+ *   - Every call returns a fargo_status; nothing calls exit().  On error,
+ *     fargo_last_error(ctx) returns a one-line description.
+ *   - One context = one disk (or one batch of disks) on one CUDA device,
+ *     with its own stream.  Contexts are independent; a context must be used
+ *     from one host thread at a time.
+ *   - Grid fields are ring-major float32, (NRAD+1)*NSEC values, element
+ *     [i*NSEC + j] = ring i, sector j; row NRAD is the outer ghost row of the
+ *     reference (used by v_r).
+ */
+#ifndef FARGO_B200_H
+#define FARGO_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FARGO_ABI_VERSION 1
+#define FARGO_MAXPLANETS 100   /* RungeKutta.cu:4 static arrays of 100 */
+#define FARGO_DIMFXY 11        /* Main.cu:71 dimfxy: Hill-cut levels of ComputeForce */
+#define FARGO_STRLEN 512
+
+typedef enum fargo_status {
+  FARGO_OK = 0,
+  FARGO_EINVAL = 1,      /* bad argument or parameter combination          */
+  FARGO_ECUDA = 2,       /* CUDA runtime error                             */
+  FARGO_ECUFFT = 3,      /* cuFFT error (self-gravity)                     */
+  FARGO_ENONFINITE = 4,  /* NaN/Inf or non-positive density detected       */
+  FARGO_ETIMEOUT = 5,    /* a bounded device-side wait gave up             */
+  FARGO_EOOM = 6,        /* device allocation failed                       */
+  FARGO_EIO = 7,         /* file missing / unreadable / unwritable         */
+  FARGO_ENODEV = 8       /* no CUDA device, or the kernels are not loaded  */
+} fargo_status;
+
+/*
+ * Parameters of a run: the .par variables of the reference with the same
+ * names and defaults (Param.cuh:9-63 declarations, Interpret.cu:35-95
+ * parsing), the switches that ReadVariables derives from them
+ * (Interpret.cu:23-31,126-202) and the command-line switches that matter on
+ * the hot path (Main.cu:101-174).
+ */
+typedef struct fargo_params {
+  /* numeric .par variables */
+  float DT, SIGMA0;
+  int NINTERM, NTOT;
+  float MASSTAPER;
+  int NRAD, NSEC;
+  float RMIN, RMAX, THICKNESSSMOOTHING, ROCHESMOOTHING, ASPECTRATIO;
+  float VISCOSITY, ALPHAVISCOSITY, SIGMASLOPE, RELEASERADIUS, RELEASEDATE;
+  float OMEGAFRAME, IMPOSEDDISKDRIFT, FLARINGINDEX, ECCENTRICITY;
+  float CAVITYRADIUS, CAVITYRATIO, CAVITYWIDTH;
+  float TRANSITIONRADIUS, TRANSITIONRATIO, TRANSITIONWIDTH, LAMBDADOUBLING;
+  float ADIABATICINDEX, COOLINGTIME0;
+  /* string .par variables (first token after the key, as sscanf %s reads it) */
+  char OUTPUTDIR[FARGO_STRLEN];
+  char PLANETCONFIG[FARGO_STRLEN];
+  char INNERBOUNDARY[64], LABELADVECTION[64], TRANSPORT[64], RADIALSPACING[64];
+  char DISK[64], FRAME[64], OUTERSOURCEMASS[64], WRITEDENSITY[64], WRITEVELOCITY[64];
+  char WRITEENERGY[64], WRITETEMPERATURE[64], WRITEQPLUS[64], INDIRECTTERM[64];
+  char EXCLUDEHILL[64], SELFGRAVITY[64], CICPLANET[64], FORCEDCIRCULAR[64];
+  char ZMPLUS[64], ADIABATIC[64], COOLING[64];
+  /* switches derived by ReadVariables (Interpret.cu:126-202); 1 = YES */
+  int AdvecteLabel, OuterSourceMass, FastTransport, OpenInner, NonReflecting;
+  int Evanescent, LogGrid, IsDisk, Corotating, GuidingCenter;
+  int Write_Density, Write_Velocity, Write_Energy, Write_Temperature, Write_DivV;
+  int Write_Qplus, Indirect_Term, SelfGravity, SGZeroMode, ZMPluss;
+  int Adiabatic, Cooling, ExcludeHill, CICPlanet, ForcedCircular;
+  int ViscosityAlpha, RocheSmoothing;
+  /* command-line switches (Main.cu:110-174) */
+  int SloppyCFL;        /* -c */
+  float ScalingFactor;  /* -f */
+} fargo_params;
+
+/* Planetary system, FP64 (Types.cuh:2-15 planetary_system). */
+typedef struct fargo_planets {
+  int nb;
+  double mass[FARGO_MAXPLANETS], x[FARGO_MAXPLANETS], y[FARGO_MAXPLANETS];
+  double vx[FARGO_MAXPLANETS], vy[FARGO_MAXPLANETS], acc[FARGO_MAXPLANETS];
+  int feeldisk[FARGO_MAXPLANETS], feelothers[FARGO_MAXPLANETS];
+  char name[FARGO_MAXPLANETS][64];
+} fargo_planets;
+
+/* Scalars of the last advanced DT (for logs, bigplanet files and tests). */
+typedef struct fargo_scalars {
+  float physical_time;      /* PhysicalTime (Viscosity.cu:15), float as in the reference */
+  float omega_frame;        /* OmegaFrame */
+  float mdcp1;              /* CircumPlanetaryMass of planet 0 (SourceEuler.cu:539-553) */
+  float lost_mass;          /* LostMass (TransportEuler.cu:17,71) */
+  int nsub_last_dt;         /* hydro substeps taken by the last DT */
+  int nsub_total;           /* hydro substeps since fargo_create */
+  double mass;              /* FP64 sum of Sigma*Surf over active cells */
+  double angular_momentum;  /* FP64 sum of Sigma*Surf*r*(v_theta + r*OmegaFrame) (cell-centred) */
+  double last_dt;           /* dt of the last substep */
+} fargo_scalars;
+
+typedef struct fargo_ctx fargo_ctx;
+
+/* ---- parameter / configuration handling (host only, no GPU needed) ---- */
+
+/* Reference defaults of every variable (Param.cuh:9-63, Interpret.cu:23-31). */
+fargo_status fargo_params_default(fargo_params* p);
+
+/* ReadVariables (Interpret.cu:97-208) + SearchVariable (Interpret.cu:35-95):
+   case-insensitive keys, first token as value, unknown keys ignored, the
+   same consistency checks (reported as FARGO_EINVAL instead of exit(1)). */
+fargo_status fargo_params_read(const char* parfile, fargo_params* p);
+
+/* Re-derive the YES/NO switches from the string variables
+   (Interpret.cu:126-202); use after editing strings by hand. */
+fargo_status fargo_params_derive(fargo_params* p);
+
+/* InitPlanetarySystem (Psys.cu:159-208) with FindNumberOfPlanets
+   (Psys.cu:83-99).  p supplies ECCENTRICITY and the grid for CICPLANET. */
+fargo_status fargo_planets_read(const char* cfgfile, const fargo_params* p,
+                                fargo_planets* out);
+
+/* FillPolar1DArrays (SourceEuler.cu:76-173): interface radii, NRAD+1 doubles
+   (the values written to used_rad.dat) and the float tables used on device. */
+fargo_status fargo_grid_radii(const fargo_params* p, double* radii_out /* NRAD+1 */);
+
+/* ---- context lifetime ---- */
+
+/* Everything main() does between ReadVariables and the DT loop
+   (Main.cu:198-344): grid tables, initial Sigma/energy/velocities, sound
+   speed, pressure, per-ring viscosity, planets; device memory, stream and
+   graphs.  radii may be NULL (computed from RMIN/RMAX/RadialSpacing) or
+   point to NRAD+1 interface radii (the reference's radii.dat path).
+   device < 0 selects the current device. */
+fargo_status fargo_create(const fargo_params* p, const fargo_planets* planets,
+                          const double* radii, int device, fargo_ctx** out);
+void fargo_destroy(fargo_ctx* ctx);
+const char* fargo_last_error(const fargo_ctx* ctx);
+
+/* Re-run the initialisation of main() from InitGasDensity on (Main.cu:292-344:
+   self-gravity start-up, OmegaFrame, sound speed, viscosity table, initial
+   velocities) with the given surface density and energy in place of the
+   reference's axisymmetric profiles.  This is where the reference would see
+   a perturbed initial density.  dens/energy may be NULL (profiles). */
+fargo_status fargo_init_state(fargo_ctx* ctx, const float* dens, const float* energy);
+
+/* Replace the disk state (H2D), e.g. seeded noisy initial conditions.
+   Any pointer may be NULL to keep that field.  (Cudamalloc, Main.cu:700-867) */
+fargo_status fargo_upload(fargo_ctx* ctx, const float* dens, const float* vrad,
+                          const float* vtheta, const float* energy);
+
+/* Read the disk state (D2H).  Any pointer may be NULL.  temperature and
+   qplus are the reference's output-only fields (DeviceToHostcudaMemcpy,
+   Main.cu:643-654; ComputeTemperatureField, SourceEuler.cu:458-463). */
+fargo_status fargo_download(fargo_ctx* ctx, float* dens, float* vrad, float* vtheta,
+                            float* energy, float* temperature, float* qplus);
+
+fargo_status fargo_get_planets(fargo_ctx* ctx, fargo_planets* out);
+fargo_status fargo_set_planets(fargo_ctx* ctx, const fargo_planets* in);
+
+/* One DT of the hydro loop: the body of AlgoGas (SourceEuler.cu:208-301),
+   all CFL substeps, planet kicks and RK5 on the device.  nsub_out (may be
+   NULL) receives the number of substeps taken. */
+fargo_status fargo_advance_dt(fargo_ctx* ctx, int* nsub_out);
+
+/* ndt DTs back to back without host synchronisation in between (one CUDA
+   graph launch per DT), then wait.  Scalars are those of the last DT. */
+fargo_status fargo_advance(fargo_ctx* ctx, int ndt);
+/* Same without the final wait (pair with fargo_sync). */
+fargo_status fargo_advance_async(fargo_ctx* ctx, int ndt);
+
+/* Wait for the context's stream. */
+fargo_status fargo_sync(fargo_ctx* ctx);
+
+/* ComputeForce (Force.cu:31-67) as UpdateLog uses it (Force.cu:102):
+   disk force on a body at (x,y), all FARGO_DIMFXY Hill-cut levels.
+   globalforce[k + m*dimfxy], m = 0 fx_inner, 1 fx_outer, 2 fy_inner,
+   3 fy_outer; FP64 sums of the FP32 per-cell forces. */
+fargo_status fargo_disk_force(fargo_ctx* ctx, double x, double y, double rsmoothing,
+                              double mass, int dimfxy, double* globalforce);
+
+/* Scalars after the last DT (also recomputes mdcp1, mass, angular momentum). */
+fargo_status fargo_get_scalars(fargo_ctx* ctx, fargo_scalars* out);
+
+/* Per-substep record of the last DT, for bit-exact parity checks:
+   nshift[s*NRAD + i] = FARGO integer shift of ring i in substep s
+   (ComputeConstantResidualKernel, Kernels.cu:1218-1221), dt[s] = substep dt.
+   cap = room in substeps; *nsub receives the count. */
+fargo_status fargo_get_substep_log(fargo_ctx* ctx, int cap, int* nshift, double* dt, int* nsub);
+
+/* ---- batched form: many independent disks, one launch per kernel ---- */
+
+/* n contexts' worth of disks in one batch (different NRAD/NSEC/parameters).
+   Each disk keeps its own CFL substep sequence; one fargo_batch_advance_dt
+   advances every disk by its own DT. */
+typedef struct fargo_batch fargo_batch;
+fargo_status fargo_batch_create(int n, const fargo_params* params, const fargo_planets* planets,
+                                int device, fargo_batch** out);
+void fargo_batch_destroy(fargo_batch* b);
+const char* fargo_batch_last_error(const fargo_batch* b);
+fargo_status fargo_batch_upload(fargo_batch* b, int disk, const float* dens, const float* vrad,
+                                const float* vtheta, const float* energy);
+fargo_status fargo_batch_download(fargo_batch* b, int disk, float* dens, float* vrad,
+                                  float* vtheta, float* energy);
+fargo_status fargo_batch_init_state(fargo_batch* b, int disk, const float* dens, const float* energy);
+fargo_status fargo_batch_advance(fargo_batch* b, int ndt);
+fargo_status fargo_batch_advance_async(fargo_batch* b, int ndt);
+fargo_status fargo_batch_sync(fargo_batch* b);
+fargo_status fargo_batch_get_scalars(fargo_batch* b, int disk, fargo_scalars* out);
+fargo_status fargo_batch_get_planets(fargo_batch* b, int disk, fargo_planets* out);
+
+/* Library facts for tests and tools. */
+int fargo_abi_version(void);
+/* Kernel launches of this library on the context outside the DT graph. */
+long long fargo_kernel_launches(const fargo_ctx* ctx);
+/* All kernel launches of this library on the batch since creation,
+   including those inside the DT graphs (substeps x kernels per substep). */
+long long fargo_batch_count_launches(fargo_batch* b);
+long long fargo_batch_kernel_launches(const fargo_batch* b);
+/* 1 (default): one CUDA graph launch per DT with a device-driven WHILE node
+   over the substeps; 0: host loop with one wait per substep. */
+fargo_status fargo_set_graph_mode(fargo_ctx* ctx, int use_graph);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FARGO_B200_H */
