@@ -1,0 +1,490 @@
+#!/usr/bin/env python
+"""Throughput of the FARGO hydro step on B200: cell-updates/s.
+
+A cell-update is one active cell (NRAD*NSEC, ghost row excluded) advanced
+through one hydro substep.  One bench *step* is one DT of every disk of the
+workload (each disk takes its own CFL substeps inside the DT).
+
+Workloads (--workload):
+  c4  (default) 64 isothermal disks of uneven size and physics, batched: one
+      launch per kernel advances all of them (the "batched" form)
+  c4plain  the same 64 disks advanced one after another (the "plain" form)
+  c1, c2, c3, c5  single disks of the other configurations
+
+Output: one JSON line (rank 0).  `value` is device-resident throughput
+(CUDA events on the library's stream); `e2e` goes through the C ABI with
+page-locked host buffers: every step uploads every disk's state, advances
+one DT and downloads the state.  `--impl reference` times the reference's
+own CUDA build (oracle/_ref/fargo_ref, from the reference sources) on a
+bounded sample of the same disks, with its own AlgoGas timer.
+
+Multi-GPU: `torchrun --nproc-per-node N bench.py --gpus N`; every rank
+advances its own 64-disk batch (disjoint seeds), no collective in the data
+path (weak scaling); the timed region is bracketed by barriers and the max
+over ranks is taken.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic bytes per cell and launch of each substep kernel (the fields it
+# must read and write once; isothermal / adiabatic), for the roofline figure.
+KERNEL_BYTES = {
+    "k_cfl_force": (12, 20),       # Sigma, v_r, v_theta (+cs) read
+    "k_source1": (20, 24),         # Sigma, v_r, v_theta (+e) read; VradInt, VthetaInt written
+    "k_visc_tau": (24, 24),        # VradInt, VthetaInt, Sigma read; 3 stresses written
+    "k_visc_update": (28, 28),     # 3 stresses, Sigma, VradInt, VthetaInt read; 2 written
+    "k_source2": (20, 28),         # VradInt, VthetaInt, Sigma (+e) read; v_r, v_theta (+e) written
+    "k_energy": (0, 24),           # v_r, v_theta, Sigma, e read; e, Q+ written
+    "k_transport": (32, 40),       # Sigma, v_r, v_theta (+e) read; Sigma + 4 momenta (+e) written
+    "k_velocities": (32, 40),      # Sigma + 4 momenta (+e) read; v_r, v_theta, Sigma (+e) written
+    "k_substep_end": (0, 0),
+}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                smax.append(float(parts[2].split()[0]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        import torch
+        pg.barrier(device_ids=[torch.cuda.current_device()])
+
+
+def allmax(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allsum(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def workload_disks(name, seed_shift=0):
+    from cudaprotoplanetarydisksfloat_b200 import configs
+    if name in ("c4", "c4plain"):
+        return configs.c4(64, seed=42 + seed_shift)
+    fn = {"c1": configs.c1, "c2": configs.c2, "c3": configs.c3, "c5": configs.c5}[name]
+    return [fn()]
+
+
+def materialise_all(disks, tmp):
+    from cudaprotoplanetarydisksfloat_b200 import configs, read_params, read_planets
+    P, L = [], []
+    for k, (p, pl) in enumerate(disks):
+        par, cfg, out = configs.materialise(p, pl, tmp, "disk%02d" % k)
+        P.append(read_params(par))
+        L.append(read_planets(cfg, P[-1]))
+    return P, L
+
+
+def noisy_init(batch, P, seed0):
+    from cudaprotoplanetarydisksfloat_b200 import noise
+    for d, p in enumerate(P):
+        f = batch.fields(d)
+        dens = noise.perturb_density(f["dens"].reshape(-1), p.NRAD, p.NSEC, seed0 + d)
+        batch.init_state(d, dens=dens)
+
+
+def ours(args, world, rank, local, pg):
+    import torch
+
+    from cudaprotoplanetarydisksfloat_b200 import Batch
+    from cudaprotoplanetarydisksfloat_b200._abi import lib
+
+    torch.cuda.set_device(local)
+    tmp = tempfile.mkdtemp(prefix="fargo_bench_")
+    disks = workload_disks(args.workload, seed_shift=rank)
+    P, L = materialise_all(disks, tmp)
+    cells = np.array([p.NRAD * p.NSEC for p in P], dtype=np.int64)
+    plain = args.workload == "c4plain"
+    groups = [[d] for d in range(len(P))] if plain else [list(range(len(P)))]
+    batches = [Batch([P[d] for d in g], [L[d] for d in g], device=local) for g in groups]
+    for b, g in zip(batches, groups):
+        noisy_init(b, [P[d] for d in g], 20261203 + 1000 * rank + g[0])
+    streams = [torch.cuda.ExternalStream(lib.fargo_batch_stream(b.b), device=local) for b in batches]
+
+    def nsub_total():
+        return np.array([b.scalars(k)["nsub_total"] for b, g in zip(batches, groups) for k in range(len(g))],
+                        dtype=np.int64)
+
+    def run(k):
+        for b in batches:
+            b.advance_async(k)
+
+    # warm-up
+    run(args.warmup)
+    for b in batches:
+        b.sync()
+    n0 = nsub_total()
+    l0 = sum(lib.fargo_batch_count_launches(b.b) for b in batches)
+    barrier(pg)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in batches]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in batches]
+    t_wall = time.time()
+    if plain:
+        # one disk after another on its own stream: serialise through stream 0's events
+        ev0[0].record(streams[0])
+        for i, b in enumerate(batches):
+            if i > 0:
+                streams[i].wait_event(ev1[i - 1])
+            b.advance_async(args.steps)
+            ev1[i].record(streams[i])
+        for b in batches:
+            b.sync()
+        ms = ev0[0].elapsed_time(ev1[-1])
+    else:
+        ev0[0].record(streams[0])
+        run(args.steps)
+        ev1[0].record(streams[0])
+        batches[0].sync()
+        ms = ev0[0].elapsed_time(ev1[0])
+    torch.cuda.synchronize()
+    t_wall = time.time() - t_wall
+    clocks = clk.stop()
+    barrier(pg)
+    n1 = nsub_total()
+    l1 = sum(lib.fargo_batch_count_launches(b.b) for b in batches)
+    upd = float(np.sum(cells * (n1 - n0)))
+    ms_max = allmax(pg, ms)
+    upd_all = allsum(pg, upd)
+    value = upd_all / (ms_max * 1e-3)
+
+    # end to end through the C ABI with page-locked host buffers
+    pinned = []
+    for b, g in zip(batches, groups):
+        for k, d in enumerate(g):
+            n = (P[d].NRAD + 1) * P[d].NSEC
+            arrs = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(3)]
+            f = b.fields(k)
+            for a, key in zip(arrs, ("dens", "vrad", "vtheta")):
+                a.numpy()[:] = f[key].reshape(-1)
+            pinned.append((b, k, arrs))
+    fp = C.POINTER(C.c_float)
+
+    def e2e_step():
+        for b, k, arrs in pinned:
+            ptrs = [C.cast(a.data_ptr(), fp) for a in arrs]
+            lib.fargo_batch_upload_async(b.b, k, ptrs[0], ptrs[1], ptrs[2], None)
+        for b in batches:
+            lib.fargo_batch_advance_async(b.b, 1)
+        for b, k, arrs in pinned:
+            ptrs = [C.cast(a.data_ptr(), fp) for a in arrs]
+            lib.fargo_batch_download_async(b.b, k, ptrs[0], ptrs[1], ptrs[2], None)
+
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    for _ in range(2):
+        e2e_step()
+    for b in batches:
+        b.sync()
+    n0 = nsub_total()
+    barrier(pg)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(streams[0])
+    for _ in range(e2e_steps):
+        e2e_step()
+        if plain:
+            for b in batches:
+                b.sync()
+    e1.record(streams[-1])
+    for b in batches:
+        b.sync()
+    torch.cuda.synchronize()
+    e_ms = e0.elapsed_time(e1)
+    n1 = nsub_total()
+    e_upd = allsum(pg, float(np.sum(cells * (n1 - n0))))
+    e_ms = allmax(pg, e_ms)
+    bytes_io = sum(4 * 3 * (P[d].NRAD + 1) * P[d].NSEC for d in range(len(P)))
+    e2e = {"value": e_upd / (e_ms * 1e-3), "unit": "cell-updates/s", "h2d_bytes_per_step": bytes_io * world,
+           "d2h_bytes_per_step": bytes_io * world, "steps": e2e_steps}
+
+    # per-kernel device time (host loop with events around every launch)
+    roof = None
+    if rank == 0:
+        nk = lib.fargo_profile_kernel_count()
+        ms_k = np.zeros(nk)
+        n0 = nsub_total()
+        for b in batches:
+            arr = (C.c_double * 16)()
+            ns = C.c_int(0)
+            st = lib.fargo_batch_profile(b.b, args.profile_steps, arr, C.byref(ns))
+            if st == 0:
+                ms_k += np.array(arr[:nk])
+        n1 = nsub_total()
+        upd_prof = float(np.sum(cells * (n1 - n0)))
+        names = [lib.fargo_profile_kernel_name(k).decode() for k in range(nk)]
+        top = int(np.argmax(ms_k[:nk - 1]))
+        name = names[top]
+        adi = int(P[0].Adiabatic)
+        bpc = KERNEL_BYTES[name][adi]
+        launches = int(np.sum(n1 - n0)) if plain else int(max(1, (n1 - n0).max()))
+        peak, kind = load_peaks()
+        achieved = bpc * upd_prof / (ms_k[top] * 1e-3) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        try:
+            tj = json.load(open(tpath))
+            if name in tj:
+                traffic = float(tj[name]["dram_bytes_per_cell"]) * upd_prof / launches
+        except Exception:
+            pass
+        roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
+                "peak_kind": kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": traffic, "alg_bytes_per_launch": bpc * upd_prof / launches,
+                "kernel_ms_share": {names[k]: round(float(ms_k[k] / ms_k.sum()), 4) for k in range(nk)
+                                    if ms_k[k] > 0}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args, disks)
+    for b in batches:
+        b.close()
+    return {
+        "value": value, "ms_per_step": ms_max / args.steps, "e2e": e2e, "roofline": roof,
+        "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(l1 - l0) * world,
+        "wall_s": t_wall, "cells": int(cells.sum()) * world, "disks": len(P) * world,
+    }
+
+
+def cpu_baseline(args, disks):
+    """The oracle (CPU restatement, OpenMP, all host cores) on one disk of the
+    workload for a bounded number of DTs."""
+    from cudaprotoplanetarydisksfloat_b200 import noise
+    from oracle.oracle import Oracle, set_threads
+    tmp = tempfile.mkdtemp(prefix="fargo_cpu_")
+    sizes = [int(p["Nrad"]) * int(p["Nsec"]) for p, _ in disks]
+    k = int(np.argsort(sizes)[len(sizes) // 2])
+    P, L = materialise_all([disks[k]], tmp)
+    cores = os.cpu_count() or 1
+    set_threads(cores)
+    o = Oracle(P[0], L[0])
+    f = o.fields()
+    o.set_fields(dens=noise.perturb_density(f["dens"].reshape(-1), P[0].NRAD, P[0].NSEC, 7))
+    o.advance_dt()
+    t0 = time.time()
+    nsub = 0
+    ndt = 0
+    while ndt < args.cpu_max_dt and time.time() - t0 < args.cpu_seconds:
+        nsub += o.advance_dt()
+        ndt += 1
+    dt = time.time() - t0
+    cells = P[0].NRAD * P[0].NSEC
+    return {"value": cells * nsub / dt, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+            "sample": "oracle f32, disk %d of the workload (%dx%d), %d DTs, %d substeps, %.1f s"
+                      % (k, P[0].NRAD, P[0].NSEC, ndt, nsub, dt)}
+
+
+def reference(args, world, rank):
+    """The reference's own CUDA build on a sample of the workload's disks."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "fargo_ref")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/fargo_ref is not built (needs the reference sources at build time)"}
+    from cudaprotoplanetarydisksfloat_b200 import configs
+    disks = workload_disks(args.workload)
+    if args.workload in ("c4", "c4plain"):
+        sizes = np.array([int(p["Nrad"]) * int(p["Nsec"]) for p, _ in disks])
+        order = np.argsort(sizes)
+        pick = [int(order[int(q * (len(order) - 1))]) for q in np.linspace(0, 1, args.ref_disks)]
+    else:
+        pick = [0]
+    tmp = tempfile.mkdtemp(prefix="fargo_ref_")
+    tot_upd, tot_s, tot_dt, samples = 0.0, 0.0, 0, []
+    for k in pick:
+        p, pl = disks[k]
+        ndt = args.warmup + args.ref_steps
+        p = dict(p, Ntot=str(ndt - 1), Ninterm="100000")
+        d = os.path.join(tmp, "disk%02d" % k)
+        par, cfg, out = configs.materialise(p, pl, d, "run", relative=True)
+        env = dict(os.environ, FARGO_REF_DUMP="dump_", FARGO_REF_NOISE_SEED=str(20261203 + k))
+        r = subprocess.run([exe, "run.par"], cwd=d, env=env, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                           timeout=1200)
+        if r.returncode != 0:
+            return {"unavailable": "reference run failed with exit code %d" % r.returncode}
+        alg = np.loadtxt(os.path.join(d, "dump_algogas.txt"), ndmin=2)
+        nrad, nsec = int(p["Nrad"]), int(p["Nsec"])
+        raw = np.fromfile(os.path.join(d, "dump_nshift.bin"), dtype=np.uint8)
+        rec = 8 + 4 * nrad
+        dts = raw[: (raw.size // rec) * rec].reshape(-1, rec)[:, :8].copy().view(np.float64).reshape(-1)
+        # substeps per DT from the dt sequence (each DT sums to DT)
+        DT = float(p["DT"])
+        per_dt, acc, cnt = [], 0.0, 0
+        for x in dts:
+            acc += x
+            cnt += 1
+            if acc >= 0.999999999 * np.float32(DT):
+                per_dt.append(cnt)
+                acc, cnt = 0.0, 0
+        per_dt = np.array(per_dt[: alg.shape[0]])
+        sel = slice(args.warmup, alg.shape[0])
+        tot_upd += float(np.sum(per_dt[sel])) * nrad * nsec
+        tot_s += float(np.sum(alg[sel, 1]))
+        tot_dt += alg.shape[0] - args.warmup
+        samples.append("%dx%d" % (nrad, nsec))
+    value = tot_upd / tot_s
+    return {"value": value, "ms_per_step": 1e3 * tot_s / max(1, tot_dt), "sample": samples, "dts": tot_dt}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c4", choices=["c4", "c4plain", "c1", "c2", "c3", "c5"])
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--profile-steps", type=int, default=2)
+    ap.add_argument("--ref-disks", type=int, default=6)
+    ap.add_argument("--ref-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-max-dt", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local, pg = dist_setup(args)
+    wl_desc = {"c4": "64 isothermal disks (Nrad in {128..512}, Nsec=3*Nrad), batched, one DT each",
+               "c4plain": "64 isothermal disks (Nrad in {128..512}, Nsec=3*Nrad), one after another",
+               "c1": "isothermal 128x384, 1 planet", "c2": "adiabatic 256x768, alpha viscosity, 2 live planets",
+               "c3": "self-gravitating 512x1024, 1 planet", "c5": "adiabatic+SG 2048x6144, 3 live planets"}
+    config = {"workload": args.workload, "description": wl_desc[args.workload],
+              "parallelism": "disk-parallel, one 64-disk batch per GPU" if args.workload.startswith("c4") else
+              "single disk per GPU", "l2": "working set larger than L2" if args.workload in ("c4", "c4plain", "c5")
+              else "working set L2-resident (launch-bound)"}
+    metric = "cell-updates/s"
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        r = reference(args, world, rank)
+        line = {"metric": metric, "impl": "reference", "unit": "cell-updates/s", "n_gpus": 1,
+                "steps": args.ref_steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded noise)", "config": config}
+        if "unavailable" in r:
+            line = {"impl": "reference", "unavailable": r["unavailable"]}
+        else:
+            line.update({"value": r["value"], "ms_per_step": r["ms_per_step"],
+                         "e2e": {"value": r["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                                 "d2h_bytes_per_step": 0},
+                         "cpu_baseline": {"value": r["value"], "unit": "cell-updates/s", "cores": 1,
+                                          "kind": "reference",
+                                          "sample": "the reference's own CUDA build on the B200 (its only "
+                                                    "implementation), disks %s, %d DTs, AlgoGas wall time"
+                                                    % (",".join(r["sample"]), r["dts"])}})
+        print(json.dumps(line), flush=True)
+        return 0
+    r = ours(args, world, rank, local, pg)
+    if rank == 0:
+        line = {"metric": metric, "value": r["value"], "unit": "cell-updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded parameters and density noise)",
+                "config": dict(config, disks=r["disks"], cells=r["cells"]),
+                "e2e": r["e2e"], "roofline": r["roofline"], "cpu_baseline": r["cpu_baseline"],
+                "clocks": r["clocks"], "gpu_launches": r["gpu_launches"]}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

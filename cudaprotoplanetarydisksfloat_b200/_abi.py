@@ -83,7 +83,9 @@ EXPORTS = [
     "fargo_batch_init_state", "fargo_batch_upload", "fargo_batch_download", "fargo_batch_advance",
     "fargo_batch_advance_async", "fargo_batch_sync", "fargo_batch_get_scalars",
     "fargo_batch_get_planets", "fargo_batch_count_launches", "fargo_batch_kernel_launches", "fargo_abi_version",
-    "fargo_kernel_launches", "fargo_set_graph_mode",
+    "fargo_kernel_launches", "fargo_set_graph_mode", "fargo_stream", "fargo_batch_stream",
+    "fargo_ctx_batch", "fargo_batch_upload_async", "fargo_batch_download_async", "fargo_batch_profile",
+    "fargo_profile_kernel_name", "fargo_profile_kernel_count",
 ]
 
 
@@ -94,7 +96,7 @@ class FargoError(RuntimeError):
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            "libfargo_b200.so is not built (run `python -m cudaprotoplanetarydisksfloat_b200.build`); "
+            "libfargo_b200.so is not built (run `python cudaprotoplanetarydisksfloat_b200/build.py`); "
             "there is no CPU fallback of the CUDA hot path")
     lib = C.CDLL(LIB_PATH)
     P = C.POINTER
@@ -138,6 +140,14 @@ def _load():
         "fargo_abi_version": (C.c_int, []),
         "fargo_kernel_launches": (C.c_longlong, [vp]),
         "fargo_set_graph_mode": (C.c_int, [vp, C.c_int]),
+        "fargo_stream": (vp, [vp]),
+        "fargo_batch_stream": (vp, [vp]),
+        "fargo_ctx_batch": (vp, [vp]),
+        "fargo_batch_upload_async": (C.c_int, [vp, C.c_int, fp, fp, fp, fp]),
+        "fargo_batch_download_async": (C.c_int, [vp, C.c_int, fp, fp, fp, fp]),
+        "fargo_batch_profile": (C.c_int, [vp, C.c_int, dp, P(C.c_int)]),
+        "fargo_profile_kernel_name": (C.c_char_p, [C.c_int]),
+        "fargo_profile_kernel_count": (C.c_int, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -1,6 +1,6 @@
 """Build the in-tree CUDA library (sm_100a) and the drop-in driver binary.
 
-    python -m cudaprotoplanetarydisksfloat_b200.build
+    python cudaprotoplanetarydisksfloat_b200/build.py
 
 Outputs, next to this file:
     libfargo_b200.so   the C ABI of include/fargo_b200.h

@@ -115,13 +115,21 @@ def write_par(path, params, cfg_path, outdir):
         f.write("OutputDir\t\t%s\n" % outdir)
 
 
-def materialise(params, planets, directory, name="run"):
-    """Write <name>.par / <name>.cfg and an output directory; return the paths."""
+def materialise(params, planets, directory, name="run", relative=False):
+    """Write <name>.par / <name>.cfg and an output directory; return the paths.
+
+    relative=True writes the paths inside the .par relative to `directory`
+    (run the program from there): the reference copies PlanetConfig and
+    OutputDir-derived names into 100-character buffers (Main.cu:104,283;
+    SourceEuler.cu:106-110), so long absolute paths get truncated."""
     os.makedirs(directory, exist_ok=True)
     cfg = os.path.join(directory, name + ".cfg")
     par = os.path.join(directory, name + ".par")
     out = os.path.join(directory, name + "_out") + "/"
     os.makedirs(out, exist_ok=True)
     write_cfg(cfg, planets)
-    write_par(par, params, cfg, out)
+    if relative:
+        write_par(par, params, name + ".cfg", name + "_out/")
+    else:
+        write_par(par, params, cfg, out)
     return par, cfg, out

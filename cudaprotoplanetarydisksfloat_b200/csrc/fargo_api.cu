@@ -46,6 +46,8 @@ struct fargo_batch {
   int* d_ring_off = nullptr;
   int4* d_theta = nullptr;
   int* d_flags = nullptr;
+  int* d_act = nullptr;  // every compacted-list array in one allocation
+  long long* d_act_cell = nullptr;
   double* d_red = nullptr;  // reduction scratch for force/diagnostic kernels
   int red_blocks = 0;
   int max_nsec = 0;
@@ -175,12 +177,12 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   if ((st = dalloc(b, h, &(ptr), (n)))) \
     return st;
   A(D.dens, ng) A(D.vrad, ng) A(D.vtheta, ng) A(D.energy, ng) A(D.vri, ng) A(D.vti, ng) A(D.trr, ng)
-  A(D.tpp, ng) A(D.trp, ng) A(D.qplus, ng) A(D.a0, ng) A(D.a1, ng) A(D.a2, ng) A(D.a3, ng) A(D.a4, ng)
+  A(D.tpp, ng) A(D.trp, ng) A(D.qplus, ng) A(D.a0, ng)
   if (p->Adiabatic) {
-    A(D.cs, ng) A(D.a5, ng)
+    A(D.cs, ng) A(D.a1, ng)
   } else {
     D.cs = nullptr;
-    D.a5 = D.a4;  // never written in isothermal runs
+    D.a1 = D.a0;  // never written in isothermal runs
   }
   A(D.pres, ng)
   A(D.visc, n1) A(D.cs_ring, n1) A(D.csmean, n1) A(D.vmoy, n1) A(D.ringmin, n1) A(D.nshift, n1)
@@ -271,7 +273,7 @@ fargo_status init_disk_state(fargo_batch* b, int d, const float* dens, const flo
   if (energy) std::memcpy(E.data(), energy, sizeof(float) * ng);
   CK(cudaMemcpyAsync(D.dens, S.data(), sizeof(float) * ng, cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(D.energy, E.data(), sizeof(float) * ng, cudaMemcpyHostToDevice, b->stream));
-  float* scratch[] = {D.vrad, D.vtheta, D.vri, D.vti, D.trr, D.tpp, D.trp, D.qplus, D.a0, D.a1, D.a2, D.a3, D.a4};
+  float* scratch[] = {D.vrad, D.vtheta, D.vri, D.vti, D.trr, D.tpp, D.trp, D.qplus, D.a0, D.a1};
   for (float* f : scratch) CK(cudaMemsetAsync(f, 0, sizeof(float) * ng, b->stream));
   // scalars and planets
   DiskCtl c;
@@ -391,7 +393,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   b->disks.resize(n);
   std::vector<long long> cell_off(n + 1, 0);
   std::vector<int> ring_off(n + 1, 0);
-  std::vector<int4> theta;
+  std::vector<int4> theta_iso, theta_adi;
   int seg_max = 0;
   for (int d = 0; d < n; d++) {
     fargo_status st = check_params(b, &params[d], &planets[d]);
@@ -410,6 +412,8 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     b->max_nsec = std::max(b->max_nsec, nsec);
     b->any_adiabatic |= h.p.Adiabatic;
     b->n_sg += h.p.SelfGravity ? 1 : 0;
+    std::vector<int4>& theta = h.p.Adiabatic ? theta_adi : theta_iso;
+    h.dev.item0 = (int)theta.size();
     for (int i = 0; i < nrad; i++) {
       if (nsec <= kSegMax) {
         theta.push_back(make_int4(d, i, 0, nsec));
@@ -422,19 +426,30 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
         }
       }
     }
+    h.dev.nitems = (int)theta.size() - h.dev.item0;
   }
   CK(cudaMalloc(&b->d_disks, sizeof(DiskDev) * n));
   CK(cudaMalloc(&b->d_ctl, sizeof(DiskCtl) * n));
   CK(cudaMemsetAsync(b->d_ctl, 0, sizeof(DiskCtl) * n, b->stream));
   CK(cudaMalloc(&b->d_cell_off, sizeof(long long) * (n + 1)));
   CK(cudaMalloc(&b->d_ring_off, sizeof(int) * (n + 1)));
-  CK(cudaMalloc(&b->d_theta, sizeof(int4) * theta.size()));
+  CK(cudaMalloc(&b->d_theta, sizeof(int4) * (theta_iso.size() + theta_adi.size() + 1)));
   CK(cudaMalloc(&b->d_flags, sizeof(int) * 4));
+  // compacted active lists: act[4] + 3 disk lists + 3 int prefix arrays, and the cell prefix
+  CK(cudaMalloc(&b->d_act, sizeof(int) * (4 + 3 * n + 3 * (n + 1))));
+  CK(cudaMemsetAsync(b->d_act, 0, sizeof(int) * (4 + 3 * n + 3 * (n + 1)), b->stream));
+  CK(cudaMalloc(&b->d_act_cell, sizeof(long long) * (n + 1)));
+  CK(cudaMemsetAsync(b->d_act_cell, 0, sizeof(long long) * (n + 1), b->stream));
   b->red_blocks = 296;
   CK(cudaMalloc(&b->d_red, sizeof(double) * b->red_blocks * 4 * FARGO_DIMFXY));
   CK(cudaMemcpyAsync(b->d_cell_off, cell_off.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->d_ring_off, ring_off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, b->stream));
-  CK(cudaMemcpyAsync(b->d_theta, theta.data(), sizeof(int4) * theta.size(), cudaMemcpyHostToDevice, b->stream));
+  if (!theta_iso.empty())
+    CK(cudaMemcpyAsync(b->d_theta, theta_iso.data(), sizeof(int4) * theta_iso.size(), cudaMemcpyHostToDevice,
+                       b->stream));
+  if (!theta_adi.empty())
+    CK(cudaMemcpyAsync(b->d_theta + theta_iso.size(), theta_adi.data(), sizeof(int4) * theta_adi.size(),
+                       cudaMemcpyHostToDevice, b->stream));
   for (int d = 0; d < n; d++) b->disks[d].dev.ctl = b->d_ctl + d;
   for (int d = 0; d < n; d++)
     CK(cudaMemcpyAsync(b->d_disks + d, &b->disks[d].dev, sizeof(DiskDev), cudaMemcpyHostToDevice, b->stream));
@@ -445,10 +460,28 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   bd.cell_off = b->d_cell_off;
   bd.ring_off = b->d_ring_off;
   bd.disks = b->d_disks;
-  bd.theta_items = b->d_theta;
-  bd.ntheta_items = (int)theta.size();
+  bd.theta_iso = b->d_theta;
+  bd.theta_adi = b->d_theta + theta_iso.size();
+  bd.ntheta_iso = (int)theta_iso.size();
+  bd.ntheta_adi = (int)theta_adi.size();
   bd.theta_seg = seg_max;
   bd.flags = b->d_flags;
+  bd.act = b->d_act;
+  bd.act_disk = b->d_act + 4;
+  bd.act_iso_disk = bd.act_disk + n;
+  bd.act_adi_disk = bd.act_iso_disk + n;
+  bd.act_ring_off = bd.act_adi_disk + n;
+  bd.act_iso_off = bd.act_ring_off + (n + 1);
+  bd.act_adi_off = bd.act_iso_off + (n + 1);
+  bd.act_cell_off = b->d_act_cell;
+  {
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    long long cg = (bd.ncell + 255) / 256;
+    bd.cell_grid = (int)std::min<long long>(cg, (long long)nsm * 8);
+    bd.ring_grid = std::min(bd.nring, nsm * 8);
+    bd.item_grid = nsm * 2;
+  }
   CK(fargo_kernel_attributes(b->max_nsec, seg_max));
   fargo_launch_sector_tables(bd, b->max_nsec, b->stream);
   CK(cudaGetLastError());
@@ -467,7 +500,8 @@ void batch_free(fargo_batch* b) {
     if (h.sg) sg_destroy(h.sg);
     for (void* p : h.allocs) cudaFree(p);
   }
-  void* ps[] = {b->d_disks, b->d_ctl, b->d_cell_off, b->d_ring_off, b->d_theta, b->d_flags, b->d_red};
+  void* ps[] = {b->d_disks, b->d_ctl, b->d_cell_off, b->d_ring_off, b->d_theta, b->d_flags, b->d_red,
+                b->d_act, b->d_act_cell};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -836,6 +870,90 @@ fargo_status fargo_batch_get_planets(fargo_batch* b, int disk, fargo_planets* ou
 }
 
 long long fargo_batch_kernel_launches(const fargo_batch* b) { return b ? b->launches : 0; }
+
+void* fargo_batch_stream(fargo_batch* b) { return b ? (void*)b->stream : nullptr; }
+void* fargo_stream(fargo_ctx* ctx) { return ctx ? (void*)ctx->b.stream : nullptr; }
+fargo_batch* fargo_ctx_batch(fargo_ctx* ctx) { return ctx ? &ctx->b : nullptr; }
+
+// Asynchronous copies (no wait): the host buffers must stay valid and, to
+// overlap, be page-locked; pair with fargo_batch_sync.
+fargo_status fargo_batch_upload_async(fargo_batch* b, int d, const float* dens, const float* vrad,
+                                      const float* vtheta, const float* energy) {
+  if (!b || d < 0 || d >= (int)b->disks.size()) return FARGO_EINVAL;
+  const DiskDev& D = b->disks[d].dev;
+  size_t bytes = sizeof(float) * (size_t)(D.nrad + 1) * D.nsec;
+  if (dens) CK(cudaMemcpyAsync(D.dens, dens, bytes, cudaMemcpyHostToDevice, b->stream));
+  if (vrad) CK(cudaMemcpyAsync(D.vrad, vrad, bytes, cudaMemcpyHostToDevice, b->stream));
+  if (vtheta) CK(cudaMemcpyAsync(D.vtheta, vtheta, bytes, cudaMemcpyHostToDevice, b->stream));
+  if (energy) CK(cudaMemcpyAsync(D.energy, energy, bytes, cudaMemcpyHostToDevice, b->stream));
+  return FARGO_OK;
+}
+
+fargo_status fargo_batch_download_async(fargo_batch* b, int d, float* dens, float* vrad, float* vtheta,
+                                        float* energy) {
+  if (!b || d < 0 || d >= (int)b->disks.size()) return FARGO_EINVAL;
+  const DiskDev& D = b->disks[d].dev;
+  size_t bytes = sizeof(float) * (size_t)(D.nrad + 1) * D.nsec;
+  if (dens) CK(cudaMemcpyAsync(dens, D.dens, bytes, cudaMemcpyDeviceToHost, b->stream));
+  if (vrad) CK(cudaMemcpyAsync(vrad, D.vrad, bytes, cudaMemcpyDeviceToHost, b->stream));
+  if (vtheta) CK(cudaMemcpyAsync(vtheta, D.vtheta, bytes, cudaMemcpyDeviceToHost, b->stream));
+  if (energy) CK(cudaMemcpyAsync(energy, D.energy, bytes, cudaMemcpyDeviceToHost, b->stream));
+  return FARGO_OK;
+}
+
+// Per-kernel timing: ndt DTs in host-loop mode with a CUDA event before and
+// after every kernel of every substep.  ms[k] accumulates the time of
+// substep kernel k (fargo_profile_kernel_name order), the last slot the
+// self-gravity pipeline; *nsub receives the substeps run.
+int fargo_profile_kernel_count(void) { return FARGO_NKERNELS + 1; }
+
+fargo_status fargo_batch_profile(fargo_batch* b, int ndt, double* ms, int* nsub) {
+  if (!b || !ms || ndt < 1) return FARGO_EINVAL;
+  CK(cudaSetDevice(b->device));
+  const int NK = FARGO_NKERNELS;
+  cudaEvent_t ev[FARGO_NKERNELS + 1], sg0, sg1;
+  for (int k = 0; k <= NK; k++) CK(cudaEventCreate(&ev[k]));
+  CK(cudaEventCreate(&sg0));
+  CK(cudaEventCreate(&sg1));
+  for (int k = 0; k <= NK; k++) ms[k] = 0.0;
+  int* hflag = nullptr;
+  CK(cudaMallocHost(&hflag, sizeof(int)));
+  int subs = 0;
+  for (int t = 0; t < ndt; t++) {
+    fargo_launch_dt_begin(b->bd, b->stream);
+    if (b->any_adiabatic) fargo_launch_cs_refresh(b->bd, -1, b->stream);
+    int more = 1;
+    while (more) {
+      CK(cudaEventRecord(sg0, b->stream));
+      for (int d = 0; d < (int)b->disks.size(); d++)
+        if (b->disks[d].sg) sg_capture_substep(b->disks[d].sg, b->bd, d, &b->disks[d].dev, b->stream);
+      CK(cudaEventRecord(sg1, b->stream));
+      fargo_launch_substep(b->bd, 0, 0, b->stream, b->max_nsec, nullptr, ev);
+      CK(cudaMemcpyAsync(hflag, b->d_flags, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+      CK(cudaStreamSynchronize(b->stream));
+      for (int k = 0; k < NK; k++) {
+        float x = 0;
+        CK(cudaEventElapsedTime(&x, ev[k], ev[k + 1]));
+        ms[k] += x;
+      }
+      float y = 0;
+      CK(cudaEventElapsedTime(&y, sg0, sg1));
+      ms[NK] += y;
+      subs++;
+      more = *hflag;
+    }
+  }
+  cudaFreeHost(hflag);
+  for (int k = 0; k <= NK; k++) cudaEventDestroy(ev[k]);
+  cudaEventDestroy(sg0);
+  cudaEventDestroy(sg1);
+  if (nsub) *nsub = subs;
+  return finish_dts(b);
+}
+
+const char* fargo_profile_kernel_name(int k) {
+  return k == FARGO_NKERNELS ? "self_gravity" : fargo_substep_kernel_name(k);
+}
 
 // Launch counting needs the substep counts: total launches of the batch's
 // own kernels so far (pre-DT launches + substeps x kernels per substep).

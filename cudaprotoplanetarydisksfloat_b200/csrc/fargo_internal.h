@@ -75,6 +75,7 @@ struct DiskDev {
   int nrad, nsec;
   long long cell0;  // first active cell of this disk in the batch's flat index
   int ring0;        // first ring of this disk in the batch's flat ring index
+  int item0, nitems;  // its transport items in the isothermal or adiabatic list
   // parameters (floats, as the reference's globals)
   float DT, ADIABATICINDEX, ASPECTRATIO, FLARINGINDEX, SIGMASLOPE, SIGMA0;
   float TRANSITIONRADIUS, TRANSITIONRATIO, TRANSITIONWIDTH, LAMBDADOUBLING;
@@ -96,7 +97,7 @@ struct DiskDev {
   float *pres;  // isothermal: pressure at the start of the DT's last substep (temperature output)
   // scratch
   float *vri, *vti, *trr, *tpp, *trp, *qplus;
-  float *a0, *a1, *a2, *a3, *a4, *a5;  // radial-transport outputs
+  float *a0, *a1;  // transported density and energy, moved into the state by k_velocities
   // self-gravity accelerations (NRAD*NSEC), may be null
   float *sg_accr, *sg_acct;
   // ring tables
@@ -124,22 +125,39 @@ struct BatchDev {
   const long long* cell_off;  // [ndisk+1]
   const int* ring_off;        // [ndisk+1]
   DiskDev* disks;
-  // azimuthal transport work items: (disk, ring, first sector) per CTA
-  const int4* theta_items;
-  int ntheta_items;
+  // transport work items (disk, ring, first sector, sectors), one per CTA,
+  // separate lists for isothermal and adiabatic disks
+  const int4* theta_iso;
+  const int4* theta_adi;
+  int ntheta_iso, ntheta_adi;
   int theta_seg;          // largest azimuthal segment (sectors)
   int* flags;             // [0] OR of the disks' "more" flags after a substep
+  // compacted lists of the disks inside their DT (rebuilt on the device at the
+  // start of a DT and after every substep): act[0] active disks, act[1] active
+  // isothermal disks, act[2] active adiabatic disks
+  int* act;
+  int* act_disk;             // [ndisk] disk id of active index a
+  long long* act_cell_off;   // [ndisk+1] prefix of active cells
+  int* act_ring_off;         // [ndisk+1] prefix of active rings
+  int* act_iso_disk;         // [ndisk] isothermal active disks
+  int* act_iso_off;          // [ndisk+1] prefix of their transport items
+  int* act_adi_disk;
+  int* act_adi_off;
+  int cell_grid, ring_grid, item_grid;  // fixed grid sizes of the grid-stride kernels
 };
 
 // kernel entry points (kernels_step.cu), launched by fargo_api.cu
-size_t fargo_theta_smem_bytes(int seg);
+#define FARGO_NKERNELS 9  // kernels per substep
+size_t fargo_transport_smem_bytes(int seg, int adiabatic);
 cudaError_t fargo_kernel_attributes(int max_nsec, int seg);
 void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s);
 // only_disk >= 0: that disk; -1: every disk still inside its DT
 void fargo_launch_cs_refresh(const BatchDev& b, int only_disk, cudaStream_t s);
 void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s);
+// ev (optional): FARGO_NKERNELS+1 events, before each kernel and after the last
 void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int use_handle, cudaStream_t s,
-                          int max_nsec, long long* launches);
+                          int max_nsec, long long* launches, cudaEvent_t* ev = nullptr);
+const char* fargo_substep_kernel_name(int k);
 void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s);
 void fargo_launch_init_velocities(const BatchDev& b, int disk, long long ncell_ghost, cudaStream_t s);
 void fargo_launch_disk_force(const BatchDev& b, int disk, float x, float y, float rs, float rh, float a,

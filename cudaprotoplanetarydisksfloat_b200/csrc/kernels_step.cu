@@ -17,9 +17,10 @@
 //   k_visc_update    viscous velocity update + sub-Keplerian boundary
 //   k_source2        artificial viscosity (Substep2) + energy predictor
 //   k_energy         viscous heating and implicit energy update (Substep3)
-//   k_transport_rad  momenta + radial van Leer for every transported quantity
-//   k_transport_theta  FARGO: ring mean, integer shift, residual and constant
-//                    azimuthal van Leer sweeps, shift fused into the store
+//   k_transport      one ring per CTA: momenta + radial van Leer in
+//                    registers, FARGO ring mean, integer shift, residual and
+//                    constant azimuthal van Leer sweeps in shared memory,
+//                    shift fused into the store
 //   k_velocities     velocities from the transported momenta
 //   k_substep_end    disks still inside their DT -> graph loop condition
 //
@@ -31,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <algorithm>
 #include <cstdio>
 
 #include "fargo_internal.h"
@@ -344,6 +346,56 @@ __device__ void prepare_bodies(const DiskDev& D, DiskCtl* C) {
   C->nbody = nbody;
 }
 
+
+// Binary search in a prefix array off[0..n] (off[0] = 0): the a with off[a] <= x < off[a+1].
+template <class T>
+__device__ __forceinline__ int find_range(const T* off, int n, T x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Grid-stride walk over the cells of the disks still inside their DT.
+template <class Body>
+__device__ __forceinline__ void for_active_cells(const BatchDev& B, Body body) {
+  const int na = B.act[0];
+  if (na <= 0) return;
+  const long long total = B.act_cell_off[na];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  int a = -1;
+  long long lo = 0, hi = 0;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total; c += stride) {
+    if (c < lo || c >= hi) {
+      a = find_range(B.act_cell_off, na, c);
+      lo = B.act_cell_off[a];
+      hi = B.act_cell_off[a + 1];
+    }
+    const int d = B.act_disk[a];
+    const DiskDev& D = B.disks[d];
+    const int nsec = D.nsec;
+    const int loc = (int)(c - lo);
+    const int i = loc / nsec, j = loc - i * nsec;
+    body(D, D.ctl, i, j, (long long)loc, jwrap_m(j, nsec), jwrap_p(j, nsec));
+  }
+}
+
+#define CELL_BEGIN                                                                                      \
+  for_active_cells(B, [&](const DiskDev& D, const DiskCtl* C, const int i, const int j, const long long l, \
+                          const int jm, const int jp) {                                                 \
+    const int nsec = D.nsec, nrad = D.nrad;                                                             \
+    (void)nrad;                                                                                         \
+    (void)jm;                                                                                           \
+    (void)jp;                                                                                           \
+    if (!D.IsDisk) return;
+#define CELL_END \
+  });
+
 // -------------------------------------------------------------- reductions
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -518,12 +570,15 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
   __shared__ float s_vm;
   __shared__ unsigned s_ticket;
   __shared__ float s_b[5][FARGO_MAXBODY];
-  const int gr = blockIdx.x;
-  const int d = disk_of_ring(B, gr);
+  const int na = B.act[0];
+  const int nar = na > 0 ? B.act_ring_off[na] : 0;
+  for (int gr = blockIdx.x; gr < nar; gr += gridDim.x) {
+  __syncthreads();
+  const int a = find_range(B.act_ring_off, na, gr);
+  const int d = B.act_disk[a];
   const DiskDev& D = B.disks[d];
   DiskCtl* C = D.ctl;
-  if (!C->active) return;
-  const int i = gr - D.ring0, nsec = D.nsec, nrad = D.nrad, tid = threadIdx.x;
+  const int i = gr - B.act_ring_off[a], nsec = D.nsec, nrad = D.nrad, tid = threadIdx.x;
   const float* vt = D.vtheta + (size_t)i * nsec;
   for (int j = tid; j < nsec; j += blockDim.x) s_ring[j] = vt[j];
   const int nbody = C->nbody;
@@ -537,6 +592,7 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
   __syncthreads();
   if (tid == 0) {
     float moy = 0.0f;
+#pragma unroll 16
     for (int j = 0; j < nsec; j++) moy += s_ring[j];
     moy /= (float)nsec;
     s_vm = moy;
@@ -635,14 +691,16 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
     P[0] = inner ? acc : 0.0;  // fx_inner / fy_inner
     P[1] = inner ? 0.0 : acc;  // fx_outer / fy_outer
   }
-  // last block of this disk finishes the substep's scalar work
+  // the block that processes this disk's last ring finishes the substep's scalar work
   __threadfence();
   __syncthreads();
   if (tid == 0) s_ticket = atomicAdd(&C->counter, 1u);
   __syncthreads();
-  if (s_ticket != (unsigned)(nrad - 1)) return;
-  __threadfence();
-  finish_cfl_and_planets(D, C, s_min, nullptr);
+  if (s_ticket == (unsigned)(nrad - 1)) {
+    __threadfence();
+    finish_cfl_and_planets(D, C, s_min, nullptr);
+  }
+  }
 }
 
 // ----------------------------------------------------------- source terms
@@ -680,27 +738,12 @@ __device__ __forceinline__ float pressure_at(const DiskDev& D, long long l, int 
   return (D.ADIABATICINDEX - 1.0) * D.energy[l];
 }
 
-#define CELL_PROLOGUE                                                   \
-  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;       \
-  if (c >= B.ncell) return;                                             \
-  const int d = disk_of_cell(B, c);                                     \
-  const DiskDev& D = B.disks[d];                                        \
-  const DiskCtl* C = D.ctl;                                             \
-  if (!C->active || !D.IsDisk) return;                                  \
-  const int nsec = D.nsec, nrad = D.nrad;                               \
-  const int loc = (int)(c - D.cell0);                                   \
-  const int i = loc / nsec, j = loc - i * nsec;                         \
-  const long long l = (long long)i * nsec + j;                          \
-  const int jm = jwrap_m(j, nsec), jp = jwrap_p(j, nsec);               \
-  (void)nrad;                                                           \
-  (void)jm;                                                             \
-  (void)jp;
 
 // Substep1KernelVrad / Substep1KernelVtheta (Kernels.cu:52-88), with
 // CorrectVthetaKernel (Kernels.cu:1352-1359) applied on the fly, and the
 // self-gravity kick of Update_sgvelocityKernel (Kernels.cu:1024-1041).
 __global__ void __launch_bounds__(kThreads) k_source1(BatchDev B) {
-  CELL_PROLOGUE
+  CELL_BEGIN
   const float dt = C->dtf;
   const float OmegaFrame = C->OmegaFrame;
   const float dom = C->domega;
@@ -748,6 +791,7 @@ __global__ void __launch_bounds__(kThreads) k_source1(BatchDev B) {
     }
     D.vti[l] = vti;
   }
+  CELL_END
 }
 
 // ViscousTermsKernelDRP + ViscousTermsKernelTAURP (Kernels.cu:843-880) on
@@ -783,11 +827,12 @@ __device__ __forceinline__ Tau viscous_terms(const DiskDev& D, const float* Vr, 
 }
 
 __global__ void __launch_bounds__(kThreads) k_visc_tau(BatchDev B) {
-  CELL_PROLOGUE
+  CELL_BEGIN
   Tau t = viscous_terms(D, D.vri, D.vti, i, j, nsec);
   D.trr[l] = t.rr;
   D.tpp[l] = t.pp;
   if (i > 0) D.trp[l] = t.rp;
+  CELL_END
 }
 
 // Sub-Keplerian boundary speeds (SideEuler.cu:250-268), device double math
@@ -815,7 +860,7 @@ __device__ void vkep_pair(const DiskDev& D, const DiskCtl* C, float* vin, float*
 // UpdateVelocitiesKernel (Kernels.cu:142-160) in place, then
 // ApplySubKeplerianBoundaryKernel (Kernels.cu:1490-1503).
 __global__ void __launch_bounds__(kThreads) k_visc_update(BatchDev B) {
-  CELL_PROLOGUE
+  CELL_BEGIN
   const float DeltaT = C->dtf;
   const float* Dn = D.dens;
   const float *TRR = D.trr, *TRP = D.trp, *TPP = D.tpp;
@@ -838,6 +883,7 @@ __global__ void __launch_bounds__(kThreads) k_visc_update(BatchDev B) {
     if (i == 0) D.vti[l] = vin - D.Rmed[0] * C->OmegaFrame;
     if (i == nrad - 1) D.vti[l] = vout - D.Rmed[nrad - 1] * C->OmegaFrame;
   }
+  CELL_END
 }
 
 // Substep2Kernel + Substep2Kernel2 (Kernels.cu:570-621), then the
@@ -848,7 +894,7 @@ __device__ __forceinline__ float qvisc(float dv, float dens) {
 }
 
 __global__ void __launch_bounds__(kThreads) k_source2(BatchDev B) {
-  CELL_PROLOGUE
+  CELL_BEGIN
   const float dt = C->dtf;
   const float* Dn = D.dens;
   const float *VRI = D.vri, *VTI = D.vti;
@@ -871,6 +917,7 @@ __global__ void __launch_bounds__(kThreads) k_source2(BatchDev B) {
   D.vrad[l] = vr_new;
   D.vtheta[l] = vt_new;
   if (i == nrad - 1) D.vtheta[l + nsec] = 0.0f;  // VthetaNew's ghost row is zero
+  CELL_END
 }
 
 // Substep3Kernel + Substep3Kernel2 (Kernels.cu:91-139) with the viscous
@@ -890,7 +937,7 @@ __device__ __forceinline__ float qplus_at(const DiskDev& D, int i, int j, int ns
 }
 
 __global__ void __launch_bounds__(kThreads) k_energy(BatchDev B) {
-  CELL_PROLOGUE
+  CELL_BEGIN
   if (!D.Adiabatic) return;
   const float dt = C->dtf;
   float divv;
@@ -922,6 +969,7 @@ __global__ void __launch_bounds__(kThreads) k_energy(BatchDev B) {
   D.qplus[l] = q;
   D.energy[l] = num / den;
   if (i == nrad - 1) D.energy[l + nsec] = 0.0f;  // EnergyNew's ghost row is zero
+  CELL_END
 }
 
 // ------------------------------------------------------------- transport
@@ -934,110 +982,135 @@ __device__ __forceinline__ float vl_rad_slope(float qm, float q0, float qp, floa
   return 0.0f;
 }
 
-// LRMomentaKernel (Kernels.cu:883-896) + the radial half of Transport:
-// StarRadKernel/StarRadKernel2/VanLeerRadialKernel (Kernels.cu:909-947,
-// 1137-1154) for RadMomP, RadMomM, ThetaMomP, ThetaMomM, energy and density,
-// with DivisePolarGridKernel's quotient (Kernels.cu:1127-1134) formed per row.
-__global__ void __launch_bounds__(kThreads) k_transport_rad(BatchDev B) {
-  CELL_PROLOGUE
+// LRMomentaKernel (Kernels.cu:883-896) and the radial half of Transport for
+// one cell (i, j): StarRadKernel/StarRadKernel2/VanLeerRadialKernel
+// (Kernels.cu:909-947, 1137-1154) for RadMomP, RadMomM, ThetaMomP,
+// ThetaMomM, [energy] and density, with DivisePolarGridKernel's quotient
+// (Kernels.cu:1127-1134) formed per row.  out[0..3] momenta, out[4] energy
+// when nq == 6, out[nq-1] density.
+template <int nq>
+__device__ __forceinline__ void radial_point(const DiskDev& D, const DiskCtl* C, int i, int j, float* out) {
+  const int nsec = D.nsec, nrad = D.nrad;
+  const int jp = jwrap_p(j, nsec);
+  const long long l = (long long)i * nsec + j;
   const float dt = C->dtf;
   const float Om = C->OmegaFrame;
-  const int adi = D.Adiabatic;
+  const bool adi = (nq == 6);
   // rows i-2 .. i+2 (clamped; the clamped values are never used)
-  float S[5], M1[5], M2[5], M3[5], M4[5], E[5], Vr[6];
-  double den[5];
+  float S[5], M1[5], M2[5], M3[5], M4[5], E[5];
+  double rden[5];
+#pragma unroll
   for (int q = 0; q < 5; q++) {
     int r = i - 2 + q;
     r = r < 0 ? 0 : (r > nrad - 1 ? nrad - 1 : r);
     const long long lr = (long long)r * nsec + j;
     const long long lrp = (long long)r * nsec + jp;
-    float s = D.dens[lr];
+    float sg = D.dens[lr];
     float rm = D.Rmed[r];
-    S[q] = s;
-    M1[q] = s * D.vrad[lr + nsec];
-    M2[q] = s * D.vrad[lr];
-    M3[q] = s * (D.vtheta[lrp] + rm * Om) * rm;
-    M4[q] = s * (D.vtheta[lr] + rm * Om) * rm;
+    S[q] = sg;
+    M1[q] = sg * D.vrad[lr + nsec];
+    M2[q] = sg * D.vrad[lr];
+    M3[q] = sg * (D.vtheta[lrp] + rm * Om) * rm;
+    M4[q] = sg * (D.vtheta[lr] + rm * Om) * rm;
     E[q] = adi ? D.energy[lr] : 0.0f;
-    den[q] = (double)s + 1e-20;
+    rden[q] = 1.0 / ((double)sg + 1e-20);
   }
-  Vr[0] = D.vrad[l];
-  Vr[1] = D.vrad[l + nsec];  // row i+1 (row nrad is the zero ghost row)
-  // slope rows: r = i-1, i, i+1 ; interface rows: i, i+1
+  const float Vr0 = D.vrad[l];
+  const float Vr1 = D.vrad[l + nsec];  // row i+1 (row nrad is the zero ghost row)
   const float idm_im1 = (i - 1 >= 1) ? D.invdiffRmed[i - 1] : 0.0f;
   const float idm_i = D.invdiffRmed[i];
   const float idm_ip1 = (i + 1 <= nrad - 1) ? D.invdiffRmed[i + 1] : 0.0f;
   const float idm_ip2 = (i + 2 <= nrad - 1) ? D.invdiffRmed[i + 2] : 0.0f;
+  const float rm_im1 = (i >= 1) ? D.Rmed[i - 1] : 0.0f;
+  const float rm_i = D.Rmed[i];
+  const float rm_ip1 = (i + 1 <= nrad - 1) ? D.Rmed[i + 1] : 0.0f;  // Rmed[NRAD] only meets a zero slope
+  const float rm_ip2 = (i + 2 <= nrad - 1) ? D.Rmed[i + 2] : 0.0f;
   auto slope = [&](const float* Q, int q) -> float {
-    // slope at row r = i-2+q
-    int r = i - 2 + q;
+    int r = i - 2 + q;  // slope at ring r
     if (r <= 0 || r >= nrad - 1) return 0.0f;
     float invm = (q == 1) ? idm_im1 : (q == 2 ? idm_i : idm_ip1);
     float invp = (q == 1) ? idm_i : (q == 2 ? idm_ip1 : idm_ip2);
     return vl_rad_slope(Q[q - 1], Q[q], Q[q + 1], invm, invp);
   };
-  auto qstar = [&](const float* Q, int rr, float v) -> float {
-    // upwind interface value at ring rr (rr = i or i+1)
-    if (rr == 0 || rr >= nrad) return 0.0f;
-    int q = rr - (i - 2);
-    if (v > 0.0 && rr > 0)
-      return Q[q - 1] + (D.Rmed[rr] - D.Rmed[rr - 1] - v * dt) * 0.5 * slope(Q, q - 1);
-    float rnext = (rr + 1 <= nrad - 1) ? D.Rmed[rr + 1] : 0.0f;  // Rmed[NRAD]: times a zero slope
-    return Q[q] - (rnext - D.Rmed[rr] + v * dt) * 0.5 * slope(Q, q);
+  // upwind interface values at rings i (q = 2) and i+1 (q = 3)
+  auto qstar_i = [&](const float* Q) -> float {
+    if (i == 0) return 0.0f;
+    if (Vr0 > 0.0) return Q[1] + (rm_i - rm_im1 - Vr0 * dt) * 0.5 * slope(Q, 1);
+    return Q[2] - (rm_ip1 - rm_i + Vr0 * dt) * 0.5 * slope(Q, 2);
   };
-  const float dstar_i = qstar(S, i, Vr[0]);
-  const float dstar_ip = qstar(S, i + 1, Vr[1]);
+  auto qstar_ip = [&](const float* Q) -> float {
+    if (i + 1 >= nrad) return 0.0f;
+    if (Vr1 > 0.0) return Q[2] + (rm_ip1 - rm_i - Vr1 * dt) * 0.5 * slope(Q, 2);
+    return Q[3] - (rm_ip2 - rm_ip1 + Vr1 * dt) * 0.5 * slope(Q, 3);
+  };
+  const float dstar_i = qstar_i(S);
+  const float dstar_ip = qstar_ip(S);
   float dtheta = 2.0 * PI_D / (float)nsec;
   const float Ri = D.Rinf[i], Rs = D.Rsup[i], iS = D.invSurf[i];
   auto advect = [&](const float* Q) -> float {
     float W[5];
 #pragma unroll
-    for (int q = 0; q < 5; q++) W[q] = (double)Q[q] * (1.0 / den[q]);
-    float qi = qstar(W, i, Vr[0]);
-    float qip = qstar(W, i + 1, Vr[1]);
-    float varq = dt * dtheta * Ri * qi * dstar_i * Vr[0];
-    varq -= dt * dtheta * Rs * qip * dstar_ip * Vr[1];
+    for (int q = 0; q < 5; q++) W[q] = (double)Q[q] * rden[q];
+    float qi = qstar_i(W);
+    float qip = qstar_ip(W);
+    float varq = dt * dtheta * Ri * qi * dstar_i * Vr0;
+    varq -= dt * dtheta * Rs * qip * dstar_ip * Vr1;
     return Q[2] + varq * iS;
   };
-  D.a1[l] = advect(M1);
-  D.a2[l] = advect(M2);
-  D.a3[l] = advect(M3);
-  D.a4[l] = advect(M4);
-  if (adi) D.a5[l] = advect(E);
-  D.a0[l] = advect(S);
+  out[0] = advect(M1);
+  out[1] = advect(M2);
+  out[2] = advect(M3);
+  out[3] = advect(M4);
+  if (adi) out[4] = advect(E);
+  out[nq - 1] = advect(S);
 }
 
-// Azimuthal half of Transport for one ring segment (OneWindTheta,
-// TransportEuler.cu:171-219): ring mean (serial, as
-// ComputeAverageThetaVelocitiesKernel), residual, Nshift and constant
-// residual (ComputeConstantResidualKernel, Kernels.cu:1201-1232), the
-// residual and the constant-residual van Leer sweeps (StarThetaKernel,
-// StarThetaKernel2, VanLeerThetaKernel, Kernels.cu:1157-1273) on the
-// quantities of k_transport_rad, and AdvectSHIFTKernel (Kernels.cu:1276-1289)
-// fused into the store.
-__global__ void __launch_bounds__(kThreads) k_transport_theta(BatchDev B) {
+constexpr int kTT = 512;   // threads of the transport kernel
+constexpr int kMaxK = 5;   // window points per thread: (2048 + 8) / 512 rounded up
+
+// One ring (or one segment of a wide ring) of Transport (TransportEuler.cu:24-35):
+// the radial half for every point of the window (radial_point, results kept
+// in registers), then OneWindTheta (TransportEuler.cu:171-219): ring mean of
+// v_theta (serial, as ComputeAverageThetaVelocitiesKernel), residual,
+// Nshift and constant residual (ComputeConstantResidualKernel,
+// Kernels.cu:1201-1232), the residual and constant-residual van Leer
+// sweeps (StarThetaKernel, StarThetaKernel2, VanLeerThetaKernel,
+// Kernels.cu:1157-1273) in shared memory, and AdvectSHIFTKernel
+// (Kernels.cu:1276-1289) fused into the store.  Final density / energy go to
+// scratch (a0 / a1) because neighbouring rings still read the old ones; the
+// velocity kernel moves them into the state.
+template <int nq>
+__global__ void __launch_bounds__(kTT) k_transport(BatchDev B, const int4* __restrict__ items) {
   extern __shared__ float sm[];
   __shared__ float s_vmed;
   __shared__ int s_nshift;
   __shared__ float s_vconst;
-  const int4 it = B.theta_items[blockIdx.x];
-  const DiskDev& D = B.disks[it.x];
+  const int nak = (nq == 5) ? B.act[1] : B.act[2];
+  const int* aoff = (nq == 5) ? B.act_iso_off : B.act_adi_off;
+  const int* adisk = (nq == 5) ? B.act_iso_disk : B.act_adi_disk;
+  const int nai = nak > 0 ? aoff[nak] : 0;
+  for (int t = blockIdx.x; t < nai; t += gridDim.x) {
+  __syncthreads();
+  const int a = find_range(aoff, nak, t);
+  const DiskDev& D = B.disks[adisk[a]];
+  const int4 it = items[D.item0 + (t - aoff[a])];
   const DiskCtl* C = D.ctl;
-  if (!C->active || !D.IsDisk) return;
-  const int i = it.y, j0 = it.z, S = it.w;  // S sectors of output
+  if (!D.IsDisk) continue;
+  const int i = it.y, j0 = it.z, S = it.w;  // S output sectors starting at j0
   const int nsec = D.nsec, tid = threadIdx.x;
-  const int L = S + 8;
-  const int nq = D.Adiabatic ? 6 : 5;  // M1..M4, [E], Sigma last
-  float* Q = sm;                    // nq * L
-  float* Vres = Q + 6 * L;          // L
-  float* dstar = Vres + L;          // L
-  float* work = dstar + L;          // L
-  float* dqa = work + L;            // L
-  float* qrs = dqa + L;             // L
+  const int L = S + 8;  // window: 4 points of halo on each side
+  float* sS = sm;           // density of the window (pre-sweep)
+  float* sV = sS + L;       // residual velocity
+  float* sD = sV + L;       // DensStar of the sweep
+  float* sW = sD + L;       // nq * L: DivisePolarGrid quotients
   const float dt = C->dtf;
   const float* vt = D.vtheta + (size_t)i * nsec;
+  const bool whole = (S == nsec);
+  float q[nq][kMaxK];
+  float tmp[nq];
   if (tid == 0) {
     float moy = 0.0f;
+#pragma unroll 16
     for (int j = 0; j < nsec; j++) moy += vt[j];
     float VMed = moy / (float)nsec;
     float invdt = 1.0 / dt;
@@ -1054,23 +1127,53 @@ __global__ void __launch_bounds__(kThreads) k_transport_theta(BatchDev B) {
       if (sidx >= 0 && sidx < FARGO_MAXLOG) D.log_nshift[(size_t)sidx * D.nrad + i] = (int)nitemp;
     }
   }
+  if (whole) {
+    // a whole ring: window sectors -4 .. nsec+3 (periodic), independent of the shift
+#pragma unroll
+    for (int k = 0; k < kMaxK; k++) {
+      int p = tid + k * kTT;
+      if (p < L) {
+        int g = p - 4;
+        g = g < 0 ? g + nsec : (g >= nsec ? g - nsec : g);
+        radial_point<nq>(D, C, i, g, tmp);
+#pragma unroll
+        for (int c = 0; c < nq; c++) q[c][k] = tmp[c];
+      }
+    }
+  }
   __syncthreads();
   const int ns = s_nshift;
   const float VMed = s_vmed;
   float vconst = s_vconst;
   const bool fast = D.FastTransport;
-  // source window: sectors js-4 .. js+S+3, js = j0 - Nshift (mod nsec)
-  int js = (j0 - ns) % nsec;
-  if (js < 0) js += nsec;
-  const float* srcs[6] = {D.a1, D.a2, D.a3, D.a4, D.Adiabatic ? D.a5 : D.a0, D.a0};
-  for (int p = tid; p < L; p += blockDim.x) {
-    int g = (js - 4 + p) % nsec;
-    if (g < 0) g += nsec;
-    const long long lg = (long long)i * nsec + g;
-    for (int q = 0; q < nq; q++) Q[q * L + p] = srcs[q == nq - 1 ? 5 : q][lg];
-    float vres = vt[g] - VMed;
-    if (!fast) vres = vconst + vres;
-    Vres[p] = vres;
+  int js = 0;
+  if (!whole) {
+    // segment of a wide ring: source window js-4 .. js+S+3, js = j0 - Nshift
+    js = (j0 - ns) % nsec;
+    if (js < 0) js += nsec;
+#pragma unroll
+    for (int k = 0; k < kMaxK; k++) {
+      int p = tid + k * kTT;
+      if (p < L) {
+        int g = (js - 4 + p) % nsec;
+        if (g < 0) g += nsec;
+        radial_point<nq>(D, C, i, g, tmp);
+#pragma unroll
+        for (int c = 0; c < nq; c++) q[c][k] = tmp[c];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kMaxK; k++) {
+    int p = tid + k * kTT;
+    if (p < L) {
+      int g = (js - 4 + p) % nsec;
+      if (g < 0) g += nsec;
+      float vres = vt[g] - VMed;
+      if (!fast) vres = vconst + vres;
+      sV[p] = vres;
+      sS[p] = q[nq - 1][k];
+    }
   }
   if (!fast) vconst = 0.0f;
   __syncthreads();
@@ -1079,80 +1182,90 @@ __global__ void __launch_bounds__(kThreads) k_transport_theta(BatchDev B) {
   float invdxtheta = 1.0 / dxtheta;
   float invsurf = 1.0 / D.Surf[i];
   float dxrad = (D.Rsup[i] - D.Rinf[i]) * dt;
-  const float* Sg = Q + (nq - 1) * L;  // density: updated last in each sweep
+  // van Leer slope of StarThetaKernel at window point x (0 at the window edges)
+  auto dqat = [&](const float* W, int x) -> float {
+    if (x <= 0 || x >= L - 1) return 0.0f;
+    float dqm = (W[x] - W[x - 1]);
+    float dqp = (W[x + 1] - W[x]);
+    if (dqp * dqm > 0.0) return dqp * dqm / (dqp + dqm) * invdxtheta;
+    return 0.0f;
+  };
+  // upwind value of StarThetaKernel2 at window point x with velocity v
+  auto qst = [&](const float* W, int x, float v) -> float {
+    float ksi = v * dt;
+    if (ksi > 0.0) return (x > 0) ? W[x - 1] + (dxtheta - ksi) * dqat(W, x - 1) : 0.0f;
+    return W[x] - (dxtheta + ksi) * dqat(W, x);
+  };
   for (int sweep = 0; sweep < 2; sweep++) {
     const bool uni = (sweep == 1);
-    // StarTheta of the density with this sweep's velocity -> DensStar
-    for (int p = tid; p < L; p += blockDim.x) {
-      float dqv = 0.0f;
-      if (p > 0 && p < L - 1) {
-        float dqm = (Sg[p] - Sg[p - 1]);
-        float dqp = (Sg[p + 1] - Sg[p]);
-        if (dqp * dqm > 0.0) dqv = dqp * dqm / (dqp + dqm) * invdxtheta;
+    // pass A: DivisePolarGrid by the pre-sweep density, DensStar
+#pragma unroll
+    for (int k = 0; k < kMaxK; k++) {
+      int p = tid + k * kTT;
+      if (p < L) {
+        const double den = (double)sS[p] + 1e-20;
+#pragma unroll
+        for (int c = 0; c < nq; c++) sW[c * L + p] = (double)q[c][k] / den;
+        sD[p] = qst(sS, p, uni ? vconst : sV[p]);
       }
-      dqa[p] = dqv;
     }
     __syncthreads();
-    for (int p = tid; p < L; p += blockDim.x) {
-      float v = uni ? vconst : Vres[p];
-      float ksi = v * dt;
-      float qsv;
-      if (ksi > 0.0)
-        qsv = (p > 0) ? Sg[p - 1] + (dxtheta - ksi) * dqa[p - 1] : 0.0f;
-      else
-        qsv = Sg[p] - (dxtheta + ksi) * dqa[p];
-      dstar[p] = qsv;
-    }
-    __syncthreads();
-    for (int q = 0; q < nq; q++) {
-      float* Qq = Q + q * L;
-      // DivisePolarGrid by the pre-sweep density (DensInt)
-      for (int p = tid; p < L; p += blockDim.x) work[p] = (double)Qq[p] / ((double)Sg[p] + 1e-20);
-      __syncthreads();
-      for (int p = tid; p < L; p += blockDim.x) {
-        float dqv = 0.0f;
-        if (p > 0 && p < L - 1) {
-          float dqm = (work[p] - work[p - 1]);
-          float dqp = (work[p + 1] - work[p]);
-          if (dqp * dqm > 0.0) dqv = dqp * dqm / (dqp + dqm) * invdxtheta;
+    // pass B: VanLeerThetaKernel for every quantity (density last is implied:
+    // all quotients were formed from the pre-sweep density)
+#pragma unroll
+    for (int k = 0; k < kMaxK; k++) {
+      int p = tid + k * kTT;
+      if (p < L - 1) {
+        const float v0 = uni ? vconst : sV[p];
+        const float v1 = uni ? vconst : sV[p + 1];
+        const float d0 = sD[p], d1 = sD[p + 1];
+#pragma unroll
+        for (int c = 0; c < nq; c++) {
+          const float* W = sW + c * L;
+          float qr0 = qst(W, p, v0);
+          float qr1 = qst(W, p + 1, v1);
+          float varq = dxrad * qr0 * d0 * v0;
+          varq -= dxrad * qr1 * d1 * v1;
+          q[c][k] += varq * invsurf;
         }
-        dqa[p] = dqv;
       }
-      __syncthreads();
-      for (int p = tid; p < L; p += blockDim.x) {
-        float v = uni ? vconst : Vres[p];
-        float ksi = v * dt;
-        float qsv;
-        if (ksi > 0.0)
-          qsv = (p > 0) ? work[p - 1] + (dxtheta - ksi) * dqa[p - 1] : 0.0f;
-        else
-          qsv = work[p] - (dxtheta + ksi) * dqa[p];
-        qrs[p] = qsv;
+    }
+    if (sweep == 0) {
+#pragma unroll
+      for (int k = 0; k < kMaxK; k++) {
+        int p = tid + k * kTT;
+        if (p < L) sS[p] = q[nq - 1][k];
       }
-      __syncthreads();
-      for (int p = tid; p < L - 1; p += blockDim.x) {
-        float v0 = uni ? vconst : Vres[p];
-        float v1 = uni ? vconst : Vres[p + 1];
-        float varq = dxrad * qrs[p] * dstar[p] * v0;
-        varq -= dxrad * qrs[p + 1] * dstar[p + 1] * v1;
-        Qq[p] += varq * invsurf;
+    }
+    __syncthreads();
+  }
+  // shifted store: output sector j takes the swept value of sector j - Nshift
+  float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.a1, D.a0};
+#pragma unroll
+  for (int k = 0; k < kMaxK; k++) {
+    int p = tid + k * kTT;
+    if (p >= 4 && p < L - 4) {
+      int j;
+      if (whole) {
+        j = (p - 4 + ns) % nsec;
+        if (j < 0) j += nsec;
+      } else {
+        j = j0 + p - 4;
       }
-      __syncthreads();
+      const long long lo = (long long)i * nsec + j;
+#pragma unroll
+      for (int c = 0; c < nq; c++) dsts[c == nq - 1 ? 5 : c][lo] = q[c][k];
     }
   }
-  // shifted store: out sector j0+t <- source window position t+4
-  float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.energy, D.dens};
-  for (int t = tid; t < S; t += blockDim.x) {
-    const long long lo = (long long)i * nsec + j0 + t;
-    for (int q = 0; q < nq; q++) dsts[q == nq - 1 ? 5 : q][lo] = Q[q * L + t + 4];
   }
 }
 
-// ComputeVelocitiesKernel, Kernels.cu:1292-1306 (momenta after the shift
-// sit in vri, vti, trr, tpp).
+// ComputeVelocitiesKernel, Kernels.cu:1292-1306, from the transported
+// momenta (vri, vti, trr, tpp) and density (a0); then the transported
+// density (and energy, a1) become the state.
 __global__ void __launch_bounds__(kThreads) k_velocities(BatchDev B) {
-  CELL_PROLOGUE
-  const float* Dn = D.dens;
+  CELL_BEGIN
+  const float* Dn = D.a0;
   const long long lmj = (long long)i * nsec + jm;
   float vr;
   if (i == 0)
@@ -1162,6 +1275,44 @@ __global__ void __launch_bounds__(kThreads) k_velocities(BatchDev B) {
   float vt = (D.trr[lmj] + D.tpp[l]) / (Dn[l] + Dn[lmj] + 1e-15) / D.Rmed[i] - D.Rmed[i] * C->OmegaFrame;
   D.vrad[l] = vr;
   D.vtheta[l] = vt;
+  D.dens[l] = Dn[l];
+  if (D.Adiabatic) D.energy[l] = D.a1[l];
+  CELL_END
+}
+
+// Compacted lists of the disks inside their DT (one thread; disks are few).
+__device__ void compact_active(const BatchDev& B) {
+  int na = 0, ni = 0, nd = 0;
+  long long cc = 0;
+  int rr = 0, ii = 0, ia = 0;
+  for (int d = 0; d < B.ndisk; d++) {
+    const DiskDev& D = B.disks[d];
+    if (!D.ctl->active) continue;
+    B.act_disk[na] = d;
+    B.act_cell_off[na] = cc;
+    B.act_ring_off[na] = rr;
+    cc += (long long)D.nrad * D.nsec;
+    rr += D.nrad;
+    na++;
+    if (D.Adiabatic) {
+      B.act_adi_disk[nd] = d;
+      B.act_adi_off[nd] = ia;
+      ia += D.nitems;
+      nd++;
+    } else {
+      B.act_iso_disk[ni] = d;
+      B.act_iso_off[ni] = ii;
+      ii += D.nitems;
+      ni++;
+    }
+  }
+  B.act_cell_off[na] = cc;
+  B.act_ring_off[na] = rr;
+  B.act_iso_off[ni] = ii;
+  B.act_adi_off[nd] = ia;
+  B.act[0] = na;
+  B.act[1] = ni;
+  B.act[2] = nd;
 }
 
 // End of a substep: which disks take another one; drives the graph's loop.
@@ -1174,23 +1325,26 @@ __global__ void k_substep_end(BatchDev B, cudaGraphConditionalHandle h, int use_
   }
   any = __syncthreads_or(any);
   if (threadIdx.x == 0) {
+    compact_active(B);
     B.flags[0] = any;
     if (use_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
   }
 }
 
-// Start of a DT (AlgoGas entry, SourceEuler.cu:211-229).
+// Start of a DT (AlgoGas entry, SourceEuler.cu:211-229) for every disk.
 __global__ void k_dt_begin(BatchDev B) {
-  int d = blockIdx.x;
-  if (d >= B.ndisk || threadIdx.x != 0) return;
-  const DiskDev& D = B.disks[d];
-  DiskCtl* C = D.ctl;
-  C->dtemp = 0.0;
-  C->nsub = 0;
-  C->active = 1;
-  C->more = 1;
-  C->counter = 0;
-  prepare_bodies(D, C);
+  for (int d = threadIdx.x; d < B.ndisk; d += blockDim.x) {
+    const DiskDev& D = B.disks[d];
+    DiskCtl* C = D.ctl;
+    C->dtemp = 0.0;
+    C->nsub = 0;
+    C->active = 1;
+    C->more = 1;
+    C->counter = 0;
+    prepare_bodies(D, C);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) compact_active(B);
 }
 
 // ComputeSoundSpeedKernel, adiabatic branch (Kernels.cu:190-191)
@@ -1400,9 +1554,8 @@ __global__ void __launch_bounds__(kThreads) k_diagnostics(BatchDev B, int disk, 
 
 static inline unsigned cell_blocks(long long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
-size_t fargo_theta_smem_bytes(int seg) { return sizeof(float) * 11 * (size_t)(seg + 8); }
 
-void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s) { k_dt_begin<<<b.ndisk, 32, 0, s>>>(b); }
+void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s) { k_dt_begin<<<1, 128, 0, s>>>(b); }
 
 void fargo_launch_cs_refresh(const BatchDev& b, int only_disk, cudaStream_t s) {
   k_cs_adiabatic<<<cell_blocks(b.ncell), kThreads, 0, s>>>(b, only_disk);
@@ -1413,23 +1566,54 @@ void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s
   k_cs_isothermal<<<(unsigned)((b.nring + 127) / 128), 128, 0, s>>>(b, only_disk);
 }
 
-int fargo_kernels_per_substep(int adiabatic) { return adiabatic ? 10 : 9; }
+int fargo_kernels_per_substep(int adiabatic) { return FARGO_NKERNELS; }
+
+const char* fargo_substep_kernel_name(int k) {
+  static const char* names[] = {"k_cfl_force", "k_source1",   "k_visc_tau",   "k_visc_update", "k_source2",
+                                "k_energy",    "k_transport", "k_velocities", "k_substep_end"};
+  return (k >= 0 && k < FARGO_NKERNELS) ? names[k] : "";
+}
+
+size_t fargo_transport_smem_bytes(int seg, int adiabatic) {
+  return sizeof(float) * (size_t)(3 + (adiabatic ? 6 : 5)) * (size_t)(seg + 8);
+}
 
 void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int use_handle, cudaStream_t s,
-                          int max_nsec, long long* launches) {
-  unsigned cb = cell_blocks(b.ncell);
+                          int max_nsec, long long* launches, cudaEvent_t* ev) {
+  const unsigned cb = (unsigned)b.cell_grid;
   size_t ring_smem = sizeof(float) * (size_t)max_nsec;
-  k_cfl_force<<<b.nring, kThreads, ring_smem, s>>>(b);
+  int k = 0;
+#define REC()                                  \
+  do {                                         \
+    if (ev) cudaEventRecord(ev[k], s);         \
+    k++;                                       \
+  } while (0)
+  REC();
+  k_cfl_force<<<b.ring_grid, kThreads, ring_smem, s>>>(b);
+  REC();
   k_source1<<<cb, kThreads, 0, s>>>(b);
+  REC();
   k_visc_tau<<<cb, kThreads, 0, s>>>(b);
+  REC();
   k_visc_update<<<cb, kThreads, 0, s>>>(b);
+  REC();
   k_source2<<<cb, kThreads, 0, s>>>(b);
+  REC();
   k_energy<<<cb, kThreads, 0, s>>>(b);
-  k_transport_rad<<<cb, kThreads, 0, s>>>(b);
-  k_transport_theta<<<b.ntheta_items, kThreads, fargo_theta_smem_bytes(b.theta_seg), s>>>(b);
+  REC();
+  if (b.ntheta_iso)
+    k_transport<5><<<std::min(b.item_grid, b.ntheta_iso), kTT, fargo_transport_smem_bytes(b.theta_seg, 0), s>>>(
+        b, b.theta_iso);
+  if (b.ntheta_adi)
+    k_transport<6><<<std::min(b.item_grid, b.ntheta_adi), kTT, fargo_transport_smem_bytes(b.theta_seg, 1), s>>>(
+        b, b.theta_adi);
+  REC();
   k_velocities<<<cb, kThreads, 0, s>>>(b);
+  REC();
   k_substep_end<<<1, 128, 0, s>>>(b, h, use_handle);
-  if (launches) *launches += 10;
+  REC();
+#undef REC
+  if (launches) *launches += FARGO_NKERNELS;
 }
 
 void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s) {
@@ -1454,6 +1638,9 @@ cudaError_t fargo_kernel_attributes(int max_nsec, int seg) {
   cudaError_t e = cudaFuncSetAttribute(k_cfl_force, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(sizeof(float) * max_nsec));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_transport_theta, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)fargo_theta_smem_bytes(seg));
+  e = cudaFuncSetAttribute(k_transport<5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)fargo_transport_smem_bytes(seg, 0));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_transport<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)fargo_transport_smem_bytes(seg, 1));
 }

@@ -222,6 +222,25 @@ long long fargo_kernel_launches(const fargo_ctx* ctx);
    including those inside the DT graphs (substeps x kernels per substep). */
 long long fargo_batch_count_launches(fargo_batch* b);
 long long fargo_batch_kernel_launches(const fargo_batch* b);
+/* The CUDA stream (cudaStream_t) every call of the context/batch uses, so a
+   caller can order its own work or record timing events on it. */
+void* fargo_stream(fargo_ctx* ctx);
+void* fargo_batch_stream(fargo_batch* b);
+/* The one-disk batch inside a context (to use the batch calls on it). */
+fargo_batch* fargo_ctx_batch(fargo_ctx* ctx);
+/* Copies without the final wait; host buffers must stay valid until
+   fargo_batch_sync (page-locked buffers let them overlap). */
+fargo_status fargo_batch_upload_async(fargo_batch* b, int disk, const float* dens, const float* vrad,
+                                      const float* vtheta, const float* energy);
+fargo_status fargo_batch_download_async(fargo_batch* b, int disk, float* dens, float* vrad,
+                                        float* vtheta, float* energy);
+/* Per-kernel device time of ndt DTs run with one CUDA event pair per kernel
+   launch (host loop over substeps): ms[k] for the fargo_profile_kernel_count()
+   slots named by fargo_profile_kernel_name(k): the substep kernels in launch
+   order, then the self-gravity pipeline. */
+fargo_status fargo_batch_profile(fargo_batch* b, int ndt, double* ms /* >= 16 */, int* nsub);
+int fargo_profile_kernel_count(void);
+const char* fargo_profile_kernel_name(int k);
 /* 1 (default): one CUDA graph launch per DT with a device-driven WHILE node
    over the substeps; 0: host loop with one wait per substep. */
 fargo_status fargo_set_graph_mode(fargo_ctx* ctx, int use_graph);

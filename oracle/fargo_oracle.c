@@ -96,7 +96,7 @@ struct orc {
   float PhysicalTime, PhysicalTimeInitial, OmegaFrame, MassTaper, HillRadius, LostMass, mdcp1;
   real invdphi, onethird, dphi;
   float Xplanet_mark, Yplanet_mark; /* Psys.cu:79 static float Xplanet, Yplanet */
-  fargo_planets sys;
+  fargo_planets sys, sys0;
   pairr DiskOnPrimaryAcceleration, IndirectTerm;
   /* substep log */
   int nsub;
@@ -1530,19 +1530,12 @@ int orc_create(const fargo_params* pin, const fargo_planets* planets, const doub
 
   fill_polar_1d(o, radii);
   fill_misc_tables(o);
-  o->sys = *planets;
-  if (o->sys.nb > 0) o->HillRadius = o->sys.x[0] * pow(o->sys.mass[0] / 3., 1. / 3.); /* Psys.cu:206 */
-  /* InitGasDensity / FillSigma, Pframeforce.cu:173-182, Theo.cu:23-29 */
+  o->sys0 = *planets;
+  /* FillSigma / FillEnergy profiles, Theo.cu:23-29,42-51 */
   for (int i = 0; i < nrad; i++) {
     o->SigmaMed[i] = sigma_profile(o, o->Rmed[i]);
     o->SigmaInf[i] = sigma_profile(o, o->Rinf[i]);
-  }
-  for (int i = 0; i < nrad; i++)
-    for (int j = 0; j < nsec; j++) o->Dens[j + i * nsec] = o->SigmaMed[i];
-  if (p->Adiabatic) {
-    for (int i = 0; i < nrad; i++) o->EnergyMed[i] = energy_profile(o, o->Rmed[i]);
-    for (int i = 0; i < nrad; i++)
-      for (int j = 0; j < nsec; j++) o->Energy[i * nsec + j] = o->EnergyMed[i];
+    if (p->Adiabatic) o->EnergyMed[i] = energy_profile(o, o->Rmed[i]);
   }
   if (p->SelfGravity) {
     size_t n2 = (size_t)2 * nrad * nsec;
@@ -1557,6 +1550,42 @@ int orc_create(const fargo_params* pin, const fargo_planets* planets, const doub
     o->SGP_rstep = RLOG(o->Radii[nrad] / o->Radii[0]) / (float)nrad;
     o->SGP_tstep = 2.0 * PI / (float)nsec;
     sg_init_kernel(o);
+  }
+  *out = o;
+  orc_init_state(o, NULL, NULL);
+  return 0;
+}
+
+/* The initialisation of main() from InitGasDensity on (Main.cu:292-344),
+   with an optional perturbed density / energy in place of the profiles. */
+void orc_init_state(orc* o, const float* dens, const float* energy) {
+  const fargo_params* p = &o->p;
+  int nrad = o->nrad, nsec = o->nsec;
+  size_t ng = o->size_grid;
+  for (size_t l = 0; l < ng; l++) {
+    o->Dens[l] = 0;
+    o->Energy[l] = 0;
+    o->Vrad[l] = 0;
+    o->Vtheta[l] = 0;
+  }
+  /* InitGasDensity / InitGasEnergy, Pframeforce.cu:173-192 */
+  for (int i = 0; i < nrad; i++)
+    for (int j = 0; j < nsec; j++) {
+      o->Dens[j + i * nsec] = o->SigmaMed[i];
+      if (p->Adiabatic) o->Energy[i * nsec + j] = o->EnergyMed[i];
+    }
+  if (dens)
+    for (size_t l = 0; l < ng; l++) o->Dens[l] = dens[l];
+  if (energy)
+    for (size_t l = 0; l < ng; l++) o->Energy[l] = energy[l];
+  o->sys = o->sys0;
+  o->PhysicalTime = 0.0f;
+  o->PhysicalTimeInitial = 0.0f;
+  o->LostMass = 0.0f;
+  o->nsub = 0;
+  o->nsub_total = 0;
+  if (o->sys.nb > 0) o->HillRadius = o->sys.x[0] * pow(o->sys.mass[0] / 3., 1. / 3.); /* Psys.cu:206 */
+  if (p->SelfGravity) {
     /* compute_selfgravity(..., init=1) without the velocity update, then
        Init_planetarysys_withSG (Main.cu:322-328) */
     sg_accelerations(o);
@@ -1571,11 +1600,7 @@ int orc_create(const fargo_params* pin, const fargo_planets* planets, const doub
   compute_pressure(o);
   compute_temperature(o);
   /* InitGasVelocities (Pframeforce.cu:194-255) */
-  if (!p->SelfGravity) {
-    /* Vtheta initialised by the kernel below */
-  } else {
-    init_vtheta_with_sg(o);
-  }
+  if (p->SelfGravity) init_vtheta_with_sg(o);
   if (p->ViscosityAlpha) ring_mean(o, o->SoundSpeed, o->GLOBAL_bufarray);
   if (p->Cooling) {
     for (int i = 0; i < nrad; i++) o->CoolingTimeMed[i] = cooling_time(o, o->Rmed[i]);
@@ -1586,9 +1611,8 @@ int orc_create(const fargo_params* pin, const fargo_planets* planets, const doub
   o->viscosity_array[nrad] = fviscosity(o, o->Rmed[nrad - 1]);
   init_gas_velocities_kernel(o);
   o->PhysicalTimeInitial = o->PhysicalTime;
-  *out = o;
-  return 0;
 }
+
 
 void orc_destroy(orc* o) {
   if (!o) return;

@@ -30,6 +30,9 @@ typedef struct orc orc;
 /* Setup as main() does it (Main.cu:198-344).  radii may be NULL. */
 int orc_create(const fargo_params* p, const fargo_planets* planets, const double* radii, orc** out);
 void orc_destroy(orc* o);
+/* Re-run the initialisation from InitGasDensity on (Main.cu:292-344) with a
+   perturbed density / energy (float32, (NRAD+1)*NSEC; NULL = profile). */
+void orc_init_state(orc* o, const float* dens, const float* energy);
 
 /* Element size of the grid fields of this build (4 or 8). */
 int orc_real_size(void);

@@ -37,6 +37,7 @@ def _lib(prec):
     lib.orc_create.restype = C.c_int
     lib.orc_create.argtypes = [vp, vp, dp, C.POINTER(vp)]
     lib.orc_destroy.argtypes = [vp]
+    lib.orc_init_state.argtypes = [vp, fp, fp]
     lib.orc_set_fields_f32.argtypes = [vp, fp, fp, fp, fp]
     lib.orc_get_fields_f32.argtypes = [vp, fp, fp, fp, fp, fp, fp]
     lib.orc_set_fields.argtypes = [vp, vp, vp, vp, vp]
@@ -79,6 +80,12 @@ class Oracle:
     @property
     def size_grid(self):
         return (self.nrad + 1) * self.nsec
+
+    def init_state(self, dens=None, energy=None):
+        """Re-run the initialisation with a perturbed density (as fargo_init_state)."""
+        fp = C.POINTER(C.c_float)
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1) for a in (dens, energy)]
+        self.lib.orc_init_state(self.h, *[None if a is None else a.ctypes.data_as(fp) for a in arrs])
 
     def set_fields(self, dens=None, vrad=None, vtheta=None, energy=None):
         fp = C.POINTER(C.c_float)

@@ -41,6 +41,7 @@ def cases():
 
 
 def run(rawdir):
+    rawdir = os.path.abspath(rawdir)
     exe = os.path.join(ROOT, "oracle", "_ref", "fargo_ref")
     if not os.path.exists(exe):
         raise SystemExit("build the reference first: make -f oracle/ref/Makefile.ref")
@@ -48,12 +49,12 @@ def run(rawdir):
     for name, (p, pl, seed, ndt) in cases().items():
         d = os.path.join(rawdir, name)
         p = dict(p, Ntot=str(ndt), Ninterm=str(ndt))
-        par, cfg, out = configs.materialise(p, pl, d, "run")
-        env = dict(os.environ, FARGO_REF_DUMP=os.path.join(d, "dump_"))
+        par, cfg, out = configs.materialise(p, pl, d, "run", relative=True)
+        env = dict(os.environ, FARGO_REF_DUMP="dump_")
         if seed is not None:
             env["FARGO_REF_NOISE_SEED"] = str(seed)
         with open(os.path.join(d, "stdout.txt"), "w") as f:
-            r = subprocess.run([exe, par], cwd=d, env=env, stdout=f, stderr=subprocess.STDOUT, timeout=600)
+            r = subprocess.run([exe, "run.par"], cwd=d, env=env, stdout=f, stderr=subprocess.STDOUT, timeout=600)
         print(name, "exit", r.returncode)
         status |= r.returncode
     return status
@@ -64,6 +65,7 @@ def _read_field(path, nrad, nsec):
 
 
 def collect(rawdir):
+    rawdir = os.path.abspath(rawdir)
     for name, (p, pl, seed, ndt) in cases().items():
         d = os.path.join(rawdir, name)
         out = os.path.join(d, "run_out")

@@ -1,0 +1,65 @@
+"""The CUDA path against the reference's own CUDA build.
+
+Fixtures tests/golden/ref_*.npz come from the reference compiled from its
+unmodified sources and run on a B200 with seeded noisy initial conditions
+(tests/golden/make_ref_golden.py).  This library, initialised from the same
+parameters and the same noise, must reproduce the reference's initial
+fields, its substep counts, dt and FARGO shift counts exactly, its planet
+orbits, and its fields after 10 DTs within the stated tolerances."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from cudaprotoplanetarydisksfloat_b200 import Disk, noise, planets_dict
+from tests.golden import make_ref_golden as G
+from tests.helpers import make, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_*.npz")))
+
+# rel-L2 after 10 DTs.  Same compiler, same FP32 expressions and contraction
+# as the reference; the only arithmetic differences are the FP64 (here) vs
+# FP32 (reference) force sums and the summation order of those sums.
+TOL = {"dens": 1e-5, "vtheta": 1e-5, "energy": 1e-5, "temperature": 1e-5, "vrad": 1e-4}
+
+
+@pytest.mark.skipif(not FIXTURES, reason="no reference fixtures")
+@pytest.mark.parametrize("path", FIXTURES, ids=os.path.basename)
+def test_matches_reference(gpu, path):
+    z = np.load(path)
+    name = os.path.basename(path)[:-4]
+    p, pl, seed, ndt = G.cases()[name]
+    P, L, _ = make(dict(p, Ntot=str(ndt), Ninterm=str(ndt)), pl, name)
+    d = Disk(P, L)
+    if seed is not None:
+        f = d.fields()
+        d.init_state(dens=noise.perturb_density(f["dens"].reshape(-1), P.NRAD, P.NSEC, seed))
+    nrad = P.NRAD
+    f0 = d.fields(temperature=True)
+    for k in ("dens", "vrad", "vtheta", "energy"):
+        if k + "0" in z:
+            assert rel_l2(f0[k][:nrad], z[k + "0"]) <= 1e-7, k
+    s = 0
+    big = z["bigplanet"]
+    for t in range(ndt):
+        # bigplanet line t is written before AlgoGas(t): planet state after t DTs
+        pd = planets_dict(d.planets())
+        for k in range(pd["x"].size):
+            assert abs(np.float32(pd["x"][k]) - big[k, t, 1]) <= 1e-6 * max(1.0, abs(big[k, t, 1]))
+            assert abs(np.float32(pd["y"][k]) - big[k, t, 2]) <= 1e-6 * max(1.0, abs(big[k, t, 1]))
+        n = d.advance_dt()
+        ns, dt = d.substep_log()
+        assert np.array_equal(ns, z["sub_nshift"][s:s + n]), "FARGO shift counts differ from the reference"
+        assert np.array_equal(dt.astype(np.float32), z["sub_dt"][s:s + n].astype(np.float32))
+        s += n
+    f1 = d.fields(temperature=True)
+    errs = {}
+    for k in TOL:
+        if k + "1" in z:
+            errs[k] = rel_l2(f1[k][:nrad], z[k + "1"])
+    for k, e in errs.items():
+        assert e <= TOL[k], (k, e, errs)
