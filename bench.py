@@ -42,12 +42,14 @@ sys.path.insert(0, ROOT)
 # Algorithmic bytes per cell and launch of each substep kernel (the fields it
 # must read and write once; isothermal / adiabatic), for the roofline figure.
 KERNEL_BYTES = {
+    "k_ring_mean_cfl": (4, 4),     # v_theta read
     "k_cfl_force": (12, 20),       # Sigma, v_r, v_theta (+cs) read
     "k_source1": (20, 24),         # Sigma, v_r, v_theta (+e) read; VradInt, VthetaInt written
     "k_visc_tau": (24, 24),        # VradInt, VthetaInt, Sigma read; 3 stresses written
     "k_visc_update": (28, 28),     # 3 stresses, Sigma, VradInt, VthetaInt read; 2 written
     "k_source2": (20, 28),         # VradInt, VthetaInt, Sigma (+e) read; v_r, v_theta (+e) written
     "k_energy": (0, 24),           # v_r, v_theta, Sigma, e read; e, Q+ written
+    "k_ring_mean_tr": (4, 4),      # v_theta read
     "k_transport": (32, 40),       # Sigma, v_r, v_theta (+e) read; Sigma + 4 momenta (+e) written
     "k_velocities": (32, 40),      # Sigma + 4 momenta (+e) read; v_r, v_theta, Sigma (+e) written
     "k_substep_end": (0, 0),

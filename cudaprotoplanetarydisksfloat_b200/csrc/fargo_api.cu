@@ -21,8 +21,6 @@
 
 namespace {
 
-constexpr int kSegMax = 2048;  // rings up to this many sectors are one azimuthal segment
-constexpr int kSeg = 1024;     // segment length for wider rings
 
 struct DiskHost {
   fargo_params p;
@@ -185,8 +183,11 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
     D.a1 = D.a0;  // never written in isothermal runs
   }
   A(D.pres, ng)
-  A(D.visc, n1) A(D.cs_ring, n1) A(D.csmean, n1) A(D.vmoy, n1) A(D.ringmin, n1) A(D.nshift, n1)
-  A(D.log_nshift, (size_t)FARGO_MAXLOG * p->NRAD) A(D.partials, n1 * 4 * FARGO_MAXBODY)
+  size_t nct = n1;
+  A(D.visc, n1) A(D.cs_ring, n1) A(D.csmean, n1) A(D.vmoy, n1) A(D.ringmin, nct) A(D.nshift, n1)
+  A(D.tvmed, n1) A(D.tvconst, n1)
+  A(D.log_nshift, (size_t)FARGO_MAXLOG * p->NRAD) A(D.partials, nct * 4 * FARGO_MAXBODY)
+  A(D.log_dt, (size_t)FARGO_MAXLOG) A(D.rk_work, (size_t)FARGO_RK_WORK(FARGO_MAXPLANETS_DEV))
   float *cp, *sp, *cc, *sc;
   A(cp, (size_t)p->NSEC) A(sp, (size_t)p->NSEC) A(cc, (size_t)p->NSEC) A(sc, (size_t)p->NSEC)
 #undef A
@@ -216,12 +217,12 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
 
 DiskCtl ctl_header(const fargo_batch* b, int d, cudaError_t* e) {
   DiskCtl c;
-  *e = cudaMemcpy(&c, b->d_ctl + d, offsetof(DiskCtl, log_dt), cudaMemcpyDeviceToHost);
+  *e = cudaMemcpy(&c, b->d_ctl + d, sizeof(DiskCtl), cudaMemcpyDeviceToHost);
   return c;
 }
 
 fargo_status put_ctl_header(fargo_batch* b, int d, const DiskCtl& c) {
-  CK(cudaMemcpyAsync(b->d_ctl + d, &c, offsetof(DiskCtl, log_dt), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_ctl + d, &c, sizeof(DiskCtl), cudaMemcpyHostToDevice, b->stream));
   CK(cudaStreamSynchronize(b->stream));
   return FARGO_OK;
 }
@@ -277,7 +278,7 @@ fargo_status init_disk_state(fargo_batch* b, int d, const float* dens, const flo
   for (float* f : scratch) CK(cudaMemsetAsync(f, 0, sizeof(float) * ng, b->stream));
   // scalars and planets
   DiskCtl c;
-  std::memset(&c, 0, offsetof(DiskCtl, log_dt));
+  std::memset(&c, 0, sizeof(DiskCtl));
   fargo_planets pl = h.planets0;
   c.PhysicalTime = 0.0f;
   c.PhysicalTimeInitial = 0.0f;
@@ -414,16 +415,15 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     b->n_sg += h.p.SelfGravity ? 1 : 0;
     std::vector<int4>& theta = h.p.Adiabatic ? theta_adi : theta_iso;
     h.dev.item0 = (int)theta.size();
-    for (int i = 0; i < nrad; i++) {
-      if (nsec <= kSegMax) {
-        theta.push_back(make_int4(d, i, 0, nsec));
-        seg_max = std::max(seg_max, nsec);
-      } else {
-        for (int j0 = 0; j0 < nsec; j0 += kSeg) {
-          int S = std::min(kSeg, nsec - j0);
-          theta.push_back(make_int4(d, i, j0, S));
-          seg_max = std::max(seg_max, S);
-        }
+    // bands of FARGO_BAND rings, each in nseg near-equal azimuthal segments
+    // of at most FARGO_SEG_OUT sectors
+    const int nseg = (nsec + FARGO_SEG_OUT - 1) / FARGO_SEG_OUT;
+    const int seg = (nsec + nseg - 1) / nseg;
+    for (int i = 0; i < nrad; i += FARGO_BAND) {
+      for (int j0 = 0; j0 < nsec; j0 += seg) {
+        int S = std::min(seg, nsec - j0);
+        theta.push_back(make_int4(d, i, j0, S));
+        seg_max = std::max(seg_max, S);
       }
     }
     h.dev.nitems = (int)theta.size() - h.dev.item0;
@@ -436,8 +436,8 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   CK(cudaMalloc(&b->d_theta, sizeof(int4) * (theta_iso.size() + theta_adi.size() + 1)));
   CK(cudaMalloc(&b->d_flags, sizeof(int) * 4));
   // compacted active lists: act[4] + 3 disk lists + 3 int prefix arrays, and the cell prefix
-  CK(cudaMalloc(&b->d_act, sizeof(int) * (4 + 3 * n + 3 * (n + 1))));
-  CK(cudaMemsetAsync(b->d_act, 0, sizeof(int) * (4 + 3 * n + 3 * (n + 1)), b->stream));
+  CK(cudaMalloc(&b->d_act, sizeof(int) * (4 + 3 * n + 6 * (n + 1))));
+  CK(cudaMemsetAsync(b->d_act, 0, sizeof(int) * (4 + 3 * n + 6 * (n + 1)), b->stream));
   CK(cudaMalloc(&b->d_act_cell, sizeof(long long) * (n + 1)));
   CK(cudaMemsetAsync(b->d_act_cell, 0, sizeof(long long) * (n + 1), b->stream));
   b->red_blocks = 296;
@@ -473,16 +473,20 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   bd.act_ring_off = bd.act_adi_disk + n;
   bd.act_iso_off = bd.act_ring_off + (n + 1);
   bd.act_adi_off = bd.act_iso_off + (n + 1);
+  bd.act_grp_off = bd.act_adi_off + (n + 1);
+  bd.act_tile_off = bd.act_grp_off + (n + 1);
+  bd.act_ctile_off = bd.act_tile_off + (n + 1);
   bd.act_cell_off = b->d_act_cell;
   {
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     long long cg = (bd.ncell + 255) / 256;
     bd.cell_grid = (int)std::min<long long>(cg, (long long)nsm * 8);
-    bd.ring_grid = std::min(bd.nring, nsm * 8);
-    bd.item_grid = nsm * 2;
+    bd.ring_grid = std::min(bd.nring, nsm * 6);
+    bd.item_grid = std::min((int)(theta_iso.size() + theta_adi.size()), nsm * 8);
+    bd.grp_grid = std::min((bd.nring + 31 * n + 31) / 32, nsm * 3);
   }
-  CK(fargo_kernel_attributes(b->max_nsec, seg_max));
+  CK(fargo_kernel_attributes(b->max_nsec));
   fargo_launch_sector_tables(bd, b->max_nsec, b->stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(b->stream));
@@ -803,7 +807,7 @@ fargo_status fargo_get_substep_log(fargo_ctx* ctx, int cap, int* nshift, double*
   if (nshift && n > 0)
     CK(cudaMemcpy(nshift, D.log_nshift, sizeof(int) * (size_t)n * D.nrad, cudaMemcpyDeviceToHost));
   if (dt && n > 0)
-    CK(cudaMemcpy(dt, (const char*)(b->d_ctl) + offsetof(DiskCtl, log_dt), sizeof(double) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dt, D.log_dt, sizeof(double) * n, cudaMemcpyDeviceToHost));
   if (nsub) *nsub = c.nsub;
   return FARGO_OK;
 }
@@ -973,6 +977,12 @@ fargo_status fargo_set_graph_mode(fargo_ctx* ctx, int use_graph) {
   if (!ctx) return FARGO_EINVAL;
   ctx->b.use_graph = use_graph != 0;
   return build_graph(&ctx->b);
+}
+
+fargo_status fargo_batch_set_graph_mode(fargo_batch* b, int use_graph) {
+  if (!b) return FARGO_EINVAL;
+  b->use_graph = use_graph != 0;
+  return build_graph(b);
 }
 
 }  // extern "C"

@@ -65,11 +65,10 @@ struct DiskCtl {
   float brh[FARGO_MAXBODY], ba[FARGO_MAXBODY];
   // self-gravity axisymmetric accelerations at rings 0 and NRAD-1
   float axisg_in, axisg_out;
-  // logs of the current DT
-  double log_dt[FARGO_MAXLOG];
-  // scratch of the device RK5 (q0, q1, k1..k6), used by one thread
-  double rk_work[14 * 4 * FARGO_MAXPLANETS_DEV];
 };
+
+// scratch of the device RK5 (q0, q1, k1..k6, distances): 33 doubles per planet
+#define FARGO_RK_WORK(nb) (33 * (nb))
 
 struct DiskDev {
   int nrad, nsec;
@@ -110,8 +109,12 @@ struct DiskDev {
   float* vmoy;           // ConditionCFLKernel1D ring mean
   float* ringmin;        // newDT per ring
   int* nshift;           // Nshift per ring of the current substep
+  float* tvmed;          // transport: ring-mean v_theta of the current substep
+  float* tvconst;        // transport: constant residual per ring
   int* log_nshift;       // [FARGO_MAXLOG][nrad]
   double* partials;      // [nrad][4*FARGO_MAXBODY] force partial sums per ring
+  double* log_dt;        // [FARGO_MAXLOG] substep dt of the current DT
+  double* rk_work;       // [FARGO_RK_WORK(FARGO_MAXPLANETS_DEV)] RK5 scratch of large systems
   // sector tables
   const float *cos_pot, *sin_pot;    // cosf/sinf of (float)j/(float)nsec*2.0*PI
   const float *cos_cell, *sin_cell;  // cosf/sinf of 2.0*PI*(float)j/(float)nsec
@@ -143,13 +146,17 @@ struct BatchDev {
   int* act_iso_off;          // [ndisk+1] prefix of their transport items
   int* act_adi_disk;
   int* act_adi_off;
-  int cell_grid, ring_grid, item_grid;  // fixed grid sizes of the grid-stride kernels
+  int* act_grp_off;          // [ndisk+1] prefix of 32-ring groups of active disks
+  int* act_tile_off;         // [ndisk+1] prefix of cell tiles (one block's cells) of active disks
+  int* act_ctile_off;        // [ndisk+1] prefix of rings of active disks (CFL tiles)
+  int cell_grid, ring_grid, item_grid, grp_grid;  // fixed grid sizes of the grid-stride kernels
 };
 
 // kernel entry points (kernels_step.cu), launched by fargo_api.cu
-#define FARGO_NKERNELS 9  // kernels per substep
-size_t fargo_transport_smem_bytes(int seg, int adiabatic);
-cudaError_t fargo_kernel_attributes(int max_nsec, int seg);
+#define FARGO_NKERNELS 11  // kernels per substep
+#define FARGO_SEG_OUT 192  // largest azimuthal transport segment (output sectors per CTA)
+#define FARGO_BAND 8       // rings per transport CTA
+cudaError_t fargo_kernel_attributes(int max_nsec);
 void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s);
 // only_disk >= 0: that disk; -1: every disk still inside its DT
 void fargo_launch_cs_refresh(const BatchDev& b, int only_disk, cudaStream_t s);

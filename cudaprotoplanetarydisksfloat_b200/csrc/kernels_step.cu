@@ -3,11 +3,12 @@
 // The reference runs ~120 single-purpose kernels, ~50 host-side reductions
 // (each with cudaMalloc/cudaFree) and ~15 full-grid device copies per
 // substep, with a device synchronisation after every launch
-// (SourceEuler.cu:230-299).  Here one substep is 8-9 launches that read and
-// write only the disk state and a few scratch fields, with the CFL count,
-// the disk forces and the planet integrator kept on the device:
+// (SourceEuler.cu:230-299).  Here one substep is 11-12 launches that read
+// and write only the disk state and a few scratch fields, with the CFL
+// count, the disk forces and the planet integrator kept on the device:
 //
-//   k_cfl_force      ring means, CFL minimum, disk-on-body forces; the last
+//   k_ring_mean<0>   serial FP32 ring means of v_theta for the CFL
+//   k_cfl_force      CFL minimum, disk-on-body forces; the last
 //                    block of each disk finishes the substep's scalar work
 //                    (dt, mass taper, potential parameters, planet kicks,
 //                    FP64 RK5, frame rotation, per-ring viscosity)
@@ -17,10 +18,10 @@
 //   k_visc_update    viscous velocity update + sub-Keplerian boundary
 //   k_source2        artificial viscosity (Substep2) + energy predictor
 //   k_energy         viscous heating and implicit energy update (Substep3)
-//   k_transport      one ring per CTA: momenta + radial van Leer in
-//                    registers, FARGO ring mean, integer shift, residual and
-//                    constant azimuthal van Leer sweeps in shared memory,
-//                    shift fused into the store
+//   k_ring_mean<1>   ring means of v_theta for FARGO: Nshift, residual
+//   k_transport      one azimuthal segment per CTA: momenta + radial van
+//                    Leer in registers, residual and constant azimuthal van
+//                    Leer sweeps in shared memory, shift fused into the load
 //   k_velocities     velocities from the transported momenta
 //   k_substep_end    disks still inside their DT -> graph loop condition
 //
@@ -135,10 +136,9 @@ __device__ double compute_smoothing(const DiskDev& D, double r, float PT, float 
 // DerivMotionRK5, RungeKutta.cu:9-46; the planet-planet term divides by the
 // cube of the perturber's distance to the star, as the reference does.
 __device__ void deriv_motion(const DiskDev& D, const DiskCtl* C, const double* q, double* deriv, int nb,
-                             float dt) {
+                             float dt, double* Dist) {
   const double *x = q, *y = q + nb, *vx = q + 2 * nb, *vy = q + 3 * nb;
   double *dx = deriv, *dy = deriv + nb, *dvx = deriv + 2 * nb, *dvy = deriv + 3 * nb;
-  double Dist[FARGO_MAXPLANETS_DEV];
   for (int i = 0; i < nb; i++) Dist[i] = sqrt(x[i] * x[i] + y[i] * y[i]);
   for (int i = 0; i < nb; i++) {
     dx[i] = vx[i];
@@ -161,7 +161,7 @@ __device__ void deriv_motion(const DiskDev& D, const DiskCtl* C, const double* q
 
 // RungeKutta, RungeKutta.cu:55-74 (Cash-Karp coefficients of the reference)
 __device__ void runge_kutta(const DiskDev& D, const DiskCtl* C, const double* q0, float dt, double* q1,
-                            double* k, int nb) {
+                            double* k, int nb, double* Dist) {
   const double c[5][5] = {{0.2, 0.0, 0.0, 0.0, 0.0},
                           {0.075, 0.225, 0.0, 0.0, 0.0},
                           {0.3, -0.9, 1.2, 0.0, 0.0},
@@ -169,25 +169,26 @@ __device__ void runge_kutta(const DiskDev& D, const DiskCtl* C, const double* q0
                           {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
   int n4 = 4 * nb;
   for (int s = 0; s < 6 * n4; s++) k[s] = 0.0;
-  deriv_motion(D, C, q0, k, nb, dt);
+  deriv_motion(D, C, q0, k, nb, dt, Dist);
   for (int s = 0; s < 5; s++) {
     for (int i = 0; i < n4; i++)
       q1[i] = q0[i] + c[s][0] * k[i] + c[s][1] * k[n4 + i] + c[s][2] * k[2 * n4 + i] +
               c[s][3] * k[3 * n4 + i] + c[s][4] * k[4 * n4 + i];
-    deriv_motion(D, C, q1, k + (s + 1) * n4, nb, dt);
+    deriv_motion(D, C, q1, k + (s + 1) * n4, nb, dt, Dist);
   }
   for (int i = 0; i < n4; i++)
     q1[i] = q0[i] + 37.0 / 378.0 * k[i] + 250.0 / 621.0 * k[2 * n4 + i] + 125.0 / 594.0 * k[3 * n4 + i] +
             512.0 / 1771.0 * k[5 * n4 + i];
 }
 
-// AdvanceSystemRK5, Pframeforce.cu:94-157
+// AdvanceSystemRK5, Pframeforce.cu:94-157; work holds FARGO_RK_WORK(nb) doubles
 __device__ void advance_system_rk5(const DiskDev& D, DiskCtl* C, float dt, float PT, double* work) {
   int nb = C->nb;
   double dtheta, omega, rdot, x, y, r, new_r, vx, vy, theta, denom;
   double* q0 = work;
-  double* q1 = work + 4 * FARGO_MAXPLANETS_DEV;
-  double* k = work + 8 * FARGO_MAXPLANETS_DEV;
+  double* q1 = work + 4 * nb;
+  double* k = work + 8 * nb;
+  double* Dist = work + 32 * nb;
   if (!D.ForcedCircular && nb > 0) {
     for (int i = 0; i < nb; i++) {
       q0[i] = C->x[i];
@@ -195,7 +196,7 @@ __device__ void advance_system_rk5(const DiskDev& D, DiskCtl* C, float dt, float
       q0[i + 2 * nb] = C->vx[i];
       q0[i + 3 * nb] = C->vy[i];
     }
-    runge_kutta(D, C, q0, dt, q1, k, nb);
+    runge_kutta(D, C, q0, dt, q1, k, nb, Dist);
   }
   for (int i = 1 - (PT >= D.RELEASEDATE); i < nb; i++) {
     if (!D.ForcedCircular) {
@@ -361,27 +362,42 @@ __device__ __forceinline__ int find_range(const T* off, int n, T x) {
   return lo;
 }
 
-// Grid-stride walk over the cells of the disks still inside their DT.
+// Walk over the cells of the disks still inside their DT, in tiles of
+// kThreads consecutive cells of one disk.  Each block takes a contiguous run
+// of tiles, so it meets few disks; on entering a disk the block copies its
+// DiskDev to shared memory, and the body's field reads then neither chase
+// global pointers nor reload after its stores.
+static_assert(sizeof(DiskDev) % 4 == 0, "DiskDev copy by words");
+__device__ __forceinline__ void copy_words(void* dst, const void* src, int bytes) {
+  const int* s = reinterpret_cast<const int*>(src);
+  int* d = reinterpret_cast<int*>(dst);
+  for (int k = threadIdx.x; k < bytes / 4; k += blockDim.x) d[k] = s[k];
+}
+
 template <class Body>
 __device__ __forceinline__ void for_active_cells(const BatchDev& B, Body body) {
+  __shared__ DiskDev sD;
   const int na = B.act[0];
   if (na <= 0) return;
-  const long long total = B.act_cell_off[na];
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  int a = -1;
-  long long lo = 0, hi = 0;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total; c += stride) {
-    if (c < lo || c >= hi) {
-      a = find_range(B.act_cell_off, na, c);
-      lo = B.act_cell_off[a];
-      hi = B.act_cell_off[a + 1];
+  const int ntile = B.act_tile_off[na];
+  const int per = (ntile + gridDim.x - 1) / gridDim.x;
+  const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
+  int lo = 0, hi = -1;
+  for (int t = t0; t < t1; t++) {
+    if (t >= hi) {  // block-uniform
+      const int a = find_range(B.act_tile_off, na, t);
+      lo = B.act_tile_off[a];
+      hi = B.act_tile_off[a + 1];
+      __syncthreads();
+      copy_words(&sD, B.disks + B.act_disk[a], sizeof(DiskDev));
+      __syncthreads();
     }
-    const int d = B.act_disk[a];
-    const DiskDev& D = B.disks[d];
-    const int nsec = D.nsec;
-    const int loc = (int)(c - lo);
-    const int i = loc / nsec, j = loc - i * nsec;
-    body(D, D.ctl, i, j, (long long)loc, jwrap_m(j, nsec), jwrap_p(j, nsec));
+    const int nsec = sD.nsec;
+    const int loc = (t - lo) * kThreads + threadIdx.x;
+    if (loc < sD.nrad * nsec) {
+      const int i = loc / nsec, j = loc - i * nsec;
+      body(sD, sD.ctl, i, j, (long long)loc, jwrap_m(j, nsec), jwrap_p(j, nsec));
+    }
   }
 }
 
@@ -433,39 +449,64 @@ __device__ float block_min_f(float v, float* sh) {
 // -------------------------------------------------------------- CFL + forces
 
 // Last block of a disk: the scalar part of the substep (SourceEuler.cu:231-264).
-__device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* C, float* shf, double* shd) {
+// Substep scalars of one disk, run by the block that completed the disk's
+// last CFL tile.  Tile minima and force partials were written by other SMs
+// in this launch: read through L2.  The serial part runs on a shared-memory
+// copy of the disk's control block (sC), written back at the end.
+constexpr int kRkShared = 16;  // planets whose RK5 scratch fits in shared memory
+__device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const double* s_sum, double* work);
+__device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* Cg, DiskCtl* sC, float* shf, double* s_sum,
+                                       double* s_work) {
   const int nrad = D.nrad, nsec = D.nsec, tid = threadIdx.x;
-  __shared__ double s_sum[4 * FARGO_MAXBODY];
+  const int nct = nrad;
   // ConditionCFL host part (SourceEuler.cu:513-535): minimum over the ring
-  // minima, the shear limit DT1D (ConditionCFLKernel2D2, Kernels.cu:1425-1428)
-  // and DeltaT.
+  // minima of rings 1 .. NRAD-1, the shear limit DT1D (ConditionCFLKernel2D2,
+  // Kernels.cu:1425-1428) and DeltaT.
   float m = 1e30f;
   bool first = true;
-  for (int i = 1 + tid; i < nrad; i += blockDim.x) {
-    float v = D.ringmin[i];
+#pragma unroll 4
+  for (int t = 1 + tid; t < nct; t += blockDim.x) {
+    float v = __ldcg(D.ringmin + t);
     if (first || v < m) m = v;
     first = false;
   }
+#pragma unroll 4
   for (int i = tid; i < nrad - 1; i += blockDim.x) {
     float dt1 = 2.0 * PI_D * CFLSEC / (float)nsec / fabsf(D.vmoy[i] * D.invRmed[i] - D.vmoy[i + 1] * D.invRmed[i + 1]);
     if (dt1 < m) m = dt1;
   }
   float newdt = block_min_f(m, shf);
-  // disk-force sums: fixed order, one warp per sum
-  int nbody = C->nbody, nsum = 4 * nbody;
-  int w = tid >> 5, l = tid & 31;
-  for (int s = w; s < nsum; s += blockDim.x >> 5) {
+  // disk-force sums over the rings in a fixed order, one warp per sum
+  const int nbody = Cg->nbody, nsum = 4 * nbody;
+  const int w = tid >> 5, l = tid & 31;
+  for (int q = w; q < nsum; q += blockDim.x >> 5) {
     double acc = 0.0;
-    for (int r = l; r < nrad; r += 32) acc += D.partials[(size_t)r * 4 * FARGO_MAXBODY + s];
+#pragma unroll 4
+    for (int t = l; t < nct; t += 32) acc += __ldcg(D.partials + (size_t)t * 4 * FARGO_MAXBODY + q);
     acc = warp_sum_d(acc);
-    if (l == 0) s_sum[s] = acc;
+    if (l == 0) s_sum[q] = acc;
   }
   // FViscosity per ring for this substep (Viscosity.cu:84-85, SourceEuler.cu:350)
-  float PT = C->PhysicalTime;
-  for (int i = tid; i < nrad; i += blockDim.x) D.visc[i] = fviscosity_ring(D, i, PT, C->PhysicalTimeInitial);
+  const float PT = Cg->PhysicalTime;
+  for (int i = tid; i < nrad; i += blockDim.x) D.visc[i] = fviscosity_ring(D, i, PT, Cg->PhysicalTimeInitial);
+  {
+    const int* src = reinterpret_cast<const int*>(Cg);
+    int* dst = reinterpret_cast<int*>(sC);
+    for (int k = tid; k < (int)(sizeof(DiskCtl) / 4); k += blockDim.x) dst[k] = src[k];
+  }
   __syncthreads();
-  if (tid != 0) return;
+  if (tid == 0) finish_serial(D, sC, newdt, s_sum, sC->nb <= kRkShared ? s_work : D.rk_work);
+  __syncthreads();
+  {
+    const int* src = reinterpret_cast<const int*>(sC);
+    int* dst = reinterpret_cast<int*>(Cg);
+    for (int k = tid; k < (int)(sizeof(DiskCtl) / 4); k += blockDim.x) dst[k] = src[k];
+  }
+}
 
+__device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const double* s_sum, double* work) {
+  const int nbody = C->nbody;
+  const float PT = C->PhysicalTime;
   double DTd = (double)D.DT;
   // MassTaper, SourceEuler.cu:231-232
   float mt = PT / (D.MASSTAPER * 2.0 * M_PI);
@@ -492,7 +533,7 @@ __device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* C, float* shf,
   C->dt = dt;
   C->dtf = (float)dt;
   C->dtemp += dt;
-  if (C->nsub < FARGO_MAXLOG) C->log_dt[C->nsub] = dt;
+  if (C->nsub < FARGO_MAXLOG) D.log_dt[C->nsub] = dt;
   float dtf = (float)dt;
   if (D.Corotating) get_psys_info(D, C, 1);
   // DiskOnPrimaryAcceleration (ComputeAccel for the star, SideEuler.cu:151-164):
@@ -536,7 +577,7 @@ __device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* C, float* shf,
       C->vy[k] += dtf * C->ity;
     }
   }
-  advance_system_rk5(D, C, dtf, PT, C->rk_work);
+  advance_system_rk5(D, C, dtf, PT, work);
   C->domega = 0.0f;
   if (D.Corotating) {
     double OmegaNew = get_psys_info(D, C, 0) / dt;
@@ -556,150 +597,150 @@ __device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* C, float* shf,
   }
   prepare_bodies(D, C);
   C->counter = 0;
-  (void)shd;
 }
 
-// One block per ring: ConditionCFLKernel1D + ConditionCFLKernel2D1 + the ring
-// minimum of ConditionCFLKernel2D2 (Kernels.cu:1363-1422), and the disk force
-// of ComputeForceKernel (Kernels.cu:804-839) for the star and every FeelDisk
-// planet, accumulated in double.
+// One block per ring: ConditionCFLKernel1D + ConditionCFLKernel2D1 + the
+// ring minimum of ConditionCFLKernel2D2 (Kernels.cu:1363-1422), and the disk
+// force of ComputeForceKernel (Kernels.cu:804-839) for the star and every
+// FeelDisk planet, accumulated in double; per-ring results, so that the
+// finishing sums run in a fixed order.  Each block takes a contiguous run of
+// rings.  The block that completes a disk's last ring finishes the
+// substep's scalar work.
 __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
-  extern __shared__ float s_ring[];
+  __shared__ DiskDev sD;
+  __shared__ DiskCtl sC;
+  __shared__ float s_b[5][FARGO_MAXBODY];
   __shared__ float s_min[32];
   __shared__ double s_red[2 * FARGO_MAXBODY][kThreads / 32];
-  __shared__ float s_vm;
+  __shared__ double s_sum[4 * FARGO_MAXBODY];
+  __shared__ double s_work[FARGO_RK_WORK(kRkShared)];
   __shared__ unsigned s_ticket;
-  __shared__ float s_b[5][FARGO_MAXBODY];
+  const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
   const int na = B.act[0];
-  const int nar = na > 0 ? B.act_ring_off[na] : 0;
-  for (int gr = blockIdx.x; gr < nar; gr += gridDim.x) {
-  __syncthreads();
-  const int a = find_range(B.act_ring_off, na, gr);
-  const int d = B.act_disk[a];
-  const DiskDev& D = B.disks[d];
-  DiskCtl* C = D.ctl;
-  const int i = gr - B.act_ring_off[a], nsec = D.nsec, nrad = D.nrad, tid = threadIdx.x;
-  const float* vt = D.vtheta + (size_t)i * nsec;
-  for (int j = tid; j < nsec; j += blockDim.x) s_ring[j] = vt[j];
-  const int nbody = C->nbody;
-  if (tid < nbody) {
-    s_b[0][tid] = C->bx[tid];
-    s_b[1][tid] = C->by[tid];
-    s_b[2][tid] = C->brs[tid];
-    s_b[3][tid] = C->brh[tid];
-    s_b[4][tid] = C->ba[tid];
-  }
-  __syncthreads();
-  if (tid == 0) {
-    float moy = 0.0f;
-#pragma unroll 16
-    for (int j = 0; j < nsec; j++) moy += s_ring[j];
-    moy /= (float)nsec;
-    s_vm = moy;
-    D.vmoy[i] = moy;
-  }
-  __syncthreads();
-  const float vm = s_vm;
-  const float* vr = D.vrad + (size_t)i * nsec;
-  float lmin = 1e30f;
-  if (i > 0 && D.IsDisk) {
-    const float dxrad = D.Rsup[i] - D.Rinf[i];
-    const float dxt = D.dxtheta[i];
-    const float csr = D.Adiabatic ? 0.0f : D.cs_ring[i];
-    for (int j = tid; j < nsec; j += blockDim.x) {
-      float cs = D.Adiabatic ? D.cs[(size_t)i * nsec + j] : csr;
-      float vres = D.FastTransport ? s_ring[j] - vm : s_ring[j];
-      float invdt1 = cs / (min2(dxrad, dxt));
-      float invdt2 = fabsf(vr[j]) / dxrad;
-      float invdt3 = fabsf(vres) / dxt;
-      float dvr = vr[j + nsec] - vr[j];
-      float dvt = s_ring[jwrap_p(j, nsec)] - s_ring[j];
-      if (dvr >= 0.0)
-        dvr = 1e-10;
-      else
-        dvr = -dvr;
-      if (dvt >= 0.0)
-        dvt = 1e-10;
-      else
-        dvt = -dvt;
-      float invdt4 = max2(dvr / dxrad, dvt / dxt);
-      invdt4 *= 4.0 * CVNR * CVNR;
-      float dt2d = CFLSEC / sqrtf(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 + invdt4 * invdt4);
-      if (dt2d < lmin) lmin = dt2d;
+  const int ntile = na > 0 ? B.act_ctile_off[na] : 0;
+  const int per = (ntile + gridDim.x - 1) / gridDim.x;
+  const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
+  int lo = 0, hi = -1;
+  for (int t = t0; t < t1; t++) {
+    if (t >= hi) {  // block-uniform: entering a disk
+      const int a = find_range(B.act_ctile_off, na, t);
+      lo = B.act_ctile_off[a];
+      hi = B.act_ctile_off[a + 1];
+      __syncthreads();
+      copy_words(&sD, B.disks + B.act_disk[a], sizeof(DiskDev));
+      __syncthreads();
+      const DiskCtl* C = sD.ctl;
+      if (tid < C->nbody) {
+        s_b[0][tid] = C->bx[tid];
+        s_b[1][tid] = C->by[tid];
+        s_b[2][tid] = C->brs[tid];
+        s_b[3][tid] = C->brh[tid];
+        s_b[4][tid] = C->ba[tid];
+      }
+      __syncthreads();
     }
-  }
-  float rmin = block_min_f(lmin, s_min);
-  if (tid == 0 && i > 0) D.ringmin[i] = rmin;
-
-  // disk forces of this ring
-  double sfx[FARGO_MAXBODY], sfy[FARGO_MAXBODY];
+    const DiskDev& D = sD;
+    DiskCtl* C = D.ctl;
+    const int nbody = C->nbody;
+    const int nsec = D.nsec;
+    const int i = t - lo;  // ring
+    float lmin = 1e30f;
+    double sfx[FARGO_MAXBODY], sfy[FARGO_MAXBODY];
 #pragma unroll
-  for (int b = 0; b < FARGO_MAXBODY; b++) sfx[b] = sfy[b] = 0.0;
-  const int k = D.ExcludeHill ? FARGO_DIMFXY - 1 : 0;
-  const float hillcutfactor = (float)k / (float)(FARGO_DIMFXY - 1);
-  if (D.IsDisk) {
-    const float Rm = D.Rmed[i], Sf = D.Surf[i];
-    const float* dn = D.dens + (size_t)i * nsec;
-    for (int j = tid; j < nsec; j += blockDim.x) {
-      float cellmass = Sf * dn[j];
-      float cx = Rm * D.cos_cell[j];
-      float cy = Rm * D.sin_cell[j];
+    for (int b = 0; b < FARGO_MAXBODY; b++) sfx[b] = sfy[b] = 0.0;
+    if (D.IsDisk) {
+      const float vm = D.vmoy[i];  // k_ring_mean<0>
+      const float dxrad = D.Rsup[i] - D.Rinf[i];
+      const float dxt = D.dxtheta[i];
+      const float csr = D.Adiabatic ? 0.0f : D.cs_ring[i];
+      const int k = D.ExcludeHill ? FARGO_DIMFXY - 1 : 0;
+      const float hillcutfactor = (float)k / (float)(FARGO_DIMFXY - 1);
+      const float Rm = D.Rmed[i], Sf = D.Surf[i];
+      const float* vt = D.vtheta + (size_t)i * nsec;
+      const float* vr = D.vrad + (size_t)i * nsec;
+      const float* dn = D.dens + (size_t)i * nsec;
+#pragma unroll 2
+      for (int j = tid; j < nsec; j += kThreads) {
+        if (i > 0) {
+          float cs = D.Adiabatic ? D.cs[(size_t)i * nsec + j] : csr;
+          const float v0 = vt[j];
+          float vres = D.FastTransport ? v0 - vm : v0;
+          float invdt1 = cs / (min2(dxrad, dxt));
+          float invdt2 = fabsf(vr[j]) / dxrad;
+          float invdt3 = fabsf(vres) / dxt;
+          float dvr = vr[j + nsec] - vr[j];
+          float dvt = vt[jwrap_p(j, nsec)] - v0;
+          if (dvr >= 0.0)
+            dvr = 1e-10;
+          else
+            dvr = -dvr;
+          if (dvt >= 0.0)
+            dvt = 1e-10;
+          else
+            dvt = -dvt;
+          float invdt4 = max2(dvr / dxrad, dvt / dxt);
+          invdt4 *= 4.0 * CVNR * CVNR;
+          float dt2d = CFLSEC / sqrtf(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 + invdt4 * invdt4);
+          if (dt2d < lmin) lmin = dt2d;
+        }
+        float cellmass = Sf * dn[j];
+        float cx = Rm * D.cos_cell[j];
+        float cy = Rm * D.sin_cell[j];
 #pragma unroll
-      for (int b = 0; b < FARGO_MAXBODY; b++) {
-        if (b < nbody) {
-          float dx = cx - s_b[0][b];
-          float dy = cy - s_b[1][b];
-          float rs = s_b[2][b];
-          float d2 = dx * dx + dy * dy;
-          float dist2 = d2 + rs * rs;
-          float distance = sqrtf(dist2);
-          // 1.0/dist2/distance: one division of the exact double product
-          float InvDist3 = 1.0 / ((double)dist2 * (double)distance);
-          float hill_cut;
-          if (k != 0) {
-            float rh = s_b[3][b] * hillcutfactor;
-            hill_cut = 1. - expf(-d2 / (rh * rh));
-          } else
-            hill_cut = 1.;
-          float fx = 1.0 * cellmass * dx * InvDist3 * hill_cut;
-          float fy = 1.0 * cellmass * dy * InvDist3 * hill_cut;
-          sfx[b] += fx;
-          sfy[b] += fy;
+        for (int b = 0; b < FARGO_MAXBODY; b++) {
+          if (b < nbody) {
+            float dx = cx - s_b[0][b];
+            float dy = cy - s_b[1][b];
+            float rs = s_b[2][b];
+            float d2 = dx * dx + dy * dy;
+            float dist2 = d2 + rs * rs;
+            float distance = sqrtf(dist2);
+            // 1.0/dist2/distance, as one float reciprocal
+            float InvDist3 = __frcp_rn(dist2 * distance);
+            float hill_cut;
+            if (k != 0) {
+              float rh = s_b[3][b] * hillcutfactor;
+              hill_cut = 1. - expf(-d2 / (rh * rh));
+            } else
+              hill_cut = 1.;
+            sfx[b] += cellmass * dx * InvDist3 * hill_cut;
+            sfy[b] += cellmass * dy * InvDist3 * hill_cut;
+          }
         }
       }
     }
-  }
-  const int w = tid >> 5, l = tid & 31;
+    float rmin = block_min_f(lmin, s_min);
+    if (tid == 0) D.ringmin[i] = rmin;
 #pragma unroll
-  for (int b = 0; b < FARGO_MAXBODY; b++) {
-    if (b < nbody) {
-      double a = warp_sum_d(sfx[b]);
-      double c = warp_sum_d(sfy[b]);
-      if (l == 0) {
-        s_red[2 * b][w] = a;
-        s_red[2 * b + 1][w] = c;
+    for (int b = 0; b < FARGO_MAXBODY; b++) {
+      if (b < nbody) {
+        double fx = warp_sum_d(sfx[b]);
+        double fy = warp_sum_d(sfy[b]);
+        if (l == 0) {
+          s_red[2 * b][w] = fx;
+          s_red[2 * b + 1][w] = fy;
+        }
       }
     }
-  }
-  __syncthreads();
-  if (tid < 2 * nbody) {
-    double acc = 0.0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); q++) acc += s_red[tid][q];
-    int b = tid >> 1, comp = tid & 1;  // comp 0: x, 1: y
-    bool inner = D.Rmed[i] < s_b[4][b];
-    double* P = D.partials + (size_t)i * 4 * FARGO_MAXBODY + 4 * b + 2 * comp;
-    P[0] = inner ? acc : 0.0;  // fx_inner / fy_inner
-    P[1] = inner ? 0.0 : acc;  // fx_outer / fy_outer
-  }
-  // the block that processes this disk's last ring finishes the substep's scalar work
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) s_ticket = atomicAdd(&C->counter, 1u);
-  __syncthreads();
-  if (s_ticket == (unsigned)(nrad - 1)) {
+    __syncthreads();
+    if (tid < 2 * nbody) {
+      double acc = 0.0;
+      for (int q = 0; q < kThreads / 32; q++) acc += s_red[tid][q];
+      const int b = tid >> 1, comp = tid & 1;  // comp 0: x, 1: y
+      const bool inner = D.Rmed[i] < s_b[4][b];
+      double* P = D.partials + (size_t)i * 4 * FARGO_MAXBODY + 4 * b + 2 * comp;
+      P[0] = inner ? acc : 0.0;  // f*_inner
+      P[1] = inner ? 0.0 : acc;  // f*_outer
+    }
+    // the block that completes this disk's last ring finishes the substep
     __threadfence();
-    finish_cfl_and_planets(D, C, s_min, nullptr);
-  }
+    __syncthreads();
+    if (tid == 0) s_ticket = atomicAdd(&C->counter, 1u);
+    __syncthreads();
+    if (s_ticket == (unsigned)(D.nrad - 1)) {
+      __threadfence();
+      finish_cfl_and_planets(D, C, &sC, s_min, s_sum, s_work);
+    }
   }
 }
 
@@ -718,7 +759,7 @@ __device__ __forceinline__ float potential_at(const DiskDev& D, const DiskCtl* C
     float distance = (x - xp) * (x - xp) + (y - yp) * (y - yp);
     float distancesmooth = sqrtf(distance + C->psmooth[k]);
     float pot = __fdiv_rn(-mp, distancesmooth);  // -G*mplanet/distancesmooth
-    if (D.Indirect_Term) pot += 1.0 * mp * C->pipd3[k] * (x * xp + y * yp);
+    if (D.Indirect_Term) pot += mp * C->pipd3[k] * (x * xp + y * yp);
     P += pot;
     if (k == 0) {
       float InvDistance = __fdiv_rn(1.0f, Rm);
@@ -735,14 +776,14 @@ __device__ __forceinline__ float pressure_at(const DiskDev& D, long long l, int 
     float cs = D.cs_ring[i];
     return D.dens[l] * cs * cs;
   }
-  return (D.ADIABATICINDEX - 1.0) * D.energy[l];
+  return (D.ADIABATICINDEX - 1.0f) * D.energy[l];
 }
 
 
 // Substep1KernelVrad / Substep1KernelVtheta (Kernels.cu:52-88), with
 // CorrectVthetaKernel (Kernels.cu:1352-1359) applied on the fly, and the
 // self-gravity kick of Update_sgvelocityKernel (Kernels.cu:1024-1041).
-__global__ void __launch_bounds__(kThreads) k_source1(BatchDev B) {
+__global__ void __launch_bounds__(kThreads, 4) k_source1(BatchDev B) {
   CELL_BEGIN
   const float dt = C->dtf;
   const float OmegaFrame = C->OmegaFrame;
@@ -759,11 +800,11 @@ __global__ void __launch_bounds__(kThreads) k_source1(BatchDev B) {
     const long long lm = l - nsec;
     const float Pm = pressure_at(D, lm, i - 1);
     const float Phim = potential_at(D, C, i - 1, j);
-    float gradp = (P0 - Pm) * 2.0 / (Dn[l] + Dn[lm]) * D.invdiffRmed[i];
+    float gradp = (P0 - Pm) * 2.0f / (Dn[l] + Dn[lm]) * D.invdiffRmed[i];
     float gradphi = (Phi0 - Phim) * D.invdiffRmed[i];
     const long long lp = (long long)i * nsec + jp;
     float vt2 = vth(l, i) + vth(lp, i) + vth(lm, i - 1) + vth(lp - nsec, i - 1);
-    vt2 = vt2 / 4.0 + D.Rinf[i] * OmegaFrame;
+    vt2 = vt2 * 0.25f + D.Rinf[i] * OmegaFrame;
     vt2 = vt2 * vt2;
     float vri = D.vrad[l] + dt * (-gradp - gradphi + vt2 * D.invRinf[i]);
     if (D.SelfGravity)
@@ -775,11 +816,11 @@ __global__ void __launch_bounds__(kThreads) k_source1(BatchDev B) {
   }
   {
     const long long la = (long long)i * nsec + jm;
-    float dxtheta = 2.0 * PI_D / (float)nsec * D.Rmed[i];
-    float invdxtheta = 1.0 / dxtheta;
+    float dxtheta = 2.0f * (float)PI_D / (float)nsec * D.Rmed[i];
+    float invdxtheta = 1.0f / dxtheta;
     const float Pa = pressure_at(D, la, i);
     const float Phia = potential_at(D, C, i, jm);
-    float gradp = (P0 - Pa) * 2.0 / (Dn[l] + Dn[la]) * invdxtheta;
+    float gradp = (P0 - Pa) * 2.0f / (Dn[l] + Dn[la]) * invdxtheta;
     float gradphi = (Phi0 - Phia) * invdxtheta;
     float vti = vth(l, i) - dt * (gradp + gradphi);
     vti += dt * D.supp_torque[i];
@@ -787,7 +828,7 @@ __global__ void __launch_bounds__(kThreads) k_source1(BatchDev B) {
       // the reference reads SG_Acct[i*nsec + (j-1)%nsec]: for j = 0 that is
       // the last sector of ring i-1 (ring 0: taken from ring 0 itself)
       long long lq = (j > 0) ? l - 1 : (i > 0 ? l - 1 : (long long)nsec - 1);
-      vti += 0.5 * dt * (D.sg_acct[l] + D.sg_acct[lq]);
+      vti += 0.5f * dt * (D.sg_acct[l] + D.sg_acct[lq]);
     }
     D.vti[l] = vti;
   }
@@ -810,18 +851,18 @@ __device__ __forceinline__ Tau viscous_terms(const DiskDev& D, const float* Vr, 
   const float nu = D.visc[i];
   Tau t;
   float DRR = (Vr[l + nsec] - Vr[l]) * D.invdiffRsup[i];
-  float DPP = (Va[lp] - Va[l]) * D.invdphi * D.invRmed[i] + 0.5 * (Vr[l + nsec] + Vr[l]) * D.invRmed[i];
+  float DPP = (Va[lp] - Va[l]) * D.invdphi * D.invRmed[i] + 0.5f * (Vr[l + nsec] + Vr[l]) * D.invRmed[i];
   float divV = (Vr[l + nsec] * D.Rsup[i] - Vr[l] * D.Rinf[i]) * D.invdiffRsup[i] * D.invRmed[i];
   divV += (Va[lp] - Va[l]) * D.invdphi * D.invRmed[i];
   t.divv = divV;
-  t.rr = 2.0 * Dn[l] * nu * (DRR - D.onethird * divV);
-  t.pp = 2.0 * Dn[l] * nu * (DPP - D.onethird * divV);
+  t.rr = 2.0f * Dn[l] * nu * (DRR - D.onethird * divV);
+  t.pp = 2.0f * Dn[l] * nu * (DPP - D.onethird * divV);
   t.rp = 0.0f;
   if (i > 0) {
     const long long lm = (long long)i * nsec + jm;
-    float DRP = 0.5 * (D.Rinf[i] * (Va[l] * D.invRmed[i] - Va[l - nsec] * D.invRmed[i - 1]) * D.invdiffRmed[i] +
-                       (Vr[l] - Vr[lm]) * D.invdphi * D.invRinf[i]);
-    t.rp = 2.0 * 0.25 * (Dn[l] + Dn[l - nsec] + Dn[(long long)i * nsec] + Dn[lm - nsec]) * nu * DRP;
+    float DRP = 0.5f * (D.Rinf[i] * (Va[l] * D.invRmed[i] - Va[l - nsec] * D.invRmed[i - 1]) * D.invdiffRmed[i] +
+                        (Vr[l] - Vr[lm]) * D.invdphi * D.invRinf[i]);
+    t.rp = 0.5f * (Dn[l] + Dn[l - nsec] + Dn[(long long)i * nsec] + Dn[lm - nsec]) * nu * DRP;
   }
   return t;
 }
@@ -868,14 +909,14 @@ __global__ void __launch_bounds__(kThreads) k_visc_update(BatchDev B) {
   if (i > 0 && i < nrad - 1) {
     D.vti[l] += DeltaT * D.invRmed[i] *
                 ((D.Rsup[i] * TRP[l + nsec] - D.Rinf[i] * TRP[l]) * D.invdiffRsup[i] +
-                 (TPP[l] - TPP[lmj]) * D.invdphi + 0.5 * (TRP[l] + TRP[l + nsec])) /
-                (0.5 * (Dn[l] + Dn[lmj]));
+                 (TPP[l] - TPP[lmj]) * D.invdphi + 0.5f * (TRP[l] + TRP[l + nsec])) /
+                (0.5f * (Dn[l] + Dn[lmj]));
   }
   if (i > 0) {
     D.vri[l] += DeltaT * D.invRinf[i] *
                 ((D.Rmed[i] * TRR[l] - D.Rmed[i - 1] * TRR[l - nsec]) * D.invdiffRmed[i] +
-                 (TRP[lpj] - TRP[l]) * D.invdphi - 0.5 * (TPP[l] + TPP[l - nsec])) /
-                (0.5 * (Dn[l] + Dn[l - nsec]));
+                 (TRP[lpj] - TRP[l]) * D.invdphi - 0.5f * (TPP[l] + TPP[l - nsec])) /
+                (0.5f * (Dn[l] + Dn[l - nsec]));
   }
   if (!D.Evanescent && (i == 0 || i == nrad - 1)) {
     float vin, vout;
@@ -889,7 +930,7 @@ __global__ void __launch_bounds__(kThreads) k_visc_update(BatchDev B) {
 // Substep2Kernel + Substep2Kernel2 (Kernels.cu:570-621), then the
 // ActualiseGasVrad/Vtheta copies become direct stores into the state.
 __device__ __forceinline__ float qvisc(float dv, float dens) {
-  if (dv < 0.0) return CVNR * CVNR * dens * dv * dv;
+  if (dv < 0.0f) return (float)(CVNR * CVNR) * dens * dv * dv;
   return 0.0f;
 }
 
@@ -904,12 +945,12 @@ __global__ void __launch_bounds__(kThreads) k_source2(BatchDev B) {
   float vr_new = 0.0f;
   if (i > 0) {
     float qrm = qvisc(VRI[l] - VRI[l - nsec], Dn[l - nsec]);
-    vr_new = VRI[l] - dt * 2.0 / (Dn[l] + Dn[l - nsec]) * (qr - qrm) * D.invdiffRmed[i];
+    vr_new = VRI[l] - dt * 2.0f / (Dn[l] + Dn[l - nsec]) * (qr - qrm) * D.invdiffRmed[i];
   }
   float qtm = qvisc(VTI[l] - VTI[lmj], Dn[lmj]);
-  float dxtheta = 2.0 * PI_D / (float)nsec * D.Rmed[i];
-  float invdxtheta = 1.0 / dxtheta;
-  float vt_new = VTI[l] - dt * 2.0 / (Dn[l] + Dn[lmj]) * (qt - qtm) * invdxtheta;
+  float dxtheta = 2.0f * (float)PI_D / (float)nsec * D.Rmed[i];
+  float invdxtheta = 1.0f / dxtheta;
+  float vt_new = VTI[l] - dt * 2.0f / (Dn[l] + Dn[lmj]) * (qt - qtm) * invdxtheta;
   if (D.Adiabatic) {
     D.energy[l] = D.energy[l] - dt * qr * (VRI[l + nsec] - VRI[l]) * D.invdiffRsup[i] -
                   dt * qt * (VTI[lpj] - VTI[l]) * invdxtheta;
@@ -928,15 +969,15 @@ __device__ __forceinline__ float qplus_at(const DiskDev& D, int i, int j, int ns
   const long long l = (long long)i * nsec + j;
   const float nu = D.visc[i];
   float q;
-  if (nu != 0.0) {
-    q = 0.5 / nu / D.dens[l] * (t.rr * t.rr + +t.rp * t.rp + t.pp * t.pp);
-    q += (2.0 / 9.0) * nu * D.dens[l] * t.divv * t.divv;
+  if (nu != 0.0f) {
+    q = 0.5f / nu / D.dens[l] * (t.rr * t.rr + +t.rp * t.rp + t.pp * t.pp);
+    q += (float)(2.0 / 9.0) * nu * D.dens[l] * t.divv * t.divv;
   } else
-    q = 0.0;
+    q = 0.0f;
   return q;
 }
 
-__global__ void __launch_bounds__(kThreads) k_energy(BatchDev B) {
+__global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
   CELL_BEGIN
   if (!D.Adiabatic) return;
   const float dt = C->dtf;
@@ -960,11 +1001,11 @@ __global__ void __launch_bounds__(kThreads) k_energy(BatchDev B) {
   float num, den;
   if (!D.Cooling) {
     num = dt * q + e_int;
-    den = 1.0 + (D.ADIABATICINDEX - 1.0) * dt * divv;
+    den = 1.0f + (D.ADIABATICINDEX - 1.0f) * dt * divv;
   } else {
     num = D.EnergyMed[i] * dt * Dl / D.SigmaMed[i] + D.CoolingTimeMed[i] * e_int +
           dt * D.CoolingTimeMed[i] * (q - D.QplusMed[i] * Dl / D.SigmaMed[i]);
-    den = dt + D.CoolingTimeMed[i] + (D.ADIABATICINDEX - 1.0) * dt * D.CoolingTimeMed[i] * divv;
+    den = dt + D.CoolingTimeMed[i] + (D.ADIABATICINDEX - 1.0f) * dt * D.CoolingTimeMed[i] * divv;
   }
   D.qplus[l] = q;
   D.energy[l] = num / den;
@@ -974,289 +1015,405 @@ __global__ void __launch_bounds__(kThreads) k_energy(BatchDev B) {
 
 // ------------------------------------------------------------- transport
 
+// Transport arithmetic is FP32 throughout.  The reference writes several
+// of these expressions with double literals (0.5, 2.0, 1e-20), which
+// promotes them to double; here each is the same expression in float, the
+// quotient Q / (Sigma + 1e-20) is Q times the float reciprocal, and the
+// results differ by at most a few ulps per operation, the size of the
+// fused-multiply-add differences between two builds of the reference
+// itself.  (FP64 conversions and divisions run on the SM's transcendental
+// pipe at 1/8 of the FP32 rate and made this kernel issue-bound.)  Slope
+// quotients use the fast reciprocal division (2 ulp): their operands are
+// differences of O(1e-12 .. 1) quantities, far from the range where it
+// differs from IEEE division by more than that.
+
 // van Leer slope of StarRadKernel (Kernels.cu:917-927)
 __device__ __forceinline__ float vl_rad_slope(float qm, float q0, float qp, float invdm, float invdp) {
   float dqm = (q0 - qm) * invdm;
   float dqp = (qp - q0) * invdp;
-  if (dqp * dqm > 0.0) return 2.0 * dqp * dqm / (dqp + dqm);
+  if (dqp * dqm > 0.0f) return __fdividef(2.0f * dqp * dqm, dqp + dqm);
   return 0.0f;
 }
 
-// LRMomentaKernel (Kernels.cu:883-896) and the radial half of Transport for
-// one cell (i, j): StarRadKernel/StarRadKernel2/VanLeerRadialKernel
-// (Kernels.cu:909-947, 1137-1154) for RadMomP, RadMomM, ThetaMomP,
-// ThetaMomM, [energy] and density, with DivisePolarGridKernel's quotient
-// (Kernels.cu:1127-1134) formed per row.  out[0..3] momenta, out[4] energy
-// when nq == 6, out[nq-1] density.
+// One row sample of the radial half of Transport at column g: the
+// LRMomentaKernel quantities (Kernels.cu:883-896) RadMomP, RadMomM,
+// ThetaMomP, ThetaMomM, [energy], density, and their DivisePolarGridKernel
+// quotients by the density (Kernels.cu:1127-1134).
 template <int nq>
-__device__ __forceinline__ void radial_point(const DiskDev& D, const DiskCtl* C, int i, int j, float* out) {
-  const int nsec = D.nsec, nrad = D.nrad;
-  const int jp = jwrap_p(j, nsec);
-  const long long l = (long long)i * nsec + j;
-  const float dt = C->dtf;
-  const float Om = C->OmegaFrame;
-  const bool adi = (nq == 6);
-  // rows i-2 .. i+2 (clamped; the clamped values are never used)
-  float S[5], M1[5], M2[5], M3[5], M4[5], E[5];
-  double rden[5];
+struct RadRow {
+  float S;      // density
+  float Q[nq];  // quantities, Q[nq-1] = S
+  float W[nq];  // quotients Q / (S + 1e-20)
+};
+
+template <int nq>
+__device__ __forceinline__ RadRow<nq> rad_row(const DiskDev& D, int r, int g, int gp, float Om) {
+  const int nsec = D.nsec;
+  r = r < 0 ? 0 : (r > D.nrad - 1 ? D.nrad - 1 : r);  // clamped rows only meet zero slopes
+  const long long lr = (long long)r * nsec + g;
+  const long long lrp = (long long)r * nsec + gp;
+  RadRow<nq> R;
+  const float sg = __ldg(D.dens + lr);
+  const float rm = __ldg(D.Rmed + r);
+  R.S = sg;
+  R.Q[0] = sg * __ldg(D.vrad + lr + nsec);
+  R.Q[1] = sg * __ldg(D.vrad + lr);
+  R.Q[2] = sg * (__ldg(D.vtheta + lrp) + rm * Om) * rm;
+  R.Q[3] = sg * (__ldg(D.vtheta + lr) + rm * Om) * rm;
+  if (nq == 6) R.Q[4] = __ldg(D.energy + lr);
+  R.Q[nq - 1] = sg;
+  const float rden = __fdividef(1.0f, sg + 1e-20f);
 #pragma unroll
-  for (int q = 0; q < 5; q++) {
-    int r = i - 2 + q;
-    r = r < 0 ? 0 : (r > nrad - 1 ? nrad - 1 : r);
-    const long long lr = (long long)r * nsec + j;
-    const long long lrp = (long long)r * nsec + jp;
-    float sg = D.dens[lr];
-    float rm = D.Rmed[r];
-    S[q] = sg;
-    M1[q] = sg * D.vrad[lr + nsec];
-    M2[q] = sg * D.vrad[lr];
-    M3[q] = sg * (D.vtheta[lrp] + rm * Om) * rm;
-    M4[q] = sg * (D.vtheta[lr] + rm * Om) * rm;
-    E[q] = adi ? D.energy[lr] : 0.0f;
-    rden[q] = 1.0 / ((double)sg + 1e-20);
-  }
-  const float Vr0 = D.vrad[l];
-  const float Vr1 = D.vrad[l + nsec];  // row i+1 (row nrad is the zero ghost row)
-  const float idm_im1 = (i - 1 >= 1) ? D.invdiffRmed[i - 1] : 0.0f;
-  const float idm_i = D.invdiffRmed[i];
-  const float idm_ip1 = (i + 1 <= nrad - 1) ? D.invdiffRmed[i + 1] : 0.0f;
-  const float idm_ip2 = (i + 2 <= nrad - 1) ? D.invdiffRmed[i + 2] : 0.0f;
-  const float rm_im1 = (i >= 1) ? D.Rmed[i - 1] : 0.0f;
-  const float rm_i = D.Rmed[i];
-  const float rm_ip1 = (i + 1 <= nrad - 1) ? D.Rmed[i + 1] : 0.0f;  // Rmed[NRAD] only meets a zero slope
-  const float rm_ip2 = (i + 2 <= nrad - 1) ? D.Rmed[i + 2] : 0.0f;
-  auto slope = [&](const float* Q, int q) -> float {
-    int r = i - 2 + q;  // slope at ring r
-    if (r <= 0 || r >= nrad - 1) return 0.0f;
-    float invm = (q == 1) ? idm_im1 : (q == 2 ? idm_i : idm_ip1);
-    float invp = (q == 1) ? idm_i : (q == 2 ? idm_ip1 : idm_ip2);
-    return vl_rad_slope(Q[q - 1], Q[q], Q[q + 1], invm, invp);
-  };
-  // upwind interface values at rings i (q = 2) and i+1 (q = 3)
-  auto qstar_i = [&](const float* Q) -> float {
-    if (i == 0) return 0.0f;
-    if (Vr0 > 0.0) return Q[1] + (rm_i - rm_im1 - Vr0 * dt) * 0.5 * slope(Q, 1);
-    return Q[2] - (rm_ip1 - rm_i + Vr0 * dt) * 0.5 * slope(Q, 2);
-  };
-  auto qstar_ip = [&](const float* Q) -> float {
-    if (i + 1 >= nrad) return 0.0f;
-    if (Vr1 > 0.0) return Q[2] + (rm_ip1 - rm_i - Vr1 * dt) * 0.5 * slope(Q, 2);
-    return Q[3] - (rm_ip2 - rm_ip1 + Vr1 * dt) * 0.5 * slope(Q, 3);
-  };
-  const float dstar_i = qstar_i(S);
-  const float dstar_ip = qstar_ip(S);
-  float dtheta = 2.0 * PI_D / (float)nsec;
-  const float Ri = D.Rinf[i], Rs = D.Rsup[i], iS = D.invSurf[i];
-  auto advect = [&](const float* Q) -> float {
-    float W[5];
-#pragma unroll
-    for (int q = 0; q < 5; q++) W[q] = (double)Q[q] * rden[q];
-    float qi = qstar_i(W);
-    float qip = qstar_ip(W);
-    float varq = dt * dtheta * Ri * qi * dstar_i * Vr0;
-    varq -= dt * dtheta * Rs * qip * dstar_ip * Vr1;
-    return Q[2] + varq * iS;
-  };
-  out[0] = advect(M1);
-  out[1] = advect(M2);
-  out[2] = advect(M3);
-  out[3] = advect(M4);
-  if (adi) out[4] = advect(E);
-  out[nq - 1] = advect(S);
+  for (int c = 0; c < nq; c++) R.W[c] = R.Q[c] * rden;
+  return R;
 }
 
-constexpr int kTT = 512;   // threads of the transport kernel
-constexpr int kMaxK = 5;   // window points per thread: (2048 + 8) / 512 rounded up
-
-// One ring (or one segment of a wide ring) of Transport (TransportEuler.cu:24-35):
-// the radial half for every point of the window (radial_point, results kept
-// in registers), then OneWindTheta (TransportEuler.cu:171-219): ring mean of
-// v_theta (serial, as ComputeAverageThetaVelocitiesKernel), residual,
-// Nshift and constant residual (ComputeConstantResidualKernel,
-// Kernels.cu:1201-1232), the residual and constant-residual van Leer
-// sweeps (StarThetaKernel, StarThetaKernel2, VanLeerThetaKernel,
-// Kernels.cu:1157-1273) in shared memory, and AdvectSHIFTKernel
-// (Kernels.cu:1276-1289) fused into the store.  Final density / energy go to
-// scratch (a0 / a1) because neighbouring rings still read the old ones; the
-// velocity kernel moves them into the state.
+// van Leer slopes at row r from rows r-1, r, r+1 (StarRadKernel; zero on the
+// first and last ring): g[c] for the quotients, gs for the density.
 template <int nq>
-__global__ void __launch_bounds__(kTT) k_transport(BatchDev B, const int4* __restrict__ items) {
-  extern __shared__ float sm[];
-  __shared__ float s_vmed;
-  __shared__ int s_nshift;
-  __shared__ float s_vconst;
+__device__ __forceinline__ void rad_slopes(const DiskDev& D, int r, const RadRow<nq>& A, const RadRow<nq>& Bm,
+                                           const RadRow<nq>& Cp, float* g, float& gs) {
+  if (r <= 0 || r >= D.nrad - 1) {
+#pragma unroll
+    for (int c = 0; c < nq; c++) g[c] = 0.0f;
+    gs = 0.0f;
+    return;
+  }
+  const float im = __ldg(D.invdiffRmed + r), ip = __ldg(D.invdiffRmed + r + 1);
+#pragma unroll
+  for (int c = 0; c < nq; c++) g[c] = vl_rad_slope(A.W[c], Bm.W[c], Cp.W[c], im, ip);
+  gs = vl_rad_slope(A.S, Bm.S, Cp.S, im, ip);
+}
+
+// Upwind interface values at the boundary b between rows b-1 (lo) and b
+// (hi) for radial velocity vr (StarRadKernel2, Kernels.cu:929-947); zero on
+// the inner edge and beyond the outer ring.
+template <int nq>
+__device__ __forceinline__ void rad_face(const DiskDev& D, int b, float vr, float dt, const RadRow<nq>& lo,
+                                         const RadRow<nq>& hi, const float* glo, float gslo, const float* ghi,
+                                         float gshi, float* qs, float& ds) {
+  const int nrad = D.nrad;
+  if (b <= 0 || b >= nrad) {
+#pragma unroll
+    for (int c = 0; c < nq; c++) qs[c] = 0.0f;
+    ds = 0.0f;
+    return;
+  }
+  if (vr > 0.0f) {
+    const float h = (__ldg(D.Rmed + b) - __ldg(D.Rmed + b - 1) - vr * dt) * 0.5f;
+#pragma unroll
+    for (int c = 0; c < nq; c++) qs[c] = lo.W[c] + h * glo[c];
+    ds = lo.S + h * gslo;
+  } else {
+    const float rp = (b + 1 <= nrad - 1) ? __ldg(D.Rmed + b + 1) : 0.0f;  // only meets a zero slope
+    const float h = (rp - __ldg(D.Rmed + b) + vr * dt) * 0.5f;
+#pragma unroll
+    for (int c = 0; c < nq; c++) qs[c] = hi.W[c] - h * ghi[c];
+    ds = hi.S - h * gshi;
+  }
+}
+
+// Radial half of Transport (VanLeerRadialKernel, Kernels.cu:1137-1154) for
+// rings ia .. ib-1 at column g, marching outwards: each ring loads one new
+// row, one new slope and one new interface.  out[k][c] at stride ostride.
+template <int nq>
+__device__ __forceinline__ void rad_march(const DiskDev& D, int ia, int ib, int g, float dt, float Om,
+                                          float dtheta, float* out, int ostride_c, int ostride_r) {
+  const int nsec = D.nsec;
+  const int gp = g + 1 == nsec ? 0 : g + 1;
+  RadRow<nq> R0 = rad_row<nq>(D, ia - 1, g, gp, Om);  // row i-1 for the first slope
+  RadRow<nq> R1 = rad_row<nq>(D, ia, g, gp, Om);      // row i
+  RadRow<nq> R2 = rad_row<nq>(D, ia + 1, g, gp, Om);  // row i+1
+  float G0[nq], G1[nq], gs0, gs1, qs[nq], ds;
+  {
+    RadRow<nq> Rm = rad_row<nq>(D, ia - 2, g, gp, Om);
+    rad_slopes<nq>(D, ia - 1, Rm, R0, R1, G0, gs0);  // slope at row i-1
+  }
+  rad_slopes<nq>(D, ia, R0, R1, R2, G1, gs1);  // slope at row i
+  float vr0 = __ldg(D.vrad + (long long)ia * nsec + g);
+  rad_face<nq>(D, ia, vr0, dt, R0, R1, G0, gs0, G1, gs1, qs, ds);
+  for (int i = ia; i < ib; i++) {
+    RadRow<nq> R3 = rad_row<nq>(D, i + 2, g, gp, Om);
+    float G2[nq], gs2;
+    rad_slopes<nq>(D, i + 1, R1, R2, R3, G2, gs2);  // slope at row i+1
+    const float vr1 = __ldg(D.vrad + (long long)(i + 1) * nsec + g);  // row nrad is the zero ghost row
+    float qs1[nq], ds1;
+    rad_face<nq>(D, i + 1, vr1, dt, R1, R2, G1, gs1, G2, gs2, qs1, ds1);
+    const float Ri = __ldg(D.Rinf + i), Rs = __ldg(D.Rsup + i), iS = __ldg(D.invSurf + i);
+    float* o = out + (i - ia) * ostride_r;
+#pragma unroll
+    for (int c = 0; c < nq; c++) {
+      float varq = dt * dtheta * Ri * qs[c] * ds * vr0;
+      varq -= dt * dtheta * Rs * qs1[c] * ds1 * vr1;
+      o[c * ostride_c] = R1.Q[c] + varq * iS;
+    }
+    R1 = R2;
+    R2 = R3;
+#pragma unroll
+    for (int c = 0; c < nq; c++) {
+      G1[c] = G2[c];
+      qs[c] = qs1[c];
+    }
+    gs1 = gs2;
+    ds = ds1;
+    vr0 = vr1;
+  }
+}
+
+// ---------------------------------------------------------- ring means
+
+// Serial FP32 ring means of v_theta, j = 0 .. NSEC-1 in order as one thread
+// of ConditionCFLKernel1D (Kernels.cu:352-356) and of
+// ComputeAverageThetaVelocitiesKernel (Kernels.cu:1184-1198) sum them: the
+// FARGO shift floor(Ntilde + 0.5) and the CFL dt depend on the last bit.
+// One CTA takes 32 rings of one disk.  All its threads stream the rings
+// through shared memory in chunks of kRMW sectors (coalesced, 32 loads in
+// flight per thread) while warp 0, lane r owning ring i0 + r, adds the
+// previous chunk's row in order.
+//   mode 0: vmoy[i] (CFL, substep start)
+//   mode 1: transport VMed, Nshift and constant residual (OneWindTheta,
+//           TransportEuler.cu:171-219 with ComputeConstantResidualKernel,
+//           Kernels.cu:1201-1232), and the Nshift log of the DT.
+constexpr int kRMT = 256;  // threads
+constexpr int kRMW = 256;  // sectors per chunk
+size_t fargo_ring_mean_smem_bytes() { return sizeof(float) * 2 * 32 * (kRMW + 1); }
+template <int mode>
+__global__ void __launch_bounds__(kRMT) k_ring_mean(BatchDev B) {
+  extern __shared__ float rm_sm[];  // [2][32][kRMW + 1]
+  const int na = B.act[0];
+  const int ng = na > 0 ? B.act_grp_off[na] : 0;
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int g = blockIdx.x; g < ng; g += gridDim.x) {
+    const int a = find_range(B.act_grp_off, na, g);
+    const DiskDev& D = B.disks[B.act_disk[a]];
+    const int i0 = (g - B.act_grp_off[a]) * 32;
+    const int nsec = D.nsec, nrad = D.nrad;
+    const int nr = min(32, nrad - i0);
+    const float* base = D.vtheta + (size_t)i0 * nsec;
+    const int nchunk = (nsec + kRMW - 1) / kRMW;
+    float r[32];
+    auto load = [&](int c) {
+      const int col = c * kRMW + tid;
+#pragma unroll
+      for (int k = 0; k < 32; k++) r[k] = (c < nchunk && k < nr && col < nsec) ? __ldg(base + (size_t)k * nsec + col) : 0.0f;
+    };
+    auto store = [&](int c) {
+      float* buf = rm_sm + (c & 1) * 32 * (kRMW + 1);
+#pragma unroll
+      for (int k = 0; k < 32; k++) buf[k * (kRMW + 1) + tid] = r[k];
+    };
+    float moy = 0.0f;
+    __syncthreads();
+    load(0);
+    store(0);
+    __syncthreads();
+    for (int c = 0; c < nchunk; c++) {
+      load(c + 1);
+      if (tid < 32) {
+        const float* row = rm_sm + (c & 1) * 32 * (kRMW + 1) + lane * (kRMW + 1);
+        const int w = min(kRMW, nsec - c * kRMW);
+        if (w == kRMW) {
+#pragma unroll 32
+          for (int k = 0; k < kRMW; k++) moy += row[k];
+        } else {
+          for (int k = 0; k < w; k++) moy += row[k];
+        }
+      }
+      if (c + 1 < nchunk) store(c + 1);
+      __syncthreads();
+    }
+    const int i = i0 + lane;
+    if (tid < 32 && lane < nr) {
+      if (mode == 0) {
+        D.vmoy[i] = moy / (float)nsec;
+      } else {
+        const DiskCtl* C = D.ctl;
+        const float dt = C->dtf;
+        float VMed = moy / (float)nsec;
+        float invdt = 1.0 / dt;
+        float dpinvns = 2.0 * PI_D / (float)nsec;
+        float Ntilde = VMed * D.invRmed[i] * dt * (float)nsec / 2.0 / PI_D;
+        float Nround = floor(Ntilde + 0.5);
+        long nitemp = (long)Nround;
+        D.tvmed[i] = VMed;
+        D.tvconst[i] = (Ntilde - Nround) * D.Rmed[i] * invdt * dpinvns;
+        D.nshift[i] = (int)nitemp;
+        int sidx = C->nsub - 1;
+        if (sidx >= 0 && sidx < FARGO_MAXLOG) D.log_nshift[(size_t)sidx * nrad + i] = (int)nitemp;
+      }
+    }
+  }
+}
+
+constexpr int kTT = 256;  // threads of the transport kernel: one window point each
+constexpr int kBR = FARGO_BAND;  // rings per transport band
+static_assert(FARGO_SEG_OUT + 8 <= kTT, "transport window must fit the CTA");
+
+size_t fargo_transport_smem_bytes(int adiabatic) {
+  const int nq = adiabatic ? 6 : 5;
+  return sizeof(float) * (size_t)kTT * (size_t)(kBR * nq + 4 + 3 * nq);
+}
+
+// Transport (TransportEuler.cu:24-35) of a band of up to kBR rings i0 ..
+// and one azimuthal segment of output sectors j0 .. j0+S-1.  The output
+// sector j of ring i takes the swept value of source sector j - Nshift_i
+// (AdvectSHIFTKernel, Kernels.cu:1276-1289), so ring i works on the source
+// window j0 - Nshift_i - 4 .. + S + 8.  The rings are taken in sub-bands
+// whose windows fit one union window of kTT sectors: the radial half
+// (rad_march) runs over the union, one thread per column marching down the
+// sub-band, into shared memory; then, ring by ring, the residual and
+// constant-residual van Leer sweeps of OneWindTheta (StarThetaKernel,
+// StarThetaKernel2, VanLeerThetaKernel, Kernels.cu:1157-1273) on the ring's
+// window; the 4-point halo covers the sweeps' stencils.  VMed, Nshift and
+// the constant residual come from k_ring_mean<1>.  Final density / energy
+// go to scratch (a0 / a1) because neighbouring rings still read the old
+// ones; the velocity kernel moves them into the state.
+template <int nq>
+__global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __restrict__ items) {
+  extern __shared__ float tr_sm[];
+  float* sR = tr_sm;                 // [kBR][nq][kTT] radial results on the union window
+  float* sS = sR + kBR * nq * kTT;   // density of the ring's window (pre-sweep)
+  float* sG = sS + kTT;              // its azimuthal slope
+  float* sV = sG + kTT;              // residual velocity
+  float* sD = sV + kTT;              // DensStar of the sweep
+  float* sW = sD + kTT;              // [nq][kTT] DivisePolarGrid quotients
+  float* sQ = sW + nq * kTT;         // [nq][kTT] their slopes
+  float* sF = sQ + nq * kTT;         // [nq][kTT] their fluxes
+  __shared__ int s_ns[kBR];
+  __shared__ float s_vmed[kBR], s_vc[kBR];
   const int nak = (nq == 5) ? B.act[1] : B.act[2];
   const int* aoff = (nq == 5) ? B.act_iso_off : B.act_adi_off;
   const int* adisk = (nq == 5) ? B.act_iso_disk : B.act_adi_disk;
   const int nai = nak > 0 ? aoff[nak] : 0;
+  const int p = threadIdx.x;
   for (int t = blockIdx.x; t < nai; t += gridDim.x) {
-  __syncthreads();
-  const int a = find_range(aoff, nak, t);
-  const DiskDev& D = B.disks[adisk[a]];
-  const int4 it = items[D.item0 + (t - aoff[a])];
-  const DiskCtl* C = D.ctl;
-  if (!D.IsDisk) continue;
-  const int i = it.y, j0 = it.z, S = it.w;  // S output sectors starting at j0
-  const int nsec = D.nsec, tid = threadIdx.x;
-  const int L = S + 8;  // window: 4 points of halo on each side
-  float* sS = sm;           // density of the window (pre-sweep)
-  float* sV = sS + L;       // residual velocity
-  float* sD = sV + L;       // DensStar of the sweep
-  float* sW = sD + L;       // nq * L: DivisePolarGrid quotients
-  const float dt = C->dtf;
-  const float* vt = D.vtheta + (size_t)i * nsec;
-  const bool whole = (S == nsec);
-  float q[nq][kMaxK];
-  float tmp[nq];
-  if (tid == 0) {
-    float moy = 0.0f;
-#pragma unroll 16
-    for (int j = 0; j < nsec; j++) moy += vt[j];
-    float VMed = moy / (float)nsec;
-    float invdt = 1.0 / dt;
-    float dpinvns = 2.0 * PI_D / (float)nsec;
-    float Ntilde = VMed * D.invRmed[i] * dt * (float)nsec / 2.0 / PI_D;
-    float Nround = floor(Ntilde + 0.5);
-    long nitemp = (long)Nround;
-    s_nshift = (int)nitemp;
-    s_vmed = VMed;
-    s_vconst = (Ntilde - Nround) * D.Rmed[i] * invdt * dpinvns;
-    if (j0 == 0) {
-      D.nshift[i] = (int)nitemp;
-      int sidx = C->nsub - 1;
-      if (sidx >= 0 && sidx < FARGO_MAXLOG) D.log_nshift[(size_t)sidx * D.nrad + i] = (int)nitemp;
-    }
-  }
-  if (whole) {
-    // a whole ring: window sectors -4 .. nsec+3 (periodic), independent of the shift
-#pragma unroll
-    for (int k = 0; k < kMaxK; k++) {
-      int p = tid + k * kTT;
-      if (p < L) {
-        int g = p - 4;
-        g = g < 0 ? g + nsec : (g >= nsec ? g - nsec : g);
-        radial_point<nq>(D, C, i, g, tmp);
-#pragma unroll
-        for (int c = 0; c < nq; c++) q[c][k] = tmp[c];
-      }
-    }
-  }
-  __syncthreads();
-  const int ns = s_nshift;
-  const float VMed = s_vmed;
-  float vconst = s_vconst;
-  const bool fast = D.FastTransport;
-  int js = 0;
-  if (!whole) {
-    // segment of a wide ring: source window js-4 .. js+S+3, js = j0 - Nshift
-    js = (j0 - ns) % nsec;
-    if (js < 0) js += nsec;
-#pragma unroll
-    for (int k = 0; k < kMaxK; k++) {
-      int p = tid + k * kTT;
-      if (p < L) {
-        int g = (js - 4 + p) % nsec;
-        if (g < 0) g += nsec;
-        radial_point<nq>(D, C, i, g, tmp);
-#pragma unroll
-        for (int c = 0; c < nq; c++) q[c][k] = tmp[c];
-      }
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < kMaxK; k++) {
-    int p = tid + k * kTT;
-    if (p < L) {
-      int g = (js - 4 + p) % nsec;
-      if (g < 0) g += nsec;
-      float vres = vt[g] - VMed;
-      if (!fast) vres = vconst + vres;
-      sV[p] = vres;
-      sS[p] = q[nq - 1][k];
-    }
-  }
-  if (!fast) vconst = 0.0f;
-  __syncthreads();
-  const float Rm = D.Rmed[i];
-  float dxtheta = 2.0 * PI_D / (float)nsec * Rm;
-  float invdxtheta = 1.0 / dxtheta;
-  float invsurf = 1.0 / D.Surf[i];
-  float dxrad = (D.Rsup[i] - D.Rinf[i]) * dt;
-  // van Leer slope of StarThetaKernel at window point x (0 at the window edges)
-  auto dqat = [&](const float* W, int x) -> float {
-    if (x <= 0 || x >= L - 1) return 0.0f;
-    float dqm = (W[x] - W[x - 1]);
-    float dqp = (W[x + 1] - W[x]);
-    if (dqp * dqm > 0.0) return dqp * dqm / (dqp + dqm) * invdxtheta;
-    return 0.0f;
-  };
-  // upwind value of StarThetaKernel2 at window point x with velocity v
-  auto qst = [&](const float* W, int x, float v) -> float {
-    float ksi = v * dt;
-    if (ksi > 0.0) return (x > 0) ? W[x - 1] + (dxtheta - ksi) * dqat(W, x - 1) : 0.0f;
-    return W[x] - (dxtheta + ksi) * dqat(W, x);
-  };
-  for (int sweep = 0; sweep < 2; sweep++) {
-    const bool uni = (sweep == 1);
-    // pass A: DivisePolarGrid by the pre-sweep density, DensStar
-#pragma unroll
-    for (int k = 0; k < kMaxK; k++) {
-      int p = tid + k * kTT;
-      if (p < L) {
-        const double den = (double)sS[p] + 1e-20;
-#pragma unroll
-        for (int c = 0; c < nq; c++) sW[c * L + p] = (double)q[c][k] / den;
-        sD[p] = qst(sS, p, uni ? vconst : sV[p]);
-      }
+    __syncthreads();
+    const int a = find_range(aoff, nak, t);
+    const DiskDev& D = B.disks[adisk[a]];
+    if (!D.IsDisk) continue;
+    const int4 it = items[D.item0 + (t - aoff[a])];
+    const DiskCtl* C = D.ctl;
+    const int i0 = it.y, j0 = it.z, S = it.w;
+    const int nsec = D.nsec, nrad = D.nrad;
+    const int nb = min(kBR, nrad - i0);
+    const int L = S + 8;
+    const float dt = C->dtf;
+    const float Om = C->OmegaFrame;
+    const bool fast = D.FastTransport;
+    const float dtheta = 2.0f * (float)PI_D / (float)nsec;
+    if (p < nb) {
+      s_ns[p] = D.nshift[i0 + p];
+      s_vmed[p] = D.tvmed[i0 + p];
+      s_vc[p] = D.tvconst[i0 + p];
     }
     __syncthreads();
-    // pass B: VanLeerThetaKernel for every quantity (density last is implied:
-    // all quotients were formed from the pre-sweep density)
+    int rb = 0;
+    while (rb < nb) {
+      // sub-band rb .. re-1: window starts (unwrapped) within kTT - L of each other
+      int lo = j0 - s_ns[rb], hi = lo, re = rb + 1;
+      while (re < nb) {
+        const int x = j0 - s_ns[re];
+        const int nlo = min(lo, x), nhi = max(hi, x);
+        if (nhi - nlo > kTT - L) break;
+        lo = nlo;
+        hi = nhi;
+        re++;
+      }
+      const int WU = hi - lo + L;  // union window width, <= kTT
+      const int u0 = lo - 4;       // first (unwrapped) sector of the union window
+      if (p < WU) {
+        int g = (u0 + p) % nsec;
+        if (g < 0) g += nsec;
+        rad_march<nq>(D, i0 + rb, i0 + re, g, dt, Om, dtheta, sR + p, kTT, nq * kTT);
+      }
+      __syncthreads();
+      for (int r = rb; r < re; r++) {
+        const int i = i0 + r;
+        const int ws = j0 - s_ns[r] - 4;  // first (unwrapped) sector of this ring's window
+        const int off = ws - u0;
+        const float VMed = s_vmed[r];
+        float vconst = s_vc[r];
+        float q[nq];
+        const bool in = p < L;
+        if (in) {
+          int g = ws + p;
+          g %= nsec;
+          if (g < 0) g += nsec;
 #pragma unroll
-    for (int k = 0; k < kMaxK; k++) {
-      int p = tid + k * kTT;
-      if (p < L - 1) {
-        const float v0 = uni ? vconst : sV[p];
-        const float v1 = uni ? vconst : sV[p + 1];
-        const float d0 = sD[p], d1 = sD[p + 1];
+          for (int c = 0; c < nq; c++) q[c] = sR[((r - rb) * nq + c) * kTT + off + p];
+          float vres = __ldg(D.vtheta + (size_t)i * nsec + g) - VMed;
+          if (!fast) vres = vconst + vres;
+          sV[p] = vres;
+          sS[p] = q[nq - 1];
+        }
+        if (!fast) vconst = 0.0f;
+        const float Rm = D.Rmed[i];
+        const float dxtheta = dtheta * Rm;
+        const float invdxtheta = 1.0f / dxtheta;
+        const float invsurf = 1.0f / D.Surf[i];
+        const float dxrad = (D.Rsup[i] - D.Rinf[i]) * dt;
+        // van Leer slope of StarThetaKernel at window point x (0 at the window edges)
+        auto dqat = [&](const float* W, int x) -> float {
+          if (x <= 0 || x >= L - 1) return 0.0f;
+          float dqm = (W[x] - W[x - 1]);
+          float dqp = (W[x + 1] - W[x]);
+          if (dqp * dqm > 0.0f) return __fdividef(dqp * dqm, dqp + dqm) * invdxtheta;
+          return 0.0f;
+        };
+        // upwind value of StarThetaKernel2 at window point x with velocity v
+        auto upw = [&](const float* W, const float* G, int x, float v) -> float {
+          float ksi = v * dt;
+          if (ksi > 0.0f) return (x > 0) ? W[x - 1] + (dxtheta - ksi) * G[x - 1] : 0.0f;
+          return W[x] - (dxtheta + ksi) * G[x];
+        };
+        __syncthreads();
+        for (int sweep = 0; sweep < 2; sweep++) {
+          const float v = (sweep == 1) ? vconst : (in ? sV[p] : 0.0f);
+          // quotients by the pre-sweep density, density slope
+          if (in) {
+            const float rr = __fdividef(1.0f, sS[p] + 1e-20f);
 #pragma unroll
-        for (int c = 0; c < nq; c++) {
-          const float* W = sW + c * L;
-          float qr0 = qst(W, p, v0);
-          float qr1 = qst(W, p + 1, v1);
-          float varq = dxrad * qr0 * d0 * v0;
-          varq -= dxrad * qr1 * d1 * v1;
-          q[c][k] += varq * invsurf;
+            for (int c = 0; c < nq; c++) sW[c * kTT + p] = q[c] * rr;
+            sG[p] = dqat(sS, p);
+          }
+          __syncthreads();
+          // DensStar, slopes of the quotients
+          if (in) {
+            sD[p] = upw(sS, sG, p, v);
+#pragma unroll
+            for (int c = 0; c < nq; c++) sQ[c * kTT + p] = dqat(sW + c * kTT, p);
+          }
+          __syncthreads();
+          // fluxes through the interface at the left of point p (VanLeerThetaKernel)
+          if (in) {
+#pragma unroll
+            for (int c = 0; c < nq; c++)
+              sF[c * kTT + p] = dxrad * upw(sW + c * kTT, sQ + c * kTT, p, v) * sD[p] * v;
+          }
+          __syncthreads();
+          if (p < L - 1) {
+#pragma unroll
+            for (int c = 0; c < nq; c++) {
+              float varq = sF[c * kTT + p];
+              varq -= sF[c * kTT + p + 1];
+              q[c] += varq * invsurf;
+            }
+          }
+          // the next sweep's pre-sweep density (read after the next barrier)
+          if (sweep == 0 && in) sS[p] = q[nq - 1];
+          __syncthreads();
+        }
+        // output sector j0 + p - 4 takes window point p
+        if (p >= 4 && p < L - 4) {
+          float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.a1, D.a0};
+          const long long lo2 = (long long)i * nsec + j0 + p - 4;
+#pragma unroll
+          for (int c = 0; c < nq; c++) dsts[c == nq - 1 ? 5 : c][lo2] = q[c];
         }
       }
+      rb = re;
+      __syncthreads();
     }
-    if (sweep == 0) {
-#pragma unroll
-      for (int k = 0; k < kMaxK; k++) {
-        int p = tid + k * kTT;
-        if (p < L) sS[p] = q[nq - 1][k];
-      }
-    }
-    __syncthreads();
-  }
-  // shifted store: output sector j takes the swept value of sector j - Nshift
-  float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.a1, D.a0};
-#pragma unroll
-  for (int k = 0; k < kMaxK; k++) {
-    int p = tid + k * kTT;
-    if (p >= 4 && p < L - 4) {
-      int j;
-      if (whole) {
-        j = (p - 4 + ns) % nsec;
-        if (j < 0) j += nsec;
-      } else {
-        j = j0 + p - 4;
-      }
-      const long long lo = (long long)i * nsec + j;
-#pragma unroll
-      for (int c = 0; c < nq; c++) dsts[c == nq - 1 ? 5 : c][lo] = q[c][k];
-    }
-  }
   }
 }
 
@@ -1271,8 +1428,8 @@ __global__ void __launch_bounds__(kThreads) k_velocities(BatchDev B) {
   if (i == 0)
     vr = 0.0;
   else
-    vr = (D.vri[l - nsec] + D.vti[l]) / (Dn[l] + Dn[l - nsec] + 1e-20);
-  float vt = (D.trr[lmj] + D.tpp[l]) / (Dn[l] + Dn[lmj] + 1e-15) / D.Rmed[i] - D.Rmed[i] * C->OmegaFrame;
+    vr = (D.vri[l - nsec] + D.vti[l]) / (Dn[l] + Dn[l - nsec] + 1e-20f);
+  float vt = (D.trr[lmj] + D.tpp[l]) / (Dn[l] + Dn[lmj] + 1e-15f) / D.Rmed[i] - D.Rmed[i] * C->OmegaFrame;
   D.vrad[l] = vr;
   D.vtheta[l] = vt;
   D.dens[l] = Dn[l];
@@ -1284,15 +1441,21 @@ __global__ void __launch_bounds__(kThreads) k_velocities(BatchDev B) {
 __device__ void compact_active(const BatchDev& B) {
   int na = 0, ni = 0, nd = 0;
   long long cc = 0;
-  int rr = 0, ii = 0, ia = 0;
+  int rr = 0, ii = 0, ia = 0, gg = 0, tt = 0, ct = 0;
   for (int d = 0; d < B.ndisk; d++) {
     const DiskDev& D = B.disks[d];
     if (!D.ctl->active) continue;
     B.act_disk[na] = d;
     B.act_cell_off[na] = cc;
     B.act_ring_off[na] = rr;
+    B.act_grp_off[na] = gg;
+    B.act_tile_off[na] = tt;
+    B.act_ctile_off[na] = ct;
+    ct += D.nrad;
     cc += (long long)D.nrad * D.nsec;
+    tt += (D.nrad * D.nsec + kThreads - 1) / kThreads;
     rr += D.nrad;
+    gg += (D.nrad + 31) / 32;
     na++;
     if (D.Adiabatic) {
       B.act_adi_disk[nd] = d;
@@ -1308,6 +1471,9 @@ __device__ void compact_active(const BatchDev& B) {
   }
   B.act_cell_off[na] = cc;
   B.act_ring_off[na] = rr;
+  B.act_grp_off[na] = gg;
+  B.act_tile_off[na] = tt;
+  B.act_ctile_off[na] = ct;
   B.act_iso_off[ni] = ii;
   B.act_adi_off[nd] = ia;
   B.act[0] = na;
@@ -1569,19 +1735,16 @@ void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s
 int fargo_kernels_per_substep(int adiabatic) { return FARGO_NKERNELS; }
 
 const char* fargo_substep_kernel_name(int k) {
-  static const char* names[] = {"k_cfl_force", "k_source1",   "k_visc_tau",   "k_visc_update", "k_source2",
-                                "k_energy",    "k_transport", "k_velocities", "k_substep_end"};
+  static const char* names[] = {"k_ring_mean_cfl", "k_cfl_force",   "k_source1",    "k_visc_tau",
+                                "k_visc_update",   "k_source2",     "k_energy",     "k_ring_mean_tr",
+                                "k_transport",     "k_velocities",  "k_substep_end"};
   return (k >= 0 && k < FARGO_NKERNELS) ? names[k] : "";
-}
-
-size_t fargo_transport_smem_bytes(int seg, int adiabatic) {
-  return sizeof(float) * (size_t)(3 + (adiabatic ? 6 : 5)) * (size_t)(seg + 8);
 }
 
 void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int use_handle, cudaStream_t s,
                           int max_nsec, long long* launches, cudaEvent_t* ev) {
   const unsigned cb = (unsigned)b.cell_grid;
-  size_t ring_smem = sizeof(float) * (size_t)max_nsec;
+  (void)max_nsec;
   int k = 0;
 #define REC()                                  \
   do {                                         \
@@ -1589,7 +1752,9 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
     k++;                                       \
   } while (0)
   REC();
-  k_cfl_force<<<b.ring_grid, kThreads, ring_smem, s>>>(b);
+  k_ring_mean<0><<<b.grp_grid, kRMT, fargo_ring_mean_smem_bytes(), s>>>(b);
+  REC();
+  k_cfl_force<<<b.ring_grid, kThreads, 0, s>>>(b);
   REC();
   k_source1<<<cb, kThreads, 0, s>>>(b);
   REC();
@@ -1601,12 +1766,12 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   REC();
   k_energy<<<cb, kThreads, 0, s>>>(b);
   REC();
+  k_ring_mean<1><<<b.grp_grid, kRMT, fargo_ring_mean_smem_bytes(), s>>>(b);
+  REC();
   if (b.ntheta_iso)
-    k_transport<5><<<std::min(b.item_grid, b.ntheta_iso), kTT, fargo_transport_smem_bytes(b.theta_seg, 0), s>>>(
-        b, b.theta_iso);
+    k_transport<5><<<std::min(b.item_grid, b.ntheta_iso), kTT, fargo_transport_smem_bytes(0), s>>>(b, b.theta_iso);
   if (b.ntheta_adi)
-    k_transport<6><<<std::min(b.item_grid, b.ntheta_adi), kTT, fargo_transport_smem_bytes(b.theta_seg, 1), s>>>(
-        b, b.theta_adi);
+    k_transport<6><<<std::min(b.item_grid, b.ntheta_adi), kTT, fargo_transport_smem_bytes(1), s>>>(b, b.theta_adi);
   REC();
   k_velocities<<<cb, kThreads, 0, s>>>(b);
   REC();
@@ -1634,13 +1799,17 @@ void fargo_launch_diagnostics(const BatchDev& b, int disk, double* out3, int nbl
   k_diagnostics<<<nblocks, kThreads, 0, s>>>(b, disk, out3);
 }
 
-cudaError_t fargo_kernel_attributes(int max_nsec, int seg) {
-  cudaError_t e = cudaFuncSetAttribute(k_cfl_force, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(sizeof(float) * max_nsec));
+cudaError_t fargo_kernel_attributes(int max_nsec) {
+  (void)max_nsec;
+  cudaError_t e = cudaFuncSetAttribute(k_ring_mean<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)fargo_ring_mean_smem_bytes());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_ring_mean<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)fargo_ring_mean_smem_bytes());
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_transport<5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)fargo_transport_smem_bytes(seg, 0));
+                           (int)fargo_transport_smem_bytes(0));
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_transport<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)fargo_transport_smem_bytes(seg, 1));
+                              (int)fargo_transport_smem_bytes(1));
 }

@@ -201,6 +201,9 @@ class Batch:
     def advance_async(self, ndt):
         self._chk(lib.fargo_batch_advance_async(self.b, ndt), "fargo_batch_advance_async")
 
+    def set_graph_mode(self, on):
+        self._chk(lib.fargo_batch_set_graph_mode(self.b, 1 if on else 0), "fargo_batch_set_graph_mode")
+
     def sync(self):
         self._chk(lib.fargo_batch_sync(self.b), "fargo_batch_sync")
 

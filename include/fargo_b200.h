@@ -244,6 +244,7 @@ const char* fargo_profile_kernel_name(int k);
 /* 1 (default): one CUDA graph launch per DT with a device-driven WHILE node
    over the substeps; 0: host loop with one wait per substep. */
 fargo_status fargo_set_graph_mode(fargo_ctx* ctx, int use_graph);
+fargo_status fargo_batch_set_graph_mode(fargo_batch* b, int use_graph);
 
 #ifdef __cplusplus
 }

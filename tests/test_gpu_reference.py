@@ -5,7 +5,7 @@ unmodified sources and run on a B200 with seeded noisy initial conditions
 (tests/golden/make_ref_golden.py).  This library, initialised from the same
 parameters and the same noise, must reproduce the reference's initial
 fields, its substep counts, dt and FARGO shift counts exactly, its planet
-orbits, and its fields after 10 DTs within the stated tolerances."""
+orbits, and its fields after 10 DTs within FIELD_TOL, the rounding-order floor between two FP32 builds."""
 import glob
 import os
 
@@ -14,7 +14,7 @@ import pytest
 
 from cudaprotoplanetarydisksfloat_b200 import Disk, noise, planets_dict
 from tests.golden import make_ref_golden as G
-from tests.helpers import make, rel_l2
+from tests.helpers import FIELD_TOL, make, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -24,7 +24,7 @@ FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_*.npz")))
 # rel-L2 after 10 DTs.  Same compiler, same FP32 expressions and contraction
 # as the reference; the only arithmetic differences are the FP64 (here) vs
 # FP32 (reference) force sums and the summation order of those sums.
-TOL = {"dens": 1e-5, "vtheta": 1e-5, "energy": 1e-5, "temperature": 1e-5, "vrad": 1e-4}
+TOL = FIELD_TOL
 
 
 @pytest.mark.skipif(not FIXTURES, reason="no reference fixtures")
