@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "libfargo_b200.so")
 
 FARGO_MAXPLANETS = 100
 FARGO_DIMFXY = 11
+FARGO_NOALLOC_MAXRAD = 4096
 FARGO_STRLEN = 512
 
 STATUS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ECUFFT", 4: "ENONFINITE", 5: "ETIMEOUT", 6: "EOOM",
@@ -78,7 +79,7 @@ EXPORTS = [
     "fargo_params_default", "fargo_params_read", "fargo_params_derive", "fargo_planets_read",
     "fargo_grid_radii", "fargo_create", "fargo_destroy", "fargo_last_error", "fargo_init_state",
     "fargo_upload", "fargo_download", "fargo_get_planets", "fargo_set_planets", "fargo_advance_dt",
-    "fargo_advance", "fargo_advance_async", "fargo_sync", "fargo_disk_force", "fargo_get_scalars",
+    "fargo_advance", "fargo_advance_async", "fargo_sync", "fargo_disk_force", "fargo_disk_force_noalloc", "fargo_get_scalars",
     "fargo_get_substep_log", "fargo_batch_create", "fargo_batch_destroy", "fargo_batch_last_error",
     "fargo_batch_init_state", "fargo_batch_upload", "fargo_batch_download", "fargo_batch_advance",
     "fargo_batch_advance_async", "fargo_batch_sync", "fargo_batch_get_scalars",
@@ -122,6 +123,8 @@ def _load():
         "fargo_advance_async": (C.c_int, [vp, C.c_int]),
         "fargo_sync": (C.c_int, [vp]),
         "fargo_disk_force": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, dp]),
+        "fargo_disk_force_noalloc": (C.c_int, [vp, vp, vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_double,
+                                               C.c_double, C.c_double, C.c_int, dp, vp, C.c_char_p, C.c_int]),
         "fargo_get_scalars": (C.c_int, [vp, P(FargoScalars)]),
         "fargo_get_substep_log": (C.c_int, [vp, C.c_int, P(C.c_int), dp, P(C.c_int)]),
         "fargo_batch_create": (C.c_int, [C.c_int, P(FargoParams), P(FargoPlanets), C.c_int, P(vp)]),

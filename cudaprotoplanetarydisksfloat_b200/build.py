@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
            "-diag-suppress", "177", "-I" + os.path.join(ROOT, "include")]
 
-LIB_SOURCES = ["kernels_step.cu", "fargo_api.cu", "sg.cu", "host_params.cpp", "host_setup.cpp"]
+LIB_SOURCES = ["kernels_step.cu", "fargo_api.cu", "sg.cu", "noalloc.cu", "host_params.cpp", "host_setup.cpp"]
 
 
 def _nvcc():

@@ -29,6 +29,7 @@ extern "C" {
 #define FARGO_ABI_VERSION 1
 #define FARGO_MAXPLANETS 100   /* RungeKutta.cu:4 static arrays of 100 */
 #define FARGO_DIMFXY 11        /* Main.cu:71 dimfxy: Hill-cut levels of ComputeForce */
+#define FARGO_NOALLOC_MAXRAD 4096 /* largest NRAD of fargo_disk_force_noalloc */
 #define FARGO_STRLEN 512
 
 typedef enum fargo_status {
@@ -183,6 +184,27 @@ fargo_status fargo_sync(fargo_ctx* ctx);
    3 fy_outer; FP64 sums of the FP32 per-cell forces. */
 fargo_status fargo_disk_force(fargo_ctx* ctx, double x, double y, double rsmoothing,
                               double mass, int dimfxy, double* globalforce);
+
+/* No counterpart in the reference: fargo_disk_force for callers that keep
+   their disk in their own device arrays and must not allocate device memory
+   (they manage it themselves, or cannot afford cudaMalloc's device-wide
+   synchronisation mid-step).  Allocates nothing: its only scratch is a fixed
+   static device array of (FARGO_NOALLOC_MAXRAD + 1) * 44 doubles (1.4 MB,
+   held by every GPU that loads the library until exit); NRAD above
+   FARGO_NOALLOC_MAXRAD is rejected with FARGO_EINVAL.  Inputs are device
+   pointers in the reference's layout: dens, cell_x, cell_y [NRAD*NSEC]
+   (Dens, CellAbscissa, CellOrdinate), surf, rmed [NRAD]; globalforce is
+   host memory, filled as by fargo_disk_force.  Runs on `stream` (a
+   cudaStream_t, NULL for the default stream) on the current device and
+   waits for it.  The first call on a device looks up the scratch address
+   there: make it before any stream capture.  Calls share the scratch, so
+   calls that overlap on the GPU race.  err/errlen (may be NULL/0) receive a
+   message on failure. */
+fargo_status fargo_disk_force_noalloc(const float* dens, const float* cell_x, const float* cell_y,
+                                      const float* surf, const float* rmed, int nrad, int nsec,
+                                      double x, double y, double rsmoothing, double mass,
+                                      int dimfxy, double* globalforce, void* stream, char* err,
+                                      int errlen);
 
 /* Scalars after the last DT (also recomputes mdcp1, mass, angular momentum). */
 fargo_status fargo_get_scalars(fargo_ctx* ctx, fargo_scalars* out);
