@@ -108,8 +108,10 @@ fargo_status dupload(fargo_batch* b, DiskHost& h, const T** ptr, const std::vect
 fargo_status check_params(fargo_batch* b, const fargo_params* p, const fargo_planets* pl) {
   if (p->NRAD < 4 || p->NSEC < 4) return set_err(b, FARGO_EINVAL, "NRAD and NSEC must be >= 4");
   if (p->NSEC > 16384) return set_err(b, FARGO_EINVAL, "NSEC > 16384 is not supported");
-  if (p->OpenInner || p->NonReflecting || p->Evanescent)
-    return set_err(b, FARGO_EINVAL, "InnerBoundary %s: only RIGID/WALL boundaries are implemented", p->INNERBOUNDARY);
+  if (p->NonReflecting && p->NSEC <= 128)
+    return set_err(b, FARGO_EINVAL,
+                   "InnerBoundary NONREFLECTING needs NSEC > 128 (the reference's DeviceReduce launches no block "
+                   "for 128 or fewer values)");
   if (p->SelfGravity && !p->LogGrid)
     return set_err(b, FARGO_EINVAL, "self-gravity needs RadialSpacing LOGARITHM (Main.cu:302-306)");
   if (p->SelfGravity && p->SGZeroMode) return set_err(b, FARGO_EINVAL, "SelfGravity Z is not implemented");
@@ -164,6 +166,15 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   D.SelfGravity = p->SelfGravity;
   D.Evanescent = p->Evanescent;
   D.OpenInner = p->OpenInner;
+  D.NonReflecting = p->NonReflecting;
+  if (p->NRAD >= 3) {
+    D.nr_pow_in = std::pow((double)h.t.Rinf[1], -1.5);
+    D.nr_pow_out = std::pow((double)h.t.Rinf[p->NRAD - 2], -1.5);
+  }
+  D.ev_Tin = (float)(2.0 * FARGO_PI * std::pow((double)h.t.Rmed[0], 3. / 2));
+  D.ev_Tout = (float)(2.0 * FARGO_PI * std::pow((double)h.t.Rmed[p->NRAD - 1], 3. / 2));
+  D.ev_DRMIN = (float)(h.t.Rmed[0] * 1.25);
+  D.ev_DRMAX = (float)(h.t.Rmed[p->NRAD - 1] * 0.84);
   D.SloppyCFL = p->SloppyCFL;
   D.IsDisk = p->IsDisk;
   D.invdphi = h.t.invdphi;
@@ -188,6 +199,11 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   A(D.tvmed, n1) A(D.tvconst, n1)
   A(D.log_nshift, (size_t)FARGO_MAXLOG * p->NRAD) A(D.partials, nct * 4 * FARGO_MAXBODY)
   A(D.log_dt, (size_t)FARGO_MAXLOG) A(D.rk_work, (size_t)FARGO_RK_WORK(FARGO_MAXPLANETS_DEV))
+  if (p->OpenInner) {
+    A(D.lost, (size_t)p->NSEC)
+  } else {
+    D.lost = nullptr;
+  }
   float *cp, *sp, *cc, *sc;
   A(cp, (size_t)p->NSEC) A(sp, (size_t)p->NSEC) A(cc, (size_t)p->NSEC) A(sc, (size_t)p->NSEC)
 #undef A
@@ -395,7 +411,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   std::vector<long long> cell_off(n + 1, 0);
   std::vector<int> ring_off(n + 1, 0);
   std::vector<int4> theta_iso, theta_adi;
-  int seg_max = 0;
+  int seg_max = 0, any_bc = 0;
   for (int d = 0; d < n; d++) {
     fargo_status st = check_params(b, &params[d], &planets[d]);
     if (st) return st;
@@ -413,6 +429,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     b->max_nsec = std::max(b->max_nsec, nsec);
     b->any_adiabatic |= h.p.Adiabatic;
     b->n_sg += h.p.SelfGravity ? 1 : 0;
+    any_bc |= (h.p.OpenInner || h.p.NonReflecting || h.p.Evanescent) ? 1 : 0;
     std::vector<int4>& theta = h.p.Adiabatic ? theta_adi : theta_iso;
     h.dev.item0 = (int)theta.size();
     // bands of FARGO_BAND rings, each in nseg near-equal azimuthal segments
@@ -455,6 +472,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     CK(cudaMemcpyAsync(b->d_disks + d, &b->disks[d].dev, sizeof(DiskDev), cudaMemcpyHostToDevice, b->stream));
   BatchDev& bd = b->bd;
   bd.ndisk = n;
+  bd.any_bc = any_bc;
   bd.ncell = cell_off[n];
   bd.nring = ring_off[n];
   bd.cell_off = b->d_cell_off;
@@ -542,14 +560,12 @@ fargo_status advance_dt_async(fargo_batch* b) {
 fargo_status finish_dts(fargo_batch* b) {
   CK(cudaStreamSynchronize(b->stream));
   CK(cudaGetLastError());
-  int per = fargo_kernels_per_substep(b->any_adiabatic);
   for (int d = 0; d < (int)b->disks.size(); d++) {
     cudaError_t e;
     DiskCtl c = ctl_header(b, d, &e);
     if (e != cudaSuccess) return set_err(b, FARGO_ECUDA, "ctl read: %s", cudaGetErrorString(e));
     if (c.error == 1) return set_err(b, FARGO_ENONFINITE, "disk %d: non-finite or non-positive CFL time step", d);
     if (c.error == 2) return set_err(b, FARGO_ETIMEOUT, "disk %d: more than 1e5 substeps in one DT", d);
-    (void)per;
   }
   return FARGO_OK;
 }
@@ -970,7 +986,7 @@ long long fargo_batch_count_launches(fargo_batch* b) {
     DiskCtl c = ctl_header(b, d, &e);
     subs = std::max<long long>(subs, c.nsub_total);
   }
-  return b->launches + subs * fargo_kernels_per_substep(b->any_adiabatic);
+  return b->launches + subs * fargo_substep_launches(b->bd);
 }
 
 fargo_status fargo_set_graph_mode(fargo_ctx* ctx, int use_graph) {

@@ -83,7 +83,12 @@ struct DiskDev {
   float IMPOSEDDISKDRIFT;
   int Adiabatic, Cooling, ViscosityAlpha, FastTransport, Indirect_Term, ExcludeHill;
   int ForcedCircular, Corotating, GuidingCenter, RocheSmoothing, SelfGravity, Evanescent;
-  int OpenInner, SloppyCFL, IsDisk;
+  int OpenInner, NonReflecting, SloppyCFL, IsDisk;
+  // boundary constants computed on the host as the reference does:
+  // pow(Rinf[1], -1.5), pow(Rinf[NRAD-2], -1.5) of NonReflectingBoundary;
+  // damping zones and orbital periods of EvanescentBoundary (SideEuler.cu:127-132)
+  double nr_pow_in, nr_pow_out;
+  float ev_DRMIN, ev_DRMAX, ev_Tin, ev_Tout;
   float invdphi, onethird;
   float HillRadius;
   // constant sub-Keplerian boundary speeds (host double -> float) when they
@@ -112,6 +117,7 @@ struct DiskDev {
   float* tvmed;          // transport: ring-mean v_theta of the current substep
   float* tvconst;        // transport: constant residual per ring
   int* log_nshift;       // [FARGO_MAXLOG][nrad]
+  float* lost;           // [nsec] mass through the inner edge this substep (OPEN inner boundary)
   double* partials;      // [nrad][4*FARGO_MAXBODY] force partial sums per ring
   double* log_dt;        // [FARGO_MAXLOG] substep dt of the current DT
   double* rk_work;       // [FARGO_RK_WORK(FARGO_MAXPLANETS_DEV)] RK5 scratch of large systems
@@ -150,10 +156,11 @@ struct BatchDev {
   int* act_tile_off;         // [ndisk+1] prefix of cell tiles (one block's cells) of active disks
   int* act_ctile_off;        // [ndisk+1] prefix of rings of active disks (CFL tiles)
   int cell_grid, ring_grid, item_grid, grp_grid;  // fixed grid sizes of the grid-stride kernels
+  int any_bc;                // some disk has an OPEN, NONREFLECTING or EVANESCENT boundary
 };
 
 // kernel entry points (kernels_step.cu), launched by fargo_api.cu
-#define FARGO_NKERNELS 11  // kernels per substep
+#define FARGO_NKERNELS 14  // profiled slots per substep (boundary slots empty for rigid boundaries)
 #define FARGO_SEG_OUT 192  // largest azimuthal transport segment (output sectors per CTA)
 #define FARGO_BAND 8       // rings per transport CTA
 cudaError_t fargo_kernel_attributes(int max_nsec);
@@ -170,4 +177,4 @@ void fargo_launch_init_velocities(const BatchDev& b, int disk, long long ncell_g
 void fargo_launch_disk_force(const BatchDev& b, int disk, float x, float y, float rs, float rh, float a,
                              double* out44, int nblocks, cudaStream_t s);
 void fargo_launch_diagnostics(const BatchDev& b, int disk, double* out3, int nblocks, cudaStream_t s);
-int fargo_kernels_per_substep(int adiabatic);
+int fargo_substep_launches(const BatchDev& b);

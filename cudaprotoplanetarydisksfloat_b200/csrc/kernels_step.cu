@@ -414,6 +414,56 @@ __device__ __forceinline__ void for_active_cells(const BatchDev& B, Body body) {
 
 // -------------------------------------------------------------- reductions
 
+// DeviceReduce<float> (Kernels.cu:431-557) of f(0) .. f(n-1) in the
+// reference's order of operations, for the whole block (kThreads threads):
+// getNumBlocksAndThreads (Kernels.cu:404-429) picks the reference's block
+// count and size, each of its blocks is reduced in turn as deviceReduceKernel
+// does (Kernels.cu:269-383: the bounds-checked form, since IsPow2 is false
+// for every n > 1; shared-memory tree down to 64, the last warp by shuffles),
+// and the block sums are added in order as its host loop does.  Result in
+// every thread.  n > 128 (the reference launches no block below that).
+template <class F>
+__device__ float ref_device_reduce(F f, int n, float* sm) {
+  long np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  const long maxBlocks = np2 / 256;
+  long h = (n + 1) / 2, T2 = 1;
+  while (T2 < h) T2 <<= 1;
+  const int T = (n < 512) ? (int)T2 : 256;
+  long blocks = (n + (2L * T - 1)) / (2L * T);
+  if (blocks > maxBlocks) blocks = maxBlocks;
+  const int t = threadIdx.x;
+  float total = 0.0f;
+  for (long b = 0; b < blocks; b++) {
+    float my = 0.0f;
+    __syncthreads();
+    if (t < T) {
+      const long gridSize = 2L * T * blocks;
+      for (long i = b * 2L * T + t; i < n; i += gridSize) {
+        my += f(i);
+        if (i + T < n) my += f(i + T);
+      }
+      sm[t] = my;
+    }
+    __syncthreads();
+    for (int stride = 256; stride >= 64; stride >>= 1) {
+      if (T >= 2 * stride && t < stride) sm[t] = my = my + sm[t + stride];
+      __syncthreads();
+    }
+    if (t < 32) {
+      if (T >= 64) my = my + sm[t + 32];
+      for (int off = 16; off > 0; off >>= 1) my += __shfl_down_sync(0xffffffffu, my, off);
+      if (t == 0) total += my;
+    }
+  }
+  __syncthreads();
+  if (t == 0) sm[0] = total;
+  __syncthreads();
+  const float r = sm[0];
+  __syncthreads();
+  return r;
+}
+
 __device__ __forceinline__ double warp_sum_d(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   return v;
@@ -787,7 +837,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_source1(BatchDev B) {
   CELL_BEGIN
   const float dt = C->dtf;
   const float OmegaFrame = C->OmegaFrame;
-  const float dom = C->domega;
+  // CorrectVtheta (SideEuler.cu:184-188) on the fly; evanescent disks had it
+  // applied in place by the boundary pass that precedes this kernel
+  const float dom = D.Evanescent ? 0.0f : C->domega;
   const float* Vt = D.vtheta;
   const float* Dn = D.dens;
   auto vth = [&](long long q, int r) -> float { return dom != 0.0f ? Vt[q] - dom * D.Rmed[r] : Vt[q]; };
@@ -952,7 +1004,8 @@ __global__ void __launch_bounds__(kThreads) k_source2(BatchDev B) {
   float invdxtheta = 1.0f / dxtheta;
   float vt_new = VTI[l] - dt * 2.0f / (Dn[l] + Dn[lmj]) * (qt - qtm) * invdxtheta;
   if (D.Adiabatic) {
-    D.energy[l] = D.energy[l] - dt * qr * (VRI[l + nsec] - VRI[l]) * D.invdiffRsup[i] -
+    // EnergyInt goes to scratch: the boundary pass before Substep3 still sees the state energy
+    D.a1[l] = D.energy[l] - dt * qr * (VRI[l + nsec] - VRI[l]) * D.invdiffRsup[i] -
                   dt * qt * (VTI[lpj] - VTI[l]) * invdxtheta;
   }
   D.vrad[l] = vr_new;
@@ -996,7 +1049,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
     else
       q = 0.0;
   }
-  const float e_int = D.energy[l];
+  const float e_int = D.a1[l];  // EnergyInt from k_source2
   const float Dl = D.dens[l];
   float num, den;
   if (!D.Cooling) {
@@ -1116,9 +1169,11 @@ __device__ __forceinline__ void rad_face(const DiskDev& D, int b, float vr, floa
 // Radial half of Transport (VanLeerRadialKernel, Kernels.cu:1137-1154) for
 // rings ia .. ib-1 at column g, marching outwards: each ring loads one new
 // row, one new slope and one new interface.  out[k][c] at stride ostride.
+// lost0 (may be null): receives the density's varq at ring 0, the mass that
+// leaves through the inner edge (LostByDisk, Kernels.cu:941-944).
 template <int nq>
 __device__ __forceinline__ void rad_march(const DiskDev& D, int ia, int ib, int g, float dt, float Om,
-                                          float dtheta, float* out, int ostride_c, int ostride_r) {
+                                          float dtheta, float* out, int ostride_c, int ostride_r, float* lost0) {
   const int nsec = D.nsec;
   const int gp = g + 1 == nsec ? 0 : g + 1;
   RadRow<nq> R0 = rad_row<nq>(D, ia - 1, g, gp, Om);  // row i-1 for the first slope
@@ -1146,6 +1201,7 @@ __device__ __forceinline__ void rad_march(const DiskDev& D, int ia, int ib, int 
       float varq = dt * dtheta * Ri * qs[c] * ds * vr0;
       varq -= dt * dtheta * Rs * qs1[c] * ds1 * vr1;
       o[c * ostride_c] = R1.Q[c] + varq * iS;
+      if (c == nq - 1 && i == 0 && lost0) *lost0 = varq;
     }
     R1 = R2;
     R2 = R3;
@@ -1251,7 +1307,7 @@ static_assert(FARGO_SEG_OUT + 8 <= kTT, "transport window must fit the CTA");
 
 size_t fargo_transport_smem_bytes(int adiabatic) {
   const int nq = adiabatic ? 6 : 5;
-  return sizeof(float) * (size_t)kTT * (size_t)(kBR * nq + 4 + 3 * nq);
+  return sizeof(float) * (size_t)kTT * (size_t)(kBR * nq + 5 + 3 * nq);
 }
 
 // Transport (TransportEuler.cu:24-35) of a band of up to kBR rings i0 ..
@@ -1279,6 +1335,7 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
   float* sW = sD + kTT;              // [nq][kTT] DivisePolarGrid quotients
   float* sQ = sW + nq * kTT;         // [nq][kTT] their slopes
   float* sF = sQ + nq * kTT;         // [nq][kTT] their fluxes
+  float* sL = sF + nq * kTT;         // [kTT] mass through the inner edge (OPEN)
   __shared__ int s_ns[kBR];
   __shared__ float s_vmed[kBR], s_vc[kBR];
   const int nak = (nq == 5) ? B.act[1] : B.act[2];
@@ -1324,7 +1381,8 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
       if (p < WU) {
         int g = (u0 + p) % nsec;
         if (g < 0) g += nsec;
-        rad_march<nq>(D, i0 + rb, i0 + re, g, dt, Om, dtheta, sR + p, kTT, nq * kTT);
+        rad_march<nq>(D, i0 + rb, i0 + re, g, dt, Om, dtheta, sR + p, kTT, nq * kTT,
+                      (D.OpenInner && i0 + rb == 0) ? sL + p : nullptr);
       }
       __syncthreads();
       for (int r = rb; r < re; r++) {
@@ -1405,6 +1463,13 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
         }
         // output sector j0 + p - 4 takes window point p
         if (p >= 4 && p < L - 4) {
+          if (i == 0 && D.OpenInner) {
+            // each source sector is the core of exactly one segment's window
+            int g = ws + p;
+            g %= nsec;
+            if (g < 0) g += nsec;
+            D.lost[g] = sL[off + p];
+          }
           float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.a1, D.a0};
           const long long lo2 = (long long)i * nsec + j0 + p - 4;
 #pragma unroll
@@ -1483,6 +1548,15 @@ __device__ void compact_active(const BatchDev& B) {
 
 // End of a substep: which disks take another one; drives the graph's loop.
 __global__ void k_substep_end(BatchDev B, cudaGraphConditionalHandle h, int use_handle) {
+  __shared__ float sm[kThreads];
+  // LostMass += VanLeerRadial's DeviceReduce of LostByDisk (TransportEuler.cu:72, 145)
+  for (int d = 0; d < B.ndisk; d++) {
+    const DiskDev& D = B.disks[d];
+    if (!D.OpenInner || !D.IsDisk || !D.ctl->active) continue;
+    const float lost = ref_device_reduce([&](long j) { return D.lost[j]; }, D.nsec, sm);
+    if (threadIdx.x == 0) D.ctl->LostMass += lost;
+  }
+  __syncthreads();
   int any = 0;
   for (int d = threadIdx.x; d < B.ndisk; d += blockDim.x) {
     DiskCtl* C = B.disks[d].ctl;
@@ -1560,6 +1634,182 @@ __global__ void k_cs_ringmean(BatchDev B, int only_disk) {
     for (int j = 0; j < nsec; j++) sum += v;
   }
   D.csmean[i] = sum / (float)nsec;
+}
+
+// ------------------------------------------------------- boundary conditions
+
+// ApplyBoundaryCondition (SideEuler.cu:172-182), ring-local part, one block
+// per ring of the disks inside their DT (contiguous runs, DiskDev in shared
+// memory):
+//  - NONREFLECTING, adiabatic: ComputeSoundSpeed first (SideEuler.cu:176-177),
+//    then, for alpha viscosity, the ring-mean sound speed and the viscosity
+//    that the next ComputeViscousTerms rebuilds from it (Viscosity.cu:79-86);
+//  - EVANESCENT: EvanescentBoundaryKernel (Kernels.cu:1076-1124) in the
+//    damping zones; at the first call of a substep it is preceded by
+//    CorrectVtheta, applied here in place (k_source1 then skips it).
+// stage 0, 1, 2: the calls before Substep1, before Substep3, after Transport
+// (SourceEuler.cu:267, 285, 292).
+template <int stage>
+__global__ void __launch_bounds__(kThreads) k_bc_rings(BatchDev B) {
+  __shared__ DiskDev sD;
+  const int tid = threadIdx.x;
+  const int na = B.act[0];
+  const int ntile = na > 0 ? B.act_ctile_off[na] : 0;
+  const int per = (ntile + gridDim.x - 1) / gridDim.x;
+  const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
+  int lo = 0, hi = -1;
+  for (int t = t0; t < t1; t++) {
+    if (t >= hi) {  // block-uniform: entering a disk
+      const int a = find_range(B.act_ctile_off, na, t);
+      lo = B.act_ctile_off[a];
+      hi = B.act_ctile_off[a + 1];
+      __syncthreads();
+      copy_words(&sD, B.disks + B.act_disk[a], sizeof(DiskDev));
+      __syncthreads();
+    }
+    const DiskDev& D = sD;
+    const DiskCtl* C = D.ctl;
+    if (!D.IsDisk) continue;
+    const int i = t - lo, nsec = D.nsec;
+    const size_t r0 = (size_t)i * nsec;
+    if (D.NonReflecting && D.Adiabatic) {
+      for (int j = tid; j < nsec; j += kThreads)
+        D.cs[r0 + j] = sqrtf(D.ADIABATICINDEX * (D.ADIABATICINDEX - 1.0) * D.energy[r0 + j] / D.dens[r0 + j]);
+      if (D.ViscosityAlpha) {
+        __syncthreads();
+        if (tid == 0) {
+          float sum = 0.0f;  // Make1DprofileKernel: sectors in order
+          for (int j = 0; j < nsec; j++) sum += D.cs[r0 + j];
+          D.csmean[i] = sum / (float)nsec;
+          D.visc[i] = fviscosity_ring(D, i, C->time_start, C->PhysicalTimeInitial);
+        }
+      }
+    }
+    if (D.Evanescent) {
+      const float Rm = D.Rmed[i];
+      if (stage == 0 && C->domega != 0.0f)
+        for (int j = tid; j < nsec; j += kThreads) D.vtheta[r0 + j] = D.vtheta[r0 + j] - C->domega * Rm;
+      const float DRMIN = D.ev_DRMIN, DRMAX = D.ev_DRMAX;
+      if ((Rm < DRMIN) || (Rm > DRMAX)) {
+        float damping, lambda = 0.0f;
+        if (Rm < DRMIN) {
+          damping = (Rm - DRMIN) / (D.Rmed[0] - DRMIN);
+          lambda = damping * damping * 10.0 * C->dtf / D.ev_Tin;
+        }
+        if (Rm > DRMAX) {
+          damping = (Rm - DRMAX) / (D.Rmed[D.nrad - 1] - DRMAX);
+          lambda = damping * damping * 10.0 * C->dtf / D.ev_Tout;
+        }
+        // the self-gravity form subtracts Rmed * GLOBAL_bufarray_d[i], an
+        // array the reference never fills (zero)
+        const float AspectRatio = aspect_ratio_dev(D, Rm, C->time_start, C->PhysicalTimeInitial);
+        float vtheta0 = sqrtf(1.0 * 1.0 / Rm *
+                              (1.0 - (1.0 + D.SIGMASLOPE - 2.0 * D.FLARINGINDEX) * powf(AspectRatio, 2.0f) *
+                                         powf(Rm, (float)(2.0 * D.FLARINGINDEX))));
+        vtheta0 -= Rm * C->OmegaFrame;
+        const float vrad0 = -3.0 * D.visc[i] / Rm * (-D.SIGMASLOPE + .5);
+        const float dens0 = D.SigmaMed[i];
+        const float energy0 = D.EnergyMed[i];
+        for (int j = tid; j < nsec; j += kThreads) {
+          const size_t l = r0 + j;
+          D.vrad[l] = (D.vrad[l] + lambda * vrad0) / (1.0 + lambda);
+          D.vtheta[l] = (D.vtheta[l] + lambda * vtheta0) / (1.0 + lambda);
+          D.dens[l] = (D.dens[l] + lambda * dens0) / (1.0 + lambda);
+          if (D.Adiabatic) D.energy[l] = (D.energy[l] + lambda * energy0) / (1.0 + lambda);
+        }
+      }
+    }
+  }
+}
+
+// ApplyBoundaryCondition, edge-ring part, one block per disk inside its DT:
+// OpenBoundaryKernel (Kernels.cu:623-637) and NonReflectingBoundary
+// (SideEuler.cu:70-101: ReduceCs, the angular offsets i_angle / i_angle2,
+// NonReflectingBoundaryKernel, ReduceMean, MinusMeanKernel,
+// Kernels.cu:640-722), with the ring means reduced in DeviceReduce's order.
+__global__ void __launch_bounds__(kThreads) k_bc_disk(BatchDev B) {
+  __shared__ float sm[kThreads];
+  __shared__ int s_angle[2];
+  const int tid = threadIdx.x;
+  const int na = B.act[0];
+  for (int a = blockIdx.x; a < na; a += gridDim.x) {
+    const DiskDev& D = B.disks[B.act_disk[a]];
+    if (!D.IsDisk || !(D.OpenInner || D.NonReflecting)) continue;
+    const int nsec = D.nsec, nrad = D.nrad;
+    float* Dn = D.dens;
+    float* En = D.energy;
+    float* Vr = D.vrad;
+    if (D.OpenInner) {
+      const float SigmaMed = D.SigmaMed[0];
+      for (int j = tid; j < nsec; j += kThreads) {
+        const int i = 1;
+        Dn[(i - 1) * nsec + j] = Dn[i * nsec + j];
+        En[(i - 1) * nsec + j] = En[i * nsec + j];
+        if (Vr[(i + 1) * nsec + j] > 0.0 || (Dn[i * nsec + j] < SigmaMed))
+          Vr[i * nsec + j] = 0.0;
+        else
+          Vr[i * nsec + j] = Vr[(i + 1) * nsec + j];
+      }
+    }
+    if (D.NonReflecting) {
+      auto csr = [&](int r) {
+        return [&, r](long j) -> float {
+          return D.Adiabatic ? D.cs[(size_t)r * nsec + j] : D.cs_ring[r];
+        };
+      };
+      const float cs0_r = ref_device_reduce(csr(0), nsec, sm) / (float)nsec;
+      const float cs1_r = ref_device_reduce(csr(1), nsec, sm) / (float)nsec;
+      const float csnrm1_r = ref_device_reduce(csr(nrad - 1), nsec, sm) / (float)nsec;
+      const float csnrm2_r = ref_device_reduce(csr(nrad - 2), nsec, sm) / (float)nsec;
+      if (tid == 0) {
+        // host arithmetic of NonReflectingBoundary, pow() of the radii from the host
+        double dangle = (D.nr_pow_in - 1.0) / (.5 * (cs0_r + cs1_r));
+        dangle *= (D.Rmed[1] - D.Rmed[0]);
+        s_angle[0] = (int)(dangle / 2.0 / PI_D * (float)nsec + .5);
+        double dangle2 = (D.nr_pow_out - 1.0) / (.5 * (csnrm1_r + csnrm2_r));
+        dangle2 *= (D.Rmed[nrad - 1] - D.Rmed[nrad - 2]);
+        s_angle[1] = (int)(dangle2 / 2.0 / PI_D * (float)nsec + .5);
+      }
+      __syncthreads();
+      const int i_angle = s_angle[0], i_angle2 = s_angle[1];
+      const float* cs = D.cs;
+      const float SigmaMed = D.SigmaMed[1], SigmaMed2 = D.SigmaMed[nrad - 2];
+      for (int j = tid; j < nsec; j += kThreads) {
+        int i = 1, jp = j + i_angle;
+        if (jp >= nsec) jp -= nsec;
+        if (jp < 0) jp += nsec;
+        float csv = D.Adiabatic ? cs[(size_t)i * nsec + j] : D.cs_ring[i];
+        Dn[jp] = Dn[i * nsec + j];
+        En[jp] = En[i * nsec + j];
+        float Vrad_med = -csv * (Dn[i * nsec + j] - SigmaMed) / SigmaMed;
+        Vr[i * nsec + j] = 2. * Vrad_med - Vr[(i + 1) * nsec + j];
+        i = nrad - 1;
+        jp = j - i_angle2;
+        if (jp >= nsec) jp -= nsec;
+        if (jp < 0) jp += nsec;
+        csv = D.Adiabatic ? cs[(size_t)i * nsec + j] : D.cs_ring[i];
+        Dn[i * nsec + j] = Dn[jp + (i - 1) * nsec];
+        En[i * nsec + j] = En[jp + (i - 1) * nsec];
+        Vrad_med = csv * (Dn[(i - 1) * nsec + j] - SigmaMed2) / SigmaMed2;
+        Vr[i * nsec + j] = 2. * Vrad_med - Vr[(i - 1) * nsec + j];
+      }
+      __syncthreads();
+      const size_t lo = (size_t)(nrad - 1) * nsec;
+      const float mean_dens_r = ref_device_reduce([&](long j) { return Dn[j]; }, nsec, sm) / (float)nsec;
+      const float mean_dens_r2 = ref_device_reduce([&](long j) { return Dn[lo + j]; }, nsec, sm) / (float)nsec;
+      const float mean_energy_r = ref_device_reduce([&](long j) { return En[j]; }, nsec, sm) / (float)nsec;
+      const float mean_energy_r2 = ref_device_reduce([&](long j) { return En[lo + j]; }, nsec, sm) / (float)nsec;
+      const float sm0 = D.SigmaMed[0], sm1 = D.SigmaMed[nrad - 1];
+      const float em0 = D.EnergyMed[0], em1 = D.EnergyMed[nrad - 1];
+      for (int j = tid; j < nsec; j += kThreads) {
+        Dn[j] += sm0 - mean_dens_r;
+        En[j] += em0 - mean_energy_r;
+        Dn[lo + j] += sm1 - mean_dens_r2;
+        En[lo + j] += em1 - mean_energy_r2;
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // Sector tables: the angle formulas of FillForcesArraysKernel
@@ -1732,12 +1982,12 @@ void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s
   k_cs_isothermal<<<(unsigned)((b.nring + 127) / 128), 128, 0, s>>>(b, only_disk);
 }
 
-int fargo_kernels_per_substep(int adiabatic) { return FARGO_NKERNELS; }
 
 const char* fargo_substep_kernel_name(int k) {
-  static const char* names[] = {"k_ring_mean_cfl", "k_cfl_force",   "k_source1",    "k_visc_tau",
-                                "k_visc_update",   "k_source2",     "k_energy",     "k_ring_mean_tr",
-                                "k_transport",     "k_velocities",  "k_substep_end"};
+  static const char* names[] = {"k_ring_mean_cfl", "k_cfl_force",  "k_boundary_0",  "k_source1",
+                                "k_visc_tau",      "k_visc_update", "k_source2",     "k_boundary_1",
+                                "k_energy",        "k_ring_mean_tr", "k_transport",  "k_velocities",
+                                "k_boundary_2",    "k_substep_end"};
   return (k >= 0 && k < FARGO_NKERNELS) ? names[k] : "";
 }
 
@@ -1756,6 +2006,11 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   REC();
   k_cfl_force<<<b.ring_grid, kThreads, 0, s>>>(b);
   REC();
+  if (b.any_bc) {
+    k_bc_rings<0><<<b.ring_grid, kThreads, 0, s>>>(b);
+    k_bc_disk<<<b.ndisk, kThreads, 0, s>>>(b);
+  }
+  REC();
   k_source1<<<cb, kThreads, 0, s>>>(b);
   REC();
   k_visc_tau<<<cb, kThreads, 0, s>>>(b);
@@ -1763,6 +2018,11 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   k_visc_update<<<cb, kThreads, 0, s>>>(b);
   REC();
   k_source2<<<cb, kThreads, 0, s>>>(b);
+  REC();
+  if (b.any_bc) {
+    k_bc_rings<1><<<b.ring_grid, kThreads, 0, s>>>(b);
+    k_bc_disk<<<b.ndisk, kThreads, 0, s>>>(b);
+  }
   REC();
   k_energy<<<cb, kThreads, 0, s>>>(b);
   REC();
@@ -1775,10 +2035,22 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   REC();
   k_velocities<<<cb, kThreads, 0, s>>>(b);
   REC();
-  k_substep_end<<<1, 128, 0, s>>>(b, h, use_handle);
+  if (b.any_bc) {
+    k_bc_rings<2><<<b.ring_grid, kThreads, 0, s>>>(b);
+    k_bc_disk<<<b.ndisk, kThreads, 0, s>>>(b);
+  }
+  REC();
+  k_substep_end<<<1, kThreads, 0, s>>>(b, h, use_handle);
   REC();
 #undef REC
-  if (launches) *launches += FARGO_NKERNELS;
+  if (launches) *launches += fargo_substep_launches(b);
+}
+
+// Launches of one substep: 11 kernels, both transport forms in a batch of
+// isothermal and adiabatic disks, two per boundary call when a disk has a
+// non-rigid boundary.
+int fargo_substep_launches(const BatchDev& b) {
+  return 11 + ((b.ntheta_iso && b.ntheta_adi) ? 1 : 0) + (b.any_bc ? 6 : 0);
 }
 
 void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s) {

@@ -96,6 +96,7 @@ struct orc {
   float PhysicalTime, PhysicalTimeInitial, OmegaFrame, MassTaper, HillRadius, LostMass, mdcp1;
   real invdphi, onethird, dphi;
   float Xplanet_mark, Yplanet_mark; /* Psys.cu:79 static float Xplanet, Yplanet */
+  int bc_angle[2];                   /* NonReflectingBoundary's i_angle, i_angle2 (last call) */
   fargo_planets sys, sys0;
   pairr DiskOnPrimaryAcceleration, IndirectTerm;
   /* substep log */
@@ -115,6 +116,7 @@ static real* zr(size_t n) { return (real*)calloc(n ? n : 1, sizeof(real)); }
 /* Kernels.cu:1459-1470 */
 static real max2(real a, real b) { return (b > a) ? b : a; }
 static real min2(real a, real b) { return (b < a) ? b : a; }
+static real device_reduce(const real* in, int n);
 
 /* AspectRatioDevice, Kernels.cu:1473-1488 (float math on the device). */
 static real aspect_ratio_dev(const orc* o, real r) {
@@ -1247,10 +1249,7 @@ static real van_leer_radial(orc* o, real* Qb, real dt, int return_lost) {
   divise_polar_grid(o, Qb, o->DensInt, o->Work);
   compute_star_rad(o, o->Work, o->QRStar, dt);
   van_leer_radial_kernel(o, Qb, dt, return_lost);
-  double lost = 0;
-  if (return_lost)
-    for (int j = 0; j < o->nsec; j++) lost += o->LostByDisk[j];
-  return (real)lost;
+  return return_lost ? device_reduce(o->LostByDisk, o->nsec) : (real)0;
 }
 
 /* OneWindRad, TransportEuler.cu:54-73. */
@@ -1432,6 +1431,187 @@ static void correct_vtheta(orc* o, real domega) {
 /* AlgoGas, SourceEuler.cu:208-301                                          */
 /* ------------------------------------------------------------------------ */
 
+/* ------------------------------------------------------------------------ */
+/* Boundary conditions (SideEuler.cu:64-182)                                */
+/* ------------------------------------------------------------------------ */
+
+static long nearest_pow2(long n) {
+  long x = 1;
+  if (!n) return n;
+  while (x < n) x <<= 1;
+  return x;
+}
+
+/* DeviceReduce<float> (Kernels.cu:431-557) in its own order of operations:
+   getNumBlocksAndThreads (Kernels.cu:404-429) picks the block count and size,
+   each block reduces with deviceReduceKernel (Kernels.cu:269-383; IsPow2 is
+   always false for n > 1 because of its operator precedence, so the bounds-
+   checked form runs), the final warp by shuffles, and the host adds the block
+   sums in order.  The reference launches no block for n <= 128 and stops
+   there with an error; the caller refuses such grids. */
+static real device_reduce(const real* in, int n) {
+  long maxBlocks = nearest_pow2(n) / 256;
+  int threads = (n < 256 * 2) ? (int)nearest_pow2((n + 1) / 2) : 256;
+  long blocks = (n + (threads * 2 - 1)) / (threads * 2);
+  if (blocks > maxBlocks) blocks = maxBlocks;
+  real s[512], w[32];
+  real sum = 0;
+  for (long b = 0; b < blocks; b++) {
+    long gridSize = (long)threads * 2 * blocks;
+    for (int t = 0; t < threads; t++) {
+      real mySum = 0;
+      long i = b * threads * 2 + t;
+      while (i < n) {
+        mySum += in[i];
+        if (i + threads < n) mySum += in[i + threads];
+        i += gridSize;
+      }
+      s[t] = mySum;
+    }
+    for (int stride = 256; stride >= 64; stride >>= 1)
+      if (threads >= 2 * stride)
+        for (int t = 0; t < stride; t++) s[t] = s[t] + s[t + stride];
+    for (int t = 0; t < 32; t++) w[t] = (threads >= 64) ? s[t] + s[t + 32] : s[t];
+    for (int off = 16; off > 0; off >>= 1) {
+      real nw[32];
+      for (int t = 0; t < 32; t++) nw[t] = (t + off < 32) ? w[t] + w[t + off] : w[t];
+      memcpy(w, nw, sizeof(w));
+    }
+    sum += w[0];
+  }
+  return sum;
+}
+
+/* OpenBoundaryKernel, Kernels.cu:623-637. */
+static void open_boundary(orc* o) {
+  int nsec = o->nsec, i = 1;
+  real* D = o->Dens;
+  real* E = o->Energy;
+  real* V = o->Vrad;
+  real SigmaMed = (float)o->SigmaMed[0];
+  for (int j = 0; j < nsec; j++) {
+    D[(i - 1) * nsec + j] = D[i * nsec + j];
+    E[(i - 1) * nsec + j] = E[i * nsec + j];
+    if (V[(i + 1) * nsec + j] > 0.0 || (D[i * nsec + j] < SigmaMed))
+      V[i * nsec + j] = 0.0;
+    else
+      V[i * nsec + j] = V[(i + 1) * nsec + j];
+  }
+}
+
+/* NonReflectingBoundary (SideEuler.cu:70-101) with ReduceCs, ReduceMean
+   (SideEuler.cu:103-122) and the kernels NonReflectingBoundaryKernel,
+   MinusMeanKernel (Kernels.cu:676-722). */
+static void non_reflecting_boundary(orc* o) {
+  int nsec = o->nsec, nrad = o->nrad, i, i_angle, i_angle2;
+  double dangle, dangle2;
+  real* D = o->Dens;
+  real* E = o->Energy;
+  real* V = o->Vrad;
+  const real* cs = o->SoundSpeed;
+  real cs0_r = device_reduce(cs, nsec) / (float)nsec;
+  real cs1_r = device_reduce(cs + nsec, nsec) / (float)nsec;
+  real csnrm1_r = device_reduce(cs + (size_t)(nrad - 1) * nsec, nsec) / (float)nsec;
+  real csnrm2_r = device_reduce(cs + (size_t)(nrad - 2) * nsec, nsec) / (float)nsec;
+  i = 1;
+  dangle = (pow(o->Rinf[i], -1.5) - 1.0) / (.5 * (cs0_r + cs1_r));
+  dangle *= (o->Rmed[i] - o->Rmed[i - 1]);
+  i_angle = (int)(dangle / 2.0 / PI * (float)nsec + .5);
+  i = nrad - 1;
+  dangle2 = (pow(o->Rinf[i - 1], -1.5) - 1.0) / (.5 * (csnrm1_r + csnrm2_r));
+  dangle2 *= (o->Rmed[i] - o->Rmed[i - 1]);
+  i_angle2 = (int)(dangle2 / 2.0 / PI * (float)nsec + .5);
+  o->bc_angle[0] = i_angle;
+  o->bc_angle[1] = i_angle2;
+  real SigmaMed = (float)o->SigmaMed[1], SigmaMed2 = (float)o->SigmaMed[nrad - 2];
+  for (int j = 0; j < nsec; j++) {
+    int jp;
+    real Vrad_med;
+    i = 1;
+    jp = j + i_angle;
+    if (jp >= nsec) jp -= nsec;
+    if (jp < 0) jp += nsec;
+    D[jp] = D[i * nsec + j];
+    E[jp] = E[i * nsec + j];
+    Vrad_med = -cs[i * nsec + j] * (D[i * nsec + j] - SigmaMed) / SigmaMed;
+    V[i * nsec + j] = 2. * Vrad_med - V[(i + 1) * nsec + j];
+    i = nrad - 1;
+    jp = j - i_angle2;
+    if (jp >= nsec) jp -= nsec;
+    if (jp < 0) jp += nsec;
+    D[i * nsec + j] = D[jp + (i - 1) * nsec];
+    E[i * nsec + j] = E[jp + (i - 1) * nsec];
+    Vrad_med = cs[i * nsec + j] * (D[(i - 1) * nsec + j] - SigmaMed2) / SigmaMed2;
+    V[i * nsec + j] = 2. * Vrad_med - V[(i - 1) * nsec + j];
+  }
+  real mean_dens_r = device_reduce(D, nsec) / (float)nsec;
+  real mean_dens_r2 = device_reduce(D + (size_t)(nrad - 1) * nsec, nsec) / (float)nsec;
+  real mean_energy_r = device_reduce(E, nsec) / (float)nsec;
+  real mean_energy_r2 = device_reduce(E + (size_t)(nrad - 1) * nsec, nsec) / (float)nsec;
+  real sm0 = (float)o->SigmaMed[0], sm1 = (float)o->SigmaMed[nrad - 1];
+  real em0 = (float)o->EnergyMed[0], em1 = (float)o->EnergyMed[nrad - 1];
+  for (int j = 0; j < nsec; j++) {
+    D[j] += sm0 - mean_dens_r;
+    E[j] += em0 - mean_energy_r;
+    D[(nrad - 1) * nsec + j] += sm1 - mean_dens_r2;
+    E[(nrad - 1) * nsec + j] += em1 - mean_energy_r2;
+  }
+}
+
+/* EvanescentBoundary (SideEuler.cu:124-141) and EvanescentBoundaryKernel
+   (Kernels.cu:1076-1124).  The kernel's GLOBAL_bufarray_d is never filled by
+   the reference (a fresh, zeroed allocation): its self-gravity term is 0. */
+static void evanescent_boundary(orc* o, real step) {
+  const fargo_params* p = &o->p;
+  int nrad = o->nrad, nsec = o->nsec;
+  double Tin_d = 2.0 * PI * pow(o->Rmed[0], 3. / 2);
+  double Tout_d = 2.0 * PI * pow(o->Rmed[nrad - 1], 3. / 2);
+  float DRMIN = o->Rmed[0] * 1.25, DRMAX = o->Rmed[nrad - 1] * 0.84;
+  float Tin = (float)Tin_d, Tout = (float)Tout_d;
+  for (int i = 0; i < nrad; i++) o->viscosity_array[i] = fviscosity(o, o->Rmed[i]);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < nrad; i++) {
+    real Rm = o->Rmed[i];
+    if (!((Rm < DRMIN) || (Rm > DRMAX))) continue;
+    real damping, lambda = 0.0, vtheta0, vrad0, energy0, dens0, AspectRatio;
+    if (Rm < DRMIN) {
+      damping = (Rm - DRMIN) / (o->Rmed[0] - DRMIN);
+      lambda = damping * damping * 10.0 * step / Tin;
+    }
+    if (Rm > DRMAX) {
+      damping = (Rm - DRMAX) / (o->Rmed[nrad - 1] - DRMAX);
+      lambda = damping * damping * 10.0 * step / Tout;
+    }
+    AspectRatio = aspect_ratio_dev(o, Rm);
+    /* the self-gravity branch subtracts Rmed * GLOBAL_bufarray_d[i] = 0 */
+    vtheta0 = RSQRT(G * 1.0 / Rm *
+                    (1.0 - (1.0 + p->SIGMASLOPE - 2.0 * p->FLARINGINDEX) * RPOW(AspectRatio, 2.0) *
+                               RPOW(Rm, 2.0 * p->FLARINGINDEX)));
+    vtheta0 -= Rm * o->OmegaFrame;
+    vrad0 = -3.0 * o->viscosity_array[i] / Rm * (-p->SIGMASLOPE + .5);
+    dens0 = o->SigmaMed[i];
+    energy0 = o->EnergyMed[i];
+    for (int j = 0; j < nsec; j++) {
+      int l = i * nsec + j;
+      o->Vrad[l] = (o->Vrad[l] + lambda * vrad0) / (1.0 + lambda);
+      o->Vtheta[l] = (o->Vtheta[l] + lambda * vtheta0) / (1.0 + lambda);
+      o->Dens[l] = (o->Dens[l] + lambda * dens0) / (1.0 + lambda);
+      if (p->Adiabatic) o->Energy[l] = (o->Energy[l] + lambda * energy0) / (1.0 + lambda);
+    }
+  }
+}
+
+/* ApplyBoundaryCondition, SideEuler.cu:172-182. */
+static void apply_boundary_condition(orc* o, real step) {
+  const fargo_params* p = &o->p;
+  if (p->OpenInner) open_boundary(o);
+  if (p->NonReflecting) {
+    if (p->Adiabatic) compute_sound_speed(o);
+    non_reflecting_boundary(o);
+  }
+  if (p->Evanescent) evanescent_boundary(o, step);
+}
+
 int orc_advance_dt(orc* o) {
   const fargo_params* p = &o->p;
   double dt, dtemp = 0.0;
@@ -1469,14 +1649,17 @@ int orc_advance_dt(orc* o) {
     rotate_psys(o, (float)(o->OmegaFrame * dt));
     if (p->IsDisk == YES) {
       real dtr = (real)(float)dt;
+      apply_boundary_condition(o, dtr);
       compute_pressure(o);
       substep1(o, dtr);
       substep2(o, dtr);
+      apply_boundary_condition(o, dtr);
       if (p->Adiabatic) {
         compute_viscous_terms(o, o->Vrad, o->Vtheta);
         substep3(o, dtr);
       }
       transport(o, dtr);
+      apply_boundary_condition(o, dtr);
       compute_temperature(o);
       o->mdcp1 = circum_planetary_mass(o);
     }
@@ -1502,7 +1685,7 @@ int orc_create(const fargo_params* pin, const fargo_planets* planets, const doub
   o->p = *pin;
   const fargo_params* p = &o->p;
   int nrad = p->NRAD, nsec = p->NSEC;
-  if (nrad < 3 || nsec < 3) {
+  if (nrad < 3 || nsec < 3 || (p->NonReflecting && nsec <= 128)) {
     free(o);
     return 1;
   }

@@ -5,8 +5,8 @@ oracle/_ref/fargo_ref (with link-level hooks that add the seeded density
 noise right after InitGasDensity and dump dt + Nshift after every Transport,
 see oracle/ref/ref_hooks.cu).  This script runs it and packs the outputs:
 
-  on a GPU box:   python tests/golden/make_ref_golden.py run <rawdir>
-  here:           python tests/golden/make_ref_golden.py collect <rawdir>
+  on a GPU box:   python tests/golden/make_ref_golden.py run <rawdir> [case ...]
+  here:           python tests/golden/make_ref_golden.py collect <rawdir> [case ...]
 
 `collect` writes tests/golden/<case>.npz with the reference's output fields
 after 0 and NDT time steps (dens/vrad/vtheta/energy/temperature dumps,
@@ -37,16 +37,30 @@ def cases():
     out["ref_adi_128x256"] = (p, pl, SEED + 1, NDT)
     p, pl = configs.c1()
     out["ref_c1_128x384"] = (p, pl, None, NDT)
+    # the non-rigid boundaries (ApplyBoundaryCondition, SideEuler.cu:172-182)
+    p, pl = configs.small("adi", 128, 256)
+    p = dict(p, InnerBoundary="NONREFLECTING", WriteEnergy="YES")
+    out["ref_nr_adi_128x256"] = (p, pl, SEED + 2, NDT)
+    p, pl = configs.small("adi", 128, 256)
+    p = dict(p, InnerBoundary="EVANESCENT", WriteEnergy="YES", Cooling="YES", CoolingTime0="31.4")
+    out["ref_ev_adi_128x256"] = (p, pl, SEED + 3, NDT)
+    p, pl = configs.small("iso", 128, 256)
+    p = dict(p, InnerBoundary="OPEN")
+    out["ref_open_iso_128x256"] = (p, pl, SEED + 4, NDT)
     return out
 
 
-def run(rawdir):
+def _selected(names):
+    return {k: v for k, v in cases().items() if not names or k in names}
+
+
+def run(rawdir, names=()):
     rawdir = os.path.abspath(rawdir)
     exe = os.path.join(ROOT, "oracle", "_ref", "fargo_ref")
     if not os.path.exists(exe):
         raise SystemExit("build the reference first: make -f oracle/ref/Makefile.ref")
     status = 0
-    for name, (p, pl, seed, ndt) in cases().items():
+    for name, (p, pl, seed, ndt) in _selected(names).items():
         d = os.path.join(rawdir, name)
         p = dict(p, Ntot=str(ndt), Ninterm=str(ndt))
         par, cfg, out = configs.materialise(p, pl, d, "run", relative=True)
@@ -64,9 +78,9 @@ def _read_field(path, nrad, nsec):
     return np.fromfile(path, dtype=np.float32).reshape(nrad, nsec)
 
 
-def collect(rawdir):
+def collect(rawdir, names=()):
     rawdir = os.path.abspath(rawdir)
-    for name, (p, pl, seed, ndt) in cases().items():
+    for name, (p, pl, seed, ndt) in _selected(names).items():
         d = os.path.join(rawdir, name)
         out = os.path.join(d, "run_out")
         nrad, nsec = int(p["Nrad"]), int(p["Nsec"])
@@ -100,8 +114,8 @@ def collect(rawdir):
 
 
 if __name__ == "__main__":
-    if len(sys.argv) != 3 or sys.argv[1] not in ("run", "collect"):
+    if len(sys.argv) < 3 or sys.argv[1] not in ("run", "collect"):
         raise SystemExit(__doc__)
     if sys.argv[1] == "run":
-        sys.exit(run(sys.argv[2]))
-    collect(sys.argv[2])
+        sys.exit(run(sys.argv[2], sys.argv[3:]))
+    collect(sys.argv[2], sys.argv[3:])

@@ -80,6 +80,41 @@ def test_self_gravity_parity(gpu):
     _compare(P, d, o, 5, planet_rtol=1e-5)
 
 
+# Non-rigid boundaries (ApplyBoundaryCondition, called three times per
+# substep).  NONREFLECTING on an adiabatic disk with alpha viscosity also
+# refreshes the sound speed and the viscosity at every call; EVANESCENT in a
+# corotating frame meets CorrectVtheta; OPEN accumulates the mass lost
+# through the inner edge.
+def test_nonreflecting_adiabatic_alpha_parity(gpu):
+    P, L, d, o, _ = _pair("adi", 48, 160, InnerBoundary="NONREFLECTING")
+    _compare(P, d, o, 10, fields=("dens", "vrad", "vtheta", "energy"), planet_rtol=1e-6)
+
+
+def test_nonreflecting_isothermal_parity(gpu):
+    P, L, d, o, _ = _pair("iso", 48, 160, InnerBoundary="NONREFLECTING")
+    _compare(P, d, o, 10)
+
+
+def test_evanescent_corotating_parity(gpu):
+    P, L, d, o, _ = _pair("adi", 48, 160, InnerBoundary="EVANESCENT", Frame="COROTATING")
+    _compare(P, d, o, 10, fields=("dens", "vrad", "vtheta", "energy"), planet_rtol=1e-6)
+
+
+def test_open_boundary_parity_and_lost_mass(gpu):
+    # Sigma rising outwards: ring 1 sits above SigmaMed[0], so the open edge lets gas out
+    P, L, d, o, _ = _pair("iso", 48, 160, InnerBoundary="OPEN", SigmaSlope="-0.5")
+    _compare(P, d, o, 10)
+    a, b = d.scalars()["lost_mass"], o.scalars()["lost_mass"]
+    assert b != 0.0
+    assert abs(a - b) <= 1e-4 * abs(b), (a, b)
+
+
+def test_nonreflecting_rejects_narrow_grid(gpu):
+    P, L, _ = small("adi", 32, 96, InnerBoundary="NONREFLECTING")
+    with pytest.raises(Exception, match="NSEC > 128"):
+        Disk(P, L)
+
+
 def test_init_parity(gpu):
     """GPU initialisation (device sound speed and velocities) vs the oracle's."""
     for kind in ("iso", "adi"):
