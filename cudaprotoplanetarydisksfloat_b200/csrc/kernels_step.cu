@@ -1301,13 +1301,115 @@ __global__ void __launch_bounds__(kRMT) k_ring_mean(BatchDev B) {
   }
 }
 
-constexpr int kTT = 256;  // threads of the transport kernel: one window point each
-constexpr int kBR = FARGO_BAND;  // rings per transport band
+constexpr int kTT = 256;         // threads of the transport kernel
+constexpr int kBR = FARGO_BAND;  // rings per transport band: one warp each in the sweeps
+constexpr int kPad = kTT + kTT / 8;  // shared row with a padding word after every 8
 static_assert(FARGO_SEG_OUT + 8 <= kTT, "transport window must fit the CTA");
+static_assert(kBR * 32 == kTT, "one warp per ring of the band");
+
+// padded shared-memory index: 8 consecutive points per lane read without
+// bank conflicts, 32 consecutive points per warp too
+__device__ __forceinline__ int pidx(int t) { return t + (t >> 3); }
 
 size_t fargo_transport_smem_bytes(int adiabatic) {
   const int nq = adiabatic ? 6 : 5;
-  return sizeof(float) * (size_t)kTT * (size_t)(kBR * nq + 5 + 3 * nq);
+  return sizeof(float) * (size_t)kPad * (size_t)(kBR * (nq + 1) + 1);
+}
+
+// The residual and constant-residual van Leer sweeps of OneWindTheta
+// (StarThetaKernel, StarThetaKernel2, VanLeerThetaKernel, Kernels.cu:1157-1273)
+// on one ring's window of L = S + 8 points, by one warp: lane l holds points
+// 8l .. 8l+7 in registers and takes its neighbours' edge values by shuffle.
+// sRr: the ring's radial results [nq][kPad] and v_theta [kPad] on the union
+// window (point x at union column off + x); the swept values go back to
+// sRr[c][pidx(x)].  The slopes are zero on the window's first and last point,
+// whose values (and those of the next point in) never reach the output.
+template <int nq>
+__device__ __forceinline__ void sweep_ring(float* sRr, int off, int L, float VMed, float vconst, bool fast,
+                                           float dt, float dxtheta, float invdxtheta, float invsurf,
+                                           float dxrad) {
+  const int lane = threadIdx.x & 31;
+  const int x0 = 8 * lane;
+  float q[nq][8], v[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const int x = x0 + k;
+    const bool in = x < L;
+    const int id = pidx(off + x);
+#pragma unroll
+    for (int c = 0; c < nq; c++) q[c][k] = in ? sRr[c * kPad + id] : 0.0f;
+    float vres = (in ? sRr[nq * kPad + id] : 0.0f) - VMed;
+    if (!fast) vres = vconst + vres;
+    v[k] = vres;
+  }
+  if (!fast) vconst = 0.0f;
+  auto slope = [&](float wm, float w0, float wp, int x) -> float {
+    if (x <= 0 || x >= L - 1) return 0.0f;
+    float dqm = (w0 - wm);
+    float dqp = (wp - w0);
+    if (dqp * dqm > 0.0f) return __fdividef(dqp * dqm, dqp + dqm) * invdxtheta;
+    return 0.0f;
+  };
+  for (int sweep = 0; sweep < 2; sweep++) {
+    float vv[8], rr[8], S[8], GS[8], sD[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      vv[k] = (sweep == 1) ? vconst : v[k];
+      S[k] = q[nq - 1][k];
+      rr[k] = __fdividef(1.0f, S[k] + 1e-20f);
+    }
+    const float Sl = __shfl_up_sync(0xffffffffu, S[7], 1);
+    const float Sr = __shfl_down_sync(0xffffffffu, S[0], 1);
+#pragma unroll
+    for (int k = 0; k < 8; k++) GS[k] = slope(k ? S[k - 1] : Sl, S[k], k < 7 ? S[k + 1] : Sr, x0 + k);
+    const float GSl = __shfl_up_sync(0xffffffffu, GS[7], 1);
+    // DensStar (StarThetaKernel2 on the density)
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const float ksi = vv[k] * dt;
+      if (ksi > 0.0f)
+        sD[k] = (x0 + k > 0) ? (k ? S[k - 1] : Sl) + (dxtheta - ksi) * (k ? GS[k - 1] : GSl) : 0.0f;
+      else
+        sD[k] = S[k] - (dxtheta + ksi) * GS[k];
+    }
+    // every quantity, density last; all quotients use the pre-sweep density
+#pragma unroll
+    for (int c = 0; c < nq; c++) {
+      float W[8], G[8], F[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) W[k] = q[c][k] * rr[k];
+      const float Wl = __shfl_up_sync(0xffffffffu, W[7], 1);
+      const float Wr = __shfl_down_sync(0xffffffffu, W[0], 1);
+#pragma unroll
+      for (int k = 0; k < 8; k++) G[k] = slope(k ? W[k - 1] : Wl, W[k], k < 7 ? W[k + 1] : Wr, x0 + k);
+      const float Gl = __shfl_up_sync(0xffffffffu, G[7], 1);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const float ksi = vv[k] * dt;
+        float qr;
+        if (ksi > 0.0f)
+          qr = (x0 + k > 0) ? (k ? W[k - 1] : Wl) + (dxtheta - ksi) * (k ? G[k - 1] : Gl) : 0.0f;
+        else
+          qr = W[k] - (dxtheta + ksi) * G[k];
+        F[k] = dxrad * qr * sD[k] * vv[k];  // flux through the left interface of point k
+      }
+      const float Fr = __shfl_down_sync(0xffffffffu, F[0], 1);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        if (x0 + k < L - 1) {
+          float varq = F[k];
+          varq -= (k < 7 ? F[k + 1] : Fr);
+          q[c][k] += varq * invsurf;
+        }
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 8; k++)
+#pragma unroll
+    for (int c = 0; c < nq; c++) sRr[c * kPad + pidx(x0 + k)] = q[c][k];
+  __syncwarp();
 }
 
 // Transport (TransportEuler.cu:24-35) of a band of up to kBR rings i0 ..
@@ -1317,32 +1419,24 @@ size_t fargo_transport_smem_bytes(int adiabatic) {
 // window j0 - Nshift_i - 4 .. + S + 8.  The rings are taken in sub-bands
 // whose windows fit one union window of kTT sectors: the radial half
 // (rad_march) runs over the union, one thread per column marching down the
-// sub-band, into shared memory; then, ring by ring, the residual and
-// constant-residual van Leer sweeps of OneWindTheta (StarThetaKernel,
-// StarThetaKernel2, VanLeerThetaKernel, Kernels.cu:1157-1273) on the ring's
-// window; the 4-point halo covers the sweeps' stencils.  VMed, Nshift and
-// the constant residual come from k_ring_mean<1>.  Final density / energy
-// go to scratch (a0 / a1) because neighbouring rings still read the old
-// ones; the velocity kernel moves them into the state.
+// sub-band, into shared memory; then one warp per ring runs the azimuthal
+// sweeps (sweep_ring) on the ring's window; the 4-point halo covers the
+// sweeps' stencils.  VMed, Nshift and the constant residual come from
+// k_ring_mean<1>.  Final density / energy go to scratch (a0 / a1) because
+// neighbouring bands still read the old ones; the velocity kernel moves them
+// into the state.
 template <int nq>
 __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __restrict__ items) {
   extern __shared__ float tr_sm[];
-  float* sR = tr_sm;                 // [kBR][nq][kTT] radial results on the union window
-  float* sS = sR + kBR * nq * kTT;   // density of the ring's window (pre-sweep)
-  float* sG = sS + kTT;              // its azimuthal slope
-  float* sV = sG + kTT;              // residual velocity
-  float* sD = sV + kTT;              // DensStar of the sweep
-  float* sW = sD + kTT;              // [nq][kTT] DivisePolarGrid quotients
-  float* sQ = sW + nq * kTT;         // [nq][kTT] their slopes
-  float* sF = sQ + nq * kTT;         // [nq][kTT] their fluxes
-  float* sL = sF + nq * kTT;         // [kTT] mass through the inner edge (OPEN)
+  float* sR = tr_sm;                         // [kBR][nq + 1][kPad] radial results + v_theta
+  float* sL = sR + kBR * (nq + 1) * kPad;    // [kPad] mass through the inner edge (OPEN)
   __shared__ int s_ns[kBR];
   __shared__ float s_vmed[kBR], s_vc[kBR];
   const int nak = (nq == 5) ? B.act[1] : B.act[2];
   const int* aoff = (nq == 5) ? B.act_iso_off : B.act_adi_off;
   const int* adisk = (nq == 5) ? B.act_iso_disk : B.act_adi_disk;
   const int nai = nak > 0 ? aoff[nak] : 0;
-  const int p = threadIdx.x;
+  const int p = threadIdx.x, warp = p >> 5, lane = p & 31;
   for (int t = blockIdx.x; t < nai; t += gridDim.x) {
     __syncthreads();
     const int a = find_range(aoff, nak, t);
@@ -1381,99 +1475,34 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
       if (p < WU) {
         int g = (u0 + p) % nsec;
         if (g < 0) g += nsec;
-        rad_march<nq>(D, i0 + rb, i0 + re, g, dt, Om, dtheta, sR + p, kTT, nq * kTT,
-                      (D.OpenInner && i0 + rb == 0) ? sL + p : nullptr);
+        float* o = sR + pidx(p);
+        rad_march<nq>(D, i0 + rb, i0 + re, g, dt, Om, dtheta, o, kPad, (nq + 1) * kPad,
+                      (D.OpenInner && i0 + rb == 0) ? sL + pidx(p) : nullptr);
+        for (int r = rb; r < re; r++) o[((r - rb) * (nq + 1) + nq) * kPad] = __ldg(D.vtheta + (size_t)(i0 + r) * nsec + g);
       }
       __syncthreads();
-      for (int r = rb; r < re; r++) {
+      const int r = rb + warp;
+      if (r < re) {
         const int i = i0 + r;
         const int ws = j0 - s_ns[r] - 4;  // first (unwrapped) sector of this ring's window
         const int off = ws - u0;
-        const float VMed = s_vmed[r];
-        float vconst = s_vc[r];
-        float q[nq];
-        const bool in = p < L;
-        if (in) {
-          int g = ws + p;
-          g %= nsec;
-          if (g < 0) g += nsec;
-#pragma unroll
-          for (int c = 0; c < nq; c++) q[c] = sR[((r - rb) * nq + c) * kTT + off + p];
-          float vres = __ldg(D.vtheta + (size_t)i * nsec + g) - VMed;
-          if (!fast) vres = vconst + vres;
-          sV[p] = vres;
-          sS[p] = q[nq - 1];
-        }
-        if (!fast) vconst = 0.0f;
+        float* sRr = sR + (size_t)(r - rb) * (nq + 1) * kPad;
         const float Rm = D.Rmed[i];
         const float dxtheta = dtheta * Rm;
-        const float invdxtheta = 1.0f / dxtheta;
-        const float invsurf = 1.0f / D.Surf[i];
-        const float dxrad = (D.Rsup[i] - D.Rinf[i]) * dt;
-        // van Leer slope of StarThetaKernel at window point x (0 at the window edges)
-        auto dqat = [&](const float* W, int x) -> float {
-          if (x <= 0 || x >= L - 1) return 0.0f;
-          float dqm = (W[x] - W[x - 1]);
-          float dqp = (W[x + 1] - W[x]);
-          if (dqp * dqm > 0.0f) return __fdividef(dqp * dqm, dqp + dqm) * invdxtheta;
-          return 0.0f;
-        };
-        // upwind value of StarThetaKernel2 at window point x with velocity v
-        auto upw = [&](const float* W, const float* G, int x, float v) -> float {
-          float ksi = v * dt;
-          if (ksi > 0.0f) return (x > 0) ? W[x - 1] + (dxtheta - ksi) * G[x - 1] : 0.0f;
-          return W[x] - (dxtheta + ksi) * G[x];
-        };
-        __syncthreads();
-        for (int sweep = 0; sweep < 2; sweep++) {
-          const float v = (sweep == 1) ? vconst : (in ? sV[p] : 0.0f);
-          // quotients by the pre-sweep density, density slope
-          if (in) {
-            const float rr = __fdividef(1.0f, sS[p] + 1e-20f);
+        sweep_ring<nq>(sRr, off, L, s_vmed[r], s_vc[r], fast, dt, dxtheta, 1.0f / dxtheta, 1.0f / D.Surf[i],
+                       (D.Rsup[i] - D.Rinf[i]) * dt);
+        // output sector j0 + x - 4 takes window point x: coalesced stores
+        float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.a1, D.a0};
+        const long long row = (long long)i * nsec + j0 - 4;
+        for (int x = 4 + lane; x < L - 4; x += 32) {
 #pragma unroll
-            for (int c = 0; c < nq; c++) sW[c * kTT + p] = q[c] * rr;
-            sG[p] = dqat(sS, p);
-          }
-          __syncthreads();
-          // DensStar, slopes of the quotients
-          if (in) {
-            sD[p] = upw(sS, sG, p, v);
-#pragma unroll
-            for (int c = 0; c < nq; c++) sQ[c * kTT + p] = dqat(sW + c * kTT, p);
-          }
-          __syncthreads();
-          // fluxes through the interface at the left of point p (VanLeerThetaKernel)
-          if (in) {
-#pragma unroll
-            for (int c = 0; c < nq; c++)
-              sF[c * kTT + p] = dxrad * upw(sW + c * kTT, sQ + c * kTT, p, v) * sD[p] * v;
-          }
-          __syncthreads();
-          if (p < L - 1) {
-#pragma unroll
-            for (int c = 0; c < nq; c++) {
-              float varq = sF[c * kTT + p];
-              varq -= sF[c * kTT + p + 1];
-              q[c] += varq * invsurf;
-            }
-          }
-          // the next sweep's pre-sweep density (read after the next barrier)
-          if (sweep == 0 && in) sS[p] = q[nq - 1];
-          __syncthreads();
-        }
-        // output sector j0 + p - 4 takes window point p
-        if (p >= 4 && p < L - 4) {
+          for (int c = 0; c < nq; c++) dsts[c == nq - 1 ? 5 : c][row + x] = sRr[c * kPad + pidx(x)];
           if (i == 0 && D.OpenInner) {
             // each source sector is the core of exactly one segment's window
-            int g = ws + p;
-            g %= nsec;
+            int g = (ws + x) % nsec;
             if (g < 0) g += nsec;
-            D.lost[g] = sL[off + p];
+            D.lost[g] = sL[pidx(off + x)];
           }
-          float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.a1, D.a0};
-          const long long lo2 = (long long)i * nsec + j0 + p - 4;
-#pragma unroll
-          for (int c = 0; c < nq; c++) dsts[c == nq - 1 ? 5 : c][lo2] = q[c];
         }
       }
       rb = re;
