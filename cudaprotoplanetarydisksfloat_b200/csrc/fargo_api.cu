@@ -105,6 +105,13 @@ fargo_status dupload(fargo_batch* b, DiskHost& h, const T** ptr, const std::vect
   return FARGO_OK;
 }
 
+// bodies of the per-substep force sums: the star and every FeelDisk planet
+int body_count(const fargo_planets* pl) {
+  int n = 1;
+  for (int k = 0; k < pl->nb; k++) n += pl->feeldisk[k] ? 1 : 0;
+  return n;
+}
+
 fargo_status check_params(fargo_batch* b, const fargo_params* p, const fargo_planets* pl) {
   if (p->NRAD < 4 || p->NSEC < 4) return set_err(b, FARGO_EINVAL, "NRAD and NSEC must be >= 4");
   if (p->NSEC > 16384) return set_err(b, FARGO_EINVAL, "NSEC > 16384 is not supported");
@@ -411,7 +418,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   std::vector<long long> cell_off(n + 1, 0);
   std::vector<int> ring_off(n + 1, 0);
   std::vector<int4> theta_iso, theta_adi;
-  int seg_max = 0, any_bc = 0;
+  int seg_max = 0, any_bc = 0, max_body = 1;
   for (int d = 0; d < n; d++) {
     fargo_status st = check_params(b, &params[d], &planets[d]);
     if (st) return st;
@@ -430,6 +437,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     b->any_adiabatic |= h.p.Adiabatic;
     b->n_sg += h.p.SelfGravity ? 1 : 0;
     any_bc |= (h.p.OpenInner || h.p.NonReflecting || h.p.Evanescent) ? 1 : 0;
+    max_body = std::max(max_body, body_count(&planets[d]));
     std::vector<int4>& theta = h.p.Adiabatic ? theta_adi : theta_iso;
     h.dev.item0 = (int)theta.size();
     // bands of FARGO_BAND rings, each in nseg near-equal azimuthal segments
@@ -473,6 +481,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   BatchDev& bd = b->bd;
   bd.ndisk = n;
   bd.any_bc = any_bc;
+  bd.max_body = max_body;
   bd.ncell = cell_off[n];
   bd.nring = ring_off[n];
   bd.cell_off = b->d_cell_off;
@@ -707,8 +716,15 @@ fargo_status fargo_set_planets(fargo_ctx* ctx, const fargo_planets* in) {
   cudaError_t e;
   DiskCtl c = ctl_header(b, 0, &e);
   if (e != cudaSuccess) return set_err(b, FARGO_ECUDA, "%s", cudaGetErrorString(e));
+  if (body_count(in) > FARGO_MAXBODY) return set_err(b, FARGO_EINVAL, "at most %d planets may feel the disk", FARGO_MAXBODY - 1);
   planets_to_ctl(in, &c);
-  return put_ctl_header(b, 0, c);
+  fargo_status st = put_ctl_header(b, 0, c);
+  if (st) return st;
+  if (body_count(in) > b->bd.max_body) {  // the force kernel was built for fewer bodies
+    b->bd.max_body = FARGO_MAXBODY;
+    return build_graph(b);
+  }
+  return FARGO_OK;
 }
 
 fargo_status fargo_advance_dt(fargo_ctx* ctx, int* nsub_out) {

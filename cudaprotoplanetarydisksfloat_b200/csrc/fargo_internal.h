@@ -157,6 +157,7 @@ struct BatchDev {
   int* act_ctile_off;        // [ndisk+1] prefix of rings of active disks (CFL tiles)
   int cell_grid, ring_grid, item_grid, grp_grid;  // fixed grid sizes of the grid-stride kernels
   int any_bc;                // some disk has an OPEN, NONREFLECTING or EVANESCENT boundary
+  int max_body;              // largest body count of the force sums (star + FeelDisk planets)
 };
 
 // kernel entry points (kernels_step.cu), launched by fargo_api.cu

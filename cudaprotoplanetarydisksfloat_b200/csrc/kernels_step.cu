@@ -656,15 +656,19 @@ __device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const d
 // finishing sums run in a fixed order.  Each block takes a contiguous run of
 // rings.  The block that completes a disk's last ring finishes the
 // substep's scalar work.
+// NB >= every disk's body count (star + FeelDisk planets): the per-thread
+// FP64 force accumulators are sized for it.
+template <int NB>
 __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
   __shared__ DiskDev sD;
   __shared__ DiskCtl sC;
-  __shared__ float s_b[5][FARGO_MAXBODY];
+  __shared__ float s_b[5][NB];
   __shared__ float s_min[32];
-  __shared__ double s_red[2 * FARGO_MAXBODY][kThreads / 32];
+  __shared__ double s_red[2 * NB][kThreads / 32];
   __shared__ double s_sum[4 * FARGO_MAXBODY];
   __shared__ double s_work[FARGO_RK_WORK(kRkShared)];
   __shared__ unsigned s_ticket;
+  __shared__ int s_nbody;
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
   const int na = B.act[0];
   const int ntile = na > 0 ? B.act_ctile_off[na] : 0;
@@ -680,7 +684,9 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
       copy_words(&sD, B.disks + B.act_disk[a], sizeof(DiskDev));
       __syncthreads();
       const DiskCtl* C = sD.ctl;
-      if (tid < C->nbody) {
+      const int nb = min(C->nbody, NB);
+      if (tid == 0) s_nbody = nb;
+      if (tid < nb) {
         s_b[0][tid] = C->bx[tid];
         s_b[1][tid] = C->by[tid];
         s_b[2][tid] = C->brs[tid];
@@ -691,13 +697,13 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
     }
     const DiskDev& D = sD;
     DiskCtl* C = D.ctl;
-    const int nbody = C->nbody;
+    const int nbody = s_nbody;
     const int nsec = D.nsec;
     const int i = t - lo;  // ring
     float lmin = 1e30f;
-    double sfx[FARGO_MAXBODY], sfy[FARGO_MAXBODY];
+    double sfx[NB], sfy[NB];
 #pragma unroll
-    for (int b = 0; b < FARGO_MAXBODY; b++) sfx[b] = sfy[b] = 0.0;
+    for (int b = 0; b < NB; b++) sfx[b] = sfy[b] = 0.0;
     if (D.IsDisk) {
       const float vm = D.vmoy[i];  // k_ring_mean<0>
       const float dxrad = D.Rsup[i] - D.Rinf[i];
@@ -737,7 +743,7 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
         float cx = Rm * D.cos_cell[j];
         float cy = Rm * D.sin_cell[j];
 #pragma unroll
-        for (int b = 0; b < FARGO_MAXBODY; b++) {
+        for (int b = 0; b < NB; b++) {
           if (b < nbody) {
             float dx = cx - s_b[0][b];
             float dy = cy - s_b[1][b];
@@ -759,10 +765,11 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
         }
       }
     }
-    float rmin = block_min_f(lmin, s_min);
-    if (tid == 0) D.ringmin[i] = rmin;
+    // ring minimum and force sums: warps by shuffle, then warp 0 over the warps
+    lmin = warp_min_f(lmin);
+    if (l == 0) s_min[w] = lmin;
 #pragma unroll
-    for (int b = 0; b < FARGO_MAXBODY; b++) {
+    for (int b = 0; b < NB; b++) {
       if (b < nbody) {
         double fx = warp_sum_d(sfx[b]);
         double fy = warp_sum_d(sfy[b]);
@@ -773,19 +780,27 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
       }
     }
     __syncthreads();
-    if (tid < 2 * nbody) {
-      double acc = 0.0;
-      for (int q = 0; q < kThreads / 32; q++) acc += s_red[tid][q];
-      const int b = tid >> 1, comp = tid & 1;  // comp 0: x, 1: y
-      const bool inner = D.Rmed[i] < s_b[4][b];
-      double* P = D.partials + (size_t)i * 4 * FARGO_MAXBODY + 4 * b + 2 * comp;
-      P[0] = inner ? acc : 0.0;  // f*_inner
-      P[1] = inner ? 0.0 : acc;  // f*_outer
+    if (w == 0) {
+      if (l == 0) {
+        float m = s_min[0];
+        for (int q = 1; q < kThreads / 32; q++)
+          if (s_min[q] < m) m = s_min[q];
+        D.ringmin[i] = m;
+      }
+      if (l < 2 * nbody) {
+        double acc = 0.0;
+        for (int q = 0; q < kThreads / 32; q++) acc += s_red[l][q];
+        const int b = l >> 1, comp = l & 1;  // comp 0: x, 1: y
+        const bool inner = D.Rmed[i] < s_b[4][b];
+        double* P = D.partials + (size_t)i * 4 * FARGO_MAXBODY + 4 * b + 2 * comp;
+        P[0] = inner ? acc : 0.0;  // f*_inner
+        P[1] = inner ? 0.0 : acc;  // f*_outer
+      }
+      // the block that completes this disk's last ring finishes the substep
+      __threadfence();
+      __syncwarp();
+      if (l == 0) s_ticket = atomicAdd(&C->counter, 1u);
     }
-    // the block that completes this disk's last ring finishes the substep
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) s_ticket = atomicAdd(&C->counter, 1u);
     __syncthreads();
     if (s_ticket == (unsigned)(D.nrad - 1)) {
       __threadfence();
@@ -2033,7 +2048,14 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   REC();
   k_ring_mean<0><<<b.grp_grid, kRMT, fargo_ring_mean_smem_bytes(), s>>>(b);
   REC();
-  k_cfl_force<<<b.ring_grid, kThreads, 0, s>>>(b);
+  if (b.max_body <= 1)
+    k_cfl_force<1><<<b.ring_grid, kThreads, 0, s>>>(b);
+  else if (b.max_body <= 2)
+    k_cfl_force<2><<<b.ring_grid, kThreads, 0, s>>>(b);
+  else if (b.max_body <= 4)
+    k_cfl_force<4><<<b.ring_grid, kThreads, 0, s>>>(b);
+  else
+    k_cfl_force<FARGO_MAXBODY><<<b.ring_grid, kThreads, 0, s>>>(b);
   REC();
   if (b.any_bc) {
     k_bc_rings<0><<<b.ring_grid, kThreads, 0, s>>>(b);
