@@ -514,6 +514,13 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     bd.grp_grid = std::min((bd.nring + 31 * n + 31) / 32, nsm * 3);
   }
   CK(fargo_kernel_attributes(b->max_nsec));
+  {
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    long long tiles = 0;
+    for (int d = 0; d < n; d++) tiles += ((long long)b->disks[d].dev.nrad * b->disks[d].dev.nsec + 255) / 256;
+    CK(fargo_size_grids(bd, nsm, tiles, (int)(theta_iso.size() + theta_adi.size())));
+  }
   fargo_launch_sector_tables(bd, b->max_nsec, b->stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(b->stream));
@@ -722,6 +729,11 @@ fargo_status fargo_set_planets(fargo_ctx* ctx, const fargo_planets* in) {
   if (st) return st;
   if (body_count(in) > b->bd.max_body) {  // the force kernel was built for fewer bodies
     b->bd.max_body = FARGO_MAXBODY;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+    int per = 1;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fargo_cfl_kernel(FARGO_MAXBODY), 256, 0));
+    b->bd.g_cfl = std::max(1, std::min(b->bd.nring, nsm * std::max(per, 1)));
     return build_graph(b);
   }
   return FARGO_OK;

@@ -158,6 +158,8 @@ struct BatchDev {
   int cell_grid, ring_grid, item_grid, grp_grid;  // fixed grid sizes of the grid-stride kernels
   int any_bc;                // some disk has an OPEN, NONREFLECTING or EVANESCENT boundary
   int max_body;              // largest body count of the force sums (star + FeelDisk planets)
+  // one-wave grids of the substep kernels (fargo_size_grids)
+  int g_cfl, g_source1, g_visc_tau, g_visc_update, g_source2, g_energy, g_velocities, g_transport;
 };
 
 // kernel entry points (kernels_step.cu), launched by fargo_api.cu
@@ -179,3 +181,5 @@ void fargo_launch_disk_force(const BatchDev& b, int disk, float x, float y, floa
                              double* out44, int nblocks, cudaStream_t s);
 void fargo_launch_diagnostics(const BatchDev& b, int disk, double* out3, int nblocks, cudaStream_t s);
 int fargo_substep_launches(const BatchDev& b);
+cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int nitems);
+const void* fargo_cfl_kernel(int max_body);

@@ -934,7 +934,7 @@ __device__ __forceinline__ Tau viscous_terms(const DiskDev& D, const float* Vr, 
   return t;
 }
 
-__global__ void __launch_bounds__(kThreads) k_visc_tau(BatchDev B) {
+__global__ void __launch_bounds__(kThreads, 6) k_visc_tau(BatchDev B) {
   CELL_BEGIN
   Tau t = viscous_terms(D, D.vri, D.vti, i, j, nsec);
   D.trr[l] = t.rr;
@@ -967,7 +967,7 @@ __device__ void vkep_pair(const DiskDev& D, const DiskCtl* C, float* vin, float*
 
 // UpdateVelocitiesKernel (Kernels.cu:142-160) in place, then
 // ApplySubKeplerianBoundaryKernel (Kernels.cu:1490-1503).
-__global__ void __launch_bounds__(kThreads) k_visc_update(BatchDev B) {
+__global__ void __launch_bounds__(kThreads, 6) k_visc_update(BatchDev B) {
   CELL_BEGIN
   const float DeltaT = C->dtf;
   const float* Dn = D.dens;
@@ -1001,7 +1001,7 @@ __device__ __forceinline__ float qvisc(float dv, float dens) {
   return 0.0f;
 }
 
-__global__ void __launch_bounds__(kThreads) k_source2(BatchDev B) {
+__global__ void __launch_bounds__(kThreads, 6) k_source2(BatchDev B) {
   CELL_BEGIN
   const float dt = C->dtf;
   const float* Dn = D.dens;
@@ -1529,7 +1529,7 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
 // ComputeVelocitiesKernel, Kernels.cu:1292-1306, from the transported
 // momenta (vri, vti, trr, tpp) and density (a0); then the transported
 // density (and energy, a1) become the state.
-__global__ void __launch_bounds__(kThreads) k_velocities(BatchDev B) {
+__global__ void __launch_bounds__(kThreads, 8) k_velocities(BatchDev B) {
   CELL_BEGIN
   const float* Dn = D.a0;
   const long long lmj = (long long)i * nsec + jm;
@@ -1594,13 +1594,15 @@ __device__ void compact_active(const BatchDev& B) {
 __global__ void k_substep_end(BatchDev B, cudaGraphConditionalHandle h, int use_handle) {
   __shared__ float sm[kThreads];
   // LostMass += VanLeerRadial's DeviceReduce of LostByDisk (TransportEuler.cu:72, 145)
-  for (int d = 0; d < B.ndisk; d++) {
-    const DiskDev& D = B.disks[d];
-    if (!D.OpenInner || !D.IsDisk || !D.ctl->active) continue;
-    const float lost = ref_device_reduce([&](long j) { return D.lost[j]; }, D.nsec, sm);
-    if (threadIdx.x == 0) D.ctl->LostMass += lost;
+  if (B.any_bc) {
+    for (int d = 0; d < B.ndisk; d++) {
+      const DiskDev& D = B.disks[d];
+      if (!D.OpenInner || !D.IsDisk || !D.ctl->active) continue;  // block-uniform
+      const float lost = ref_device_reduce([&](long j) { return D.lost[j]; }, D.nsec, sm);
+      if (threadIdx.x == 0) D.ctl->LostMass += lost;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   int any = 0;
   for (int d = threadIdx.x; d < B.ndisk; d += blockDim.x) {
     DiskCtl* C = B.disks[d].ctl;
@@ -2037,7 +2039,6 @@ const char* fargo_substep_kernel_name(int k) {
 
 void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int use_handle, cudaStream_t s,
                           int max_nsec, long long* launches, cudaEvent_t* ev) {
-  const unsigned cb = (unsigned)b.cell_grid;
   (void)max_nsec;
   int k = 0;
 #define REC()                                  \
@@ -2049,42 +2050,42 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   k_ring_mean<0><<<b.grp_grid, kRMT, fargo_ring_mean_smem_bytes(), s>>>(b);
   REC();
   if (b.max_body <= 1)
-    k_cfl_force<1><<<b.ring_grid, kThreads, 0, s>>>(b);
+    k_cfl_force<1><<<b.g_cfl, kThreads, 0, s>>>(b);
   else if (b.max_body <= 2)
-    k_cfl_force<2><<<b.ring_grid, kThreads, 0, s>>>(b);
+    k_cfl_force<2><<<b.g_cfl, kThreads, 0, s>>>(b);
   else if (b.max_body <= 4)
-    k_cfl_force<4><<<b.ring_grid, kThreads, 0, s>>>(b);
+    k_cfl_force<4><<<b.g_cfl, kThreads, 0, s>>>(b);
   else
-    k_cfl_force<FARGO_MAXBODY><<<b.ring_grid, kThreads, 0, s>>>(b);
+    k_cfl_force<FARGO_MAXBODY><<<b.g_cfl, kThreads, 0, s>>>(b);
   REC();
   if (b.any_bc) {
     k_bc_rings<0><<<b.ring_grid, kThreads, 0, s>>>(b);
     k_bc_disk<<<b.ndisk, kThreads, 0, s>>>(b);
   }
   REC();
-  k_source1<<<cb, kThreads, 0, s>>>(b);
+  k_source1<<<b.g_source1, kThreads, 0, s>>>(b);
   REC();
-  k_visc_tau<<<cb, kThreads, 0, s>>>(b);
+  k_visc_tau<<<b.g_visc_tau, kThreads, 0, s>>>(b);
   REC();
-  k_visc_update<<<cb, kThreads, 0, s>>>(b);
+  k_visc_update<<<b.g_visc_update, kThreads, 0, s>>>(b);
   REC();
-  k_source2<<<cb, kThreads, 0, s>>>(b);
+  k_source2<<<b.g_source2, kThreads, 0, s>>>(b);
   REC();
   if (b.any_bc) {
     k_bc_rings<1><<<b.ring_grid, kThreads, 0, s>>>(b);
     k_bc_disk<<<b.ndisk, kThreads, 0, s>>>(b);
   }
   REC();
-  k_energy<<<cb, kThreads, 0, s>>>(b);
+  k_energy<<<b.g_energy, kThreads, 0, s>>>(b);
   REC();
   k_ring_mean<1><<<b.grp_grid, kRMT, fargo_ring_mean_smem_bytes(), s>>>(b);
   REC();
   if (b.ntheta_iso)
-    k_transport<5><<<std::min(b.item_grid, b.ntheta_iso), kTT, fargo_transport_smem_bytes(0), s>>>(b, b.theta_iso);
+    k_transport<5><<<std::min(b.g_transport, b.ntheta_iso), kTT, fargo_transport_smem_bytes(0), s>>>(b, b.theta_iso);
   if (b.ntheta_adi)
-    k_transport<6><<<std::min(b.item_grid, b.ntheta_adi), kTT, fargo_transport_smem_bytes(1), s>>>(b, b.theta_adi);
+    k_transport<6><<<std::min(b.g_transport, b.ntheta_adi), kTT, fargo_transport_smem_bytes(1), s>>>(b, b.theta_adi);
   REC();
-  k_velocities<<<cb, kThreads, 0, s>>>(b);
+  k_velocities<<<b.g_velocities, kThreads, 0, s>>>(b);
   REC();
   if (b.any_bc) {
     k_bc_rings<2><<<b.ring_grid, kThreads, 0, s>>>(b);
@@ -2095,6 +2096,37 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   REC();
 #undef REC
   if (launches) *launches += fargo_substep_launches(b);
+}
+
+// The CFL/force kernel instance for up to max_body bodies.
+const void* fargo_cfl_kernel(int max_body) {
+  return max_body <= 1   ? (const void*)k_cfl_force<1>
+         : max_body <= 2 ? (const void*)k_cfl_force<2>
+         : max_body <= 4 ? (const void*)k_cfl_force<4>
+                         : (const void*)k_cfl_force<FARGO_MAXBODY>;
+}
+
+// Grids of the substep kernels: one wave of resident blocks (the kernels walk
+// contiguous runs of tiles, so a second partial wave would idle most SMs),
+// never more blocks than work items.
+cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int nitems) {
+  auto wave = [&](const void* fn, int threads, size_t smem, long long work, int* out) -> cudaError_t {
+    int per = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem);
+    if (e != cudaSuccess) return e;
+    long long g = (long long)nsm * (per > 0 ? per : 1);
+    *out = (int)std::max<long long>(1, std::min<long long>(g, work));
+    return cudaSuccess;
+  };
+  cudaError_t e;
+  if ((e = wave(fargo_cfl_kernel(b.max_body), kThreads, 0, b.nring, &b.g_cfl))) return e;
+  if ((e = wave((const void*)k_source1, kThreads, 0, ncell_tiles, &b.g_source1))) return e;
+  if ((e = wave((const void*)k_visc_tau, kThreads, 0, ncell_tiles, &b.g_visc_tau))) return e;
+  if ((e = wave((const void*)k_visc_update, kThreads, 0, ncell_tiles, &b.g_visc_update))) return e;
+  if ((e = wave((const void*)k_source2, kThreads, 0, ncell_tiles, &b.g_source2))) return e;
+  if ((e = wave((const void*)k_energy, kThreads, 0, ncell_tiles, &b.g_energy))) return e;
+  if ((e = wave((const void*)k_velocities, kThreads, 0, ncell_tiles, &b.g_velocities))) return e;
+  return wave((const void*)k_transport<6>, kTT, fargo_transport_smem_bytes(1), nitems, &b.g_transport);
 }
 
 // Launches of one substep: 11 kernels, both transport forms in a batch of
