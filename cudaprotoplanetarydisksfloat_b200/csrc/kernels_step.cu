@@ -663,8 +663,8 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
   __shared__ DiskDev sD;
   __shared__ DiskCtl sC;
   __shared__ float s_b[5][NB];
-  __shared__ float s_min[32];
-  __shared__ double s_red[2 * NB][kThreads / 32];
+  __shared__ float s_min[2][32];                     // double-buffered by ring parity
+  __shared__ double s_red[2][2 * NB][kThreads / 32];
   __shared__ double s_sum[4 * FARGO_MAXBODY];
   __shared__ double s_work[FARGO_RK_WORK(kRkShared)];
   __shared__ unsigned s_ticket;
@@ -674,9 +674,29 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
   const int ntile = na > 0 ? B.act_ctile_off[na] : 0;
   const int per = (ntile + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
-  int lo = 0, hi = -1;
+  int lo = 0, hi = -1, run = 0;
+  // A run of rings of one disk is done: count it on the disk's ticket; the
+  // block that completes the disk's last ring finishes the substep.  Warp 0
+  // wrote the run's results and fences them before the ticket.
+  auto finish_run = [&]() {
+    if (run == 0) return;
+    DiskCtl* Cr = sD.ctl;
+    if (w == 0) {
+      __threadfence();
+      __syncwarp();
+      if (l == 0) s_ticket = atomicAdd(&Cr->counter, (unsigned)run);
+    }
+    __syncthreads();
+    if (s_ticket + (unsigned)run == (unsigned)sD.nrad) {
+      __threadfence();
+      finish_cfl_and_planets(sD, Cr, &sC, s_min[0], s_sum, s_work);
+    }
+    run = 0;
+    __syncthreads();
+  };
   for (int t = t0; t < t1; t++) {
     if (t >= hi) {  // block-uniform: entering a disk
+      finish_run();
       const int a = find_range(B.act_ctile_off, na, t);
       lo = B.act_ctile_off[a];
       hi = B.act_ctile_off[a + 1];
@@ -696,7 +716,6 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
       __syncthreads();
     }
     const DiskDev& D = sD;
-    DiskCtl* C = D.ctl;
     const int nbody = s_nbody;
     const int nsec = D.nsec;
     const int i = t - lo;  // ring
@@ -766,47 +785,42 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
       }
     }
     // ring minimum and force sums: warps by shuffle, then warp 0 over the warps
+    // (buffers alternate by ring, so one barrier per ring suffices)
+    const int pb = t & 1;
     lmin = warp_min_f(lmin);
-    if (l == 0) s_min[w] = lmin;
+    if (l == 0) s_min[pb][w] = lmin;
 #pragma unroll
     for (int b = 0; b < NB; b++) {
       if (b < nbody) {
         double fx = warp_sum_d(sfx[b]);
         double fy = warp_sum_d(sfy[b]);
         if (l == 0) {
-          s_red[2 * b][w] = fx;
-          s_red[2 * b + 1][w] = fy;
+          s_red[pb][2 * b][w] = fx;
+          s_red[pb][2 * b + 1][w] = fy;
         }
       }
     }
     __syncthreads();
     if (w == 0) {
       if (l == 0) {
-        float m = s_min[0];
+        float m = s_min[pb][0];
         for (int q = 1; q < kThreads / 32; q++)
-          if (s_min[q] < m) m = s_min[q];
+          if (s_min[pb][q] < m) m = s_min[pb][q];
         D.ringmin[i] = m;
       }
       if (l < 2 * nbody) {
         double acc = 0.0;
-        for (int q = 0; q < kThreads / 32; q++) acc += s_red[l][q];
+        for (int q = 0; q < kThreads / 32; q++) acc += s_red[pb][l][q];
         const int b = l >> 1, comp = l & 1;  // comp 0: x, 1: y
         const bool inner = D.Rmed[i] < s_b[4][b];
         double* P = D.partials + (size_t)i * 4 * FARGO_MAXBODY + 4 * b + 2 * comp;
         P[0] = inner ? acc : 0.0;  // f*_inner
         P[1] = inner ? 0.0 : acc;  // f*_outer
       }
-      // the block that completes this disk's last ring finishes the substep
-      __threadfence();
-      __syncwarp();
-      if (l == 0) s_ticket = atomicAdd(&C->counter, 1u);
     }
-    __syncthreads();
-    if (s_ticket == (unsigned)(D.nrad - 1)) {
-      __threadfence();
-      finish_cfl_and_planets(D, C, &sC, s_min, s_sum, s_work);
-    }
+    run++;
   }
+  finish_run();
 }
 
 // ----------------------------------------------------------- source terms
@@ -1202,7 +1216,11 @@ __device__ __forceinline__ void rad_march(const DiskDev& D, int ia, int ib, int 
   rad_slopes<nq>(D, ia, R0, R1, R2, G1, gs1);  // slope at row i
   float vr0 = __ldg(D.vrad + (long long)ia * nsec + g);
   rad_face<nq>(D, ia, vr0, dt, R0, R1, G0, gs0, G1, gs1, qs, ds);
-  for (int i = ia; i < ib; i++) {
+  // at most FARGO_BAND rings: unrolled, so that later rows load early
+#pragma unroll
+  for (int k = 0; k < FARGO_BAND; k++) {
+    const int i = ia + k;
+    if (i >= ib) break;
     RadRow<nq> R3 = rad_row<nq>(D, i + 2, g, gp, Om);
     float G2[nq], gs2;
     rad_slopes<nq>(D, i + 1, R1, R2, R3, G2, gs2);  // slope at row i+1
