@@ -43,6 +43,7 @@ struct fargo_batch {
   long long* d_cell_off = nullptr;
   int* d_ring_off = nullptr;
   int4* d_theta = nullptr;
+  int seg_out = FARGO_SEG_OUT;  // transport segment width in use (autotuned)
   int* d_flags = nullptr;
   int* d_act = nullptr;  // every compacted-list array in one allocation
   long long* d_act_cell = nullptr;
@@ -405,6 +406,64 @@ fargo_status build_graph(fargo_batch* b) {
   return FARGO_OK;
 }
 
+// Transport work items of every disk: bands of FARGO_BAND rings, each in
+// nseg near-equal azimuthal segments of at most seg_out sectors; isothermal
+// and adiabatic disks in separate lists.  Sets each disk's item0 / nitems
+// (host copy) and returns the widest segment.
+int build_items(fargo_batch* b, int seg_out, std::vector<int4>& theta_iso, std::vector<int4>& theta_adi) {
+  int seg_max = 0;
+  theta_iso.clear();
+  theta_adi.clear();
+  for (int d = 0; d < (int)b->disks.size(); d++) {
+    DiskHost& h = b->disks[d];
+    const int nrad = h.p.NRAD, nsec = h.p.NSEC;
+    std::vector<int4>& theta = h.p.Adiabatic ? theta_adi : theta_iso;
+    h.dev.item0 = (int)theta.size();
+    const int nseg = (nsec + seg_out - 1) / seg_out;
+    const int seg = (nsec + nseg - 1) / nseg;
+    for (int i = 0; i < nrad; i += FARGO_BAND) {
+      for (int j0 = 0; j0 < nsec; j0 += seg) {
+        int S = std::min(seg, nsec - j0);
+        theta.push_back(make_int4(d, i, j0, S));
+        seg_max = std::max(seg_max, S);
+      }
+    }
+    h.dev.nitems = (int)theta.size() - h.dev.item0;
+  }
+  b->seg_out = seg_out;
+  return seg_max;
+}
+
+// Replace the batch's transport items (device list, per-disk item0/nitems,
+// grid) with those for seg_out.
+fargo_status install_items(fargo_batch* b, int seg_out) {
+  std::vector<int4> theta_iso, theta_adi;
+  int seg_max = build_items(b, seg_out, theta_iso, theta_adi);
+  CK(cudaStreamSynchronize(b->stream));
+  if (b->d_theta) CK(cudaFree(b->d_theta));
+  b->d_theta = nullptr;
+  CK(cudaMalloc(&b->d_theta, sizeof(int4) * (theta_iso.size() + theta_adi.size() + 1)));
+  if (!theta_iso.empty())
+    CK(cudaMemcpy(b->d_theta, theta_iso.data(), sizeof(int4) * theta_iso.size(), cudaMemcpyHostToDevice));
+  if (!theta_adi.empty())
+    CK(cudaMemcpy(b->d_theta + theta_iso.size(), theta_adi.data(), sizeof(int4) * theta_adi.size(),
+                  cudaMemcpyHostToDevice));
+  for (int d = 0; d < (int)b->disks.size(); d++)
+    CK(cudaMemcpy(&b->d_disks[d].item0, &b->disks[d].dev.item0, 2 * sizeof(int), cudaMemcpyHostToDevice));
+  BatchDev& bd = b->bd;
+  bd.theta_iso = b->d_theta;
+  bd.theta_adi = b->d_theta + theta_iso.size();
+  bd.ntheta_iso = (int)theta_iso.size();
+  bd.ntheta_adi = (int)theta_adi.size();
+  bd.theta_seg = seg_max;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+  long long tiles = 0;
+  for (auto& h : b->disks) tiles += ((long long)h.dev.nrad * h.dev.nsec + 255) / 256;
+  CK(fargo_size_grids(bd, nsm, tiles, (int)(theta_iso.size() + theta_adi.size())));
+  return FARGO_OK;
+}
+
 fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, const fargo_planets* planets,
                           const double* const* radii, int device) {
   int ndev = 0;
@@ -438,21 +497,8 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     b->n_sg += h.p.SelfGravity ? 1 : 0;
     any_bc |= (h.p.OpenInner || h.p.NonReflecting || h.p.Evanescent) ? 1 : 0;
     max_body = std::max(max_body, body_count(&planets[d]));
-    std::vector<int4>& theta = h.p.Adiabatic ? theta_adi : theta_iso;
-    h.dev.item0 = (int)theta.size();
-    // bands of FARGO_BAND rings, each in nseg near-equal azimuthal segments
-    // of at most FARGO_SEG_OUT sectors
-    const int nseg = (nsec + FARGO_SEG_OUT - 1) / FARGO_SEG_OUT;
-    const int seg = (nsec + nseg - 1) / nseg;
-    for (int i = 0; i < nrad; i += FARGO_BAND) {
-      for (int j0 = 0; j0 < nsec; j0 += seg) {
-        int S = std::min(seg, nsec - j0);
-        theta.push_back(make_int4(d, i, j0, S));
-        seg_max = std::max(seg_max, S);
-      }
-    }
-    h.dev.nitems = (int)theta.size() - h.dev.item0;
   }
+  seg_max = build_items(b, FARGO_SEG_OUT, theta_iso, theta_adi);
   CK(cudaMalloc(&b->d_disks, sizeof(DiskDev) * n));
   CK(cudaMalloc(&b->d_ctl, sizeof(DiskCtl) * n));
   CK(cudaMemsetAsync(b->d_ctl, 0, sizeof(DiskCtl) * n, b->stream));
@@ -1021,6 +1067,53 @@ fargo_status fargo_set_graph_mode(fargo_ctx* ctx, int use_graph) {
   if (!ctx) return FARGO_EINVAL;
   ctx->b.use_graph = use_graph != 0;
   return build_graph(&ctx->b);
+}
+
+// Autotuner of the transport tile: the azimuthal segment width (output
+// sectors per CTA) decides the threads left idle in the last segment of a
+// ring, the halo overhead and the number of CTAs.  Each candidate is
+// installed and the transport kernels are timed on the current state (they
+// write only scratch); the fastest stays and the graph is rebuilt.
+fargo_status batch_autotune(fargo_batch* b, int reps, int* chosen) {
+  if (!b || reps < 1) return FARGO_EINVAL;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  static const int cand[] = {96, 128, 160, 192, 224, 248};
+  fargo_launch_dt_begin(b->bd, b->stream);  // every disk active (the next DT starts the same way)
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best_ms = 1e30f;
+  int best = b->seg_out;
+  for (int c : cand) {
+    fargo_status st = install_items(b, c);
+    if (st) return st;
+    fargo_launch_transport(b->bd, b->stream);
+    CK(cudaEventRecord(e0, b->stream));
+    for (int r = 0; r < reps; r++) fargo_launch_transport(b->bd, b->stream);
+    CK(cudaEventRecord(e1, b->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaGetLastError());
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  fargo_status st = install_items(b, best);
+  if (st) return st;
+  if (chosen) *chosen = best;
+  return build_graph(b);
+}
+
+fargo_status fargo_batch_autotune(fargo_batch* b, int reps, int* seg_out) { return batch_autotune(b, reps, seg_out); }
+
+fargo_status fargo_autotune(fargo_ctx* ctx, int reps, int* seg_out) {
+  if (!ctx) return FARGO_EINVAL;
+  return batch_autotune(&ctx->b, reps, seg_out);
 }
 
 fargo_status fargo_batch_set_graph_mode(fargo_batch* b, int use_graph) {

@@ -183,3 +183,4 @@ void fargo_launch_diagnostics(const BatchDev& b, int disk, double* out3, int nbl
 int fargo_substep_launches(const BatchDev& b);
 cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int nitems);
 const void* fargo_cfl_kernel(int max_body);
+void fargo_launch_transport(const BatchDev& b, cudaStream_t s);

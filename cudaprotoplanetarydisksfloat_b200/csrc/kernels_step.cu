@@ -1097,6 +1097,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
 
 // ------------------------------------------------------------- transport
 
+// Transport arithmetic is FP32 throughout, and free of multiply-add
+// contraction: every product that meets an addition is an explicit
+// round-to-nearest multiply (fm), so each cell's result does not depend on
+// how the work is cut into bands, segments and unrolled steps (the compiler
+// may contract the same expression differently in different code paths).
+// The reference's own arithmetic, and the oracle's, is uncontracted too.
+//
 // Transport arithmetic is FP32 throughout.  The reference writes several
 // of these expressions with double literals (0.5, 2.0, 1e-20), which
 // promotes them to double; here each is the same expression in float, the
@@ -1110,10 +1117,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
 // differs from IEEE division by more than that.
 
 // van Leer slope of StarRadKernel (Kernels.cu:917-927)
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+
 __device__ __forceinline__ float vl_rad_slope(float qm, float q0, float qp, float invdm, float invdp) {
-  float dqm = (q0 - qm) * invdm;
-  float dqp = (qp - q0) * invdp;
-  if (dqp * dqm > 0.0f) return __fdividef(2.0f * dqp * dqm, dqp + dqm);
+  float dqm = fm(q0 - qm, invdm);
+  float dqp = fm(qp - q0, invdp);
+  if (fm(dqp, dqm) > 0.0f) return __fdividef(fm(fm(2.0f, dqp), dqm), dqp + dqm);
   return 0.0f;
 }
 
@@ -1138,15 +1147,15 @@ __device__ __forceinline__ RadRow<nq> rad_row(const DiskDev& D, int r, int g, in
   const float sg = __ldg(D.dens + lr);
   const float rm = __ldg(D.Rmed + r);
   R.S = sg;
-  R.Q[0] = sg * __ldg(D.vrad + lr + nsec);
-  R.Q[1] = sg * __ldg(D.vrad + lr);
-  R.Q[2] = sg * (__ldg(D.vtheta + lrp) + rm * Om) * rm;
-  R.Q[3] = sg * (__ldg(D.vtheta + lr) + rm * Om) * rm;
+  R.Q[0] = fm(sg, __ldg(D.vrad + lr + nsec));
+  R.Q[1] = fm(sg, __ldg(D.vrad + lr));
+  R.Q[2] = fm(fm(sg, __ldg(D.vtheta + lrp) + fm(rm, Om)), rm);
+  R.Q[3] = fm(fm(sg, __ldg(D.vtheta + lr) + fm(rm, Om)), rm);
   if (nq == 6) R.Q[4] = __ldg(D.energy + lr);
   R.Q[nq - 1] = sg;
   const float rden = __fdividef(1.0f, sg + 1e-20f);
 #pragma unroll
-  for (int c = 0; c < nq; c++) R.W[c] = R.Q[c] * rden;
+  for (int c = 0; c < nq; c++) R.W[c] = fm(R.Q[c], rden);
   return R;
 }
 
@@ -1182,16 +1191,16 @@ __device__ __forceinline__ void rad_face(const DiskDev& D, int b, float vr, floa
     return;
   }
   if (vr > 0.0f) {
-    const float h = (__ldg(D.Rmed + b) - __ldg(D.Rmed + b - 1) - vr * dt) * 0.5f;
+    const float h = fm(__ldg(D.Rmed + b) - __ldg(D.Rmed + b - 1) - fm(vr, dt), 0.5f);
 #pragma unroll
-    for (int c = 0; c < nq; c++) qs[c] = lo.W[c] + h * glo[c];
-    ds = lo.S + h * gslo;
+    for (int c = 0; c < nq; c++) qs[c] = lo.W[c] + fm(h, glo[c]);
+    ds = lo.S + fm(h, gslo);
   } else {
     const float rp = (b + 1 <= nrad - 1) ? __ldg(D.Rmed + b + 1) : 0.0f;  // only meets a zero slope
-    const float h = (rp - __ldg(D.Rmed + b) + vr * dt) * 0.5f;
+    const float h = fm(rp - __ldg(D.Rmed + b) + fm(vr, dt), 0.5f);
 #pragma unroll
-    for (int c = 0; c < nq; c++) qs[c] = hi.W[c] - h * ghi[c];
-    ds = hi.S - h * gshi;
+    for (int c = 0; c < nq; c++) qs[c] = hi.W[c] - fm(h, ghi[c]);
+    ds = hi.S - fm(h, gshi);
   }
 }
 
@@ -1231,9 +1240,9 @@ __device__ __forceinline__ void rad_march(const DiskDev& D, int ia, int ib, int 
     float* o = out + (i - ia) * ostride_r;
 #pragma unroll
     for (int c = 0; c < nq; c++) {
-      float varq = dt * dtheta * Ri * qs[c] * ds * vr0;
-      varq -= dt * dtheta * Rs * qs1[c] * ds1 * vr1;
-      o[c * ostride_c] = R1.Q[c] + varq * iS;
+      float varq = fm(fm(fm(fm(fm(dt, dtheta), Ri), qs[c]), ds), vr0);
+      varq -= fm(fm(fm(fm(fm(dt, dtheta), Rs), qs1[c]), ds1), vr1);
+      o[c * ostride_c] = R1.Q[c] + fm(varq, iS);
       if (c == nq - 1 && i == 0 && lost0) *lost0 = varq;
     }
     R1 = R2;
@@ -1380,7 +1389,7 @@ __device__ __forceinline__ void sweep_ring(float* sRr, int off, int L, float VMe
     if (x <= 0 || x >= L - 1) return 0.0f;
     float dqm = (w0 - wm);
     float dqp = (wp - w0);
-    if (dqp * dqm > 0.0f) return __fdividef(dqp * dqm, dqp + dqm) * invdxtheta;
+    if (fm(dqp, dqm) > 0.0f) return fm(__fdividef(fm(dqp, dqm), dqp + dqm), invdxtheta);
     return 0.0f;
   };
   for (int sweep = 0; sweep < 2; sweep++) {
@@ -1399,18 +1408,18 @@ __device__ __forceinline__ void sweep_ring(float* sRr, int off, int L, float VMe
     // DensStar (StarThetaKernel2 on the density)
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-      const float ksi = vv[k] * dt;
+      const float ksi = fm(vv[k], dt);
       if (ksi > 0.0f)
-        sD[k] = (x0 + k > 0) ? (k ? S[k - 1] : Sl) + (dxtheta - ksi) * (k ? GS[k - 1] : GSl) : 0.0f;
+        sD[k] = (x0 + k > 0) ? (k ? S[k - 1] : Sl) + fm(dxtheta - ksi, k ? GS[k - 1] : GSl) : 0.0f;
       else
-        sD[k] = S[k] - (dxtheta + ksi) * GS[k];
+        sD[k] = S[k] - fm(dxtheta + ksi, GS[k]);
     }
     // every quantity, density last; all quotients use the pre-sweep density
 #pragma unroll
     for (int c = 0; c < nq; c++) {
       float W[8], G[8], F[8];
 #pragma unroll
-      for (int k = 0; k < 8; k++) W[k] = q[c][k] * rr[k];
+      for (int k = 0; k < 8; k++) W[k] = fm(q[c][k], rr[k]);
       const float Wl = __shfl_up_sync(0xffffffffu, W[7], 1);
       const float Wr = __shfl_down_sync(0xffffffffu, W[0], 1);
 #pragma unroll
@@ -1418,13 +1427,13 @@ __device__ __forceinline__ void sweep_ring(float* sRr, int off, int L, float VMe
       const float Gl = __shfl_up_sync(0xffffffffu, G[7], 1);
 #pragma unroll
       for (int k = 0; k < 8; k++) {
-        const float ksi = vv[k] * dt;
+        const float ksi = fm(vv[k], dt);
         float qr;
         if (ksi > 0.0f)
-          qr = (x0 + k > 0) ? (k ? W[k - 1] : Wl) + (dxtheta - ksi) * (k ? G[k - 1] : Gl) : 0.0f;
+          qr = (x0 + k > 0) ? (k ? W[k - 1] : Wl) + fm(dxtheta - ksi, k ? G[k - 1] : Gl) : 0.0f;
         else
-          qr = W[k] - (dxtheta + ksi) * G[k];
-        F[k] = dxrad * qr * sD[k] * vv[k];  // flux through the left interface of point k
+          qr = W[k] - fm(dxtheta + ksi, G[k]);
+        F[k] = fm(fm(fm(dxrad, qr), sD[k]), vv[k]);  // flux through the left interface of point k
       }
       const float Fr = __shfl_down_sync(0xffffffffu, F[0], 1);
 #pragma unroll
@@ -1432,7 +1441,7 @@ __device__ __forceinline__ void sweep_ring(float* sRr, int off, int L, float VMe
         if (x0 + k < L - 1) {
           float varq = F[k];
           varq -= (k < 7 ? F[k + 1] : Fr);
-          q[c][k] += varq * invsurf;
+          q[c][k] += fm(varq, invsurf);
         }
       }
     }
@@ -1521,9 +1530,9 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
         const int off = ws - u0;
         float* sRr = sR + (size_t)(r - rb) * (nq + 1) * kPad;
         const float Rm = D.Rmed[i];
-        const float dxtheta = dtheta * Rm;
+        const float dxtheta = fm(dtheta, Rm);
         sweep_ring<nq>(sRr, off, L, s_vmed[r], s_vc[r], fast, dt, dxtheta, 1.0f / dxtheta, 1.0f / D.Surf[i],
-                       (D.Rsup[i] - D.Rinf[i]) * dt);
+                       fm(D.Rsup[i] - D.Rinf[i], dt));
         // output sector j0 + x - 4 takes window point x: coalesced stores
         float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.a1, D.a0};
         const long long row = (long long)i * nsec + j0 - 4;
@@ -2114,6 +2123,15 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   REC();
 #undef REC
   if (launches) *launches += fargo_substep_launches(b);
+}
+
+// The transport kernels alone (both forms), for the autotuner: they read the
+// state and the last substep's ring means and write only scratch.
+void fargo_launch_transport(const BatchDev& b, cudaStream_t s) {
+  if (b.ntheta_iso)
+    k_transport<5><<<std::min(b.g_transport, b.ntheta_iso), kTT, fargo_transport_smem_bytes(0), s>>>(b, b.theta_iso);
+  if (b.ntheta_adi)
+    k_transport<6><<<std::min(b.g_transport, b.ntheta_adi), kTT, fargo_transport_smem_bytes(1), s>>>(b, b.theta_adi);
 }
 
 // The CFL/force kernel instance for up to max_body bodies.

@@ -143,6 +143,12 @@ class Disk:
     def set_graph_mode(self, on):
         self._chk(lib.fargo_set_graph_mode(self.ctx, 1 if on else 0), "fargo_set_graph_mode")
 
+    def autotune(self, reps=3):
+        """Pick the transport segment width by timing (between DTs); returns it."""
+        seg = C.c_int(0)
+        self._chk(lib.fargo_autotune(self.ctx, reps, C.byref(seg)), "fargo_autotune")
+        return seg.value
+
     def close(self):
         if self.ctx:
             lib.fargo_destroy(self.ctx)
@@ -203,6 +209,12 @@ class Batch:
 
     def set_graph_mode(self, on):
         self._chk(lib.fargo_batch_set_graph_mode(self.b, 1 if on else 0), "fargo_batch_set_graph_mode")
+
+    def autotune(self, reps=3):
+        """Pick the transport segment width by timing (between DTs); returns it."""
+        seg = C.c_int(0)
+        self._chk(lib.fargo_batch_autotune(self.b, reps, C.byref(seg)), "fargo_batch_autotune")
+        return seg.value
 
     def sync(self):
         self._chk(lib.fargo_batch_sync(self.b), "fargo_batch_sync")

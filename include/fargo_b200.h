@@ -267,6 +267,11 @@ const char* fargo_profile_kernel_name(int k);
    over the substeps; 0: host loop with one wait per substep. */
 fargo_status fargo_set_graph_mode(fargo_ctx* ctx, int use_graph);
 fargo_status fargo_batch_set_graph_mode(fargo_batch* b, int use_graph);
+/* (new) Tile autotuner: times the transport kernels on the current state for
+   azimuthal segment widths 96..248 sectors and keeps the fastest (*seg_out).
+   Call between DTs; the state is not advanced. */
+fargo_status fargo_batch_autotune(fargo_batch* b, int reps, int* seg_out);
+fargo_status fargo_autotune(fargo_ctx* ctx, int reps, int* seg_out);
 
 #ifdef __cplusplus
 }
