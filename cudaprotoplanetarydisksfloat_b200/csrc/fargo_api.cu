@@ -1079,7 +1079,6 @@ fargo_status batch_autotune(fargo_batch* b, int reps, int* chosen) {
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
   static const int cand[] = {96, 128, 160, 192, 224, 248};
-  fargo_launch_dt_begin(b->bd, b->stream);  // every disk active (the next DT starts the same way)
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -1088,6 +1087,9 @@ fargo_status batch_autotune(fargo_batch* b, int reps, int* chosen) {
   for (int c : cand) {
     fargo_status st = install_items(b, c);
     if (st) return st;
+    // every disk active, and the compacted item prefixes rebuilt for these
+    // items (the next DT starts the same way)
+    fargo_launch_dt_begin(b->bd, b->stream);
     fargo_launch_transport(b->bd, b->stream);
     CK(cudaEventRecord(e0, b->stream));
     for (int r = 0; r < reps; r++) fargo_launch_transport(b->bd, b->stream);
