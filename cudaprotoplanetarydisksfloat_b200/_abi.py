@@ -84,7 +84,8 @@ EXPORTS = [
     "fargo_batch_init_state", "fargo_batch_upload", "fargo_batch_download", "fargo_batch_advance",
     "fargo_batch_advance_async", "fargo_batch_sync", "fargo_batch_get_scalars",
     "fargo_batch_get_planets", "fargo_batch_count_launches", "fargo_batch_kernel_launches", "fargo_abi_version",
-    "fargo_kernel_launches", "fargo_set_graph_mode", "fargo_batch_set_graph_mode", "fargo_batch_autotune", "fargo_autotune", "fargo_stream", "fargo_batch_stream",
+    "fargo_kernel_launches", "fargo_set_graph_mode", "fargo_batch_set_graph_mode", "fargo_batch_autotune", "fargo_autotune", "fargo_checkpoint_bytes", "fargo_checkpoint_save",
+    "fargo_checkpoint_load", "fargo_stream", "fargo_batch_stream",
     "fargo_ctx_batch", "fargo_batch_upload_async", "fargo_batch_download_async", "fargo_batch_profile",
     "fargo_profile_kernel_name", "fargo_profile_kernel_count",
 ]
@@ -146,6 +147,9 @@ def _load():
         "fargo_batch_set_graph_mode": (C.c_int, [vp, C.c_int]),
         "fargo_batch_autotune": (C.c_int, [vp, C.c_int, P(C.c_int)]),
         "fargo_autotune": (C.c_int, [vp, C.c_int, P(C.c_int)]),
+        "fargo_checkpoint_bytes": (C.c_size_t, [vp]),
+        "fargo_checkpoint_save": (C.c_int, [vp, vp, C.c_size_t]),
+        "fargo_checkpoint_load": (C.c_int, [vp, vp, C.c_size_t]),
         "fargo_stream": (vp, [vp]),
         "fargo_batch_stream": (vp, [vp]),
         "fargo_ctx_batch": (vp, [vp]),

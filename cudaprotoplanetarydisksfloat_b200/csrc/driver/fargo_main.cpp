@@ -5,11 +5,24 @@
 // path (AlgoGas) running through the C ABI of libfargo_b200.so.  Output
 // formats are kept byte-compatible on purpose, so the reference's
 // post-processing (plot2d.py and friends) reads them unchanged.
+//
+// Two additions: every output also writes checkpointN.bin (the device state,
+// fargo_checkpoint_save), so that -s N, which the reference parses but never
+// acts on, restarts from output N and continues the run bit for bit; and
+// output files are written by a writer thread while the next DTs run (the
+// console messages stay in the reference's order, printed by the main
+// thread).
 #include <sys/stat.h>
 #include <sys/types.h>
 
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <thread>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -112,27 +125,74 @@ static void die(fargo_ctx* ctx, fargo_status st, const char* what) {
   std::exit(1);
 }
 
-// WriteDiskPolar, Output.cu:104-135
-static void write_disk_polar(const std::string& outdir, const float* a, const char* name, int number, int nrad,
-                             int nsec) {
+// Output files are written here, in order, while the main thread advances.
+class Writer {
+ public:
+  Writer() : t_([this] { loop(); }) {}
+  ~Writer() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      done_ = true;
+    }
+    cv_.notify_one();
+    t_.join();
+  }
+  void push(std::function<void()> job) {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      q_.push_back(std::move(job));
+    }
+    cv_.notify_one();
+  }
+
+ private:
+  void loop() {
+    for (;;) {
+      std::function<void()> job;
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [this] { return done_ || !q_.empty(); });
+        if (q_.empty()) return;
+        job = std::move(q_.front());
+        q_.pop_front();
+      }
+      job();
+    }
+  }
+  std::mutex m_;
+  std::condition_variable cv_;
+  std::deque<std::function<void()>> q_;
+  bool done_ = false;
+  std::thread t_;
+};
+
+static void write_file(const std::string& fn, const void* data, size_t bytes) {
+  FILE* f = std::fopen(fn.c_str(), "wb");
+  if (!f) {
+    std::fprintf(stderr, "Unable to open '%s'\n", fn.c_str());
+    std::exit(1);
+  }
+  std::fwrite(data, 1, bytes, f);
+  std::fclose(f);
+}
+
+// WriteDiskPolar, Output.cu:104-135: the message now, the file by the writer
+static void write_disk_polar(Writer& w, const std::string& outdir, const std::vector<float>& a, const char* name,
+                             int number, int nrad, int nsec) {
   std::string url = outdir + name;
   struct stat st;
   if (stat(url.c_str(), &st) == -1) mkdir(url.c_str(), 0700);
   char fn[1024];
   std::snprintf(fn, sizeof(fn), "%s%s/%s%d.dat", outdir.c_str(), name, name, number);
-  FILE* f = std::fopen(fn, "w");
-  if (!f) {
-    std::fprintf(stderr, "Unable to open '%s'\n", fn);
-    std::exit(1);
-  }
   std::printf("Writting '%s%d.dat'... ", name, number);
-  std::fwrite(a, sizeof(float), (size_t)nrad * nsec, f);
-  std::fclose(f);
+  auto copy = std::make_shared<std::vector<float>>(a.begin(), a.begin() + (size_t)nrad * nsec);
+  std::string path = fn;
+  w.push([copy, path] { write_file(path, copy->data(), copy->size() * sizeof(float)); });
   std::printf("done\n");
 }
 
 int main(int argc, char** argv) {
-  int disable = 0, verbose = 0, sloppy = 0, restart = 0, overrides = 0;
+  int disable = 0, verbose = 0, sloppy = 0, restart = 0, overrides = 0, nb_restart = 0;
   float scaling = 1.0f;
   char parfile[1024] = "";
   std::string newout;
@@ -150,6 +210,7 @@ int main(int argc, char** argv) {
           std::printf("Incorrect restart number\n");
           usage(argv[0]);
         }
+        nb_restart = std::atoi(argv[i]);
       }
       if (std::strchr(argv[i], 'o')) {
         overrides = 1;
@@ -168,7 +229,6 @@ int main(int argc, char** argv) {
       std::snprintf(parfile, sizeof(parfile), "%s", argv[i]);
     }
   }
-  (void)restart;
   if (parfile[0] == 0) usage(argv[0]);
   fargo_params p;
   fargo_status st = fargo_params_read(parfile, &p);
@@ -318,8 +378,29 @@ int main(int argc, char** argv) {
   std::memset(&sc, 0, sizeof(sc));
   float mdcp1 = 0.0f, lost = 0.0f;
   int TimeStep = 0;
+  int begin_i = 0;
+  if (restart) {
+    // the state saved with output nb_restart; the loop resumes at that output
+    char fn[1024];
+    std::snprintf(fn, sizeof(fn), "%scheckpoint%d.bin", outdir.c_str(), nb_restart);
+    FILE* f = std::fopen(fn, "rb");
+    if (!f) {
+      std::fprintf(stderr, "Can't read restart file %s\n", fn);
+      return 1;
+    }
+    std::vector<char> ck(fargo_checkpoint_bytes(ctx));
+    size_t got = std::fread(ck.data(), 1, ck.size(), f);
+    std::fclose(f);
+    st = fargo_checkpoint_load(ctx, ck.data(), got);
+    if (st != FARGO_OK) die(ctx, st, "fargo_checkpoint_load");
+    fargo_get_scalars(ctx, &sc);
+    mdcp1 = sc.mdcp1;
+    lost = sc.lost_mass;
+    begin_i = nb_restart * p.NINTERM;
+  }
+  Writer writer;
   auto start = std::chrono::steady_clock::now();
-  for (int i = 0; i <= p.NTOT; i++) {
+  for (int i = begin_i; i <= p.NTOT; i++) {
     fargo_get_planets(ctx, &sys);
     // WriteBigPlanetSystemFile (every DT, Main.cu:349-355; Output.cu:70-102):
     // the planet values pass through static floats
@@ -390,16 +471,23 @@ int main(int argc, char** argv) {
       if (st != FARGO_OK) die(ctx, st, "fargo_download");
       std::printf("\n*** OUTPUT %d ***\n", TimeStep);
       if (p.IsDisk) {
-        if (p.Write_Density) write_disk_polar(outdir, dens.data(), "dens", TimeStep, NRAD, NSEC);
+        if (p.Write_Density) write_disk_polar(writer, outdir, dens, "dens", TimeStep, NRAD, NSEC);
         if (p.Write_Velocity) {
-          write_disk_polar(outdir, vrad.data(), "vrad", TimeStep, NRAD, NSEC);
-          write_disk_polar(outdir, vtheta.data(), "vtheta", TimeStep, NRAD, NSEC);
+          write_disk_polar(writer, outdir, vrad, "vrad", TimeStep, NRAD, NSEC);
+          write_disk_polar(writer, outdir, vtheta, "vtheta", TimeStep, NRAD, NSEC);
         }
-        if (p.Write_Energy) write_disk_polar(outdir, energy.data(), "energy", TimeStep, NRAD, NSEC);
-        if (p.Write_Temperature) write_disk_polar(outdir, temperature.data(), "temperature", TimeStep, NRAD, NSEC);
-        if (p.Write_Qplus) write_disk_polar(outdir, qplus.data(), "qplus", TimeStep, NRAD, NSEC);
-        if (p.AdvecteLabel) write_disk_polar(outdir, label.data(), "label", TimeStep, NRAD, NSEC);
+        if (p.Write_Energy) write_disk_polar(writer, outdir, energy, "energy", TimeStep, NRAD, NSEC);
+        if (p.Write_Temperature) write_disk_polar(writer, outdir, temperature, "temperature", TimeStep, NRAD, NSEC);
+        if (p.Write_Qplus) write_disk_polar(writer, outdir, qplus, "qplus", TimeStep, NRAD, NSEC);
+        if (p.AdvecteLabel) write_disk_polar(writer, outdir, label, "label", TimeStep, NRAD, NSEC);
       }
+      auto ck = std::make_shared<std::vector<char>>(fargo_checkpoint_bytes(ctx));
+      st = fargo_checkpoint_save(ctx, ck->data(), ck->size());
+      if (st != FARGO_OK) die(ctx, st, "fargo_checkpoint_save");
+      char fn[1024];
+      std::snprintf(fn, sizeof(fn), "%scheckpoint%d.bin", outdir.c_str(), TimeStep);
+      std::string path = fn;
+      writer.push([ck, path] { write_file(path, ck->data(), ck->size()); });
     }
     int nsub = 0;
     st = fargo_advance_dt(ctx, &nsub);

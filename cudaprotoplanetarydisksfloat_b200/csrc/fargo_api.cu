@@ -745,6 +745,81 @@ fargo_status fargo_download(fargo_ctx* ctx, float* dens, float* vrad, float* vth
   return download_impl(&ctx->b, 0, dens, vrad, vtheta, energy, temperature, qplus);
 }
 
+// ---------------------------------------------------------------- checkpoints
+
+// Everything a later DT reads from the device that the next DT does not
+// rebuild itself: the control block (time, frame, planets, DT bookkeeping),
+// the state fields with their ghost rows, the temperature-output pressure,
+// Q+, the adiabatic sound speed and the per-ring sound speed, mean sound
+// speed and viscosity.
+struct CkptPart {
+  void* dev;
+  size_t bytes;
+};
+static std::vector<CkptPart> ckpt_parts(fargo_batch* b, int d) {
+  const DiskHost& h = b->disks[d];
+  const DiskDev& D = h.dev;
+  const size_t ng = sizeof(float) * (size_t)(D.nrad + 1) * D.nsec, n1 = sizeof(float) * (size_t)(D.nrad + 1);
+  std::vector<CkptPart> v = {{b->d_ctl + d, sizeof(DiskCtl)}, {D.dens, ng},  {D.vrad, ng},    {D.vtheta, ng},
+                             {D.energy, ng},                 {D.pres, ng},  {D.qplus, ng},   {D.visc, n1},
+                             {D.cs_ring, n1},                {D.csmean, n1}};
+  if (h.p.Adiabatic) v.push_back({D.cs, ng});
+  return v;
+}
+static const unsigned kCkptMagic = 0x43324246u;  // "FB2C"
+struct CkptHeader {
+  unsigned magic, version;
+  int nrad, nsec, adiabatic, ctl_bytes;
+};
+static size_t ckpt_bytes(fargo_batch* b, int d) {
+  size_t n = sizeof(CkptHeader);
+  for (auto& p : ckpt_parts(b, d)) n += p.bytes;
+  return n;
+}
+
+size_t fargo_checkpoint_bytes(fargo_ctx* ctx) { return ctx ? ckpt_bytes(&ctx->b, 0) : 0; }
+
+fargo_status fargo_checkpoint_save(fargo_ctx* ctx, void* buf, size_t bytes) {
+  if (!ctx || !buf) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  if (bytes < ckpt_bytes(b, 0)) return set_err(b, FARGO_EINVAL, "checkpoint buffer too small");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  const DiskHost& h = b->disks[0];
+  CkptHeader hd = {kCkptMagic, 1u, h.p.NRAD, h.p.NSEC, h.p.Adiabatic, (int)sizeof(DiskCtl)};
+  char* o = static_cast<char*>(buf);
+  std::memcpy(o, &hd, sizeof(hd));
+  o += sizeof(hd);
+  for (auto& p : ckpt_parts(b, 0)) {
+    CK(cudaMemcpy(o, p.dev, p.bytes, cudaMemcpyDeviceToHost));
+    o += p.bytes;
+  }
+  return FARGO_OK;
+}
+
+fargo_status fargo_checkpoint_load(fargo_ctx* ctx, const void* buf, size_t bytes) {
+  if (!ctx || !buf) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  const DiskHost& h = b->disks[0];
+  CkptHeader hd;
+  if (bytes < sizeof(hd)) return set_err(b, FARGO_EINVAL, "checkpoint truncated");
+  std::memcpy(&hd, buf, sizeof(hd));
+  if (hd.magic != kCkptMagic || hd.version != 1u)
+    return set_err(b, FARGO_EINVAL, "not a checkpoint of this library");
+  if (hd.nrad != h.p.NRAD || hd.nsec != h.p.NSEC || hd.adiabatic != h.p.Adiabatic ||
+      hd.ctl_bytes != (int)sizeof(DiskCtl))
+    return set_err(b, FARGO_EINVAL, "checkpoint of a different grid or build (%dx%d)", hd.nrad, hd.nsec);
+  if (bytes < ckpt_bytes(b, 0)) return set_err(b, FARGO_EINVAL, "checkpoint truncated");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  const char* in = static_cast<const char*>(buf) + sizeof(hd);
+  for (auto& p : ckpt_parts(b, 0)) {
+    CK(cudaMemcpy(p.dev, in, p.bytes, cudaMemcpyHostToDevice));
+    in += p.bytes;
+  }
+  return FARGO_OK;
+}
+
 static fargo_status get_planets_impl(fargo_batch* b, int d, fargo_planets* out) {
   if (!b || !out || d < 0 || d >= (int)b->disks.size()) return FARGO_EINVAL;
   CK(cudaSetDevice(b->device));

@@ -149,6 +149,18 @@ class Disk:
         self._chk(lib.fargo_autotune(self.ctx, reps, C.byref(seg)), "fargo_autotune")
         return seg.value
 
+    def checkpoint(self):
+        """The device state as bytes (between DTs)."""
+        n = lib.fargo_checkpoint_bytes(self.ctx)
+        buf = C.create_string_buffer(n)
+        self._chk(lib.fargo_checkpoint_save(self.ctx, buf, n), "fargo_checkpoint_save")
+        return buf.raw
+
+    def restore(self, data):
+        """Load a state saved by checkpoint()."""
+        buf = C.create_string_buffer(data, len(data))
+        self._chk(lib.fargo_checkpoint_load(self.ctx, buf, len(data)), "fargo_checkpoint_load")
+
     def close(self):
         if self.ctx:
             lib.fargo_destroy(self.ctx)

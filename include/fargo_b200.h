@@ -206,6 +206,16 @@ fargo_status fargo_disk_force_noalloc(const float* dens, const float* cell_x, co
                                       int dimfxy, double* globalforce, void* stream, char* err,
                                       int errlen);
 
+/* Checkpoint / restart (new: the reference parses -s N, Main.cu:147-155, but
+   never restores a state).  A checkpoint is the device state a later DT
+   reads: control block (time, frame, planets in FP64), fields with their
+   ghost rows and the per-ring sound speed and viscosity.  Save and load
+   between DTs; loading into a context of the same grid and build continues
+   the run bit for bit. */
+size_t fargo_checkpoint_bytes(fargo_ctx* ctx);
+fargo_status fargo_checkpoint_save(fargo_ctx* ctx, void* buf, size_t bytes);
+fargo_status fargo_checkpoint_load(fargo_ctx* ctx, const void* buf, size_t bytes);
+
 /* Scalars after the last DT (also recomputes mdcp1, mass, angular momentum). */
 fargo_status fargo_get_scalars(fargo_ctx* ctx, fargo_scalars* out);
 
