@@ -507,8 +507,8 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   CK(cudaMalloc(&b->d_theta, sizeof(int4) * (theta_iso.size() + theta_adi.size() + 1)));
   CK(cudaMalloc(&b->d_flags, sizeof(int) * 4));
   // compacted active lists: act[4] + 3 disk lists + 3 int prefix arrays, and the cell prefix
-  CK(cudaMalloc(&b->d_act, sizeof(int) * (4 + 3 * n + 6 * (n + 1))));
-  CK(cudaMemsetAsync(b->d_act, 0, sizeof(int) * (4 + 3 * n + 6 * (n + 1)), b->stream));
+  CK(cudaMalloc(&b->d_act, sizeof(int) * (4 + 3 * n + 7 * (n + 1))));
+  CK(cudaMemsetAsync(b->d_act, 0, sizeof(int) * (4 + 3 * n + 7 * (n + 1)), b->stream));
   CK(cudaMalloc(&b->d_act_cell, sizeof(long long) * (n + 1)));
   CK(cudaMemsetAsync(b->d_act_cell, 0, sizeof(long long) * (n + 1), b->stream));
   b->red_blocks = 296;
@@ -549,6 +549,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   bd.act_grp_off = bd.act_adi_off + (n + 1);
   bd.act_tile_off = bd.act_grp_off + (n + 1);
   bd.act_ctile_off = bd.act_tile_off + (n + 1);
+  bd.act_vtile_off = bd.act_ctile_off + (n + 1);
   bd.act_cell_off = b->d_act_cell;
   {
     int nsm = 148;

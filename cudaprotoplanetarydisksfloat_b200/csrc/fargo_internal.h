@@ -155,15 +155,16 @@ struct BatchDev {
   int* act_grp_off;          // [ndisk+1] prefix of 32-ring groups of active disks
   int* act_tile_off;         // [ndisk+1] prefix of cell tiles (one block's cells) of active disks
   int* act_ctile_off;        // [ndisk+1] prefix of rings of active disks (CFL tiles)
+  int* act_vtile_off;        // [ndisk+1] prefix of viscosity tiles (8 x 64 cells) of active disks
   int cell_grid, ring_grid, item_grid, grp_grid;  // fixed grid sizes of the grid-stride kernels
   int any_bc;                // some disk has an OPEN, NONREFLECTING or EVANESCENT boundary
   int max_body;              // largest body count of the force sums (star + FeelDisk planets)
   // one-wave grids of the substep kernels (fargo_size_grids)
-  int g_cfl, g_source1, g_visc_tau, g_visc_update, g_source2, g_energy, g_velocities, g_transport;
+  int g_cfl, g_source1, g_viscosity, g_source2, g_energy, g_velocities, g_transport;
 };
 
 // kernel entry points (kernels_step.cu), launched by fargo_api.cu
-#define FARGO_NKERNELS 14  // profiled slots per substep (boundary slots empty for rigid boundaries)
+#define FARGO_NKERNELS 13  // profiled slots per substep (boundary slots empty for rigid boundaries)
 #define FARGO_SEG_OUT 192  // largest azimuthal transport segment (output sectors per CTA)
 #define FARGO_BAND 8       // rings per transport CTA
 cudaError_t fargo_kernel_attributes(int max_nsec);

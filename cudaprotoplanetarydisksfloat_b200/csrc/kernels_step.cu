@@ -14,8 +14,8 @@
 //                    FP64 RK5, frame rotation, per-ring viscosity)
 //   k_source1        Substep1 (pressure + potential + centrifugal kick),
 //                    potential evaluated on the fly, + self-gravity kick
-//   k_visc_tau       viscous stress tensor
-//   k_visc_update    viscous velocity update + sub-Keplerian boundary
+//   k_viscosity      viscous stress tensor + velocity update + sub-Keplerian
+//                    boundary on 8x64 tiles with halos in shared memory
 //   k_source2        artificial viscosity (Substep2) + energy predictor
 //   k_energy         viscous heating and implicit energy update (Substep3)
 //   k_ring_mean<1>   ring means of v_theta for FARGO: Nshift, residual
@@ -948,15 +948,6 @@ __device__ __forceinline__ Tau viscous_terms(const DiskDev& D, const float* Vr, 
   return t;
 }
 
-__global__ void __launch_bounds__(kThreads, 6) k_visc_tau(BatchDev B) {
-  CELL_BEGIN
-  Tau t = viscous_terms(D, D.vri, D.vti, i, j, nsec);
-  D.trr[l] = t.rr;
-  D.tpp[l] = t.pp;
-  if (i > 0) D.trp[l] = t.rp;
-  CELL_END
-}
-
 // Sub-Keplerian boundary speeds (SideEuler.cu:250-268), device double math
 // when they change with time or self-gravity.
 __device__ void vkep_pair(const DiskDev& D, const DiskCtl* C, float* vin, float* vout) {
@@ -979,33 +970,162 @@ __device__ void vkep_pair(const DiskDev& D, const DiskCtl* C, float* vin, float*
   *vout = sqrt(a1);
 }
 
-// UpdateVelocitiesKernel (Kernels.cu:142-160) in place, then
-// ApplySubKeplerianBoundaryKernel (Kernels.cu:1490-1503).
-__global__ void __launch_bounds__(kThreads, 6) k_visc_update(BatchDev B) {
-  CELL_BEGIN
-  const float DeltaT = C->dtf;
-  const float* Dn = D.dens;
-  const float *TRR = D.trr, *TRP = D.trp, *TPP = D.tpp;
-  const long long lmj = (long long)i * nsec + jm, lpj = (long long)i * nsec + jp;
-  if (i > 0 && i < nrad - 1) {
-    D.vti[l] += DeltaT * D.invRmed[i] *
-                ((D.Rsup[i] * TRP[l + nsec] - D.Rinf[i] * TRP[l]) * D.invdiffRsup[i] +
-                 (TPP[l] - TPP[lmj]) * D.invdphi + 0.5f * (TRP[l] + TRP[l + nsec])) /
-                (0.5f * (Dn[l] + Dn[lmj]));
+// ComputeViscousTerms + UpdateVelocitiesWithViscosity + the sub-Keplerian
+// boundary (Viscosity.cu:77-102, Kernels.cu:142-160, 843-880, 1490-1503)
+// fused on radial x azimuthal tiles of kVR x kVC cells.  The block stages
+// VradInt, VthetaInt and Sigma for the tile and a 2-cell halo in shared
+// memory (azimuth periodic), computes the stress tensor once for the tile
+// and a 1-cell halo into shared memory (the same arithmetic as
+// viscous_terms), then the updated velocities of its own cells.  They go to
+// the trr / tpp buffers (the stresses never reach HBM), which Substep2 then
+// reads as VradInt / VthetaInt: writing them in place would race with the
+// neighbouring tiles' halo reads.
+constexpr int kVR = 8, kVC = 64;                        // tile rows, columns
+constexpr int kSR = kVR + 4, kSC = kVC + 4;             // staged rows, columns
+constexpr int kTR = kVR + 2, kTC = kVC + 2;             // stress rows, columns
+__device__ __forceinline__ int vtiles_of(const DiskDev& D) {
+  return ((D.nrad + kVR - 1) / kVR) * ((D.nsec + kVC - 1) / kVC);
+}
+
+// 4-byte asynchronous global -> shared copy (zero-filled when !valid)
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = valid ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int n>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(n) : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
+  __shared__ DiskDev sD;
+  __shared__ float sVrb[2][kSR][kSC], sVab[2][kSR][kSC], sDnb[2][kSR][kSC], sD0b[2][kSR];
+  __shared__ float sTrr[kTR][kTC], sTpp[kTR][kTC], sTrp[kTR][kTC];
+  const int tid = threadIdx.x;
+  const int na = B.act[0];
+  const int ntile = na > 0 ? B.act_vtile_off[na] : 0;
+  const int per = (ntile + gridDim.x - 1) / gridDim.x;
+  const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
+  // issue the asynchronous staging of tile lt of the disk in sD into buffer bf:
+  // rows i0-2 .. i0+kVR+1 (row NRAD is the ghost row), columns j0-2 .. j0+kVC+1
+  auto stage = [&](int lt, int bf) {
+    const int nsec = sD.nsec, nrad = sD.nrad;
+    const int ncol = (nsec + kVC - 1) / kVC;
+    const int i0 = (lt / ncol) * kVR, j0 = (lt % ncol) * kVC;
+    for (int q = tid; q < kSR * kSC; q += kThreads) {
+      const int r = q / kSC, c = q - r * kSC;
+      const int i = i0 - 2 + r;
+      int j = (j0 - 2 + c) % nsec;
+      if (j < 0) j += nsec;
+      const bool ok = i >= 0 && i <= nrad;
+      const size_t l = ok ? (size_t)i * nsec + j : 0;
+      cp_async4(&sVrb[bf][r][c], sD.vri + l, ok);
+      cp_async4(&sVab[bf][r][c], sD.vti + l, ok);
+      cp_async4(&sDnb[bf][r][c], sD.dens + l, ok);
+    }
+    if (tid < kSR) {
+      const int i = i0 - 2 + tid;
+      const bool ok = i >= 0 && i <= nrad;
+      cp_async4(&sD0b[bf][tid], sD.dens + (ok ? (size_t)i * nsec : 0), ok);
+    }
+    cp_async_commit();
+  };
+  int lo = 0, hi = -1, bf = 0;
+  bool have = false;  // tile t already staged (prefetched) in buffer bf
+  for (int t = t0; t < t1; t++) {
+    if (t >= hi) {  // block-uniform: entering a disk
+      const int a = find_range(B.act_vtile_off, na, t);
+      lo = B.act_vtile_off[a];
+      hi = B.act_vtile_off[a + 1];
+      __syncthreads();
+      copy_words(&sD, B.disks + B.act_disk[a], sizeof(DiskDev));
+      __syncthreads();
+      have = false;
+    }
+    if (!have) stage(t - lo, bf);
+    // prefetch the next tile of the same disk while this one is computed
+    const bool pre = (t + 1 < t1) && (t + 1 < hi);
+    if (pre) {
+      stage(t + 1 - lo, bf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    float(*sVr)[kSC] = sVrb[bf];
+    float(*sVa)[kSC] = sVab[bf];
+    float(*sDn)[kSC] = sDnb[bf];
+    const float* sD0 = sD0b[bf];
+    const DiskDev& D = sD;
+    const DiskCtl* C = D.ctl;
+    const int nsec = D.nsec, nrad = D.nrad;
+    const int ncol = (nsec + kVC - 1) / kVC;
+    const int lt = t - lo;
+    const int i0 = (lt / ncol) * kVR, j0 = (lt % ncol) * kVC;
+    if (D.IsDisk) {
+      // stresses at rows i0-1 .. i0+kVR, columns j0-1 .. j0+kVC (viscous_terms)
+      for (int q = tid; q < kTR * kTC; q += kThreads) {
+        const int r = q / kTC, c = q - r * kTC;
+        const int i = i0 - 1 + r;
+        if (i < 0 || i >= nrad) continue;
+        const int rr = r + 1, cc = c + 1;  // staged indices of (i, j)
+        const float nu = D.visc[i];
+        const float iRm = D.invRmed[i];
+        float DRR = (sVr[rr + 1][cc] - sVr[rr][cc]) * D.invdiffRsup[i];
+        float DPP = (sVa[rr][cc + 1] - sVa[rr][cc]) * D.invdphi * iRm + 0.5f * (sVr[rr + 1][cc] + sVr[rr][cc]) * iRm;
+        float divV = (sVr[rr + 1][cc] * D.Rsup[i] - sVr[rr][cc] * D.Rinf[i]) * D.invdiffRsup[i] * iRm;
+        divV += (sVa[rr][cc + 1] - sVa[rr][cc]) * D.invdphi * iRm;
+        sTrr[r][c] = 2.0f * sDn[rr][cc] * nu * (DRR - D.onethird * divV);
+        sTpp[r][c] = 2.0f * sDn[rr][cc] * nu * (DPP - D.onethird * divV);
+        float rp = 0.0f;  // TAURP's ring 0 is never written: zero
+        if (i > 0) {
+          float DRP = 0.5f * (D.Rinf[i] * (sVa[rr][cc] * iRm - sVa[rr - 1][cc] * D.invRmed[i - 1]) * D.invdiffRmed[i] +
+                              (sVr[rr][cc] - sVr[rr][cc - 1]) * D.invdphi * D.invRinf[i]);
+          // TAURP's third density sample is dens[i*nsec] (Kernels.cu:876)
+          rp = 0.5f * (sDn[rr][cc] + sDn[rr - 1][cc] + sD0[rr] + sDn[rr - 1][cc - 1]) * nu * DRP;
+        }
+        sTrp[r][c] = rp;
+      }
+    }
+    __syncthreads();
+    // updated velocities of the tile's cells
+    const float DeltaT = C->dtf;
+    float vin = 0.0f, vout = 0.0f;
+    const bool kep = !D.Evanescent && (i0 == 0 || i0 + kVR >= nrad);
+    if (kep) vkep_pair(D, C, &vin, &vout);
+    for (int q = tid; q < kVR * kVC; q += kThreads) {
+      const int r = q / kVC, c = q - r * kVC;
+      const int i = i0 + r, j = j0 + c;
+      if (i >= nrad || j >= nsec) continue;
+      const size_t l = (size_t)i * nsec + j;
+      const int R = r + 1, Cc = c + 1;   // stress index of (i, j)
+      const int rr = r + 2, cc = c + 2;  // staged index of (i, j)
+      float vti = sVa[rr][cc], vri = sVr[rr][cc];
+      if (D.IsDisk) {
+        if (i > 0 && i < nrad - 1) {
+          vti += DeltaT * D.invRmed[i] *
+                 ((D.Rsup[i] * sTrp[R + 1][Cc] - D.Rinf[i] * sTrp[R][Cc]) * D.invdiffRsup[i] +
+                  (sTpp[R][Cc] - sTpp[R][Cc - 1]) * D.invdphi + 0.5f * (sTrp[R][Cc] + sTrp[R + 1][Cc])) /
+                 (0.5f * (sDn[rr][cc] + sDn[rr][cc - 1]));
+        }
+        if (i > 0) {
+          vri += DeltaT * D.invRinf[i] *
+                 ((D.Rmed[i] * sTrr[R][Cc] - D.Rmed[i - 1] * sTrr[R - 1][Cc]) * D.invdiffRmed[i] +
+                  (sTrp[R][Cc + 1] - sTrp[R][Cc]) * D.invdphi - 0.5f * (sTpp[R][Cc] + sTpp[R - 1][Cc])) /
+                 (0.5f * (sDn[rr][cc] + sDn[rr - 1][cc]));
+        }
+        if (kep && i == 0) vti = vin - D.Rmed[0] * C->OmegaFrame;
+        if (kep && i == nrad - 1) vti = vout - D.Rmed[nrad - 1] * C->OmegaFrame;
+      }
+      D.trr[l] = vri;
+      D.tpp[l] = vti;
+    }
+    __syncthreads();  // buffer bf is restaged two tiles on
+    bf ^= 1;
+    have = pre;
   }
-  if (i > 0) {
-    D.vri[l] += DeltaT * D.invRinf[i] *
-                ((D.Rmed[i] * TRR[l] - D.Rmed[i - 1] * TRR[l - nsec]) * D.invdiffRmed[i] +
-                 (TRP[lpj] - TRP[l]) * D.invdphi - 0.5f * (TPP[l] + TPP[l - nsec])) /
-                (0.5f * (Dn[l] + Dn[l - nsec]));
-  }
-  if (!D.Evanescent && (i == 0 || i == nrad - 1)) {
-    float vin, vout;
-    vkep_pair(D, C, &vin, &vout);
-    if (i == 0) D.vti[l] = vin - D.Rmed[0] * C->OmegaFrame;
-    if (i == nrad - 1) D.vti[l] = vout - D.Rmed[nrad - 1] * C->OmegaFrame;
-  }
-  CELL_END
 }
 
 // Substep2Kernel + Substep2Kernel2 (Kernels.cu:570-621), then the
@@ -1019,7 +1139,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_source2(BatchDev B) {
   CELL_BEGIN
   const float dt = C->dtf;
   const float* Dn = D.dens;
-  const float *VRI = D.vri, *VTI = D.vti;
+  const float *VRI = D.trr, *VTI = D.tpp;  // viscosity-updated VradInt / VthetaInt (k_viscosity)
   const long long lmj = (long long)i * nsec + jm, lpj = (long long)i * nsec + jp;
   float qr = qvisc(VRI[l + nsec] - VRI[l], Dn[l]);
   float qt = qvisc(VTI[lpj] - VTI[l], Dn[l]);
@@ -1577,7 +1697,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_velocities(BatchDev B) {
 __device__ void compact_active(const BatchDev& B) {
   int na = 0, ni = 0, nd = 0;
   long long cc = 0;
-  int rr = 0, ii = 0, ia = 0, gg = 0, tt = 0, ct = 0;
+  int rr = 0, ii = 0, ia = 0, gg = 0, tt = 0, ct = 0, vt = 0;
   for (int d = 0; d < B.ndisk; d++) {
     const DiskDev& D = B.disks[d];
     if (!D.ctl->active) continue;
@@ -1588,6 +1708,8 @@ __device__ void compact_active(const BatchDev& B) {
     B.act_tile_off[na] = tt;
     B.act_ctile_off[na] = ct;
     ct += D.nrad;
+    B.act_vtile_off[na] = vt;
+    vt += vtiles_of(D);
     cc += (long long)D.nrad * D.nsec;
     tt += (D.nrad * D.nsec + kThreads - 1) / kThreads;
     rr += D.nrad;
@@ -1610,6 +1732,7 @@ __device__ void compact_active(const BatchDev& B) {
   B.act_grp_off[na] = gg;
   B.act_tile_off[na] = tt;
   B.act_ctile_off[na] = ct;
+  B.act_vtile_off[na] = vt;
   B.act_iso_off[ni] = ii;
   B.act_adi_off[nd] = ia;
   B.act[0] = na;
@@ -2057,10 +2180,10 @@ void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s
 
 
 const char* fargo_substep_kernel_name(int k) {
-  static const char* names[] = {"k_ring_mean_cfl", "k_cfl_force",  "k_boundary_0",  "k_source1",
-                                "k_visc_tau",      "k_visc_update", "k_source2",     "k_boundary_1",
-                                "k_energy",        "k_ring_mean_tr", "k_transport",  "k_velocities",
-                                "k_boundary_2",    "k_substep_end"};
+  static const char* names[] = {"k_ring_mean_cfl", "k_cfl_force",    "k_boundary_0", "k_source1",
+                                "k_viscosity",     "k_source2",      "k_boundary_1", "k_energy",
+                                "k_ring_mean_tr",  "k_transport",    "k_velocities", "k_boundary_2",
+                                "k_substep_end"};
   return (k >= 0 && k < FARGO_NKERNELS) ? names[k] : "";
 }
 
@@ -2092,9 +2215,7 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   REC();
   k_source1<<<b.g_source1, kThreads, 0, s>>>(b);
   REC();
-  k_visc_tau<<<b.g_visc_tau, kThreads, 0, s>>>(b);
-  REC();
-  k_visc_update<<<b.g_visc_update, kThreads, 0, s>>>(b);
+  k_viscosity<<<b.g_viscosity, kThreads, 0, s>>>(b);
   REC();
   k_source2<<<b.g_source2, kThreads, 0, s>>>(b);
   REC();
@@ -2157,19 +2278,18 @@ cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int ni
   cudaError_t e;
   if ((e = wave(fargo_cfl_kernel(b.max_body), kThreads, 0, b.nring, &b.g_cfl))) return e;
   if ((e = wave((const void*)k_source1, kThreads, 0, ncell_tiles, &b.g_source1))) return e;
-  if ((e = wave((const void*)k_visc_tau, kThreads, 0, ncell_tiles, &b.g_visc_tau))) return e;
-  if ((e = wave((const void*)k_visc_update, kThreads, 0, ncell_tiles, &b.g_visc_update))) return e;
+  if ((e = wave((const void*)k_viscosity, kThreads, 0, ncell_tiles, &b.g_viscosity))) return e;
   if ((e = wave((const void*)k_source2, kThreads, 0, ncell_tiles, &b.g_source2))) return e;
   if ((e = wave((const void*)k_energy, kThreads, 0, ncell_tiles, &b.g_energy))) return e;
   if ((e = wave((const void*)k_velocities, kThreads, 0, ncell_tiles, &b.g_velocities))) return e;
   return wave((const void*)k_transport<6>, kTT, fargo_transport_smem_bytes(1), nitems, &b.g_transport);
 }
 
-// Launches of one substep: 11 kernels, both transport forms in a batch of
+// Launches of one substep: 10 kernels, both transport forms in a batch of
 // isothermal and adiabatic disks, two per boundary call when a disk has a
 // non-rigid boundary.
 int fargo_substep_launches(const BatchDev& b) {
-  return 11 + ((b.ntheta_iso && b.ntheta_adi) ? 1 : 0) + (b.any_bc ? 6 : 0);
+  return 10 + ((b.ntheta_iso && b.ntheta_adi) ? 1 : 0) + (b.any_bc ? 6 : 0);
 }
 
 void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s) {
