@@ -201,7 +201,7 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
     D.cs = nullptr;
     D.a1 = D.a0;  // never written in isothermal runs
   }
-  A(D.pres, ng)
+  A(D.pres, ng) A(D.phi, ng)
   size_t nct = n1;
   A(D.visc, n1) A(D.cs_ring, n1) A(D.csmean, n1) A(D.vmoy, n1) A(D.ringmin, nct) A(D.nshift, n1)
   A(D.tvmed, n1) A(D.tvconst, n1)

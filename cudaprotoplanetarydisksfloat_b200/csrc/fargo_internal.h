@@ -102,6 +102,7 @@ struct DiskDev {
   // scratch
   float *vri, *vti, *trr, *tpp, *trp, *qplus;
   float *a0, *a1;  // transported density and energy, moved into the state by k_velocities
+  float* phi;      // gravitational potential of the substep (k_potential)
   // self-gravity accelerations (NRAD*NSEC), may be null
   float *sg_accr, *sg_acct;
   // ring tables
@@ -160,11 +161,11 @@ struct BatchDev {
   int any_bc;                // some disk has an OPEN, NONREFLECTING or EVANESCENT boundary
   int max_body;              // largest body count of the force sums (star + FeelDisk planets)
   // one-wave grids of the substep kernels (fargo_size_grids)
-  int g_cfl, g_source1, g_viscosity, g_source2, g_energy, g_velocities, g_transport;
+  int g_cfl, g_source1, g_potential, g_viscosity, g_source2, g_energy, g_velocities, g_transport;
 };
 
 // kernel entry points (kernels_step.cu), launched by fargo_api.cu
-#define FARGO_NKERNELS 13  // profiled slots per substep (boundary slots empty for rigid boundaries)
+#define FARGO_NKERNELS 14  // profiled slots per substep (boundary slots empty for rigid boundaries)
 #define FARGO_SEG_OUT 192  // largest azimuthal transport segment (output sectors per CTA)
 #define FARGO_BAND 8       // rings per transport CTA
 cudaError_t fargo_kernel_attributes(int max_nsec);

@@ -850,6 +850,14 @@ __device__ __forceinline__ float potential_at(const DiskDev& D, const DiskCtl* C
   return P;
 }
 
+// FillForcesArrays (Pframeforce.cu:37-66): the potential of every cell, once
+// per substep (Substep1 reads it at three cells each).
+__global__ void __launch_bounds__(kThreads) k_potential(BatchDev B) {
+  CELL_BEGIN
+  D.phi[l] = potential_at(D, C, i, j);
+  CELL_END
+}
+
 __device__ __forceinline__ float pressure_at(const DiskDev& D, long long l, int i) {
   if (!D.Adiabatic) {
     float cs = D.cs_ring[i];
@@ -873,14 +881,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_source1(BatchDev B) {
   const float* Dn = D.dens;
   auto vth = [&](long long q, int r) -> float { return dom != 0.0f ? Vt[q] - dom * D.Rmed[r] : Vt[q]; };
   const float P0 = pressure_at(D, l, i);
-  const float Phi0 = potential_at(D, C, i, j);
+  const float Phi0 = D.phi[l];  // k_potential
   // ComputeTemperatureField divides the pressure of the substep start by the
   // final density (SourceEuler.cu:280,293): keep the last substep's pressure
   if (!D.Adiabatic && !C->more) D.pres[l] = P0;
   if (i > 0) {
     const long long lm = l - nsec;
     const float Pm = pressure_at(D, lm, i - 1);
-    const float Phim = potential_at(D, C, i - 1, j);
+    const float Phim = D.phi[l - nsec];
     float gradp = (P0 - Pm) * 2.0f / (Dn[l] + Dn[lm]) * D.invdiffRmed[i];
     float gradphi = (Phi0 - Phim) * D.invdiffRmed[i];
     const long long lp = (long long)i * nsec + jp;
@@ -900,7 +908,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_source1(BatchDev B) {
     float dxtheta = 2.0f * (float)PI_D / (float)nsec * D.Rmed[i];
     float invdxtheta = 1.0f / dxtheta;
     const float Pa = pressure_at(D, la, i);
-    const float Phia = potential_at(D, C, i, jm);
+    const float Phia = D.phi[la];
     float gradp = (P0 - Pa) * 2.0f / (Dn[l] + Dn[la]) * invdxtheta;
     float gradphi = (Phi0 - Phia) * invdxtheta;
     float vti = vth(l, i) - dt * (gradp + gradphi);
@@ -2180,10 +2188,10 @@ void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s
 
 
 const char* fargo_substep_kernel_name(int k) {
-  static const char* names[] = {"k_ring_mean_cfl", "k_cfl_force",    "k_boundary_0", "k_source1",
-                                "k_viscosity",     "k_source2",      "k_boundary_1", "k_energy",
-                                "k_ring_mean_tr",  "k_transport",    "k_velocities", "k_boundary_2",
-                                "k_substep_end"};
+  static const char* names[] = {"k_ring_mean_cfl", "k_cfl_force",    "k_potential",  "k_boundary_0",
+                                "k_source1",       "k_viscosity",    "k_source2",    "k_boundary_1",
+                                "k_energy",        "k_ring_mean_tr", "k_transport",  "k_velocities",
+                                "k_boundary_2",    "k_substep_end"};
   return (k >= 0 && k < FARGO_NKERNELS) ? names[k] : "";
 }
 
@@ -2207,6 +2215,8 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
     k_cfl_force<4><<<b.g_cfl, kThreads, 0, s>>>(b);
   else
     k_cfl_force<FARGO_MAXBODY><<<b.g_cfl, kThreads, 0, s>>>(b);
+  REC();
+  k_potential<<<b.g_potential, kThreads, 0, s>>>(b);
   REC();
   if (b.any_bc) {
     k_bc_rings<0><<<b.ring_grid, kThreads, 0, s>>>(b);
@@ -2278,6 +2288,7 @@ cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int ni
   cudaError_t e;
   if ((e = wave(fargo_cfl_kernel(b.max_body), kThreads, 0, b.nring, &b.g_cfl))) return e;
   if ((e = wave((const void*)k_source1, kThreads, 0, ncell_tiles, &b.g_source1))) return e;
+  if ((e = wave((const void*)k_potential, kThreads, 0, ncell_tiles, &b.g_potential))) return e;
   if ((e = wave((const void*)k_viscosity, kThreads, 0, ncell_tiles, &b.g_viscosity))) return e;
   if ((e = wave((const void*)k_source2, kThreads, 0, ncell_tiles, &b.g_source2))) return e;
   if ((e = wave((const void*)k_energy, kThreads, 0, ncell_tiles, &b.g_energy))) return e;
@@ -2285,11 +2296,11 @@ cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int ni
   return wave((const void*)k_transport<6>, kTT, fargo_transport_smem_bytes(1), nitems, &b.g_transport);
 }
 
-// Launches of one substep: 10 kernels, both transport forms in a batch of
+// Launches of one substep: 11 kernels, both transport forms in a batch of
 // isothermal and adiabatic disks, two per boundary call when a disk has a
 // non-rigid boundary.
 int fargo_substep_launches(const BatchDev& b) {
-  return 10 + ((b.ntheta_iso && b.ntheta_adi) ? 1 : 0) + (b.any_bc ? 6 : 0);
+  return 11 + ((b.ntheta_iso && b.ntheta_adi) ? 1 : 0) + (b.any_bc ? 6 : 0);
 }
 
 void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s) {
