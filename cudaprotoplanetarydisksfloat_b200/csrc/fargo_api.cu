@@ -407,7 +407,8 @@ fargo_status build_graph(fargo_batch* b) {
 }
 
 // Transport work items of every disk: bands of FARGO_BAND rings, each in
-// nseg near-equal azimuthal segments of at most seg_out sectors; isothermal
+// nseg near-equal azimuthal segments of at most seg_out source sectors (the
+// sectors a band reads; each ring stores them shifted by its Nshift); isothermal
 // and adiabatic disks in separate lists.  Sets each disk's item0 / nitems
 // (host copy) and returns the widest segment.
 int build_items(fargo_batch* b, int seg_out, std::vector<int4>& theta_iso, std::vector<int4>& theta_adi) {

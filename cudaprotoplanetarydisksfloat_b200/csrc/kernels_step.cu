@@ -1583,24 +1583,24 @@ __device__ __forceinline__ void sweep_ring(float* sRr, int off, int L, float VMe
 }
 
 // Transport (TransportEuler.cu:24-35) of a band of up to kBR rings i0 ..
-// and one azimuthal segment of output sectors j0 .. j0+S-1.  The output
-// sector j of ring i takes the swept value of source sector j - Nshift_i
-// (AdvectSHIFTKernel, Kernels.cu:1276-1289), so ring i works on the source
-// window j0 - Nshift_i - 4 .. + S + 8.  The rings are taken in sub-bands
-// whose windows fit one union window of kTT sectors: the radial half
-// (rad_march) runs over the union, one thread per column marching down the
-// sub-band, into shared memory; then one warp per ring runs the azimuthal
-// sweeps (sweep_ring) on the ring's window; the 4-point halo covers the
-// sweeps' stencils.  VMed, Nshift and the constant residual come from
-// k_ring_mean<1>.  Final density / energy go to scratch (a0 / a1) because
-// neighbouring bands still read the old ones; the velocity kernel moves them
-// into the state.
+// and one azimuthal segment of source sectors g0 .. g0+S-1.  The tile is
+// taken in source coordinates: the radial half (rad_march) runs over the
+// window g0-4 .. g0+S+3 of every ring of the band, one thread per column
+// marching outwards, into shared memory; then one warp per ring runs the
+// azimuthal sweeps (sweep_ring) on that window, whose 4-point halo covers
+// the sweeps' stencils.  Source sector g of ring i is then stored at output
+// sector g + Nshift_i (AdvectSHIFTKernel, Kernels.cu:1276-1289: output j
+// takes source j - Nshift): per ring a contiguous run, and the segments of
+// a ring map one to one onto its output sectors.  VMed, Nshift and the
+// constant residual come from k_ring_mean<1>.  Final density / energy go
+// to scratch (a0 / a1) because neighbouring bands still read the old ones;
+// the velocity kernel moves them into the state.
 template <int nq>
 __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __restrict__ items) {
   extern __shared__ float tr_sm[];
   float* sR = tr_sm;                         // [kBR][nq + 1][kPad] radial results + v_theta
   float* sL = sR + kBR * (nq + 1) * kPad;    // [kPad] mass through the inner edge (OPEN)
-  __shared__ int s_ns[kBR];
+  __shared__ int s_jb[kBR];
   __shared__ float s_vmed[kBR], s_vc[kBR];
   const int nak = (nq == 5) ? B.act[1] : B.act[2];
   const int* aoff = (nq == 5) ? B.act_iso_off : B.act_adi_off;
@@ -1614,7 +1614,7 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
     if (!D.IsDisk) continue;
     const int4 it = items[D.item0 + (t - aoff[a])];
     const DiskCtl* C = D.ctl;
-    const int i0 = it.y, j0 = it.z, S = it.w;
+    const int i0 = it.y, g0 = it.z, S = it.w;
     const int nsec = D.nsec, nrad = D.nrad;
     const int nb = min(kBR, nrad - i0);
     const int L = S + 8;
@@ -1623,60 +1623,40 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
     const bool fast = D.FastTransport;
     const float dtheta = 2.0f * (float)PI_D / (float)nsec;
     if (p < nb) {
-      s_ns[p] = D.nshift[i0 + p];
+      int jb = (g0 + D.nshift[i0 + p]) % nsec;  // output sector of source sector g0
+      s_jb[p] = jb < 0 ? jb + nsec : jb;
       s_vmed[p] = D.tvmed[i0 + p];
       s_vc[p] = D.tvconst[i0 + p];
     }
+    if (p < L) {
+      int g = (g0 - 4 + p) % nsec;
+      if (g < 0) g += nsec;
+      float* o = sR + pidx(p);
+      rad_march<nq>(D, i0, i0 + nb, g, dt, Om, dtheta, o, kPad, (nq + 1) * kPad,
+                    (D.OpenInner && i0 == 0) ? sL + pidx(p) : nullptr);
+      for (int r = 0; r < nb; r++) o[(r * (nq + 1) + nq) * kPad] = __ldg(D.vtheta + (size_t)(i0 + r) * nsec + g);
+    }
     __syncthreads();
-    int rb = 0;
-    while (rb < nb) {
-      // sub-band rb .. re-1: window starts (unwrapped) within kTT - L of each other
-      int lo = j0 - s_ns[rb], hi = lo, re = rb + 1;
-      while (re < nb) {
-        const int x = j0 - s_ns[re];
-        const int nlo = min(lo, x), nhi = max(hi, x);
-        if (nhi - nlo > kTT - L) break;
-        lo = nlo;
-        hi = nhi;
-        re++;
-      }
-      const int WU = hi - lo + L;  // union window width, <= kTT
-      const int u0 = lo - 4;       // first (unwrapped) sector of the union window
-      if (p < WU) {
-        int g = (u0 + p) % nsec;
-        if (g < 0) g += nsec;
-        float* o = sR + pidx(p);
-        rad_march<nq>(D, i0 + rb, i0 + re, g, dt, Om, dtheta, o, kPad, (nq + 1) * kPad,
-                      (D.OpenInner && i0 + rb == 0) ? sL + pidx(p) : nullptr);
-        for (int r = rb; r < re; r++) o[((r - rb) * (nq + 1) + nq) * kPad] = __ldg(D.vtheta + (size_t)(i0 + r) * nsec + g);
-      }
-      __syncthreads();
-      const int r = rb + warp;
-      if (r < re) {
-        const int i = i0 + r;
-        const int ws = j0 - s_ns[r] - 4;  // first (unwrapped) sector of this ring's window
-        const int off = ws - u0;
-        float* sRr = sR + (size_t)(r - rb) * (nq + 1) * kPad;
-        const float Rm = D.Rmed[i];
-        const float dxtheta = fm(dtheta, Rm);
-        sweep_ring<nq>(sRr, off, L, s_vmed[r], s_vc[r], fast, dt, dxtheta, 1.0f / dxtheta, 1.0f / D.Surf[i],
-                       fm(D.Rsup[i] - D.Rinf[i], dt));
-        // output sector j0 + x - 4 takes window point x: coalesced stores
-        float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.a1, D.a0};
-        const long long row = (long long)i * nsec + j0 - 4;
-        for (int x = 4 + lane; x < L - 4; x += 32) {
+    const int r = warp;
+    if (r < nb) {
+      const int i = i0 + r;
+      float* sRr = sR + (size_t)r * (nq + 1) * kPad;
+      const float Rm = D.Rmed[i];
+      const float dxtheta = fm(dtheta, Rm);
+      sweep_ring<nq>(sRr, 0, L, s_vmed[r], s_vc[r], fast, dt, dxtheta, 1.0f / dxtheta, 1.0f / D.Surf[i],
+                     fm(D.Rsup[i] - D.Rinf[i], dt));
+      // window point x is source sector g0 + x - 4, stored at output sector
+      // jb + x - 4 (jb < nsec and x - 4 < S <= nsec: one wrap at most)
+      float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.a1, D.a0};
+      const long long row = (long long)i * nsec;
+      const int jb = s_jb[r] - 4;
+      for (int x = 4 + lane; x < L - 4; x += 32) {
+        int j = jb + x;
+        if (j >= nsec) j -= nsec;
 #pragma unroll
-          for (int c = 0; c < nq; c++) dsts[c == nq - 1 ? 5 : c][row + x] = sRr[c * kPad + pidx(x)];
-          if (i == 0 && D.OpenInner) {
-            // each source sector is the core of exactly one segment's window
-            int g = (ws + x) % nsec;
-            if (g < 0) g += nsec;
-            D.lost[g] = sL[pidx(off + x)];
-          }
-        }
+        for (int c = 0; c < nq; c++) dsts[c == nq - 1 ? 5 : c][row + j] = sRr[c * kPad + pidx(x)];
+        if (i == 0 && D.OpenInner) D.lost[g0 + x - 4] = sL[pidx(x)];
       }
-      rb = re;
-      __syncthreads();
     }
   }
 }
