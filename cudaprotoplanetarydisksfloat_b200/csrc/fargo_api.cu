@@ -202,7 +202,7 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
     D.a1 = D.a0;  // never written in isothermal runs
   }
   A(D.pres, ng) A(D.phi, ng)
-  size_t nct = n1;
+  size_t nct = std::max<size_t>(n1, (size_t)fargo_cfl_tiles(p->NRAD, p->NSEC));
   A(D.visc, n1) A(D.cs_ring, n1) A(D.csmean, n1) A(D.vmoy, n1) A(D.ringmin, nct) A(D.nshift, n1)
   A(D.tvmed, n1) A(D.tvconst, n1)
   A(D.log_nshift, (size_t)FARGO_MAXLOG * p->NRAD) A(D.partials, nct * 4 * FARGO_MAXBODY)
@@ -531,6 +531,8 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   bd.max_body = max_body;
   bd.ncell = cell_off[n];
   bd.nring = ring_off[n];
+  bd.ncfl = 0;
+  for (int d = 0; d < n; d++) bd.ncfl += fargo_cfl_tiles(b->disks[d].dev.nrad, b->disks[d].dev.nsec);
   bd.cell_off = b->d_cell_off;
   bd.ring_off = b->d_ring_off;
   bd.disks = b->d_disks;
@@ -856,7 +858,7 @@ fargo_status fargo_set_planets(fargo_ctx* ctx, const fargo_planets* in) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
     int per = 1;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fargo_cfl_kernel(FARGO_MAXBODY), 256, 0));
-    b->bd.g_cfl = std::max(1, std::min(b->bd.nring, nsm * std::max(per, 1)));
+    b->bd.g_cfl = std::max(1, std::min(b->bd.ncfl, nsm * std::max(per, 1)));
     return build_graph(b);
   }
   return FARGO_OK;

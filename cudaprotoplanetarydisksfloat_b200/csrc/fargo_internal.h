@@ -67,6 +67,13 @@ struct DiskCtl {
   float axisg_in, axisg_out;
 };
 
+// CFL/force tiles: FARGO_CFL_TILE consecutive cells of one disk, each with its
+// own minimum and force partials
+#define FARGO_CFL_TILE 1024
+inline __host__ __device__ int fargo_cfl_tiles(int nrad, int nsec) {
+  return (int)(((long long)nrad * nsec + FARGO_CFL_TILE - 1) / FARGO_CFL_TILE);
+}
+
 // scratch of the device RK5 (q0, q1, k1..k6, distances): 33 doubles per planet
 #define FARGO_RK_WORK(nb) (33 * (nb))
 
@@ -113,13 +120,13 @@ struct DiskDev {
   float* cs_ring;        // isothermal sound speed per ring
   float* csmean;         // GLOBAL_bufarray: ring-mean sound speed
   float* vmoy;           // ConditionCFLKernel1D ring mean
-  float* ringmin;        // newDT per ring
+  float* ringmin;        // newDT per CFL tile
   int* nshift;           // Nshift per ring of the current substep
   float* tvmed;          // transport: ring-mean v_theta of the current substep
   float* tvconst;        // transport: constant residual per ring
   int* log_nshift;       // [FARGO_MAXLOG][nrad]
   float* lost;           // [nsec] mass through the inner edge this substep (OPEN inner boundary)
-  double* partials;      // [nrad][4*FARGO_MAXBODY] force partial sums per ring
+  double* partials;      // [4*FARGO_MAXBODY][CFL tiles] force partial sums per tile
   double* log_dt;        // [FARGO_MAXLOG] substep dt of the current DT
   double* rk_work;       // [FARGO_RK_WORK(FARGO_MAXPLANETS_DEV)] RK5 scratch of large systems
   // sector tables
@@ -132,6 +139,7 @@ struct BatchDev {
   int ndisk;
   long long ncell;       // total active cells
   int nring;             // total rings
+  int ncfl;              // total CFL tiles
   const long long* cell_off;  // [ndisk+1]
   const int* ring_off;        // [ndisk+1]
   DiskDev* disks;
@@ -155,7 +163,7 @@ struct BatchDev {
   int* act_adi_off;
   int* act_grp_off;          // [ndisk+1] prefix of 32-ring groups of active disks
   int* act_tile_off;         // [ndisk+1] prefix of cell tiles (one block's cells) of active disks
-  int* act_ctile_off;        // [ndisk+1] prefix of rings of active disks (CFL tiles)
+  int* act_ctile_off;        // [ndisk+1] prefix of CFL tiles (FARGO_CFL_TILE cells) of active disks
   int* act_vtile_off;        // [ndisk+1] prefix of viscosity tiles (8 x 64 cells) of active disks
   int cell_grid, ring_grid, item_grid, grp_grid;  // fixed grid sizes of the grid-stride kernels
   int any_bc;                // some disk has an OPEN, NONREFLECTING or EVANESCENT boundary

@@ -374,7 +374,10 @@ __device__ __forceinline__ void copy_words(void* dst, const void* src, int bytes
   for (int k = threadIdx.x; k < bytes / 4; k += blockDim.x) d[k] = s[k];
 }
 
-template <class Body>
+// adi_only: skip the tiles of isothermal disks (energy kernels).  A thread's
+// cell advances by kThreads sectors from one tile to the next, so the ring
+// division runs only on entering a disk.
+template <bool adi_only, class Body>
 __device__ __forceinline__ void for_active_cells(const BatchDev& B, Body body) {
   __shared__ DiskDev sD;
   const int na = B.act[0];
@@ -382,7 +385,7 @@ __device__ __forceinline__ void for_active_cells(const BatchDev& B, Body body) {
   const int ntile = B.act_tile_off[na];
   const int per = (ntile + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
-  int lo = 0, hi = -1;
+  int lo = 0, hi = -1, i = 0, j = 0;
   for (int t = t0; t < t1; t++) {
     if (t >= hi) {  // block-uniform
       const int a = find_range(B.act_tile_off, na, t);
@@ -391,24 +394,36 @@ __device__ __forceinline__ void for_active_cells(const BatchDev& B, Body body) {
       __syncthreads();
       copy_words(&sD, B.disks + B.act_disk[a], sizeof(DiskDev));
       __syncthreads();
+      if (!sD.IsDisk || (adi_only && !sD.Adiabatic)) {  // nothing to do on this disk
+        t = hi - 1;
+        continue;
+      }
+      const int loc = (t - lo) * kThreads + threadIdx.x;
+      i = loc / sD.nsec;
+      j = loc - i * sD.nsec;
+    } else {
+      const int nsec = sD.nsec;
+      j += kThreads;
+      while (j >= nsec) {
+        j -= nsec;
+        i++;
+      }
     }
-    const int nsec = sD.nsec;
-    const int loc = (t - lo) * kThreads + threadIdx.x;
-    if (loc < sD.nrad * nsec) {
-      const int i = loc / nsec, j = loc - i * nsec;
-      body(sD, sD.ctl, i, j, (long long)loc, jwrap_m(j, nsec), jwrap_p(j, nsec));
+    if (i < sD.nrad) {
+      const int ns = sD.nsec;
+      body(sD, sD.ctl, i, j, (long long)i * ns + j, jwrap_m(j, ns), jwrap_p(j, ns));
     }
   }
 }
 
-#define CELL_BEGIN                                                                                      \
-  for_active_cells(B, [&](const DiskDev& D, const DiskCtl* C, const int i, const int j, const long long l, \
-                          const int jm, const int jp) {                                                 \
+#define CELL_BEGIN_T(adi_only)                                                                          \
+  for_active_cells<adi_only>(B, [&](const DiskDev& D, const DiskCtl* C, const int i, const int j,         \
+                                    const long long l, const int jm, const int jp) {                     \
     const int nsec = D.nsec, nrad = D.nrad;                                                             \
     (void)nrad;                                                                                         \
     (void)jm;                                                                                           \
-    (void)jp;                                                                                           \
-    if (!D.IsDisk) return;
+    (void)jp;
+#define CELL_BEGIN CELL_BEGIN_T(false)
 #define CELL_END \
   });
 
@@ -508,17 +523,15 @@ __device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const d
 __device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* Cg, DiskCtl* sC, float* shf, double* s_sum,
                                        double* s_work) {
   const int nrad = D.nrad, nsec = D.nsec, tid = threadIdx.x;
-  const int nct = nrad;
-  // ConditionCFL host part (SourceEuler.cu:513-535): minimum over the ring
-  // minima of rings 1 .. NRAD-1, the shear limit DT1D (ConditionCFLKernel2D2,
-  // Kernels.cu:1425-1428) and DeltaT.
+  const int nct = fargo_cfl_tiles(nrad, nsec);
+  // ConditionCFL host part (SourceEuler.cu:513-535): minimum over the tile
+  // minima (cells of rings 1 .. NRAD-1), the shear limit DT1D
+  // (ConditionCFLKernel2D2, Kernels.cu:1425-1428) and DeltaT.
   float m = 1e30f;
-  bool first = true;
 #pragma unroll 4
-  for (int t = 1 + tid; t < nct; t += blockDim.x) {
+  for (int t = tid; t < nct; t += blockDim.x) {
     float v = __ldcg(D.ringmin + t);
-    if (first || v < m) m = v;
-    first = false;
+    if (v < m) m = v;
   }
 #pragma unroll 4
   for (int i = tid; i < nrad - 1; i += blockDim.x) {
@@ -526,15 +539,24 @@ __device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* Cg, DiskCtl* s
     if (dt1 < m) m = dt1;
   }
   float newdt = block_min_f(m, shf);
-  // disk-force sums over the rings in a fixed order, one warp per sum
+  // disk-force sums over the tiles in a fixed order: every thread a strided
+  // share (partials are [sum][tile]), the warps by shuffle, then the warps in
+  // order (s_work is free until the planet update)
   const int nbody = Cg->nbody, nsum = 4 * nbody;
-  const int w = tid >> 5, l = tid & 31;
-  for (int q = w; q < nsum; q += blockDim.x >> 5) {
+  const int w = tid >> 5, l = tid & 31, nw = blockDim.x >> 5;
+  for (int q = 0; q < nsum; q++) {
+    const double* P = D.partials + (size_t)q * nct;
     double acc = 0.0;
 #pragma unroll 4
-    for (int t = l; t < nct; t += 32) acc += __ldcg(D.partials + (size_t)t * 4 * FARGO_MAXBODY + q);
+    for (int t = tid; t < nct; t += blockDim.x) acc += __ldcg(P + t);
     acc = warp_sum_d(acc);
-    if (l == 0) s_sum[q] = acc;
+    if (l == 0) s_work[q * nw + w] = acc;
+  }
+  __syncthreads();
+  if (tid < nsum) {
+    double acc = 0.0;
+    for (int u = 0; u < nw; u++) acc += s_work[tid * nw + u];
+    s_sum[tid] = acc;
   }
   // FViscosity per ring for this substep (Viscosity.cu:84-85, SourceEuler.cu:350)
   const float PT = Cg->PhysicalTime;
@@ -649,22 +671,26 @@ __device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const d
   C->counter = 0;
 }
 
-// One block per ring: ConditionCFLKernel1D + ConditionCFLKernel2D1 + the
-// ring minimum of ConditionCFLKernel2D2 (Kernels.cu:1363-1422), and the disk
-// force of ComputeForceKernel (Kernels.cu:804-839) for the star and every
-// FeelDisk planet, accumulated in double; per-ring results, so that the
-// finishing sums run in a fixed order.  Each block takes a contiguous run of
-// rings.  The block that completes a disk's last ring finishes the
-// substep's scalar work.
+// ConditionCFLKernel1D + ConditionCFLKernel2D1 + the cell minimum of
+// ConditionCFLKernel2D2 (Kernels.cu:1363-1422), and the disk force of
+// ComputeForceKernel (Kernels.cu:804-839) for the star and every FeelDisk
+// planet, accumulated in double, on CFL tiles of FARGO_CFL_TILE consecutive
+// cells (kCflCells per thread, their loads issued together).  Each tile
+// writes its minimum and its force partials (inner / outer by the ring of
+// each cell), so that the finishing sums run in a fixed order.  Each block
+// takes a contiguous run of tiles; the block that completes a disk's last
+// tile finishes the substep's scalar work.
 // NB >= every disk's body count (star + FeelDisk planets): the per-thread
 // FP64 force accumulators are sized for it.
+constexpr int kCflCells = FARGO_CFL_TILE / kThreads;
+static_assert(kCflCells * kThreads == FARGO_CFL_TILE, "CFL tile = whole cells per thread");
 template <int NB>
-__global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
+__global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDev B) {
   __shared__ DiskDev sD;
   __shared__ DiskCtl sC;
   __shared__ float s_b[5][NB];
-  __shared__ float s_min[2][32];                     // double-buffered by ring parity
-  __shared__ double s_red[2][2 * NB][kThreads / 32];
+  __shared__ float s_min[2][32];                     // double-buffered by tile parity
+  __shared__ double s_red[2][4 * NB][kThreads / 32];
   __shared__ double s_sum[4 * FARGO_MAXBODY];
   __shared__ double s_work[FARGO_RK_WORK(kRkShared)];
   __shared__ unsigned s_ticket;
@@ -675,8 +701,8 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
   const int per = (ntile + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
   int lo = 0, hi = -1, run = 0;
-  // A run of rings of one disk is done: count it on the disk's ticket; the
-  // block that completes the disk's last ring finishes the substep.  Warp 0
+  // A run of tiles of one disk is done: count it on the disk's ticket; the
+  // block that completes the disk's last tile finishes the substep.  Warp 0
   // wrote the run's results and fences them before the ticket.
   auto finish_run = [&]() {
     if (run == 0) return;
@@ -687,7 +713,7 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
       if (l == 0) s_ticket = atomicAdd(&Cr->counter, (unsigned)run);
     }
     __syncthreads();
-    if (s_ticket + (unsigned)run == (unsigned)sD.nrad) {
+    if (s_ticket + (unsigned)run == (unsigned)fargo_cfl_tiles(sD.nrad, sD.nsec)) {
       __threadfence();
       finish_cfl_and_planets(sD, Cr, &sC, s_min[0], s_sum, s_work);
     }
@@ -717,86 +743,99 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
     }
     const DiskDev& D = sD;
     const int nbody = s_nbody;
-    const int nsec = D.nsec;
-    const int i = t - lo;  // ring
+    const int nsec = D.nsec, nrad = D.nrad;
+    const int k = t - lo;  // tile of this disk
     float lmin = 1e30f;
-    double sfx[NB], sfy[NB];
+    double acc[NB][4];     // x inner, x outer, y inner, y outer
 #pragma unroll
-    for (int b = 0; b < NB; b++) sfx[b] = sfy[b] = 0.0;
+    for (int b = 0; b < NB; b++) acc[b][0] = acc[b][1] = acc[b][2] = acc[b][3] = 0.0;
     if (D.IsDisk) {
-      const float vm = D.vmoy[i];  // k_ring_mean<0>
-      const float dxrad = D.Rsup[i] - D.Rinf[i];
-      const float dxt = D.dxtheta[i];
-      const float csr = D.Adiabatic ? 0.0f : D.cs_ring[i];
-      const int k = D.ExcludeHill ? FARGO_DIMFXY - 1 : 0;
-      const float hillcutfactor = (float)k / (float)(FARGO_DIMFXY - 1);
-      const float Rm = D.Rmed[i], Sf = D.Surf[i];
-      const float* vt = D.vtheta + (size_t)i * nsec;
-      const float* vr = D.vrad + (size_t)i * nsec;
-      const float* dn = D.dens + (size_t)i * nsec;
-#pragma unroll 2
-      for (int j = tid; j < nsec; j += kThreads) {
-        if (i > 0) {
-          float cs = D.Adiabatic ? D.cs[(size_t)i * nsec + j] : csr;
-          const float v0 = vt[j];
-          float vres = D.FastTransport ? v0 - vm : v0;
-          float invdt1 = cs / (min2(dxrad, dxt));
-          float invdt2 = fabsf(vr[j]) / dxrad;
-          float invdt3 = fabsf(vres) / dxt;
-          float dvr = vr[j + nsec] - vr[j];
-          float dvt = vt[jwrap_p(j, nsec)] - v0;
-          if (dvr >= 0.0)
-            dvr = 1e-10;
-          else
-            dvr = -dvr;
-          if (dvt >= 0.0)
-            dvt = 1e-10;
-          else
-            dvt = -dvt;
-          float invdt4 = max2(dvr / dxrad, dvt / dxt);
-          invdt4 *= 4.0 * CVNR * CVNR;
-          float dt2d = CFLSEC / sqrtf(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 + invdt4 * invdt4);
-          if (dt2d < lmin) lmin = dt2d;
-        }
-        float cellmass = Sf * dn[j];
-        float cx = Rm * D.cos_cell[j];
-        float cy = Rm * D.sin_cell[j];
+      const int kh = D.ExcludeHill ? FARGO_DIMFXY - 1 : 0;
+      const float hillcutfactor = (float)kh / (float)(FARGO_DIMFXY - 1);
+      const int c0 = k * FARGO_CFL_TILE + tid;
+      int i = c0 / nsec, j = c0 - i * nsec;
 #pragma unroll
-        for (int b = 0; b < NB; b++) {
-          if (b < nbody) {
-            float dx = cx - s_b[0][b];
-            float dy = cy - s_b[1][b];
-            float rs = s_b[2][b];
-            float d2 = dx * dx + dy * dy;
-            float dist2 = d2 + rs * rs;
-            float distance = sqrtf(dist2);
-            // 1.0/dist2/distance, as one float reciprocal
-            float InvDist3 = __frcp_rn(dist2 * distance);
-            float hill_cut;
-            if (k != 0) {
-              float rh = s_b[3][b] * hillcutfactor;
-              hill_cut = 1. - expf(-d2 / (rh * rh));
-            } else
-              hill_cut = 1.;
-            sfx[b] += cellmass * dx * InvDist3 * hill_cut;
-            sfy[b] += cellmass * dy * InvDist3 * hill_cut;
+      for (int c = 0; c < kCflCells; c++) {
+        if (i < nrad) {
+          const long long q = (long long)i * nsec + j;
+          const float v0 = D.vtheta[q];
+          const float vr0 = D.vrad[q];
+          const float dn = D.dens[q];
+          if (i > 0) {
+            const float dxrad = D.Rsup[i] - D.Rinf[i];
+            const float dxt = D.dxtheta[i];
+            float cs = D.Adiabatic ? D.cs[q] : D.cs_ring[i];
+            float vres = D.FastTransport ? v0 - D.vmoy[i] : v0;  // vmoy: k_ring_mean<0>
+            float invdt1 = cs / (min2(dxrad, dxt));
+            float invdt2 = fabsf(vr0) / dxrad;
+            float invdt3 = fabsf(vres) / dxt;
+            float dvr = D.vrad[q + nsec] - vr0;
+            float dvt = D.vtheta[q - j + jwrap_p(j, nsec)] - v0;
+            if (dvr >= 0.0)
+              dvr = 1e-10;
+            else
+              dvr = -dvr;
+            if (dvt >= 0.0)
+              dvt = 1e-10;
+            else
+              dvt = -dvt;
+            float invdt4 = max2(dvr / dxrad, dvt / dxt);
+            invdt4 *= 4.0 * CVNR * CVNR;
+            float dt2d = CFLSEC / sqrtf(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 + invdt4 * invdt4);
+            if (dt2d < lmin) lmin = dt2d;
           }
+          const float Rm = D.Rmed[i];
+          float cellmass = D.Surf[i] * dn;
+          float cx = Rm * D.cos_cell[j];
+          float cy = Rm * D.sin_cell[j];
+#pragma unroll
+          for (int b = 0; b < NB; b++) {
+            if (b < nbody) {
+              float dx = cx - s_b[0][b];
+              float dy = cy - s_b[1][b];
+              float rs = s_b[2][b];
+              float d2 = dx * dx + dy * dy;
+              float dist2 = d2 + rs * rs;
+              float distance = sqrtf(dist2);
+              // 1.0/dist2/distance, as one float reciprocal
+              float InvDist3 = __frcp_rn(dist2 * distance);
+              float hill_cut;
+              if (kh != 0) {
+                float rh = s_b[3][b] * hillcutfactor;
+                hill_cut = 1. - expf(-d2 / (rh * rh));
+              } else
+                hill_cut = 1.;
+              const double fx = cellmass * dx * InvDist3 * hill_cut;
+              const double fy = cellmass * dy * InvDist3 * hill_cut;
+              if (Rm < s_b[4][b]) {  // f*_inner (constant indices: the sums stay in registers)
+                acc[b][0] += fx;
+                acc[b][2] += fy;
+              } else {  // f*_outer
+                acc[b][1] += fx;
+                acc[b][3] += fy;
+              }
+            }
+          }
+        }
+        j += kThreads;
+        while (j >= nsec) {
+          j -= nsec;
+          i++;
         }
       }
     }
-    // ring minimum and force sums: warps by shuffle, then warp 0 over the warps
-    // (buffers alternate by ring, so one barrier per ring suffices)
+    // tile minimum and force sums: warps by shuffle, then warp 0 over the
+    // warps (buffers alternate by tile, so one barrier per tile suffices)
     const int pb = t & 1;
     lmin = warp_min_f(lmin);
     if (l == 0) s_min[pb][w] = lmin;
 #pragma unroll
     for (int b = 0; b < NB; b++) {
       if (b < nbody) {
-        double fx = warp_sum_d(sfx[b]);
-        double fy = warp_sum_d(sfy[b]);
-        if (l == 0) {
-          s_red[pb][2 * b][w] = fx;
-          s_red[pb][2 * b + 1][w] = fy;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          double v = warp_sum_d(acc[b][u]);
+          if (l == 0) s_red[pb][4 * b + u][w] = v;
         }
       }
     }
@@ -804,18 +843,15 @@ __global__ void __launch_bounds__(kThreads) k_cfl_force(BatchDev B) {
     if (w == 0) {
       if (l == 0) {
         float m = s_min[pb][0];
-        for (int q = 1; q < kThreads / 32; q++)
-          if (s_min[pb][q] < m) m = s_min[pb][q];
-        D.ringmin[i] = m;
+        for (int u = 1; u < kThreads / 32; u++)
+          if (s_min[pb][u] < m) m = s_min[pb][u];
+        D.ringmin[k] = m;
       }
-      if (l < 2 * nbody) {
-        double acc = 0.0;
-        for (int q = 0; q < kThreads / 32; q++) acc += s_red[pb][l][q];
-        const int b = l >> 1, comp = l & 1;  // comp 0: x, 1: y
-        const bool inner = D.Rmed[i] < s_b[4][b];
-        double* P = D.partials + (size_t)i * 4 * FARGO_MAXBODY + 4 * b + 2 * comp;
-        P[0] = inner ? acc : 0.0;  // f*_inner
-        P[1] = inner ? 0.0 : acc;  // f*_outer
+      const int nct = fargo_cfl_tiles(nrad, nsec);
+      for (int u = l; u < 4 * nbody; u += 32) {
+        double v = 0.0;
+        for (int x = 0; x < kThreads / 32; x++) v += s_red[pb][u][x];
+        D.partials[(size_t)u * nct + k] = v;  // [sum][tile]
       }
     }
     run++;
@@ -1188,8 +1224,7 @@ __device__ __forceinline__ float qplus_at(const DiskDev& D, int i, int j, int ns
 }
 
 __global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
-  CELL_BEGIN
-  if (!D.Adiabatic) return;
+  CELL_BEGIN_T(true)
   const float dt = C->dtf;
   float divv;
   float q = 0.0f;
@@ -1265,21 +1300,30 @@ struct RadRow {
   float W[nq];  // quotients Q / (S + 1e-20)
 };
 
+// The disk fields and ring tables the radial half reads, loaded once per
+// band into registers (the band's shared-memory stores then cannot force
+// reloads of the disk's pointers); 32-bit cell offsets, as the reference's.
+struct TrView {
+  const float *dens, *vrad, *vtheta, *energy;
+  const float *Rmed, *invdiffRmed, *Rinf, *Rsup, *invSurf;
+  int nsec, nrad;
+};
+
 template <int nq>
-__device__ __forceinline__ RadRow<nq> rad_row(const DiskDev& D, int r, int g, int gp, float Om) {
-  const int nsec = D.nsec;
-  r = r < 0 ? 0 : (r > D.nrad - 1 ? D.nrad - 1 : r);  // clamped rows only meet zero slopes
-  const long long lr = (long long)r * nsec + g;
-  const long long lrp = (long long)r * nsec + gp;
+__device__ __forceinline__ RadRow<nq> rad_row(const TrView& V, int r, int g, int gp, float Om) {
+  const int nsec = V.nsec;
+  r = r < 0 ? 0 : (r > V.nrad - 1 ? V.nrad - 1 : r);  // clamped rows only meet zero slopes
+  const int lr = r * nsec + g;
+  const int lrp = r * nsec + gp;
   RadRow<nq> R;
-  const float sg = __ldg(D.dens + lr);
-  const float rm = __ldg(D.Rmed + r);
+  const float sg = __ldg(V.dens + lr);
+  const float rm = __ldg(V.Rmed + r);
   R.S = sg;
-  R.Q[0] = fm(sg, __ldg(D.vrad + lr + nsec));
-  R.Q[1] = fm(sg, __ldg(D.vrad + lr));
-  R.Q[2] = fm(fm(sg, __ldg(D.vtheta + lrp) + fm(rm, Om)), rm);
-  R.Q[3] = fm(fm(sg, __ldg(D.vtheta + lr) + fm(rm, Om)), rm);
-  if (nq == 6) R.Q[4] = __ldg(D.energy + lr);
+  R.Q[0] = fm(sg, __ldg(V.vrad + lr + nsec));
+  R.Q[1] = fm(sg, __ldg(V.vrad + lr));
+  R.Q[2] = fm(fm(sg, __ldg(V.vtheta + lrp) + fm(rm, Om)), rm);
+  R.Q[3] = fm(fm(sg, __ldg(V.vtheta + lr) + fm(rm, Om)), rm);
+  if (nq == 6) R.Q[4] = __ldg(V.energy + lr);
   R.Q[nq - 1] = sg;
   const float rden = __fdividef(1.0f, sg + 1e-20f);
 #pragma unroll
@@ -1290,15 +1334,15 @@ __device__ __forceinline__ RadRow<nq> rad_row(const DiskDev& D, int r, int g, in
 // van Leer slopes at row r from rows r-1, r, r+1 (StarRadKernel; zero on the
 // first and last ring): g[c] for the quotients, gs for the density.
 template <int nq>
-__device__ __forceinline__ void rad_slopes(const DiskDev& D, int r, const RadRow<nq>& A, const RadRow<nq>& Bm,
+__device__ __forceinline__ void rad_slopes(const TrView& V, int r, const RadRow<nq>& A, const RadRow<nq>& Bm,
                                            const RadRow<nq>& Cp, float* g, float& gs) {
-  if (r <= 0 || r >= D.nrad - 1) {
+  if (r <= 0 || r >= V.nrad - 1) {
 #pragma unroll
     for (int c = 0; c < nq; c++) g[c] = 0.0f;
     gs = 0.0f;
     return;
   }
-  const float im = __ldg(D.invdiffRmed + r), ip = __ldg(D.invdiffRmed + r + 1);
+  const float im = __ldg(V.invdiffRmed + r), ip = __ldg(V.invdiffRmed + r + 1);
 #pragma unroll
   for (int c = 0; c < nq; c++) g[c] = vl_rad_slope(A.W[c], Bm.W[c], Cp.W[c], im, ip);
   gs = vl_rad_slope(A.S, Bm.S, Cp.S, im, ip);
@@ -1308,10 +1352,10 @@ __device__ __forceinline__ void rad_slopes(const DiskDev& D, int r, const RadRow
 // (hi) for radial velocity vr (StarRadKernel2, Kernels.cu:929-947); zero on
 // the inner edge and beyond the outer ring.
 template <int nq>
-__device__ __forceinline__ void rad_face(const DiskDev& D, int b, float vr, float dt, const RadRow<nq>& lo,
+__device__ __forceinline__ void rad_face(const TrView& V, int b, float vr, float dt, const RadRow<nq>& lo,
                                          const RadRow<nq>& hi, const float* glo, float gslo, const float* ghi,
                                          float gshi, float* qs, float& ds) {
-  const int nrad = D.nrad;
+  const int nrad = V.nrad;
   if (b <= 0 || b >= nrad) {
 #pragma unroll
     for (int c = 0; c < nq; c++) qs[c] = 0.0f;
@@ -1319,13 +1363,13 @@ __device__ __forceinline__ void rad_face(const DiskDev& D, int b, float vr, floa
     return;
   }
   if (vr > 0.0f) {
-    const float h = fm(__ldg(D.Rmed + b) - __ldg(D.Rmed + b - 1) - fm(vr, dt), 0.5f);
+    const float h = fm(__ldg(V.Rmed + b) - __ldg(V.Rmed + b - 1) - fm(vr, dt), 0.5f);
 #pragma unroll
     for (int c = 0; c < nq; c++) qs[c] = lo.W[c] + fm(h, glo[c]);
     ds = lo.S + fm(h, gslo);
   } else {
-    const float rp = (b + 1 <= nrad - 1) ? __ldg(D.Rmed + b + 1) : 0.0f;  // only meets a zero slope
-    const float h = fm(rp - __ldg(D.Rmed + b) + fm(vr, dt), 0.5f);
+    const float rp = (b + 1 <= nrad - 1) ? __ldg(V.Rmed + b + 1) : 0.0f;  // only meets a zero slope
+    const float h = fm(rp - __ldg(V.Rmed + b) + fm(vr, dt), 0.5f);
 #pragma unroll
     for (int c = 0; c < nq; c++) qs[c] = hi.W[c] - fm(h, ghi[c]);
     ds = hi.S - fm(h, gshi);
@@ -1338,38 +1382,40 @@ __device__ __forceinline__ void rad_face(const DiskDev& D, int b, float vr, floa
 // lost0 (may be null): receives the density's varq at ring 0, the mass that
 // leaves through the inner edge (LostByDisk, Kernels.cu:941-944).
 template <int nq>
-__device__ __forceinline__ void rad_march(const DiskDev& D, int ia, int ib, int g, float dt, float Om,
+__device__ __forceinline__ void rad_march(const TrView& V, int ia, int ib, int g, float dt, float Om,
                                           float dtheta, float* out, int ostride_c, int ostride_r, float* lost0) {
-  const int nsec = D.nsec;
+  const int nsec = V.nsec;
   const int gp = g + 1 == nsec ? 0 : g + 1;
-  RadRow<nq> R0 = rad_row<nq>(D, ia - 1, g, gp, Om);  // row i-1 for the first slope
-  RadRow<nq> R1 = rad_row<nq>(D, ia, g, gp, Om);      // row i
-  RadRow<nq> R2 = rad_row<nq>(D, ia + 1, g, gp, Om);  // row i+1
+  RadRow<nq> R0 = rad_row<nq>(V, ia - 1, g, gp, Om);  // row i-1 for the first slope
+  RadRow<nq> R1 = rad_row<nq>(V, ia, g, gp, Om);      // row i
+  RadRow<nq> R2 = rad_row<nq>(V, ia + 1, g, gp, Om);  // row i+1
   float G0[nq], G1[nq], gs0, gs1, qs[nq], ds;
   {
-    RadRow<nq> Rm = rad_row<nq>(D, ia - 2, g, gp, Om);
-    rad_slopes<nq>(D, ia - 1, Rm, R0, R1, G0, gs0);  // slope at row i-1
+    RadRow<nq> Rm = rad_row<nq>(V, ia - 2, g, gp, Om);
+    rad_slopes<nq>(V, ia - 1, Rm, R0, R1, G0, gs0);  // slope at row i-1
   }
-  rad_slopes<nq>(D, ia, R0, R1, R2, G1, gs1);  // slope at row i
-  float vr0 = __ldg(D.vrad + (long long)ia * nsec + g);
-  rad_face<nq>(D, ia, vr0, dt, R0, R1, G0, gs0, G1, gs1, qs, ds);
+  rad_slopes<nq>(V, ia, R0, R1, R2, G1, gs1);  // slope at row i
+  float vr0 = __ldg(V.vrad + ia * nsec + g);
+  rad_face<nq>(V, ia, vr0, dt, R0, R1, G0, gs0, G1, gs1, qs, ds);
+  const float dtdth = fm(dt, dtheta);
   // at most FARGO_BAND rings: unrolled, so that later rows load early
 #pragma unroll
   for (int k = 0; k < FARGO_BAND; k++) {
     const int i = ia + k;
     if (i >= ib) break;
-    RadRow<nq> R3 = rad_row<nq>(D, i + 2, g, gp, Om);
+    RadRow<nq> R3 = rad_row<nq>(V, i + 2, g, gp, Om);
     float G2[nq], gs2;
-    rad_slopes<nq>(D, i + 1, R1, R2, R3, G2, gs2);  // slope at row i+1
-    const float vr1 = __ldg(D.vrad + (long long)(i + 1) * nsec + g);  // row nrad is the zero ghost row
+    rad_slopes<nq>(V, i + 1, R1, R2, R3, G2, gs2);  // slope at row i+1
+    const float vr1 = __ldg(V.vrad + (i + 1) * nsec + g);  // row nrad is the zero ghost row
     float qs1[nq], ds1;
-    rad_face<nq>(D, i + 1, vr1, dt, R1, R2, G1, gs1, G2, gs2, qs1, ds1);
-    const float Ri = __ldg(D.Rinf + i), Rs = __ldg(D.Rsup + i), iS = __ldg(D.invSurf + i);
+    rad_face<nq>(V, i + 1, vr1, dt, R1, R2, G1, gs1, G2, gs2, qs1, ds1);
+    const float Ri = __ldg(V.Rinf + i), Rs = __ldg(V.Rsup + i), iS = __ldg(V.invSurf + i);
+    const float fi = fm(dtdth, Ri), fs = fm(dtdth, Rs);
     float* o = out + (i - ia) * ostride_r;
 #pragma unroll
     for (int c = 0; c < nq; c++) {
-      float varq = fm(fm(fm(fm(fm(dt, dtheta), Ri), qs[c]), ds), vr0);
-      varq -= fm(fm(fm(fm(fm(dt, dtheta), Rs), qs1[c]), ds1), vr1);
+      float varq = fm(fm(fm(fi, qs[c]), ds), vr0);
+      varq -= fm(fm(fm(fs, qs1[c]), ds1), vr1);
       o[c * ostride_c] = R1.Q[c] + fm(varq, iS);
       if (c == nq - 1 && i == 0 && lost0) *lost0 = varq;
     }
@@ -1488,59 +1534,61 @@ size_t fargo_transport_smem_bytes(int adiabatic) {
 
 // The residual and constant-residual van Leer sweeps of OneWindTheta
 // (StarThetaKernel, StarThetaKernel2, VanLeerThetaKernel, Kernels.cu:1157-1273)
-// on one ring's window of L = S + 8 points, by one warp: lane l holds points
+// on one ring's window of 256 points, by one warp: lane l holds points
 // 8l .. 8l+7 in registers and takes its neighbours' edge values by shuffle.
-// sRr: the ring's radial results [nq][kPad] and v_theta [kPad] on the union
-// window (point x at union column off + x); the swept values go back to
-// sRr[c][pidx(x)].  The slopes are zero on the window's first and last point,
-// whose values (and those of the next point in) never reach the output.
+// sRr: the ring's radial results [nq][kPad] and v_theta [kPad] (point x at
+// pidx(x)); the swept values go back to the same places.  The window's
+// points 0..3 and L-4.. (and any beyond L) are halo: each sweep's result at
+// a point depends on the points within two of it, so after the two sweeps
+// the values at 4 .. L-5 do not depend on anything outside the window and
+// the edges need no special case (their values are never stored).
 template <int nq>
-__device__ __forceinline__ void sweep_ring(float* sRr, int off, int L, float VMed, float vconst, bool fast,
-                                           float dt, float dxtheta, float invdxtheta, float invsurf,
-                                           float dxrad) {
+__device__ __forceinline__ void sweep_ring(float* sRr, float VMed, float vconst, bool fast, float dt,
+                                           float dxtheta, float invdxtheta, float invsurf, float dxrad) {
   const int lane = threadIdx.x & 31;
-  const int x0 = 8 * lane;
+  const int b0 = 9 * lane;  // pidx(8 * lane): points 8l .. 8l+7 are contiguous
   float q[nq][8], v[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) {
-    const int x = x0 + k;
-    const bool in = x < L;
-    const int id = pidx(off + x);
 #pragma unroll
-    for (int c = 0; c < nq; c++) q[c][k] = in ? sRr[c * kPad + id] : 0.0f;
-    float vres = (in ? sRr[nq * kPad + id] : 0.0f) - VMed;
+    for (int c = 0; c < nq; c++) q[c][k] = sRr[c * kPad + b0 + k];
+    float vres = sRr[nq * kPad + b0 + k] - VMed;
     if (!fast) vres = vconst + vres;
     v[k] = vres;
   }
   if (!fast) vconst = 0.0f;
-  auto slope = [&](float wm, float w0, float wp, int x) -> float {
-    if (x <= 0 || x >= L - 1) return 0.0f;
+  auto slope = [&](float wm, float w0, float wp) -> float {
     float dqm = (w0 - wm);
     float dqp = (wp - w0);
     if (fm(dqp, dqm) > 0.0f) return fm(__fdividef(fm(dqp, dqm), dqp + dqm), invdxtheta);
     return 0.0f;
   };
   for (int sweep = 0; sweep < 2; sweep++) {
-    float vv[8], rr[8], S[8], GS[8], sD[8];
+    // upwind side of each point's left interface and the distance to it:
+    // ksi > 0 takes point k-1 at dxtheta - ksi, else point k at -(dxtheta + ksi)
+    float vv[8], rr[8], S[8], GS[8], sD[8], h[8];
+    unsigned up = 0;
 #pragma unroll
     for (int k = 0; k < 8; k++) {
       vv[k] = (sweep == 1) ? vconst : v[k];
       S[k] = q[nq - 1][k];
       rr[k] = __fdividef(1.0f, S[k] + 1e-20f);
+      const float ksi = fm(vv[k], dt);
+      if (ksi > 0.0f) up |= 1u << k;
+      h[k] = (ksi > 0.0f) ? dxtheta - ksi : dxtheta + ksi;
     }
     const float Sl = __shfl_up_sync(0xffffffffu, S[7], 1);
     const float Sr = __shfl_down_sync(0xffffffffu, S[0], 1);
 #pragma unroll
-    for (int k = 0; k < 8; k++) GS[k] = slope(k ? S[k - 1] : Sl, S[k], k < 7 ? S[k + 1] : Sr, x0 + k);
+    for (int k = 0; k < 8; k++) GS[k] = slope(k ? S[k - 1] : Sl, S[k], k < 7 ? S[k + 1] : Sr);
     const float GSl = __shfl_up_sync(0xffffffffu, GS[7], 1);
-    // DensStar (StarThetaKernel2 on the density)
+    // DensStar (StarThetaKernel2 on the density); a - fm(h, g) = a + fm(h, -g)
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-      const float ksi = fm(vv[k], dt);
-      if (ksi > 0.0f)
-        sD[k] = (x0 + k > 0) ? (k ? S[k - 1] : Sl) + fm(dxtheta - ksi, k ? GS[k - 1] : GSl) : 0.0f;
-      else
-        sD[k] = S[k] - fm(dxtheta + ksi, GS[k]);
+      const bool u = (up >> k) & 1u;
+      const float su = u ? (k ? S[k - 1] : Sl) : S[k];
+      const float gu = u ? (k ? GS[k - 1] : GSl) : -GS[k];
+      sD[k] = su + fm(h[k], gu);
     }
     // every quantity, density last; all quotients use the pre-sweep density
 #pragma unroll
@@ -1551,26 +1599,22 @@ __device__ __forceinline__ void sweep_ring(float* sRr, int off, int L, float VMe
       const float Wl = __shfl_up_sync(0xffffffffu, W[7], 1);
       const float Wr = __shfl_down_sync(0xffffffffu, W[0], 1);
 #pragma unroll
-      for (int k = 0; k < 8; k++) G[k] = slope(k ? W[k - 1] : Wl, W[k], k < 7 ? W[k + 1] : Wr, x0 + k);
+      for (int k = 0; k < 8; k++) G[k] = slope(k ? W[k - 1] : Wl, W[k], k < 7 ? W[k + 1] : Wr);
       const float Gl = __shfl_up_sync(0xffffffffu, G[7], 1);
 #pragma unroll
       for (int k = 0; k < 8; k++) {
-        const float ksi = fm(vv[k], dt);
-        float qr;
-        if (ksi > 0.0f)
-          qr = (x0 + k > 0) ? (k ? W[k - 1] : Wl) + fm(dxtheta - ksi, k ? G[k - 1] : Gl) : 0.0f;
-        else
-          qr = W[k] - fm(dxtheta + ksi, G[k]);
+        const bool u = (up >> k) & 1u;
+        const float wu = u ? (k ? W[k - 1] : Wl) : W[k];
+        const float gu = u ? (k ? G[k - 1] : Gl) : -G[k];
+        const float qr = wu + fm(h[k], gu);
         F[k] = fm(fm(fm(dxrad, qr), sD[k]), vv[k]);  // flux through the left interface of point k
       }
       const float Fr = __shfl_down_sync(0xffffffffu, F[0], 1);
 #pragma unroll
       for (int k = 0; k < 8; k++) {
-        if (x0 + k < L - 1) {
-          float varq = F[k];
-          varq -= (k < 7 ? F[k + 1] : Fr);
-          q[c][k] += fm(varq, invsurf);
-        }
+        float varq = F[k];
+        varq -= (k < 7 ? F[k + 1] : Fr);
+        q[c][k] += fm(varq, invsurf);
       }
     }
   }
@@ -1578,7 +1622,7 @@ __device__ __forceinline__ void sweep_ring(float* sRr, int off, int L, float VMe
 #pragma unroll
   for (int k = 0; k < 8; k++)
 #pragma unroll
-    for (int c = 0; c < nq; c++) sRr[c * kPad + pidx(x0 + k)] = q[c][k];
+    for (int c = 0; c < nq; c++) sRr[c * kPad + b0 + k] = q[c][k];
   __syncwarp();
 }
 
@@ -1629,12 +1673,14 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
       s_vc[p] = D.tvconst[i0 + p];
     }
     if (p < L) {
+      const TrView V = {D.dens, D.vrad, D.vtheta, D.energy, D.Rmed, D.invdiffRmed, D.Rinf, D.Rsup, D.invSurf,
+                        nsec, nrad};
       int g = (g0 - 4 + p) % nsec;
       if (g < 0) g += nsec;
       float* o = sR + pidx(p);
-      rad_march<nq>(D, i0, i0 + nb, g, dt, Om, dtheta, o, kPad, (nq + 1) * kPad,
+      rad_march<nq>(V, i0, i0 + nb, g, dt, Om, dtheta, o, kPad, (nq + 1) * kPad,
                     (D.OpenInner && i0 == 0) ? sL + pidx(p) : nullptr);
-      for (int r = 0; r < nb; r++) o[(r * (nq + 1) + nq) * kPad] = __ldg(D.vtheta + (size_t)(i0 + r) * nsec + g);
+      for (int r = 0; r < nb; r++) o[(r * (nq + 1) + nq) * kPad] = __ldg(V.vtheta + (i0 + r) * nsec + g);
     }
     __syncthreads();
     const int r = warp;
@@ -1643,7 +1689,7 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
       float* sRr = sR + (size_t)r * (nq + 1) * kPad;
       const float Rm = D.Rmed[i];
       const float dxtheta = fm(dtheta, Rm);
-      sweep_ring<nq>(sRr, 0, L, s_vmed[r], s_vc[r], fast, dt, dxtheta, 1.0f / dxtheta, 1.0f / D.Surf[i],
+      sweep_ring<nq>(sRr, s_vmed[r], s_vc[r], fast, dt, dxtheta, 1.0f / dxtheta, 1.0f / D.Surf[i],
                      fm(D.Rsup[i] - D.Rinf[i], dt));
       // window point x is source sector g0 + x - 4, stored at output sector
       // jb + x - 4 (jb < nsec and x - 4 < S <= nsec: one wrap at most)
@@ -1695,7 +1741,7 @@ __device__ void compact_active(const BatchDev& B) {
     B.act_grp_off[na] = gg;
     B.act_tile_off[na] = tt;
     B.act_ctile_off[na] = ct;
-    ct += D.nrad;
+    ct += fargo_cfl_tiles(D.nrad, D.nsec);
     B.act_vtile_off[na] = vt;
     vt += vtiles_of(D);
     cc += (long long)D.nrad * D.nsec;
@@ -1838,15 +1884,15 @@ __global__ void __launch_bounds__(kThreads) k_bc_rings(BatchDev B) {
   __shared__ DiskDev sD;
   const int tid = threadIdx.x;
   const int na = B.act[0];
-  const int ntile = na > 0 ? B.act_ctile_off[na] : 0;
+  const int ntile = na > 0 ? B.act_ring_off[na] : 0;
   const int per = (ntile + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
   int lo = 0, hi = -1;
   for (int t = t0; t < t1; t++) {
     if (t >= hi) {  // block-uniform: entering a disk
-      const int a = find_range(B.act_ctile_off, na, t);
-      lo = B.act_ctile_off[a];
-      hi = B.act_ctile_off[a + 1];
+      const int a = find_range(B.act_ring_off, na, t);
+      lo = B.act_ring_off[a];
+      hi = B.act_ring_off[a + 1];
       __syncthreads();
       copy_words(&sD, B.disks + B.act_disk[a], sizeof(DiskDev));
       __syncthreads();
@@ -2214,7 +2260,7 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
     k_bc_disk<<<b.ndisk, kThreads, 0, s>>>(b);
   }
   REC();
-  k_energy<<<b.g_energy, kThreads, 0, s>>>(b);
+  if (b.ntheta_adi) k_energy<<<b.g_energy, kThreads, 0, s>>>(b);  // adiabatic disks only
   REC();
   k_ring_mean<1><<<b.grp_grid, kRMT, fargo_ring_mean_smem_bytes(), s>>>(b);
   REC();
@@ -2266,7 +2312,7 @@ cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int ni
     return cudaSuccess;
   };
   cudaError_t e;
-  if ((e = wave(fargo_cfl_kernel(b.max_body), kThreads, 0, b.nring, &b.g_cfl))) return e;
+  if ((e = wave(fargo_cfl_kernel(b.max_body), kThreads, 0, b.ncfl, &b.g_cfl))) return e;
   if ((e = wave((const void*)k_source1, kThreads, 0, ncell_tiles, &b.g_source1))) return e;
   if ((e = wave((const void*)k_potential, kThreads, 0, ncell_tiles, &b.g_potential))) return e;
   if ((e = wave((const void*)k_viscosity, kThreads, 0, ncell_tiles, &b.g_viscosity))) return e;
@@ -2276,11 +2322,11 @@ cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int ni
   return wave((const void*)k_transport<6>, kTT, fargo_transport_smem_bytes(1), nitems, &b.g_transport);
 }
 
-// Launches of one substep: 11 kernels, both transport forms in a batch of
-// isothermal and adiabatic disks, two per boundary call when a disk has a
-// non-rigid boundary.
+// Launches of one substep: 10 kernels, the energy kernel when a disk is
+// adiabatic, both transport forms in a batch of isothermal and adiabatic
+// disks, two per boundary call when a disk has a non-rigid boundary.
 int fargo_substep_launches(const BatchDev& b) {
-  return 11 + ((b.ntheta_iso && b.ntheta_adi) ? 1 : 0) + (b.any_bc ? 6 : 0);
+  return 10 + (b.ntheta_adi ? 1 : 0) + ((b.ntheta_iso && b.ntheta_adi) ? 1 : 0) + (b.any_bc ? 6 : 0);
 }
 
 void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s) {
