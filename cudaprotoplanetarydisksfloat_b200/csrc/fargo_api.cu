@@ -116,6 +116,8 @@ int body_count(const fargo_planets* pl) {
 fargo_status check_params(fargo_batch* b, const fargo_params* p, const fargo_planets* pl) {
   if (p->NRAD < 4 || p->NSEC < 4) return set_err(b, FARGO_EINVAL, "NRAD and NSEC must be >= 4");
   if (p->NSEC > 16384) return set_err(b, FARGO_EINVAL, "NSEC > 16384 is not supported");
+  if ((long long)(p->NRAD + 1) * p->NSEC > 0x7fffffffLL)
+    return set_err(b, FARGO_EINVAL, "(NRAD+1)*NSEC must fit a 32-bit cell index, as in the reference's kernels");
   if (p->NonReflecting && p->NSEC <= 128)
     return set_err(b, FARGO_EINVAL,
                    "InnerBoundary NONREFLECTING needs NSEC > 128 (the reference's DeviceReduce launches no block "

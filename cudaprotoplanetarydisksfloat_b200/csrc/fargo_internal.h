@@ -69,7 +69,7 @@ struct DiskCtl {
 
 // CFL/force tiles: FARGO_CFL_TILE consecutive cells of one disk, each with its
 // own minimum and force partials
-#define FARGO_CFL_TILE 1024
+#define FARGO_CFL_TILE 4096
 inline __host__ __device__ int fargo_cfl_tiles(int nrad, int nsec) {
   return (int)(((long long)nrad * nsec + FARGO_CFL_TILE - 1) / FARGO_CFL_TILE);
 }

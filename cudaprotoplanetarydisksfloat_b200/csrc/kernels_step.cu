@@ -376,7 +376,10 @@ __device__ __forceinline__ void copy_words(void* dst, const void* src, int bytes
 
 // adi_only: skip the tiles of isothermal disks (energy kernels).  A thread's
 // cell advances by kThreads sectors from one tile to the next, so the ring
-// division runs only on entering a disk.
+// division runs only on entering a disk.  The tiles of one disk form an
+// inner loop without barriers or shared-memory writes; as the bodies store
+// with stg (below), the compiler may keep the disk's fields in registers
+// across it.
 template <bool adi_only, class Body>
 __device__ __forceinline__ void for_active_cells(const BatchDev& B, Body body) {
   __shared__ DiskDev sD;
@@ -385,40 +388,42 @@ __device__ __forceinline__ void for_active_cells(const BatchDev& B, Body body) {
   const int ntile = B.act_tile_off[na];
   const int per = (ntile + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
-  int lo = 0, hi = -1, i = 0, j = 0;
-  for (int t = t0; t < t1; t++) {
-    if (t >= hi) {  // block-uniform
-      const int a = find_range(B.act_tile_off, na, t);
-      lo = B.act_tile_off[a];
-      hi = B.act_tile_off[a + 1];
-      __syncthreads();
-      copy_words(&sD, B.disks + B.act_disk[a], sizeof(DiskDev));
-      __syncthreads();
-      if (!sD.IsDisk || (adi_only && !sD.Adiabatic)) {  // nothing to do on this disk
-        t = hi - 1;
-        continue;
-      }
-      const int loc = (t - lo) * kThreads + threadIdx.x;
-      i = loc / sD.nsec;
-      j = loc - i * sD.nsec;
-    } else {
-      const int nsec = sD.nsec;
+  int t = t0;
+  while (t < t1) {  // block-uniform: one disk per pass
+    const int a = find_range(B.act_tile_off, na, t);
+    const int lo = B.act_tile_off[a], te = min(t1, B.act_tile_off[a + 1]);
+    __syncthreads();
+    copy_words(&sD, B.disks + B.act_disk[a], sizeof(DiskDev));
+    __syncthreads();
+    if (!sD.IsDisk || (adi_only && !sD.Adiabatic)) {  // nothing to do on this disk
+      t = te;
+      continue;
+    }
+    const int nsec = sD.nsec, nrad = sD.nrad;
+    const int loc = (t - lo) * kThreads + threadIdx.x;
+    int i = loc / nsec, j = loc - i * nsec;
+    for (; t < te; t++) {
+      if (i < nrad) body(sD, sD.ctl, i, j, i * nsec + j, jwrap_m(j, nsec), jwrap_p(j, nsec));
       j += kThreads;
       while (j >= nsec) {
         j -= nsec;
         i++;
       }
     }
-    if (i < sD.nrad) {
-      const int ns = sD.nsec;
-      body(sD, sD.ctl, i, j, (long long)i * ns + j, jwrap_m(j, ns), jwrap_p(j, ns));
-    }
   }
+}
+
+// Store to global memory for the cell kernels.  None of them reads back in
+// the same launch what it stores, so the store is not ordered against the
+// compiler's loads (no memory clobber): loads of the disk's fields from
+// shared memory need not be repeated after it.
+__device__ __forceinline__ void stg(float* p, float v) {
+  asm volatile("st.global.f32 [%0], %1;\n" ::"l"(p), "f"(v));
 }
 
 #define CELL_BEGIN_T(adi_only)                                                                          \
   for_active_cells<adi_only>(B, [&](const DiskDev& D, const DiskCtl* C, const int i, const int j,         \
-                                    const long long l, const int jm, const int jp) {                     \
+                                    const int l, const int jm, const int jp) {                           \
     const int nsec = D.nsec, nrad = D.nrad;                                                             \
     (void)nrad;                                                                                         \
     (void)jm;                                                                                           \
@@ -520,6 +525,7 @@ __device__ float block_min_f(float v, float* sh) {
 // copy of the disk's control block (sC), written back at the end.
 constexpr int kRkShared = 16;  // planets whose RK5 scratch fits in shared memory
 __device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const double* s_sum, double* work);
+template <int NB>
 __device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* Cg, DiskCtl* sC, float* shf, double* s_sum,
                                        double* s_work) {
   const int nrad = D.nrad, nsec = D.nsec, tid = threadIdx.x;
@@ -540,17 +546,26 @@ __device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* Cg, DiskCtl* s
   }
   float newdt = block_min_f(m, shf);
   // disk-force sums over the tiles in a fixed order: every thread a strided
-  // share (partials are [sum][tile]), the warps by shuffle, then the warps in
-  // order (s_work is free until the planet update)
-  const int nbody = Cg->nbody, nsum = 4 * nbody;
+  // share of the tiles for all sums at once (partials are [sum][tile]), the
+  // warps by shuffle, then the warps in order (s_work is free until the
+  // planet update)
+  const int nbody = min(Cg->nbody, NB), nsum = 4 * nbody;
   const int w = tid >> 5, l = tid & 31, nw = blockDim.x >> 5;
-  for (int q = 0; q < nsum; q++) {
-    const double* P = D.partials + (size_t)q * nct;
-    double acc = 0.0;
-#pragma unroll 4
-    for (int t = tid; t < nct; t += blockDim.x) acc += __ldcg(P + t);
-    acc = warp_sum_d(acc);
-    if (l == 0) s_work[q * nw + w] = acc;
+  double acc[4 * NB];
+#pragma unroll
+  for (int q = 0; q < 4 * NB; q++) acc[q] = 0.0;
+#pragma unroll 2
+  for (int t = tid; t < nct; t += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < 4 * NB; q++)
+      if (q < nsum) acc[q] += __ldcg(D.partials + (size_t)q * nct + t);
+  }
+#pragma unroll
+  for (int q = 0; q < 4 * NB; q++) {
+    if (q < nsum) {
+      const double v = warp_sum_d(acc[q]);
+      if (l == 0) s_work[q * nw + w] = v;
+    }
   }
   __syncthreads();
   if (tid < nsum) {
@@ -715,7 +730,7 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
     __syncthreads();
     if (s_ticket + (unsigned)run == (unsigned)fargo_cfl_tiles(sD.nrad, sD.nsec)) {
       __threadfence();
-      finish_cfl_and_planets(sD, Cr, &sC, s_min[0], s_sum, s_work);
+      finish_cfl_and_planets<NB>(sD, Cr, &sC, s_min[0], s_sum, s_work);
     }
     run = 0;
     __syncthreads();
@@ -754,7 +769,7 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
       const float hillcutfactor = (float)kh / (float)(FARGO_DIMFXY - 1);
       const int c0 = k * FARGO_CFL_TILE + tid;
       int i = c0 / nsec, j = c0 - i * nsec;
-#pragma unroll
+#pragma unroll 4
       for (int c = 0; c < kCflCells; c++) {
         if (i < nrad) {
           const long long q = (long long)i * nsec + j;
@@ -890,11 +905,11 @@ __device__ __forceinline__ float potential_at(const DiskDev& D, const DiskCtl* C
 // per substep (Substep1 reads it at three cells each).
 __global__ void __launch_bounds__(kThreads) k_potential(BatchDev B) {
   CELL_BEGIN
-  D.phi[l] = potential_at(D, C, i, j);
+  stg(D.phi + l, potential_at(D, C, i, j));
   CELL_END
 }
 
-__device__ __forceinline__ float pressure_at(const DiskDev& D, long long l, int i) {
+__device__ __forceinline__ float pressure_at(const DiskDev& D, int l, int i) {
   if (!D.Adiabatic) {
     float cs = D.cs_ring[i];
     return D.dens[l] * cs * cs;
@@ -915,19 +930,19 @@ __global__ void __launch_bounds__(kThreads, 4) k_source1(BatchDev B) {
   const float dom = D.Evanescent ? 0.0f : C->domega;
   const float* Vt = D.vtheta;
   const float* Dn = D.dens;
-  auto vth = [&](long long q, int r) -> float { return dom != 0.0f ? Vt[q] - dom * D.Rmed[r] : Vt[q]; };
+  auto vth = [&](int q, int r) -> float { return dom != 0.0f ? Vt[q] - dom * D.Rmed[r] : Vt[q]; };
   const float P0 = pressure_at(D, l, i);
   const float Phi0 = D.phi[l];  // k_potential
   // ComputeTemperatureField divides the pressure of the substep start by the
   // final density (SourceEuler.cu:280,293): keep the last substep's pressure
-  if (!D.Adiabatic && !C->more) D.pres[l] = P0;
+  if (!D.Adiabatic && !C->more) stg(D.pres + l, P0);
   if (i > 0) {
-    const long long lm = l - nsec;
+    const int lm = l - nsec;
     const float Pm = pressure_at(D, lm, i - 1);
     const float Phim = D.phi[l - nsec];
     float gradp = (P0 - Pm) * 2.0f / (Dn[l] + Dn[lm]) * D.invdiffRmed[i];
     float gradphi = (Phi0 - Phim) * D.invdiffRmed[i];
-    const long long lp = (long long)i * nsec + jp;
+    const int lp = i * nsec + jp;
     float vt2 = vth(l, i) + vth(lp, i) + vth(lm, i - 1) + vth(lp - nsec, i - 1);
     vt2 = vt2 * 0.25f + D.Rinf[i] * OmegaFrame;
     vt2 = vt2 * vt2;
@@ -935,12 +950,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_source1(BatchDev B) {
     if (D.SelfGravity)
       vri += dt * ((D.Rinf[i] - D.Rmed[i - 1]) * D.sg_accr[l] + (D.Rmed[i] - D.Rinf[i]) * D.sg_accr[lm]) *
              D.invdiffRmed[i];
-    D.vri[l] = vri;
+    stg(D.vri + l, vri);
   } else {
-    D.vri[l] = 0.0f;  // VradInt's ring 0 is never written by the reference: zero
+    stg(D.vri + l, 0.0f);  // VradInt's ring 0 is never written by the reference: zero
   }
   {
-    const long long la = (long long)i * nsec + jm;
+    const int la = i * nsec + jm;
     float dxtheta = 2.0f * (float)PI_D / (float)nsec * D.Rmed[i];
     float invdxtheta = 1.0f / dxtheta;
     const float Pa = pressure_at(D, la, i);
@@ -952,10 +967,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_source1(BatchDev B) {
     if (D.SelfGravity) {
       // the reference reads SG_Acct[i*nsec + (j-1)%nsec]: for j = 0 that is
       // the last sector of ring i-1 (ring 0: taken from ring 0 itself)
-      long long lq = (j > 0) ? l - 1 : (i > 0 ? l - 1 : (long long)nsec - 1);
+      int lq = (j > 0) ? l - 1 : (i > 0 ? l - 1 : nsec - 1);
       vti += 0.5f * dt * (D.sg_acct[l] + D.sg_acct[lq]);
     }
-    D.vti[l] = vti;
+    stg(D.vti + l, vti);
   }
   CELL_END
 }
@@ -969,9 +984,9 @@ struct Tau {
 
 __device__ __forceinline__ Tau viscous_terms(const DiskDev& D, const float* Vr, const float* Va, int i, int j,
                                              int nsec) {
-  const long long l = (long long)i * nsec + j;
+  const int l = i * nsec + j;
   const int jp = jwrap_p(j, nsec), jm = jwrap_m(j, nsec);
-  const long long lp = (long long)i * nsec + jp;
+  const int lp = i * nsec + jp;
   const float* Dn = D.dens;
   const float nu = D.visc[i];
   Tau t;
@@ -984,10 +999,10 @@ __device__ __forceinline__ Tau viscous_terms(const DiskDev& D, const float* Vr, 
   t.pp = 2.0f * Dn[l] * nu * (DPP - D.onethird * divV);
   t.rp = 0.0f;
   if (i > 0) {
-    const long long lm = (long long)i * nsec + jm;
+    const int lm = i * nsec + jm;
     float DRP = 0.5f * (D.Rinf[i] * (Va[l] * D.invRmed[i] - Va[l - nsec] * D.invRmed[i - 1]) * D.invdiffRmed[i] +
                         (Vr[l] - Vr[lm]) * D.invdphi * D.invRinf[i]);
-    t.rp = 0.5f * (Dn[l] + Dn[l - nsec] + Dn[(long long)i * nsec] + Dn[lm - nsec]) * nu * DRP;
+    t.rp = 0.5f * (Dn[l] + Dn[l - nsec] + Dn[i * nsec] + Dn[lm - nsec]) * nu * DRP;
   }
   return t;
 }
@@ -1025,7 +1040,8 @@ __device__ void vkep_pair(const DiskDev& D, const DiskCtl* C, float* vin, float*
 // reads as VradInt / VthetaInt: writing them in place would race with the
 // neighbouring tiles' halo reads.
 constexpr int kVR = 8, kVC = 64;                        // tile rows, columns
-constexpr int kSR = kVR + 4, kSC = kVC + 4;             // staged rows, columns
+constexpr int kSO = 4;                                  // staged columns left of the tile
+constexpr int kSR = kVR + 4, kSC = kVC + 2 * kSO;       // staged rows, columns (whole 16-byte chunks)
 constexpr int kTR = kVR + 2, kTC = kVC + 2;             // stress rows, columns
 __device__ __forceinline__ int vtiles_of(const DiskDev& D) {
   return ((D.nrad + kVR - 1) / kVR) * ((D.nsec + kVC - 1) / kVC);
@@ -1037,6 +1053,13 @@ __device__ __forceinline__ void cp_async4(float* smem, const float* gmem, bool v
   const int sz = valid ? 4 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz) : "memory");
 }
+// 16-byte asynchronous global -> shared copy, both addresses 16-byte
+// aligned (zero-filled when !valid)
+__device__ __forceinline__ void cp_async16(float* smem, const float* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int n>
 __device__ __forceinline__ void cp_async_wait() {
@@ -1045,7 +1068,8 @@ __device__ __forceinline__ void cp_async_wait() {
 
 __global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
   __shared__ DiskDev sD;
-  __shared__ float sVrb[2][kSR][kSC], sVab[2][kSR][kSC], sDnb[2][kSR][kSC], sD0b[2][kSR];
+  __shared__ __align__(16) float sVrb[2][kSR][kSC], sVab[2][kSR][kSC], sDnb[2][kSR][kSC];
+  __shared__ float sD0b[2][kSR];
   __shared__ float sTrr[kTR][kTC], sTpp[kTR][kTC], sTrp[kTR][kTC];
   const int tid = threadIdx.x;
   const int na = B.act[0];
@@ -1053,21 +1077,39 @@ __global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
   const int per = (ntile + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
   // issue the asynchronous staging of tile lt of the disk in sD into buffer bf:
-  // rows i0-2 .. i0+kVR+1 (row NRAD is the ghost row), columns j0-2 .. j0+kVC+1
+  // rows i0-2 .. i0+kVR+1 (row NRAD is the ghost row), columns j0-kSO ..
+  // j0+kVC+kSO-1 (azimuth periodic).  With NSEC a multiple of 4 every
+  // 4-column chunk is one aligned 16-byte copy (j0 is a multiple of 64 and a
+  // wrap moves a chunk by NSEC); otherwise column by column.
   auto stage = [&](int lt, int bf) {
     const int nsec = sD.nsec, nrad = sD.nrad;
     const int ncol = (nsec + kVC - 1) / kVC;
     const int i0 = (lt / ncol) * kVR, j0 = (lt % ncol) * kVC;
-    for (int q = tid; q < kSR * kSC; q += kThreads) {
-      const int r = q / kSC, c = q - r * kSC;
-      const int i = i0 - 2 + r;
-      int j = (j0 - 2 + c) % nsec;
-      if (j < 0) j += nsec;
-      const bool ok = i >= 0 && i <= nrad;
-      const size_t l = ok ? (size_t)i * nsec + j : 0;
-      cp_async4(&sVrb[bf][r][c], sD.vri + l, ok);
-      cp_async4(&sVab[bf][r][c], sD.vti + l, ok);
-      cp_async4(&sDnb[bf][r][c], sD.dens + l, ok);
+    if ((nsec & 3) == 0) {
+      constexpr int kCh = kSC / 4;  // chunks per staged row
+      for (int q = tid; q < kSR * kCh; q += kThreads) {
+        const int r = q / kCh, c = 4 * (q - r * kCh);
+        const int i = i0 - 2 + r;
+        int j = (j0 - kSO + c) % nsec;
+        if (j < 0) j += nsec;
+        const bool ok = i >= 0 && i <= nrad;
+        const int l = ok ? i * nsec + j : 0;
+        cp_async16(&sVrb[bf][r][c], sD.vri + l, ok);
+        cp_async16(&sVab[bf][r][c], sD.vti + l, ok);
+        cp_async16(&sDnb[bf][r][c], sD.dens + l, ok);
+      }
+    } else {
+      for (int q = tid; q < kSR * kSC; q += kThreads) {
+        const int r = q / kSC, c = q - r * kSC;
+        const int i = i0 - 2 + r;
+        int j = (j0 - kSO + c) % nsec;
+        if (j < 0) j += nsec;
+        const bool ok = i >= 0 && i <= nrad;
+        const int l = ok ? i * nsec + j : 0;
+        cp_async4(&sVrb[bf][r][c], sD.vri + l, ok);
+        cp_async4(&sVab[bf][r][c], sD.vti + l, ok);
+        cp_async4(&sDnb[bf][r][c], sD.dens + l, ok);
+      }
     }
     if (tid < kSR) {
       const int i = i0 - 2 + tid;
@@ -1114,7 +1156,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
         const int r = q / kTC, c = q - r * kTC;
         const int i = i0 - 1 + r;
         if (i < 0 || i >= nrad) continue;
-        const int rr = r + 1, cc = c + 1;  // staged indices of (i, j)
+        const int rr = r + 1, cc = c + kSO - 1;  // staged indices of (i, j)
         const float nu = D.visc[i];
         const float iRm = D.invRmed[i];
         float DRR = (sVr[rr + 1][cc] - sVr[rr][cc]) * D.invdiffRsup[i];
@@ -1145,7 +1187,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
       if (i >= nrad || j >= nsec) continue;
       const size_t l = (size_t)i * nsec + j;
       const int R = r + 1, Cc = c + 1;   // stress index of (i, j)
-      const int rr = r + 2, cc = c + 2;  // staged index of (i, j)
+      const int rr = r + 2, cc = c + kSO;  // staged index of (i, j)
       float vti = sVa[rr][cc], vri = sVr[rr][cc];
       if (D.IsDisk) {
         if (i > 0 && i < nrad - 1) {
@@ -1184,7 +1226,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_source2(BatchDev B) {
   const float dt = C->dtf;
   const float* Dn = D.dens;
   const float *VRI = D.trr, *VTI = D.tpp;  // viscosity-updated VradInt / VthetaInt (k_viscosity)
-  const long long lmj = (long long)i * nsec + jm, lpj = (long long)i * nsec + jp;
+  const int lmj = i * nsec + jm, lpj = i * nsec + jp;
   float qr = qvisc(VRI[l + nsec] - VRI[l], Dn[l]);
   float qt = qvisc(VTI[lpj] - VTI[l], Dn[l]);
   float vr_new = 0.0f;
@@ -1198,12 +1240,12 @@ __global__ void __launch_bounds__(kThreads, 6) k_source2(BatchDev B) {
   float vt_new = VTI[l] - dt * 2.0f / (Dn[l] + Dn[lmj]) * (qt - qtm) * invdxtheta;
   if (D.Adiabatic) {
     // EnergyInt goes to scratch: the boundary pass before Substep3 still sees the state energy
-    D.a1[l] = D.energy[l] - dt * qr * (VRI[l + nsec] - VRI[l]) * D.invdiffRsup[i] -
-                  dt * qt * (VTI[lpj] - VTI[l]) * invdxtheta;
+    stg(D.a1 + l, D.energy[l] - dt * qr * (VRI[l + nsec] - VRI[l]) * D.invdiffRsup[i] -
+                      dt * qt * (VTI[lpj] - VTI[l]) * invdxtheta);
   }
-  D.vrad[l] = vr_new;
-  D.vtheta[l] = vt_new;
-  if (i == nrad - 1) D.vtheta[l + nsec] = 0.0f;  // VthetaNew's ghost row is zero
+  stg(D.vrad + l, vr_new);
+  stg(D.vtheta + l, vt_new);
+  if (i == nrad - 1) stg(D.vtheta + l + nsec, 0.0f);  // VthetaNew's ghost row is zero
   CELL_END
 }
 
@@ -1212,7 +1254,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_source2(BatchDev B) {
 __device__ __forceinline__ float qplus_at(const DiskDev& D, int i, int j, int nsec, float* divv) {
   Tau t = viscous_terms(D, D.vrad, D.vtheta, i, j, nsec);
   *divv = t.divv;
-  const long long l = (long long)i * nsec + j;
+  const int l = i * nsec + j;
   const float nu = D.visc[i];
   float q;
   if (nu != 0.0f) {
@@ -1252,9 +1294,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
           dt * D.CoolingTimeMed[i] * (q - D.QplusMed[i] * Dl / D.SigmaMed[i]);
     den = dt + D.CoolingTimeMed[i] + (D.ADIABATICINDEX - 1.0f) * dt * D.CoolingTimeMed[i] * divv;
   }
-  D.qplus[l] = q;
-  D.energy[l] = num / den;
-  if (i == nrad - 1) D.energy[l + nsec] = 0.0f;  // EnergyNew's ghost row is zero
+  stg(D.qplus + l, q);
+  stg(D.energy + l, num / den);
+  if (i == nrad - 1) stg(D.energy + l + nsec, 0.0f);  // EnergyNew's ghost row is zero
   CELL_END
 }
 
@@ -1713,65 +1755,105 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
 __global__ void __launch_bounds__(kThreads, 8) k_velocities(BatchDev B) {
   CELL_BEGIN
   const float* Dn = D.a0;
-  const long long lmj = (long long)i * nsec + jm;
+  const int lmj = i * nsec + jm;
   float vr;
   if (i == 0)
     vr = 0.0;
   else
     vr = (D.vri[l - nsec] + D.vti[l]) / (Dn[l] + Dn[l - nsec] + 1e-20f);
   float vt = (D.trr[lmj] + D.tpp[l]) / (Dn[l] + Dn[lmj] + 1e-15f) / D.Rmed[i] - D.Rmed[i] * C->OmegaFrame;
-  D.vrad[l] = vr;
-  D.vtheta[l] = vt;
-  D.dens[l] = Dn[l];
-  if (D.Adiabatic) D.energy[l] = D.a1[l];
+  stg(D.vrad + l, vr);
+  stg(D.vtheta + l, vt);
+  stg(D.dens + l, Dn[l]);
+  if (D.Adiabatic) stg(D.energy + l, D.a1[l]);
   CELL_END
 }
 
-// Compacted lists of the disks inside their DT (one thread; disks are few).
+// Compacted lists of the disks inside their DT, by the whole block (at most
+// kThreads threads): the threads gather each disk's flags and sizes into
+// shared memory, a chunk of blockDim.x disks at a time, and thread 0 then
+// runs the prefix sums over shared memory (the disks' global reads are thus
+// issued in parallel, not one dependent chain per disk).
 __device__ void compact_active(const BatchDev& B) {
-  int na = 0, ni = 0, nd = 0;
-  long long cc = 0;
-  int rr = 0, ii = 0, ia = 0, gg = 0, tt = 0, ct = 0, vt = 0;
-  for (int d = 0; d < B.ndisk; d++) {
-    const DiskDev& D = B.disks[d];
-    if (!D.ctl->active) continue;
-    B.act_disk[na] = d;
-    B.act_cell_off[na] = cc;
-    B.act_ring_off[na] = rr;
-    B.act_grp_off[na] = gg;
-    B.act_tile_off[na] = tt;
-    B.act_ctile_off[na] = ct;
-    ct += fargo_cfl_tiles(D.nrad, D.nsec);
-    B.act_vtile_off[na] = vt;
-    vt += vtiles_of(D);
-    cc += (long long)D.nrad * D.nsec;
-    tt += (D.nrad * D.nsec + kThreads - 1) / kThreads;
-    rr += D.nrad;
-    gg += (D.nrad + 31) / 32;
-    na++;
-    if (D.Adiabatic) {
-      B.act_adi_disk[nd] = d;
-      B.act_adi_off[nd] = ia;
-      ia += D.nitems;
-      nd++;
-    } else {
-      B.act_iso_disk[ni] = d;
-      B.act_iso_off[ni] = ii;
-      ii += D.nitems;
-      ni++;
-    }
+  __shared__ int s_act[kThreads], s_adi[kThreads], s_items[kThreads], s_nrad[kThreads];
+  __shared__ int s_tiles[kThreads], s_ctiles[kThreads], s_vtiles[kThreads];
+  __shared__ long long s_cells[kThreads];
+  __shared__ long long s_cc;
+  __shared__ int s_cnt[10];  // na, ni, nd, rr, ii, ia, gg, tt, ct, vt
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    s_cc = 0;
+    for (int k = 0; k < 10; k++) s_cnt[k] = 0;
   }
-  B.act_cell_off[na] = cc;
-  B.act_ring_off[na] = rr;
-  B.act_grp_off[na] = gg;
-  B.act_tile_off[na] = tt;
-  B.act_ctile_off[na] = ct;
-  B.act_vtile_off[na] = vt;
-  B.act_iso_off[ni] = ii;
-  B.act_adi_off[nd] = ia;
-  B.act[0] = na;
-  B.act[1] = ni;
-  B.act[2] = nd;
+  for (int d0 = 0; d0 < B.ndisk; d0 += blockDim.x) {
+    const int d = d0 + tid;
+    if (d < B.ndisk) {
+      const DiskDev& D = B.disks[d];
+      const long long cells = (long long)D.nrad * D.nsec;
+      s_act[tid] = D.ctl->active;
+      s_adi[tid] = D.Adiabatic;
+      s_items[tid] = D.nitems;
+      s_nrad[tid] = D.nrad;
+      s_cells[tid] = cells;
+      s_tiles[tid] = (int)((cells + kThreads - 1) / kThreads);
+      s_ctiles[tid] = fargo_cfl_tiles(D.nrad, D.nsec);
+      s_vtiles[tid] = vtiles_of(D);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int na = s_cnt[0], ni = s_cnt[1], nd = s_cnt[2], rr = s_cnt[3], ii = s_cnt[4], ia = s_cnt[5];
+      int gg = s_cnt[6], tt = s_cnt[7], ct = s_cnt[8], vt = s_cnt[9];
+      long long cc = s_cc;
+      const int n = min((int)blockDim.x, B.ndisk - d0);
+      for (int k = 0; k < n; k++) {
+        if (!s_act[k]) continue;
+        const int d = d0 + k;
+        B.act_disk[na] = d;
+        B.act_cell_off[na] = cc;
+        B.act_ring_off[na] = rr;
+        B.act_grp_off[na] = gg;
+        B.act_tile_off[na] = tt;
+        B.act_ctile_off[na] = ct;
+        B.act_vtile_off[na] = vt;
+        cc += s_cells[k];
+        rr += s_nrad[k];
+        gg += (s_nrad[k] + 31) / 32;
+        tt += s_tiles[k];
+        ct += s_ctiles[k];
+        vt += s_vtiles[k];
+        na++;
+        if (s_adi[k]) {
+          B.act_adi_disk[nd] = d;
+          B.act_adi_off[nd] = ia;
+          ia += s_items[k];
+          nd++;
+        } else {
+          B.act_iso_disk[ni] = d;
+          B.act_iso_off[ni] = ii;
+          ii += s_items[k];
+          ni++;
+        }
+      }
+      s_cnt[0] = na, s_cnt[1] = ni, s_cnt[2] = nd, s_cnt[3] = rr, s_cnt[4] = ii, s_cnt[5] = ia;
+      s_cnt[6] = gg, s_cnt[7] = tt, s_cnt[8] = ct, s_cnt[9] = vt;
+      s_cc = cc;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const int na = s_cnt[0], ni = s_cnt[1], nd = s_cnt[2];
+    B.act_cell_off[na] = s_cc;
+    B.act_ring_off[na] = s_cnt[3];
+    B.act_grp_off[na] = s_cnt[6];
+    B.act_tile_off[na] = s_cnt[7];
+    B.act_ctile_off[na] = s_cnt[8];
+    B.act_vtile_off[na] = s_cnt[9];
+    B.act_iso_off[ni] = s_cnt[4];
+    B.act_adi_off[nd] = s_cnt[5];
+    B.act[0] = na;
+    B.act[1] = ni;
+    B.act[2] = nd;
+  }
 }
 
 // End of a substep: which disks take another one; drives the graph's loop.
@@ -1794,8 +1876,8 @@ __global__ void k_substep_end(BatchDev B, cudaGraphConditionalHandle h, int use_
     any |= C->active;
   }
   any = __syncthreads_or(any);
+  compact_active(B);
   if (threadIdx.x == 0) {
-    compact_active(B);
     B.flags[0] = any;
     if (use_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
   }
@@ -1814,7 +1896,7 @@ __global__ void k_dt_begin(BatchDev B) {
     prepare_bodies(D, C);
   }
   __syncthreads();
-  if (threadIdx.x == 0) compact_active(B);
+  compact_active(B);
 }
 
 // ComputeSoundSpeedKernel, adiabatic branch (Kernels.cu:190-191)
