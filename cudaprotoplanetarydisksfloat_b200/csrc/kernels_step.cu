@@ -769,23 +769,51 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
       const float hillcutfactor = (float)kh / (float)(FARGO_DIMFXY - 1);
       const int c0 = k * FARGO_CFL_TILE + tid;
       int i = c0 / nsec, j = c0 - i * nsec;
-#pragma unroll 4
-      for (int c = 0; c < kCflCells; c++) {
-        if (i < nrad) {
-          const long long q = (long long)i * nsec + j;
-          const float v0 = D.vtheta[q];
-          const float vr0 = D.vrad[q];
-          const float dn = D.dens[q];
-          if (i > 0) {
-            const float dxrad = D.Rsup[i] - D.Rinf[i];
-            const float dxt = D.dxtheta[i];
-            float cs = D.Adiabatic ? D.cs[q] : D.cs_ring[i];
-            float vres = D.FastTransport ? v0 - D.vmoy[i] : v0;  // vmoy: k_ring_mean<0>
+      // kG cells at a time: their loads are issued together (cells past
+      // the disk's end read cell 0 and are skipped); fewer with more bodies,
+      // whose accumulators take the registers
+      constexpr int kG = NB <= 2 ? 4 : (NB <= 4 ? 2 : 1);
+      for (int g = 0; g < kCflCells; g += kG) {
+        int ci[kG], cj[kG];
+        bool ok[kG];
+#pragma unroll
+        for (int u = 0; u < kG; u++) {
+          ok[u] = i < nrad;
+          ci[u] = ok[u] ? i : 0;
+          cj[u] = ok[u] ? j : 0;
+          j += kThreads;
+          while (j >= nsec) {
+            j -= nsec;
+            i++;
+          }
+        }
+        float v0[kG], vr0[kG], dn[kG], vrp[kG], vtp[kG], csv[kG], cth[kG], sth[kG];
+#pragma unroll
+        for (int u = 0; u < kG; u++) {
+          const int q = ci[u] * nsec + cj[u];
+          v0[u] = D.vtheta[q];
+          vr0[u] = D.vrad[q];
+          dn[u] = D.dens[q];
+          vrp[u] = D.vrad[q + nsec];
+          vtp[u] = D.vtheta[q - cj[u] + jwrap_p(cj[u], nsec)];
+          csv[u] = D.Adiabatic ? D.cs[q] : D.cs_ring[ci[u]];
+          cth[u] = D.cos_cell[cj[u]];
+          sth[u] = D.sin_cell[cj[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < kG; u++) {
+          if (!ok[u]) continue;
+          const int ic = ci[u];
+          if (ic > 0) {
+            const float dxrad = D.Rsup[ic] - D.Rinf[ic];
+            const float dxt = D.dxtheta[ic];
+            float cs = csv[u];
+            float vres = D.FastTransport ? v0[u] - D.vmoy[ic] : v0[u];  // vmoy: k_ring_mean<0>
             float invdt1 = cs / (min2(dxrad, dxt));
-            float invdt2 = fabsf(vr0) / dxrad;
+            float invdt2 = fabsf(vr0[u]) / dxrad;
             float invdt3 = fabsf(vres) / dxt;
-            float dvr = D.vrad[q + nsec] - vr0;
-            float dvt = D.vtheta[q - j + jwrap_p(j, nsec)] - v0;
+            float dvr = vrp[u] - vr0[u];
+            float dvt = vtp[u] - v0[u];
             if (dvr >= 0.0)
               dvr = 1e-10;
             else
@@ -799,10 +827,10 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
             float dt2d = CFLSEC / sqrtf(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 + invdt4 * invdt4);
             if (dt2d < lmin) lmin = dt2d;
           }
-          const float Rm = D.Rmed[i];
-          float cellmass = D.Surf[i] * dn;
-          float cx = Rm * D.cos_cell[j];
-          float cy = Rm * D.sin_cell[j];
+          const float Rm = D.Rmed[ic];
+          float cellmass = D.Surf[ic] * dn[u];
+          float cx = Rm * cth[u];
+          float cy = Rm * sth[u];
 #pragma unroll
           for (int b = 0; b < NB; b++) {
             if (b < nbody) {
@@ -831,11 +859,6 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
               }
             }
           }
-        }
-        j += kThreads;
-        while (j >= nsec) {
-          j -= nsec;
-          i++;
         }
       }
     }
