@@ -462,7 +462,7 @@ fargo_status install_items(fargo_batch* b, int seg_out) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
   long long tiles = 0;
-  for (auto& h : b->disks) tiles += ((long long)h.dev.nrad * h.dev.nsec + 255) / 256;
+  for (auto& h : b->disks) tiles += ((long long)h.dev.nrad * h.dev.nsec + FARGO_QTILE - 1) / FARGO_QTILE;
   CK(fargo_size_grids(bd, nsm, tiles, (int)(theta_iso.size() + theta_adi.size())));
   return FARGO_OK;
 }
@@ -570,7 +570,8 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     long long tiles = 0;
-    for (int d = 0; d < n; d++) tiles += ((long long)b->disks[d].dev.nrad * b->disks[d].dev.nsec + 255) / 256;
+    for (int d = 0; d < n; d++)
+      tiles += ((long long)b->disks[d].dev.nrad * b->disks[d].dev.nsec + FARGO_QTILE - 1) / FARGO_QTILE;
     CK(fargo_size_grids(bd, nsm, tiles, (int)(theta_iso.size() + theta_adi.size())));
   }
   fargo_launch_sector_tables(bd, b->max_nsec, b->stream);

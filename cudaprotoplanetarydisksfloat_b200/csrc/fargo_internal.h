@@ -67,6 +67,10 @@ struct DiskCtl {
   float axisg_in, axisg_out;
 };
 
+// cell tiles of the cell kernels: FARGO_QTILE consecutive cells of one disk,
+// four per thread
+#define FARGO_QTILE 1024
+
 // CFL/force tiles: FARGO_CFL_TILE consecutive cells of one disk, each with its
 // own minimum and force partials
 #define FARGO_CFL_TILE 4096
@@ -162,7 +166,7 @@ struct BatchDev {
   int* act_adi_disk;
   int* act_adi_off;
   int* act_grp_off;          // [ndisk+1] prefix of 32-ring groups of active disks
-  int* act_tile_off;         // [ndisk+1] prefix of cell tiles (one block's cells) of active disks
+  int* act_tile_off;         // [ndisk+1] prefix of cell tiles (FARGO_QTILE cells) of active disks
   int* act_ctile_off;        // [ndisk+1] prefix of CFL tiles (FARGO_CFL_TILE cells) of active disks
   int* act_vtile_off;        // [ndisk+1] prefix of viscosity tiles (8 x 64 cells) of active disks
   int cell_grid, ring_grid, item_grid, grp_grid;  // fixed grid sizes of the grid-stride kernels

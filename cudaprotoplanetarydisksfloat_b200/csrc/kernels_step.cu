@@ -35,6 +35,7 @@
 #include <cmath>
 #include <algorithm>
 #include <cstdio>
+#include <type_traits>
 
 #include "fargo_internal.h"
 
@@ -374,14 +375,27 @@ __device__ __forceinline__ void copy_words(void* dst, const void* src, int bytes
   for (int k = threadIdx.x; k < bytes / 4; k += blockDim.x) d[k] = s[k];
 }
 
-// adi_only: skip the tiles of isothermal disks (energy kernels).  A thread's
-// cell advances by kThreads sectors from one tile to the next, so the ring
-// division runs only on entering a disk.  The tiles of one disk form an
-// inner loop without barriers or shared-memory writes; as the bodies store
-// with stg (below), the compiler may keep the disk's fields in registers
-// across it.
+// Four consecutive cells c0 .. c0+3 of one disk (c0 a multiple of 4).  With
+// vec (NSEC a multiple of 4) they share a ring, start at a sector multiple
+// of 4, and their fields load and store as 16-byte vectors; otherwise each
+// cell is addressed on its own and may lie past the disk's end (!ok).
+template <bool V>
+struct Quad {
+  static constexpr bool vec = V;
+  int i[4], j[4], l[4];
+  bool ok[4];
+};
+
+// Walk over the cells of the disks still inside their DT in tiles of
+// FARGO_QTILE cells, four per thread.  Each block takes a contiguous run of
+// tiles, so it meets few disks; on entering a disk the block copies its
+// DiskDev to shared memory.  A thread's quad advances by FARGO_QTILE cells
+// from one tile to the next (no division after the disk's first tile); the
+// tiles of one disk form an inner loop without barriers.  adi_only: skip
+// isothermal disks (energy kernel).
+static_assert(FARGO_QTILE == 4 * kThreads, "four cells per thread");
 template <bool adi_only, class Body>
-__device__ __forceinline__ void for_active_cells(const BatchDev& B, Body body) {
+__device__ __forceinline__ void for_active_quads(const BatchDev& B, Body body) {
   __shared__ DiskDev sD;
   const int na = B.act[0];
   if (na <= 0) return;
@@ -400,14 +414,48 @@ __device__ __forceinline__ void for_active_cells(const BatchDev& B, Body body) {
       continue;
     }
     const int nsec = sD.nsec, nrad = sD.nrad;
-    const int loc = (t - lo) * kThreads + threadIdx.x;
-    int i = loc / nsec, j = loc - i * nsec;
-    for (; t < te; t++) {
-      if (i < nrad) body(sD, sD.ctl, i, j, i * nsec + j, jwrap_m(j, nsec), jwrap_p(j, nsec));
-      j += kThreads;
-      while (j >= nsec) {
-        j -= nsec;
-        i++;
+    const int c0 = (t - lo) * FARGO_QTILE + 4 * threadIdx.x;
+    int i = c0 / nsec, j = c0 - i * nsec;
+    if ((nsec & 3) == 0) {
+      for (; t < te; t++) {
+        if (i < nrad) {
+          Quad<true> q;
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            q.i[u] = i;
+            q.j[u] = j + u;
+            q.l[u] = i * nsec + j + u;
+            q.ok[u] = true;
+          }
+          body(sD, sD.ctl, q);
+        }
+        j += FARGO_QTILE;
+        while (j >= nsec) {
+          j -= nsec;
+          i++;
+        }
+      }
+    } else {
+      for (; t < te; t++) {
+        Quad<false> q;
+        int ii = i, jj = j;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          q.ok[u] = ii < nrad;
+          q.i[u] = q.ok[u] ? ii : 0;
+          q.j[u] = q.ok[u] ? jj : 0;
+          q.l[u] = q.i[u] * nsec + q.j[u];
+          if (++jj == nsec) {
+            jj = 0;
+            ii++;
+          }
+        }
+        if (q.ok[0]) body(sD, sD.ctl, q);
+        j += FARGO_QTILE;
+        while (j >= nsec) {
+          j -= nsec;
+          i++;
+        }
       }
     }
   }
@@ -421,15 +469,82 @@ __device__ __forceinline__ void stg(float* p, float v) {
   asm volatile("st.global.f32 [%0], %1;\n" ::"l"(p), "f"(v));
 }
 
-#define CELL_BEGIN_T(adi_only)                                                                          \
-  for_active_cells<adi_only>(B, [&](const DiskDev& D, const DiskCtl* C, const int i, const int j,         \
-                                    const int l, const int jm, const int jp) {                           \
-    const int nsec = D.nsec, nrad = D.nrad;                                                             \
-    (void)nrad;                                                                                         \
-    (void)jm;                                                                                           \
-    (void)jp;
-#define CELL_BEGIN CELL_BEGIN_T(false)
-#define CELL_END \
+__device__ __forceinline__ void stg4(float* p, float a, float b, float c, float d) {
+  asm volatile("st.global.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d));
+}
+
+// Quad loads and stores.  Row offsets: 0 (ring i), +nsec (ring i+1, the
+// ghost row for the last ring), -nsec (ring i-1: zero where i == 0).
+template <bool V>
+__device__ __forceinline__ void qld(float (&v)[4], const float* p, const Quad<V>& q, int roff = 0) {
+  if (V) {
+    if (roff < 0 && q.i[0] == 0) {
+      v[0] = v[1] = v[2] = v[3] = 0.0f;
+      return;
+    }
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p + q.l[0] + roff));
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; u++) v[u] = (q.ok[u] && (roff >= 0 || q.i[u] > 0)) ? __ldg(p + q.l[u] + roff) : 0.0f;
+  }
+}
+// values at (i, j-1) of each cell, given the same row's values c at (i, j)
+template <bool V>
+__device__ __forceinline__ void qld_jm(float (&v)[4], const float (&c)[4], const float* p, const Quad<V>& q, int nsec,
+                                       int roff = 0) {
+  if (V) {
+    v[0] = (roff < 0 && q.i[0] == 0) ? 0.0f : __ldg(p + q.i[0] * nsec + jwrap_m(q.j[0], nsec) + roff);
+    v[1] = c[0], v[2] = c[1], v[3] = c[2];
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      v[u] = (q.ok[u] && (roff >= 0 || q.i[u] > 0)) ? __ldg(p + q.i[u] * nsec + jwrap_m(q.j[u], nsec) + roff) : 0.0f;
+  }
+}
+// values at (i, j+1) of each cell, given the same row's values c at (i, j)
+template <bool V>
+__device__ __forceinline__ void qld_jp(float (&v)[4], const float (&c)[4], const float* p, const Quad<V>& q, int nsec,
+                                       int roff = 0) {
+  if (V) {
+    v[0] = c[1], v[1] = c[2], v[2] = c[3];
+    v[3] = (roff < 0 && q.i[0] == 0) ? 0.0f : __ldg(p + q.i[0] * nsec + jwrap_p(q.j[3], nsec) + roff);
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      v[u] = (q.ok[u] && (roff >= 0 || q.i[u] > 0)) ? __ldg(p + q.i[u] * nsec + jwrap_p(q.j[u], nsec) + roff) : 0.0f;
+  }
+}
+// sector-table values (index j) of each cell
+template <bool V>
+__device__ __forceinline__ void qld_sector(float (&v)[4], const float* p, const Quad<V>& q) {
+  if (V) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p + q.j[0]));
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; u++) v[u] = __ldg(p + q.j[u]);
+  }
+}
+template <bool V>
+__device__ __forceinline__ void qst(float* p, const Quad<V>& q, const float (&v)[4], int roff = 0) {
+  if (V) {
+    stg4(p + q.l[0] + roff, v[0], v[1], v[2], v[3]);
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (q.ok[u]) stg(p + q.l[u] + roff, v[u]);
+  }
+}
+
+#define QUAD_BEGIN_T(adi_only)                                                                         \
+  for_active_quads<adi_only>(B, [&](const DiskDev& D, const DiskCtl* C, const auto& q) {               \
+    constexpr bool V = std::decay_t<decltype(q)>::vec;                                                 \
+    (void)V;                                                                                           \
+    const int nsec = D.nsec, nrad = D.nrad;                                                            \
+    (void)nrad;
+#define QUAD_BEGIN QUAD_BEGIN_T(false)
+#define QUAD_END \
   });
 
 // -------------------------------------------------------------- reductions
@@ -901,10 +1016,10 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
 
 // Gravitational potential at cell (i, j): FillForcesArraysKernel
 // (Kernels.cu:1322-1349) summed over the planets in the reference's order.
-__device__ __forceinline__ float potential_at(const DiskDev& D, const DiskCtl* C, int i, int j) {
+__device__ __forceinline__ float potential_xy(const DiskDev& D, const DiskCtl* C, int i, float cosj, float sinj) {
   const float Rm = D.Rmed[i];
-  const float x = Rm * D.cos_pot[j];
-  const float y = Rm * D.sin_pot[j];
+  const float x = Rm * cosj;
+  const float y = Rm * sinj;
   float P = 0.0f;
   const int nb = C->nb;
   for (int k = 0; k < nb; k++) {
@@ -927,75 +1042,104 @@ __device__ __forceinline__ float potential_at(const DiskDev& D, const DiskCtl* C
 // FillForcesArrays (Pframeforce.cu:37-66): the potential of every cell, once
 // per substep (Substep1 reads it at three cells each).
 __global__ void __launch_bounds__(kThreads) k_potential(BatchDev B) {
-  CELL_BEGIN
-  stg(D.phi + l, potential_at(D, C, i, j));
-  CELL_END
+  QUAD_BEGIN
+  float cp[4], sp[4], phi[4];
+  qld_sector(cp, D.cos_pot, q);
+  qld_sector(sp, D.sin_pot, q);
+#pragma unroll
+  for (int u = 0; u < 4; u++) phi[u] = potential_xy(D, C, q.i[u], cp[u], sp[u]);
+  qst(D.phi, q, phi);
+  QUAD_END
 }
-
-__device__ __forceinline__ float pressure_at(const DiskDev& D, int l, int i) {
-  if (!D.Adiabatic) {
-    float cs = D.cs_ring[i];
-    return D.dens[l] * cs * cs;
-  }
-  return (D.ADIABATICINDEX - 1.0f) * D.energy[l];
-}
-
 
 // Substep1KernelVrad / Substep1KernelVtheta (Kernels.cu:52-88), with
 // CorrectVthetaKernel (Kernels.cu:1352-1359) applied on the fly, and the
 // self-gravity kick of Update_sgvelocityKernel (Kernels.cu:1024-1041).
-__global__ void __launch_bounds__(kThreads, 4) k_source1(BatchDev B) {
-  CELL_BEGIN
+__global__ void __launch_bounds__(kThreads, 2) k_source1(BatchDev B) {
+  QUAD_BEGIN
   const float dt = C->dtf;
   const float OmegaFrame = C->OmegaFrame;
   // CorrectVtheta (SideEuler.cu:184-188) on the fly; evanescent disks had it
   // applied in place by the boundary pass that precedes this kernel
   const float dom = D.Evanescent ? 0.0f : C->domega;
-  const float* Vt = D.vtheta;
-  const float* Dn = D.dens;
-  auto vth = [&](int q, int r) -> float { return dom != 0.0f ? Vt[q] - dom * D.Rmed[r] : Vt[q]; };
-  const float P0 = pressure_at(D, l, i);
-  const float Phi0 = D.phi[l];  // k_potential
-  // ComputeTemperatureField divides the pressure of the substep start by the
-  // final density (SourceEuler.cu:280,293): keep the last substep's pressure
-  if (!D.Adiabatic && !C->more) stg(D.pres + l, P0);
-  if (i > 0) {
-    const int lm = l - nsec;
-    const float Pm = pressure_at(D, lm, i - 1);
-    const float Phim = D.phi[l - nsec];
-    float gradp = (P0 - Pm) * 2.0f / (Dn[l] + Dn[lm]) * D.invdiffRmed[i];
-    float gradphi = (Phi0 - Phim) * D.invdiffRmed[i];
-    const int lp = i * nsec + jp;
-    float vt2 = vth(l, i) + vth(lp, i) + vth(lm, i - 1) + vth(lp - nsec, i - 1);
-    vt2 = vt2 * 0.25f + D.Rinf[i] * OmegaFrame;
-    vt2 = vt2 * vt2;
-    float vri = D.vrad[l] + dt * (-gradp - gradphi + vt2 * D.invRinf[i]);
-    if (D.SelfGravity)
-      vri += dt * ((D.Rinf[i] - D.Rmed[i - 1]) * D.sg_accr[l] + (D.Rmed[i] - D.Rinf[i]) * D.sg_accr[lm]) *
-             D.invdiffRmed[i];
-    stg(D.vri + l, vri);
-  } else {
-    stg(D.vri + l, 0.0f);  // VradInt's ring 0 is never written by the reference: zero
+  const bool adi = D.Adiabatic, sg = D.SelfGravity;
+  auto vth = [&](float v, int r) -> float { return dom != 0.0f ? v - dom * D.Rmed[r] : v; };
+  // (i, j), (i-1, j) and (i, j-1) samples; v_theta also at (i, j+1), (i-1, j+1)
+  float Dn0[4], Dnm[4], Dna[4], E0[4], Em[4], Ea[4], Ph0[4], Phm[4], Pha[4];
+  float Vt0[4], Vtp[4], Vtm[4], Vtmp[4], Vr0[4];
+  qld(Dn0, D.dens, q);
+  qld(Dnm, D.dens, q, -nsec);
+  qld_jm(Dna, Dn0, D.dens, q, nsec);
+  if (adi) {
+    qld(E0, D.energy, q);
+    qld(Em, D.energy, q, -nsec);
+    qld_jm(Ea, E0, D.energy, q, nsec);
   }
-  {
-    const int la = i * nsec + jm;
+  qld(Ph0, D.phi, q);  // k_potential
+  qld(Phm, D.phi, q, -nsec);
+  qld_jm(Pha, Ph0, D.phi, q, nsec);
+  qld(Vt0, D.vtheta, q);
+  qld_jp(Vtp, Vt0, D.vtheta, q, nsec);
+  qld(Vtm, D.vtheta, q, -nsec);
+  qld_jp(Vtmp, Vtm, D.vtheta, q, nsec, -nsec);
+  qld(Vr0, D.vrad, q);
+  float ar0[4], arm[4], at0[4], atq[4];
+  if (sg) {
+    qld(ar0, D.sg_accr, q);
+    qld(arm, D.sg_accr, q, -nsec);
+    qld(at0, D.sg_acct, q);
+    // the reference reads SG_Acct[i*nsec + (j-1)%nsec]: for j = 0 that is
+    // the last sector of ring i-1 (ring 0: taken from ring 0 itself), i.e.
+    // the cell before in memory
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      if (V && u > 0) {
+        atq[u] = at0[u - 1];
+      } else {
+        const int lq = q.l[u] > 0 ? q.l[u] - 1 : nsec - 1;
+        atq[u] = q.ok[u] ? __ldg(D.sg_acct + lq) : 0.0f;
+      }
+    }
+  }
+  float vri[4], vti[4], P0s[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int i = q.i[u];
+    const float cs = adi ? 0.0f : D.cs_ring[i];
+    // pressure: isothermal Sigma cs^2 per ring, adiabatic (gamma - 1) e
+    const float P0 = adi ? (D.ADIABATICINDEX - 1.0f) * E0[u] : Dn0[u] * cs * cs;
+    P0s[u] = P0;
+    if (i > 0) {
+      const float csm = adi ? 0.0f : D.cs_ring[i - 1];
+      const float Pm = adi ? (D.ADIABATICINDEX - 1.0f) * Em[u] : Dnm[u] * csm * csm;
+      float gradp = (P0 - Pm) * 2.0f / (Dn0[u] + Dnm[u]) * D.invdiffRmed[i];
+      float gradphi = (Ph0[u] - Phm[u]) * D.invdiffRmed[i];
+      float vt2 = vth(Vt0[u], i) + vth(Vtp[u], i) + vth(Vtm[u], i - 1) + vth(Vtmp[u], i - 1);
+      vt2 = vt2 * 0.25f + D.Rinf[i] * OmegaFrame;
+      vt2 = vt2 * vt2;
+      float v = Vr0[u] + dt * (-gradp - gradphi + vt2 * D.invRinf[i]);
+      if (sg)
+        v += dt * ((D.Rinf[i] - D.Rmed[i - 1]) * ar0[u] + (D.Rmed[i] - D.Rinf[i]) * arm[u]) * D.invdiffRmed[i];
+      vri[u] = v;
+    } else {
+      vri[u] = 0.0f;  // VradInt's ring 0 is never written by the reference: zero
+    }
     float dxtheta = 2.0f * (float)PI_D / (float)nsec * D.Rmed[i];
     float invdxtheta = 1.0f / dxtheta;
-    const float Pa = pressure_at(D, la, i);
-    const float Phia = D.phi[la];
-    float gradp = (P0 - Pa) * 2.0f / (Dn[l] + Dn[la]) * invdxtheta;
-    float gradphi = (Phi0 - Phia) * invdxtheta;
-    float vti = vth(l, i) - dt * (gradp + gradphi);
-    vti += dt * D.supp_torque[i];
-    if (D.SelfGravity) {
-      // the reference reads SG_Acct[i*nsec + (j-1)%nsec]: for j = 0 that is
-      // the last sector of ring i-1 (ring 0: taken from ring 0 itself)
-      int lq = (j > 0) ? l - 1 : (i > 0 ? l - 1 : nsec - 1);
-      vti += 0.5f * dt * (D.sg_acct[l] + D.sg_acct[lq]);
-    }
-    stg(D.vti + l, vti);
+    const float Pa = adi ? (D.ADIABATICINDEX - 1.0f) * Ea[u] : Dna[u] * cs * cs;
+    float gradp = (P0 - Pa) * 2.0f / (Dn0[u] + Dna[u]) * invdxtheta;
+    float gradphi = (Ph0[u] - Pha[u]) * invdxtheta;
+    float v = vth(Vt0[u], i) - dt * (gradp + gradphi);
+    v += dt * D.supp_torque[i];
+    if (sg) v += 0.5f * dt * (at0[u] + atq[u]);
+    vti[u] = v;
   }
-  CELL_END
+  // ComputeTemperatureField divides the pressure of the substep start by the
+  // final density (SourceEuler.cu:280,293): keep the last substep's pressure
+  if (!adi && !C->more) qst(D.pres, q, P0s);
+  qst(D.vri, q, vri);
+  qst(D.vti, q, vti);
+  QUAD_END
 }
 
 // ViscousTermsKernelDRP + ViscousTermsKernelTAURP (Kernels.cu:843-880) on
@@ -1113,8 +1257,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
       for (int q = tid; q < kSR * kCh; q += kThreads) {
         const int r = q / kCh, c = 4 * (q - r * kCh);
         const int i = i0 - 2 + r;
-        int j = (j0 - kSO + c) % nsec;
+        int j = j0 - kSO + c;  // j0 - kSO >= -kSO: at most one wrap below
         if (j < 0) j += nsec;
+        while (j >= nsec) j -= nsec;
         const bool ok = i >= 0 && i <= nrad;
         const int l = ok ? i * nsec + j : 0;
         cp_async16(&sVrb[bf][r][c], sD.vri + l, ok);
@@ -1208,7 +1353,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
       const int r = q / kVC, c = q - r * kVC;
       const int i = i0 + r, j = j0 + c;
       if (i >= nrad || j >= nsec) continue;
-      const size_t l = (size_t)i * nsec + j;
+      const int l = i * nsec + j;
       const int R = r + 1, Cc = c + 1;   // stress index of (i, j)
       const int rr = r + 2, cc = c + kSO;  // staged index of (i, j)
       float vti = sVa[rr][cc], vri = sVr[rr][cc];
@@ -1228,8 +1373,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
         if (kep && i == 0) vti = vin - D.Rmed[0] * C->OmegaFrame;
         if (kep && i == nrad - 1) vti = vout - D.Rmed[nrad - 1] * C->OmegaFrame;
       }
-      D.trr[l] = vri;
-      D.tpp[l] = vti;
+      stg(D.trr + l, vri);
+      stg(D.tpp + l, vti);
     }
     __syncthreads();  // buffer bf is restaged two tiles on
     bf ^= 1;
@@ -1244,32 +1389,53 @@ __device__ __forceinline__ float qvisc(float dv, float dens) {
   return 0.0f;
 }
 
-__global__ void __launch_bounds__(kThreads, 6) k_source2(BatchDev B) {
-  CELL_BEGIN
+__global__ void __launch_bounds__(kThreads, 3) k_source2(BatchDev B) {
+  QUAD_BEGIN
   const float dt = C->dtf;
-  const float* Dn = D.dens;
-  const float *VRI = D.trr, *VTI = D.tpp;  // viscosity-updated VradInt / VthetaInt (k_viscosity)
-  const int lmj = i * nsec + jm, lpj = i * nsec + jp;
-  float qr = qvisc(VRI[l + nsec] - VRI[l], Dn[l]);
-  float qt = qvisc(VTI[lpj] - VTI[l], Dn[l]);
-  float vr_new = 0.0f;
-  if (i > 0) {
-    float qrm = qvisc(VRI[l] - VRI[l - nsec], Dn[l - nsec]);
-    vr_new = VRI[l] - dt * 2.0f / (Dn[l] + Dn[l - nsec]) * (qr - qrm) * D.invdiffRmed[i];
-  }
-  float qtm = qvisc(VTI[l] - VTI[lmj], Dn[lmj]);
-  float dxtheta = 2.0f * (float)PI_D / (float)nsec * D.Rmed[i];
-  float invdxtheta = 1.0f / dxtheta;
-  float vt_new = VTI[l] - dt * 2.0f / (Dn[l] + Dn[lmj]) * (qt - qtm) * invdxtheta;
-  if (D.Adiabatic) {
+  const bool adi = D.Adiabatic;
+  // viscosity-updated VradInt / VthetaInt (k_viscosity) and the density
+  float R0[4], Ru[4], Rd[4], T0[4], Tp[4], Tm[4], N0[4], Nd[4], Nm[4], E0[4];
+  qld(R0, D.trr, q);
+  qld(Ru, D.trr, q, nsec);
+  qld(Rd, D.trr, q, -nsec);
+  qld(T0, D.tpp, q);
+  qld_jp(Tp, T0, D.tpp, q, nsec);
+  qld_jm(Tm, T0, D.tpp, q, nsec);
+  qld(N0, D.dens, q);
+  qld(Nd, D.dens, q, -nsec);
+  qld_jm(Nm, N0, D.dens, q, nsec);
+  if (adi) qld(E0, D.energy, q);
+  float vrn[4], vtn[4], ein[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int i = q.i[u];
+    float qr = qvisc(Ru[u] - R0[u], N0[u]);
+    float qt = qvisc(Tp[u] - T0[u], N0[u]);
+    float vr_new = 0.0f;
+    if (i > 0) {
+      float qrm = qvisc(R0[u] - Rd[u], Nd[u]);
+      vr_new = R0[u] - dt * 2.0f / (N0[u] + Nd[u]) * (qr - qrm) * D.invdiffRmed[i];
+    }
+    float qtm = qvisc(T0[u] - Tm[u], Nm[u]);
+    float dxtheta = 2.0f * (float)PI_D / (float)nsec * D.Rmed[i];
+    float invdxtheta = 1.0f / dxtheta;
+    vtn[u] = T0[u] - dt * 2.0f / (N0[u] + Nm[u]) * (qt - qtm) * invdxtheta;
+    vrn[u] = vr_new;
     // EnergyInt goes to scratch: the boundary pass before Substep3 still sees the state energy
-    stg(D.a1 + l, D.energy[l] - dt * qr * (VRI[l + nsec] - VRI[l]) * D.invdiffRsup[i] -
-                      dt * qt * (VTI[lpj] - VTI[l]) * invdxtheta);
+    if (adi) ein[u] = E0[u] - dt * qr * (Ru[u] - R0[u]) * D.invdiffRsup[i] - dt * qt * (Tp[u] - T0[u]) * invdxtheta;
   }
-  stg(D.vrad + l, vr_new);
-  stg(D.vtheta + l, vt_new);
-  if (i == nrad - 1) stg(D.vtheta + l + nsec, 0.0f);  // VthetaNew's ghost row is zero
-  CELL_END
+  if (adi) qst(D.a1, q, ein);
+  qst(D.vrad, q, vrn);
+  qst(D.vtheta, q, vtn);
+  // VthetaNew's ghost row is zero
+  if (V) {
+    if (q.i[0] == nrad - 1) stg4(D.vtheta + q.l[0] + nsec, 0.0f, 0.0f, 0.0f, 0.0f);
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (q.ok[u] && q.i[u] == nrad - 1) stg(D.vtheta + q.l[u] + nsec, 0.0f);
+  }
+  QUAD_END
 }
 
 // Substep3Kernel + Substep3Kernel2 (Kernels.cu:91-139) with the viscous
@@ -1289,38 +1455,56 @@ __device__ __forceinline__ float qplus_at(const DiskDev& D, int i, int j, int ns
 }
 
 __global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
-  CELL_BEGIN_T(true)
+  QUAD_BEGIN_T(true)
   const float dt = C->dtf;
-  float divv;
-  float q = 0.0f;
-  if (i > 0) {
-    q = qplus_at(D, i, j, nsec, &divv);
-  } else {
-    float dv1, dv2;
-    float q1 = qplus_at(D, 1, j, nsec, &dv1);
-    float q2 = qplus_at(D, 2, j, nsec, &dv2);
-    Tau t0 = viscous_terms(D, D.vrad, D.vtheta, 0, j, nsec);
-    divv = t0.divv;
-    if (D.visc[nrad - 1] != 0.0)
-      q = q1 * expf(logf(q1 / q2) * logf(D.Rmed[0] / D.Rmed[1]) / logf(D.Rmed[1] / D.Rmed[2]));
-    else
-      q = 0.0;
+  float qv[4], ev[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int i = q.i[u], j = q.j[u], l = q.l[u];
+    if (!q.ok[u]) {
+      qv[u] = ev[u] = 0.0f;
+      continue;
+    }
+    float divv;
+    float qp = 0.0f;
+    if (i > 0) {
+      qp = qplus_at(D, i, j, nsec, &divv);
+    } else {
+      float dv1, dv2;
+      float q1 = qplus_at(D, 1, j, nsec, &dv1);
+      float q2 = qplus_at(D, 2, j, nsec, &dv2);
+      Tau t0 = viscous_terms(D, D.vrad, D.vtheta, 0, j, nsec);
+      divv = t0.divv;
+      if (D.visc[nrad - 1] != 0.0)
+        qp = q1 * expf(logf(q1 / q2) * logf(D.Rmed[0] / D.Rmed[1]) / logf(D.Rmed[1] / D.Rmed[2]));
+      else
+        qp = 0.0;
+    }
+    const float e_int = D.a1[l];  // EnergyInt from k_source2
+    const float Dl = D.dens[l];
+    float num, den;
+    if (!D.Cooling) {
+      num = dt * qp + e_int;
+      den = 1.0f + (D.ADIABATICINDEX - 1.0f) * dt * divv;
+    } else {
+      num = D.EnergyMed[i] * dt * Dl / D.SigmaMed[i] + D.CoolingTimeMed[i] * e_int +
+            dt * D.CoolingTimeMed[i] * (qp - D.QplusMed[i] * Dl / D.SigmaMed[i]);
+      den = dt + D.CoolingTimeMed[i] + (D.ADIABATICINDEX - 1.0f) * dt * D.CoolingTimeMed[i] * divv;
+    }
+    qv[u] = qp;
+    ev[u] = num / den;
   }
-  const float e_int = D.a1[l];  // EnergyInt from k_source2
-  const float Dl = D.dens[l];
-  float num, den;
-  if (!D.Cooling) {
-    num = dt * q + e_int;
-    den = 1.0f + (D.ADIABATICINDEX - 1.0f) * dt * divv;
+  qst(D.qplus, q, qv);
+  qst(D.energy, q, ev);
+  // EnergyNew's ghost row is zero
+  if (V) {
+    if (q.i[0] == nrad - 1) stg4(D.energy + q.l[0] + nsec, 0.0f, 0.0f, 0.0f, 0.0f);
   } else {
-    num = D.EnergyMed[i] * dt * Dl / D.SigmaMed[i] + D.CoolingTimeMed[i] * e_int +
-          dt * D.CoolingTimeMed[i] * (q - D.QplusMed[i] * Dl / D.SigmaMed[i]);
-    den = dt + D.CoolingTimeMed[i] + (D.ADIABATICINDEX - 1.0f) * dt * D.CoolingTimeMed[i] * divv;
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (q.ok[u] && q.i[u] == nrad - 1) stg(D.energy + q.l[u] + nsec, 0.0f);
   }
-  stg(D.qplus + l, q);
-  stg(D.energy + l, num / den);
-  if (i == nrad - 1) stg(D.energy + l + nsec, 0.0f);  // EnergyNew's ghost row is zero
-  CELL_END
+  QUAD_END
 }
 
 // ------------------------------------------------------------- transport
@@ -1775,21 +1959,34 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
 // ComputeVelocitiesKernel, Kernels.cu:1292-1306, from the transported
 // momenta (vri, vti, trr, tpp) and density (a0); then the transported
 // density (and energy, a1) become the state.
-__global__ void __launch_bounds__(kThreads, 8) k_velocities(BatchDev B) {
-  CELL_BEGIN
-  const float* Dn = D.a0;
-  const int lmj = i * nsec + jm;
-  float vr;
-  if (i == 0)
-    vr = 0.0;
-  else
-    vr = (D.vri[l - nsec] + D.vti[l]) / (Dn[l] + Dn[l - nsec] + 1e-20f);
-  float vt = (D.trr[lmj] + D.tpp[l]) / (Dn[l] + Dn[lmj] + 1e-15f) / D.Rmed[i] - D.Rmed[i] * C->OmegaFrame;
-  stg(D.vrad + l, vr);
-  stg(D.vtheta + l, vt);
-  stg(D.dens + l, Dn[l]);
-  if (D.Adiabatic) stg(D.energy + l, D.a1[l]);
-  CELL_END
+__global__ void __launch_bounds__(kThreads, 4) k_velocities(BatchDev B) {
+  QUAD_BEGIN
+  const float Om = C->OmegaFrame;
+  float A0[4], Ad[4], Am[4], Rd[4], T0[4], P0[4], Pm[4], S0[4], E1[4];
+  qld(A0, D.a0, q);  // transported density
+  qld(Ad, D.a0, q, -nsec);
+  qld_jm(Am, A0, D.a0, q, nsec);
+  qld(Rd, D.vri, q, -nsec);
+  qld(T0, D.vti, q);
+  qld(P0, D.trr, q);
+  qld_jm(Pm, P0, D.trr, q, nsec);
+  qld(S0, D.tpp, q);
+  if (D.Adiabatic) qld(E1, D.a1, q);
+  float vr[4], vt[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int i = q.i[u];
+    if (i == 0)
+      vr[u] = 0.0;
+    else
+      vr[u] = (Rd[u] + T0[u]) / (A0[u] + Ad[u] + 1e-20f);
+    vt[u] = (Pm[u] + S0[u]) / (A0[u] + Am[u] + 1e-15f) / D.Rmed[i] - D.Rmed[i] * Om;
+  }
+  qst(D.vrad, q, vr);
+  qst(D.vtheta, q, vt);
+  qst(D.dens, q, A0);
+  if (D.Adiabatic) qst(D.energy, q, E1);
+  QUAD_END
 }
 
 // Compacted lists of the disks inside their DT, by the whole block (at most
@@ -1818,7 +2015,7 @@ __device__ void compact_active(const BatchDev& B) {
       s_items[tid] = D.nitems;
       s_nrad[tid] = D.nrad;
       s_cells[tid] = cells;
-      s_tiles[tid] = (int)((cells + kThreads - 1) / kThreads);
+      s_tiles[tid] = (int)((cells + FARGO_QTILE - 1) / FARGO_QTILE);
       s_ctiles[tid] = fargo_cfl_tiles(D.nrad, D.nsec);
       s_vtiles[tid] = vtiles_of(D);
     }
