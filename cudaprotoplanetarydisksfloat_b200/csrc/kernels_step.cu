@@ -1206,10 +1206,13 @@ __device__ void vkep_pair(const DiskDev& D, const DiskCtl* C, float* vin, float*
 // the trr / tpp buffers (the stresses never reach HBM), which Substep2 then
 // reads as VradInt / VthetaInt: writing them in place would race with the
 // neighbouring tiles' halo reads.
-constexpr int kVR = 8, kVC = 64;                        // tile rows, columns
+constexpr int kVR = 16, kVC = 64;                       // tile rows, columns
 constexpr int kSO = 4;                                  // staged columns left of the tile
 constexpr int kSR = kVR + 4, kSC = kVC + 2 * kSO;       // staged rows, columns (whole 16-byte chunks)
 constexpr int kTR = kVR + 2, kTC = kVC + 2;             // stress rows, columns
+constexpr int kTQ = (kTC + 3) / 4;                      // stress quads per row
+constexpr int kTCp = 4 * kTQ;                           // stress row length in shared memory
+static_assert(kVR * kVC == 4 * kThreads, "one quad of the tile per thread in the update");
 __device__ __forceinline__ int vtiles_of(const DiskDev& D) {
   return ((D.nrad + kVR - 1) / kVR) * ((D.nsec + kVC - 1) / kVC);
 }
@@ -1233,11 +1236,15 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(n) : "memory");
 }
 
-__global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
+constexpr size_t kViscSmem = sizeof(float) * 3 * 2 * kSR * kSC;  // dynamic: the staged tiles
+__global__ void __launch_bounds__(kThreads, 3) k_viscosity(BatchDev B) {
   __shared__ DiskDev sD;
-  __shared__ __align__(16) float sVrb[2][kSR][kSC], sVab[2][kSR][kSC], sDnb[2][kSR][kSC];
+  extern __shared__ __align__(16) float vs_sm[];
+  float(*sVrb)[kSR][kSC] = reinterpret_cast<float(*)[kSR][kSC]>(vs_sm);  // [2][kSR][kSC] each
+  float(*sVab)[kSR][kSC] = sVrb + 2;
+  float(*sDnb)[kSR][kSC] = sVab + 2;
   __shared__ float sD0b[2][kSR];
-  __shared__ float sTrr[kTR][kTC], sTpp[kTR][kTC], sTrp[kTR][kTC];
+  __shared__ float sTrr[kTR][kTCp], sTpp[kTR][kTCp], sTrp[kTR][kTCp];
   const int tid = threadIdx.x;
   const int na = B.act[0];
   const int ntile = na > 0 ? B.act_vtile_off[na] : 0;
@@ -1282,7 +1289,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
     if (tid < kSR) {
       const int i = i0 - 2 + tid;
       const bool ok = i >= 0 && i <= nrad;
-      cp_async4(&sD0b[bf][tid], sD.dens + (ok ? (size_t)i * nsec : 0), ok);
+      cp_async4(&sD0b[bf][tid], sD.dens + (ok ? i * nsec : 0), ok);
     }
     cp_async_commit();
   };
@@ -1318,63 +1325,125 @@ __global__ void __launch_bounds__(kThreads, 4) k_viscosity(BatchDev B) {
     const int ncol = (nsec + kVC - 1) / kVC;
     const int lt = t - lo;
     const int i0 = (lt / ncol) * kVR, j0 = (lt % ncol) * kVC;
+    const float invdphi = D.invdphi, onethird = D.onethird;
     if (D.IsDisk) {
-      // stresses at rows i0-1 .. i0+kVR, columns j0-1 .. j0+kVC (viscous_terms)
-      for (int q = tid; q < kTR * kTC; q += kThreads) {
-        const int r = q / kTC, c = q - r * kTC;
+      // stresses at rows i0-1 .. i0+kVR, columns j0-1 .. j0+kVC (viscous_terms),
+      // four consecutive columns of one row per thread: the row's tables are
+      // read once and neighbouring samples are shared in registers
+      for (int it = tid; it < kTR * kTQ; it += kThreads) {
+        const int r = it / kTQ, c0 = 4 * (it - r * kTQ);
         const int i = i0 - 1 + r;
         if (i < 0 || i >= nrad) continue;
-        const int rr = r + 1, cc = c + kSO - 1;  // staged indices of (i, j)
+        const int rr = r + 1, cc = c0 + kSO - 1;  // staged indices of (i, j) for the first column
         const float nu = D.visc[i];
         const float iRm = D.invRmed[i];
-        float DRR = (sVr[rr + 1][cc] - sVr[rr][cc]) * D.invdiffRsup[i];
-        float DPP = (sVa[rr][cc + 1] - sVa[rr][cc]) * D.invdphi * iRm + 0.5f * (sVr[rr + 1][cc] + sVr[rr][cc]) * iRm;
-        float divV = (sVr[rr + 1][cc] * D.Rsup[i] - sVr[rr][cc] * D.Rinf[i]) * D.invdiffRsup[i] * iRm;
-        divV += (sVa[rr][cc + 1] - sVa[rr][cc]) * D.invdphi * iRm;
-        sTrr[r][c] = 2.0f * sDn[rr][cc] * nu * (DRR - D.onethird * divV);
-        sTpp[r][c] = 2.0f * sDn[rr][cc] * nu * (DPP - D.onethird * divV);
-        float rp = 0.0f;  // TAURP's ring 0 is never written: zero
-        if (i > 0) {
-          float DRP = 0.5f * (D.Rinf[i] * (sVa[rr][cc] * iRm - sVa[rr - 1][cc] * D.invRmed[i - 1]) * D.invdiffRmed[i] +
-                              (sVr[rr][cc] - sVr[rr][cc - 1]) * D.invdphi * D.invRinf[i]);
-          // TAURP's third density sample is dens[i*nsec] (Kernels.cu:876)
-          rp = 0.5f * (sDn[rr][cc] + sDn[rr - 1][cc] + sD0[rr] + sDn[rr - 1][cc - 1]) * nu * DRP;
+        const float idRs = D.invdiffRsup[i], Rs = D.Rsup[i], Ri = D.Rinf[i];
+        float vr[5], vr1[4], va[5], vam[4], dn[4], dnm[5];
+#pragma unroll
+        for (int u = 0; u < 5; u++) {
+          vr[u] = sVr[rr][cc - 1 + u];   // columns c0-1 .. c0+3
+          va[u] = sVa[rr][cc + u];       // columns c0 .. c0+4
+          dnm[u] = sDn[rr - 1][cc - 1 + u];
         }
-        sTrp[r][c] = rp;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          vr1[u] = sVr[rr + 1][cc + u];
+          vam[u] = sVa[rr - 1][cc + u];
+          dn[u] = sDn[rr][cc + u];
+        }
+        const float d0 = sD0[rr];
+        const float iRm1 = i > 0 ? D.invRmed[i - 1] : 0.0f;
+        const float idRm = D.invdiffRmed[i], iRi = D.invRinf[i];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int c = c0 + u;
+          if (c >= kTC) break;
+          const float v0 = vr[u + 1], vp = vr1[u], a0 = va[u], ap = va[u + 1];
+          float DRR = (vp - v0) * idRs;
+          float DPP = (ap - a0) * invdphi * iRm + 0.5f * (vp + v0) * iRm;
+          float divV = (vp * Rs - v0 * Ri) * idRs * iRm;
+          divV += (ap - a0) * invdphi * iRm;
+          sTrr[r][c] = 2.0f * dn[u] * nu * (DRR - onethird * divV);
+          sTpp[r][c] = 2.0f * dn[u] * nu * (DPP - onethird * divV);
+          float rp = 0.0f;  // TAURP's ring 0 is never written: zero
+          if (i > 0) {
+            float DRP = 0.5f * (Ri * (a0 * iRm - vam[u] * iRm1) * idRm + (v0 - vr[u]) * invdphi * iRi);
+            // TAURP's third density sample is dens[i*nsec] (Kernels.cu:876)
+            rp = 0.5f * (dn[u] + dnm[u + 1] + d0 + dnm[u]) * nu * DRP;
+          }
+          sTrp[r][c] = rp;
+        }
       }
     }
     __syncthreads();
-    // updated velocities of the tile's cells
+    // updated velocities of the tile's cells: one quad per thread
     const float DeltaT = C->dtf;
     float vin = 0.0f, vout = 0.0f;
     const bool kep = !D.Evanescent && (i0 == 0 || i0 + kVR >= nrad);
     if (kep) vkep_pair(D, C, &vin, &vout);
-    for (int q = tid; q < kVR * kVC; q += kThreads) {
-      const int r = q / kVC, c = q - r * kVC;
-      const int i = i0 + r, j = j0 + c;
-      if (i >= nrad || j >= nsec) continue;
-      const int l = i * nsec + j;
-      const int R = r + 1, Cc = c + 1;   // stress index of (i, j)
-      const int rr = r + 2, cc = c + kSO;  // staged index of (i, j)
-      float vti = sVa[rr][cc], vri = sVr[rr][cc];
-      if (D.IsDisk) {
-        if (i > 0 && i < nrad - 1) {
-          vti += DeltaT * D.invRmed[i] *
-                 ((D.Rsup[i] * sTrp[R + 1][Cc] - D.Rinf[i] * sTrp[R][Cc]) * D.invdiffRsup[i] +
-                  (sTpp[R][Cc] - sTpp[R][Cc - 1]) * D.invdphi + 0.5f * (sTrp[R][Cc] + sTrp[R + 1][Cc])) /
-                 (0.5f * (sDn[rr][cc] + sDn[rr][cc - 1]));
+    {
+      const int r = tid / (kVC / 4), c0 = 4 * (tid - r * (kVC / 4));
+      const int i = i0 + r, j = j0 + c0;
+      if (i < nrad && j < nsec) {
+        const int R = r + 1, Cc = c0 + 1;   // stress index of (i, j)
+        const int rr = r + 2, cc = c0 + kSO;  // staged index of (i, j)
+        float vti[4], vri[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          vti[u] = sVa[rr][cc + u];
+          vri[u] = sVr[rr][cc + u];
         }
-        if (i > 0) {
-          vri += DeltaT * D.invRinf[i] *
-                 ((D.Rmed[i] * sTrr[R][Cc] - D.Rmed[i - 1] * sTrr[R - 1][Cc]) * D.invdiffRmed[i] +
-                  (sTrp[R][Cc + 1] - sTrp[R][Cc]) * D.invdphi - 0.5f * (sTpp[R][Cc] + sTpp[R - 1][Cc])) /
-                 (0.5f * (sDn[rr][cc] + sDn[rr - 1][cc]));
+        if (D.IsDisk) {
+          const float iRm = D.invRmed[i], Rs = D.Rsup[i], Ri = D.Rinf[i], idRs = D.invdiffRsup[i];
+          const float iRi = D.invRinf[i], Rm = D.Rmed[i];
+          const float Rm1 = i > 0 ? D.Rmed[i - 1] : 0.0f, idRm = D.invdiffRmed[i];
+          float trp0[5], trp1[4], tpp0[5], tpp1[4], trr0[4], trr1[4], dn[5], dnm[4];
+#pragma unroll
+          for (int u = 0; u < 5; u++) {
+            trp0[u] = sTrp[R][Cc + u];       // columns c0 .. c0+4
+            tpp0[u] = sTpp[R][Cc - 1 + u];   // columns c0-1 .. c0+3
+            dn[u] = sDn[rr][cc - 1 + u];     // columns c0-1 .. c0+3
+          }
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            trp1[u] = sTrp[R + 1][Cc + u];
+            tpp1[u] = sTpp[R - 1][Cc + u];
+            trr0[u] = sTrr[R][Cc + u];
+            trr1[u] = sTrr[R - 1][Cc + u];
+            dnm[u] = sDn[rr - 1][cc + u];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            if (i > 0 && i < nrad - 1) {
+              vti[u] += DeltaT * iRm *
+                        ((Rs * trp1[u] - Ri * trp0[u]) * idRs + (tpp0[u + 1] - tpp0[u]) * invdphi +
+                         0.5f * (trp0[u] + trp1[u])) /
+                        (0.5f * (dn[u + 1] + dn[u]));
+            }
+            if (i > 0) {
+              vri[u] += DeltaT * iRi *
+                        ((Rm * trr0[u] - Rm1 * trr1[u]) * idRm + (trp0[u + 1] - trp0[u]) * invdphi -
+                         0.5f * (tpp0[u + 1] + tpp1[u])) /
+                        (0.5f * (dn[u + 1] + dnm[u]));
+            }
+            if (kep && i == 0) vti[u] = vin - D.Rmed[0] * C->OmegaFrame;
+            if (kep && i == nrad - 1) vti[u] = vout - D.Rmed[nrad - 1] * C->OmegaFrame;
+          }
         }
-        if (kep && i == 0) vti = vin - D.Rmed[0] * C->OmegaFrame;
-        if (kep && i == nrad - 1) vti = vout - D.Rmed[nrad - 1] * C->OmegaFrame;
+        const int l = i * nsec + j;
+        if ((nsec & 3) == 0) {  // the quad lies inside the ring, 16-byte aligned
+          stg4(D.trr + l, vri[0], vri[1], vri[2], vri[3]);
+          stg4(D.tpp + l, vti[0], vti[1], vti[2], vti[3]);
+        } else {
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            if (j + u < nsec) {
+              stg(D.trr + l + u, vri[u]);
+              stg(D.tpp + l + u, vti[u]);
+            }
+          }
+        }
       }
-      stg(D.trr + l, vri);
-      stg(D.tpp + l, vti);
     }
     __syncthreads();  // buffer bf is restaged two tiles on
     bf ^= 1;
@@ -2553,7 +2622,7 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   REC();
   k_source1<<<b.g_source1, kThreads, 0, s>>>(b);
   REC();
-  k_viscosity<<<b.g_viscosity, kThreads, 0, s>>>(b);
+  k_viscosity<<<b.g_viscosity, kThreads, kViscSmem, s>>>(b);
   REC();
   k_source2<<<b.g_source2, kThreads, 0, s>>>(b);
   REC();
@@ -2617,7 +2686,7 @@ cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int ni
   if ((e = wave(fargo_cfl_kernel(b.max_body), kThreads, 0, b.ncfl, &b.g_cfl))) return e;
   if ((e = wave((const void*)k_source1, kThreads, 0, ncell_tiles, &b.g_source1))) return e;
   if ((e = wave((const void*)k_potential, kThreads, 0, ncell_tiles, &b.g_potential))) return e;
-  if ((e = wave((const void*)k_viscosity, kThreads, 0, ncell_tiles, &b.g_viscosity))) return e;
+  if ((e = wave((const void*)k_viscosity, kThreads, kViscSmem, ncell_tiles, &b.g_viscosity))) return e;
   if ((e = wave((const void*)k_source2, kThreads, 0, ncell_tiles, &b.g_source2))) return e;
   if ((e = wave((const void*)k_energy, kThreads, 0, ncell_tiles, &b.g_energy))) return e;
   if ((e = wave((const void*)k_velocities, kThreads, 0, ncell_tiles, &b.g_velocities))) return e;
@@ -2656,6 +2725,8 @@ cudaError_t fargo_kernel_attributes(int max_nsec) {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_ring_mean<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)fargo_ring_mean_smem_bytes());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_viscosity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kViscSmem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_transport<5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)fargo_transport_smem_bytes(0));
