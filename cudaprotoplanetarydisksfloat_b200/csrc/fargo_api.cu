@@ -423,7 +423,10 @@ int build_items(fargo_batch* b, int seg_out, std::vector<int4>& theta_iso, std::
     std::vector<int4>& theta = h.p.Adiabatic ? theta_adi : theta_iso;
     h.dev.item0 = (int)theta.size();
     const int nseg = (nsec + seg_out - 1) / seg_out;
-    const int seg = (nsec + nseg - 1) / nseg;
+    int seg = (nsec + nseg - 1) / nseg;
+    // segment starts on 4-sector boundaries when NSEC allows: the transport
+    // kernel then stages its rows by 16-byte copies (seg_out is a multiple of 4)
+    if ((nsec & 3) == 0 && (seg_out & 3) == 0) seg = (seg + 3) & ~3;
     for (int i = 0; i < nrad; i += FARGO_BAND) {
       for (int j0 = 0; j0 < nsec; j0 += seg) {
         int S = std::min(seg, nsec - j0);

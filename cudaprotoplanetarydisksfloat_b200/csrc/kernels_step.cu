@@ -1680,18 +1680,15 @@ __device__ __forceinline__ void rad_face(const TrView& V, int b, float vr, float
     ds = 0.0f;
     return;
   }
-  if (vr > 0.0f) {
-    const float h = fm(__ldg(V.Rmed + b) - __ldg(V.Rmed + b - 1) - fm(vr, dt), 0.5f);
+  // upwind side by selection (columns differ in sign): vr > 0 takes row b-1
+  // at + h, else row b at -h; a - fm(h, g) = a + fm(h, -g)
+  const bool pos = vr > 0.0f;
+  const float rm = __ldg(V.Rmed + b), rl = __ldg(V.Rmed + b - 1);
+  const float rp = (b + 1 <= nrad - 1) ? __ldg(V.Rmed + b + 1) : 0.0f;  // only meets a zero slope
+  const float h = pos ? fm(rm - rl - fm(vr, dt), 0.5f) : fm(rp - rm + fm(vr, dt), 0.5f);
 #pragma unroll
-    for (int c = 0; c < nq; c++) qs[c] = lo.W[c] + fm(h, glo[c]);
-    ds = lo.S + fm(h, gslo);
-  } else {
-    const float rp = (b + 1 <= nrad - 1) ? __ldg(V.Rmed + b + 1) : 0.0f;  // only meets a zero slope
-    const float h = fm(rp - __ldg(V.Rmed + b) + fm(vr, dt), 0.5f);
-#pragma unroll
-    for (int c = 0; c < nq; c++) qs[c] = hi.W[c] - fm(h, ghi[c]);
-    ds = hi.S - fm(h, gshi);
-  }
+  for (int c = 0; c < nq; c++) qs[c] = (pos ? lo.W[c] : hi.W[c]) + fm(h, pos ? glo[c] : -ghi[c]);
+  ds = (pos ? lo.S : hi.S) + fm(h, pos ? gslo : -gshi);
 }
 
 // Radial half of Transport (VanLeerRadialKernel, Kernels.cu:1137-1154) for
@@ -1730,6 +1727,89 @@ __device__ __forceinline__ void rad_march(const TrView& V, int ia, int ib, int g
     const float Ri = __ldg(V.Rinf + i), Rs = __ldg(V.Rsup + i), iS = __ldg(V.invSurf + i);
     const float fi = fm(dtdth, Ri), fs = fm(dtdth, Rs);
     float* o = out + (i - ia) * ostride_r;
+#pragma unroll
+    for (int c = 0; c < nq; c++) {
+      float varq = fm(fm(fm(fi, qs[c]), ds), vr0);
+      varq -= fm(fm(fm(fs, qs1[c]), ds1), vr1);
+      o[c * ostride_c] = R1.Q[c] + fm(varq, iS);
+      if (c == nq - 1 && i == 0 && lost0) *lost0 = varq;
+    }
+    R1 = R2;
+    R2 = R3;
+#pragma unroll
+    for (int c = 0; c < nq; c++) {
+      G1[c] = G2[c];
+      qs[c] = qs1[c];
+    }
+    gs1 = gs2;
+    ds = ds1;
+    vr0 = vr1;
+  }
+}
+
+// The band's input rows staged in shared memory (k_transport): logical row
+// k holds ring i0-2+k on the window's columns (L + 1 of them: v_theta is
+// also read one column to the right); dens and v_theta rings i0-2 ..
+// i0+kBR+1, v_r rings i0-2 .. i0+kBR+2 (its ghost row NRAD included).
+// Rings outside the disk are zero-filled: they only feed zero slopes and
+// zero interface fluxes, whose values do not depend on them.
+constexpr int kRow = 264;                    // staged row length (>= window + 1, 16-byte multiple)
+constexpr int kInD = 0, kInR = 12, kInT = 25;  // first staged row of dens, v_r, v_theta
+constexpr int kInRows = 37;
+static_assert(kInR - kInD == FARGO_BAND + 4 && kInT - kInR == FARGO_BAND + 5 &&
+                  kInRows - kInT == FARGO_BAND + 4, "staged rows of one band");
+
+template <int nq>
+__device__ __forceinline__ RadRow<nq> rad_row_s(const TrView& V, const float* sIn, int r, int k, int p, int g,
+                                                float Om) {
+  const int rc = r < 0 ? 0 : (r > V.nrad - 1 ? V.nrad - 1 : r);
+  RadRow<nq> R;
+  const float sg = sIn[(kInD + k) * kRow + p];
+  const float rm = __ldg(V.Rmed + rc);
+  R.S = sg;
+  R.Q[0] = fm(sg, sIn[(kInR + k + 1) * kRow + p]);
+  R.Q[1] = fm(sg, sIn[(kInR + k) * kRow + p]);
+  R.Q[2] = fm(fm(sg, sIn[(kInT + k) * kRow + p + 1] + fm(rm, Om)), rm);
+  R.Q[3] = fm(fm(sg, sIn[(kInT + k) * kRow + p] + fm(rm, Om)), rm);
+  if (nq == 6) R.Q[4] = __ldg(V.energy + rc * V.nsec + g);
+  R.Q[nq - 1] = sg;
+  const float rden = __fdividef(1.0f, sg + 1e-20f);
+#pragma unroll
+  for (int c = 0; c < nq; c++) R.W[c] = fm(R.Q[c], rden);
+  return R;
+}
+
+// rad_march on the staged rows of the band starting at ring i0 (ia = i0):
+// window column p, global column g.
+template <int nq>
+__device__ __forceinline__ void rad_march_s(const TrView& V, const float* sIn, int ia, int ib, int p, int g,
+                                            float dt, float Om, float dtheta, float* out, int ostride_c,
+                                            int ostride_r, float* lost0) {
+  RadRow<nq> R0 = rad_row_s<nq>(V, sIn, ia - 1, 1, p, g, Om);  // row i-1 for the first slope
+  RadRow<nq> R1 = rad_row_s<nq>(V, sIn, ia, 2, p, g, Om);      // row i
+  RadRow<nq> R2 = rad_row_s<nq>(V, sIn, ia + 1, 3, p, g, Om);  // row i+1
+  float G0[nq], G1[nq], gs0, gs1, qs[nq], ds;
+  {
+    RadRow<nq> Rm = rad_row_s<nq>(V, sIn, ia - 2, 0, p, g, Om);
+    rad_slopes<nq>(V, ia - 1, Rm, R0, R1, G0, gs0);  // slope at row i-1
+  }
+  rad_slopes<nq>(V, ia, R0, R1, R2, G1, gs1);  // slope at row i
+  float vr0 = sIn[(kInR + 2) * kRow + p];
+  rad_face<nq>(V, ia, vr0, dt, R0, R1, G0, gs0, G1, gs1, qs, ds);
+  const float dtdth = fm(dt, dtheta);
+#pragma unroll
+  for (int k = 0; k < FARGO_BAND; k++) {
+    const int i = ia + k;
+    if (i >= ib) break;
+    RadRow<nq> R3 = rad_row_s<nq>(V, sIn, i + 2, k + 4, p, g, Om);
+    float G2[nq], gs2;
+    rad_slopes<nq>(V, i + 1, R1, R2, R3, G2, gs2);  // slope at row i+1
+    const float vr1 = sIn[(kInR + k + 3) * kRow + p];  // row nrad is the zero ghost row
+    float qs1[nq], ds1;
+    rad_face<nq>(V, i + 1, vr1, dt, R1, R2, G1, gs1, G2, gs2, qs1, ds1);
+    const float Ri = __ldg(V.Rinf + i), Rs = __ldg(V.Rsup + i), iS = __ldg(V.invSurf + i);
+    const float fi = fm(dtdth, Ri), fs = fm(dtdth, Rs);
+    float* o = out + k * ostride_r;
 #pragma unroll
     for (int c = 0; c < nq; c++) {
       float varq = fm(fm(fm(fi, qs[c]), ds), vr0);
@@ -1847,8 +1927,9 @@ __device__ __forceinline__ int pidx(int t) { return t + (t >> 3); }
 
 size_t fargo_transport_smem_bytes(int adiabatic) {
   const int nq = adiabatic ? 6 : 5;
-  return sizeof(float) * (size_t)kPad * (size_t)(kBR * (nq + 1) + 1);
+  return sizeof(float) * ((size_t)kPad * (size_t)(kBR * (nq + 1) + 1) + (size_t)kInRows * kRow);
 }
+static_assert((kPad * 4) % 16 == 0 && (kRow * 4) % 16 == 0, "staged rows 16-byte aligned");
 
 // The residual and constant-residual van Leer sweeps of OneWindTheta
 // (StarThetaKernel, StarThetaKernel2, VanLeerThetaKernel, Kernels.cu:1157-1273)
@@ -1944,24 +2025,82 @@ __device__ __forceinline__ void sweep_ring(float* sRr, float VMed, float vconst,
   __syncwarp();
 }
 
+// Issue the asynchronous staging of transport item t's input rows (see
+// kRow): 16-byte copies when NSEC and the segment start are multiples of 4
+// (every 4-column chunk then lies inside the ring), else 4-byte copies.
+template <int nq>
+__device__ __forceinline__ void tr_stage(const BatchDev& B, const int4* __restrict__ items, int t, float* sIn) {
+  const int nak = (nq == 5) ? B.act[1] : B.act[2];
+  const int* aoff = (nq == 5) ? B.act_iso_off : B.act_adi_off;
+  const int* adisk = (nq == 5) ? B.act_iso_disk : B.act_adi_disk;
+  const int a = find_range(aoff, nak, t);
+  const DiskDev& D = B.disks[adisk[a]];
+  const int4 it = items[D.item0 + (t - aoff[a])];
+  const int i0 = it.y, g0 = it.z, W = it.w + 9;  // window + 1 columns
+  const int nsec = D.nsec, nrad = D.nrad;
+  const float *dens = D.dens, *vrad = D.vrad, *vth = D.vtheta;
+  auto src = [&](int row, int& r, int& lim) -> const float* {
+    if (row < kInR) {
+      r = i0 - 2 + row - kInD;
+      lim = nrad - 1;
+      return dens;
+    }
+    if (row < kInT) {
+      r = i0 - 2 + row - kInR;
+      lim = nrad;  // the ghost row
+      return vrad;
+    }
+    r = i0 - 2 + row - kInT;
+    lim = nrad - 1;
+    return vth;
+  };
+  if ((nsec & 3) == 0 && (g0 & 3) == 0) {
+    constexpr int nch = kRow / 4;  // whole staged rows: a constant divisor
+    for (int q = threadIdx.x; q < kInRows * nch; q += kTT) {
+      const int row = q / nch, ch = q - row * nch;
+      int r, lim;
+      const float* base = src(row, r, lim);
+      const bool ok = r >= 0 && r <= lim;
+      int g = g0 - 4 + 4 * ch;
+      if (g < 0) g += nsec;
+      while (g >= nsec) g -= nsec;
+      cp_async16(sIn + row * kRow + 4 * ch, base + (ok ? r * nsec + g : 0), ok);
+    }
+  } else {
+    for (int q = threadIdx.x; q < kInRows * W; q += kTT) {
+      const int row = q / W, c = q - row * W;
+      int r, lim;
+      const float* base = src(row, r, lim);
+      const bool ok = r >= 0 && r <= lim;
+      int g = (g0 - 4 + c) % nsec;
+      if (g < 0) g += nsec;
+      cp_async4(sIn + row * kRow + c, base + (ok ? r * nsec + g : 0), ok);
+    }
+  }
+  cp_async_commit();
+}
+
 // Transport (TransportEuler.cu:24-35) of a band of up to kBR rings i0 ..
 // and one azimuthal segment of source sectors g0 .. g0+S-1.  The tile is
-// taken in source coordinates: the radial half (rad_march) runs over the
+// taken in source coordinates: the radial half (rad_march_s) runs over the
 // window g0-4 .. g0+S+3 of every ring of the band, one thread per column
-// marching outwards, into shared memory; then one warp per ring runs the
-// azimuthal sweeps (sweep_ring) on that window, whose 4-point halo covers
-// the sweeps' stencils.  Source sector g of ring i is then stored at output
-// sector g + Nshift_i (AdvectSHIFTKernel, Kernels.cu:1276-1289: output j
-// takes source j - Nshift): per ring a contiguous run, and the segments of
-// a ring map one to one onto its output sectors.  VMed, Nshift and the
-// constant residual come from k_ring_mean<1>.  Final density / energy go
-// to scratch (a0 / a1) because neighbouring bands still read the old ones;
-// the velocity kernel moves them into the state.
+// marching outwards, on input rows staged in shared memory, into shared
+// memory; then one warp per ring runs the azimuthal sweeps (sweep_ring) on
+// that window, whose 4-point halo covers the sweeps' stencils.  The next
+// item's rows are staged while the sweeps run.  Source sector g of ring i
+// is then stored at output sector g + Nshift_i (AdvectSHIFTKernel,
+// Kernels.cu:1276-1289: output j takes source j - Nshift): per ring a
+// contiguous run, and the segments of a ring map one to one onto its output
+// sectors.  VMed, Nshift and the constant residual come from
+// k_ring_mean<1>.  Final density / energy go to scratch (a0 / a1) because
+// neighbouring bands still read the old ones; the velocity kernel moves
+// them into the state.
 template <int nq>
 __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __restrict__ items) {
-  extern __shared__ float tr_sm[];
+  extern __shared__ __align__(16) float tr_sm[];
   float* sR = tr_sm;                         // [kBR][nq + 1][kPad] radial results + v_theta
   float* sL = sR + kBR * (nq + 1) * kPad;    // [kPad] mass through the inner edge (OPEN)
+  float* sIn = sL + kPad;                    // [kInRows][kRow] staged input rows
   __shared__ int s_jb[kBR];
   __shared__ float s_vmed[kBR], s_vc[kBR];
   const int nak = (nq == 5) ? B.act[1] : B.act[2];
@@ -1969,11 +2108,17 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
   const int* adisk = (nq == 5) ? B.act_iso_disk : B.act_adi_disk;
   const int nai = nak > 0 ? aoff[nak] : 0;
   const int p = threadIdx.x, warp = p >> 5, lane = p & 31;
+  if ((int)blockIdx.x < nai) tr_stage<nq>(B, items, blockIdx.x, sIn);
   for (int t = blockIdx.x; t < nai; t += gridDim.x) {
-    __syncthreads();
+    const int tn = t + gridDim.x;  // this block's next item
     const int a = find_range(aoff, nak, t);
     const DiskDev& D = B.disks[adisk[a]];
-    if (!D.IsDisk) continue;
+    cp_async_wait<0>();
+    __syncthreads();  // staged rows visible; the previous item's sweeps are done
+    if (!D.IsDisk) {
+      if (tn < nai) tr_stage<nq>(B, items, tn, sIn);
+      continue;
+    }
     const int4 it = items[D.item0 + (t - aoff[a])];
     const DiskCtl* C = D.ctl;
     const int i0 = it.y, g0 = it.z, S = it.w;
@@ -1996,11 +2141,12 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
       int g = (g0 - 4 + p) % nsec;
       if (g < 0) g += nsec;
       float* o = sR + pidx(p);
-      rad_march<nq>(V, i0, i0 + nb, g, dt, Om, dtheta, o, kPad, (nq + 1) * kPad,
-                    (D.OpenInner && i0 == 0) ? sL + pidx(p) : nullptr);
-      for (int r = 0; r < nb; r++) o[(r * (nq + 1) + nq) * kPad] = __ldg(V.vtheta + (i0 + r) * nsec + g);
+      rad_march_s<nq>(V, sIn, i0, i0 + nb, p, g, dt, Om, dtheta, o, kPad, (nq + 1) * kPad,
+                      (D.OpenInner && i0 == 0) ? sL + pidx(p) : nullptr);
+      for (int r = 0; r < nb; r++) o[(r * (nq + 1) + nq) * kPad] = sIn[(kInT + r + 2) * kRow + p];
     }
-    __syncthreads();
+    __syncthreads();  // radial results complete; the staged rows are free
+    if (tn < nai) tr_stage<nq>(B, items, tn, sIn);
     const int r = warp;
     if (r < nb) {
       const int i = i0 + r;
@@ -2023,6 +2169,7 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
       }
     }
   }
+  cp_async_wait<0>();
 }
 
 // ComputeVelocitiesKernel, Kernels.cu:1292-1306, from the transported
