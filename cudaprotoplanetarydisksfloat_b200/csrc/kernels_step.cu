@@ -1014,41 +1014,46 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
 
 // ----------------------------------------------------------- source terms
 
-// Gravitational potential at cell (i, j): FillForcesArraysKernel
-// (Kernels.cu:1322-1349) summed over the planets in the reference's order.
-__device__ __forceinline__ float potential_xy(const DiskDev& D, const DiskCtl* C, int i, float cosj, float sinj) {
-  const float Rm = D.Rmed[i];
-  const float x = Rm * cosj;
-  const float y = Rm * sinj;
-  float P = 0.0f;
-  const int nb = C->nb;
-  for (int k = 0; k < nb; k++) {
-    const float xp = C->pxp[k], yp = C->pyp[k], mp = C->pmass[k];
-    float distance = (x - xp) * (x - xp) + (y - yp) * (y - yp);
-    float distancesmooth = sqrtf(distance + C->psmooth[k]);
-    float pot = __fdiv_rn(-mp, distancesmooth);  // -G*mplanet/distancesmooth
-    if (D.Indirect_Term) pot += mp * C->pipd3[k] * (x * xp + y * yp);
-    P += pot;
-    if (k == 0) {
-      float InvDistance = __fdiv_rn(1.0f, Rm);
-      pot = -InvDistance;
-      pot -= C->itx * x + C->ity * y;
-      P += pot;
-    }
-  }
-  return P;
-}
-
 // FillForcesArrays (Pframeforce.cu:37-66): the potential of every cell, once
-// per substep (Substep1 reads it at three cells each).
+// per substep (Substep1 reads it at three cells each), summed over the
+// planets in the reference's order (FillForcesArraysKernel,
+// Kernels.cu:1322-1349); each planet's parameters are read once per quad.
 __global__ void __launch_bounds__(kThreads) k_potential(BatchDev B) {
   QUAD_BEGIN
-  float cp[4], sp[4], phi[4];
+  float cp[4], sp[4], x[4], y[4], P[4];
   qld_sector(cp, D.cos_pot, q);
   qld_sector(sp, D.sin_pot, q);
 #pragma unroll
-  for (int u = 0; u < 4; u++) phi[u] = potential_xy(D, C, q.i[u], cp[u], sp[u]);
-  qst(D.phi, q, phi);
+  for (int u = 0; u < 4; u++) {
+    const float Rm = D.Rmed[q.i[u]];
+    x[u] = Rm * cp[u];
+    y[u] = Rm * sp[u];
+    P[u] = 0.0f;
+  }
+  const int nb = C->nb;
+  const bool ind = D.Indirect_Term;
+  for (int k = 0; k < nb; k++) {
+    const float xp = C->pxp[k], yp = C->pyp[k], mp = C->pmass[k], sm = C->psmooth[k], ip3 = C->pipd3[k];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      float distance = (x[u] - xp) * (x[u] - xp) + (y[u] - yp) * (y[u] - yp);
+      float distancesmooth = sqrtf(distance + sm);
+      float pot = __fdiv_rn(-mp, distancesmooth);  // -G*mplanet/distancesmooth
+      if (ind) pot += mp * ip3 * (x[u] * xp + y[u] * yp);
+      P[u] += pot;
+    }
+    if (k == 0) {  // the star
+      const float itx = C->itx, ity = C->ity;
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        float InvDistance = __fdiv_rn(1.0f, D.Rmed[q.i[u]]);
+        float pot = -InvDistance;
+        pot -= itx * x[u] + ity * y[u];
+        P[u] += pot;
+      }
+    }
+  }
+  qst(D.phi, q, P);
   QUAD_END
 }
 
