@@ -542,6 +542,7 @@ __device__ __forceinline__ void qst(float* p, const Quad<V>& q, const float (&v)
     constexpr bool V = std::decay_t<decltype(q)>::vec;                                                 \
     (void)V;                                                                                           \
     const int nsec = D.nsec, nrad = D.nrad;                                                            \
+    (void)nsec;                                                                                        \
     (void)nrad;
 #define QUAD_BEGIN QUAD_BEGIN_T(false)
 #define QUAD_END \
@@ -1632,28 +1633,6 @@ struct TrView {
   int nsec, nrad;
 };
 
-template <int nq>
-__device__ __forceinline__ RadRow<nq> rad_row(const TrView& V, int r, int g, int gp, float Om) {
-  const int nsec = V.nsec;
-  r = r < 0 ? 0 : (r > V.nrad - 1 ? V.nrad - 1 : r);  // clamped rows only meet zero slopes
-  const int lr = r * nsec + g;
-  const int lrp = r * nsec + gp;
-  RadRow<nq> R;
-  const float sg = __ldg(V.dens + lr);
-  const float rm = __ldg(V.Rmed + r);
-  R.S = sg;
-  R.Q[0] = fm(sg, __ldg(V.vrad + lr + nsec));
-  R.Q[1] = fm(sg, __ldg(V.vrad + lr));
-  R.Q[2] = fm(fm(sg, __ldg(V.vtheta + lrp) + fm(rm, Om)), rm);
-  R.Q[3] = fm(fm(sg, __ldg(V.vtheta + lr) + fm(rm, Om)), rm);
-  if (nq == 6) R.Q[4] = __ldg(V.energy + lr);
-  R.Q[nq - 1] = sg;
-  const float rden = __fdividef(1.0f, sg + 1e-20f);
-#pragma unroll
-  for (int c = 0; c < nq; c++) R.W[c] = fm(R.Q[c], rden);
-  return R;
-}
-
 // van Leer slopes at row r from rows r-1, r, r+1 (StarRadKernel; zero on the
 // first and last ring): g[c] for the quotients, gs for the density.
 template <int nq>
@@ -1696,62 +1675,6 @@ __device__ __forceinline__ void rad_face(const TrView& V, int b, float vr, float
   ds = (pos ? lo.S : hi.S) + fm(h, pos ? gslo : -gshi);
 }
 
-// Radial half of Transport (VanLeerRadialKernel, Kernels.cu:1137-1154) for
-// rings ia .. ib-1 at column g, marching outwards: each ring loads one new
-// row, one new slope and one new interface.  out[k][c] at stride ostride.
-// lost0 (may be null): receives the density's varq at ring 0, the mass that
-// leaves through the inner edge (LostByDisk, Kernels.cu:941-944).
-template <int nq>
-__device__ __forceinline__ void rad_march(const TrView& V, int ia, int ib, int g, float dt, float Om,
-                                          float dtheta, float* out, int ostride_c, int ostride_r, float* lost0) {
-  const int nsec = V.nsec;
-  const int gp = g + 1 == nsec ? 0 : g + 1;
-  RadRow<nq> R0 = rad_row<nq>(V, ia - 1, g, gp, Om);  // row i-1 for the first slope
-  RadRow<nq> R1 = rad_row<nq>(V, ia, g, gp, Om);      // row i
-  RadRow<nq> R2 = rad_row<nq>(V, ia + 1, g, gp, Om);  // row i+1
-  float G0[nq], G1[nq], gs0, gs1, qs[nq], ds;
-  {
-    RadRow<nq> Rm = rad_row<nq>(V, ia - 2, g, gp, Om);
-    rad_slopes<nq>(V, ia - 1, Rm, R0, R1, G0, gs0);  // slope at row i-1
-  }
-  rad_slopes<nq>(V, ia, R0, R1, R2, G1, gs1);  // slope at row i
-  float vr0 = __ldg(V.vrad + ia * nsec + g);
-  rad_face<nq>(V, ia, vr0, dt, R0, R1, G0, gs0, G1, gs1, qs, ds);
-  const float dtdth = fm(dt, dtheta);
-  // at most FARGO_BAND rings: unrolled, so that later rows load early
-#pragma unroll
-  for (int k = 0; k < FARGO_BAND; k++) {
-    const int i = ia + k;
-    if (i >= ib) break;
-    RadRow<nq> R3 = rad_row<nq>(V, i + 2, g, gp, Om);
-    float G2[nq], gs2;
-    rad_slopes<nq>(V, i + 1, R1, R2, R3, G2, gs2);  // slope at row i+1
-    const float vr1 = __ldg(V.vrad + (i + 1) * nsec + g);  // row nrad is the zero ghost row
-    float qs1[nq], ds1;
-    rad_face<nq>(V, i + 1, vr1, dt, R1, R2, G1, gs1, G2, gs2, qs1, ds1);
-    const float Ri = __ldg(V.Rinf + i), Rs = __ldg(V.Rsup + i), iS = __ldg(V.invSurf + i);
-    const float fi = fm(dtdth, Ri), fs = fm(dtdth, Rs);
-    float* o = out + (i - ia) * ostride_r;
-#pragma unroll
-    for (int c = 0; c < nq; c++) {
-      float varq = fm(fm(fm(fi, qs[c]), ds), vr0);
-      varq -= fm(fm(fm(fs, qs1[c]), ds1), vr1);
-      o[c * ostride_c] = R1.Q[c] + fm(varq, iS);
-      if (c == nq - 1 && i == 0 && lost0) *lost0 = varq;
-    }
-    R1 = R2;
-    R2 = R3;
-#pragma unroll
-    for (int c = 0; c < nq; c++) {
-      G1[c] = G2[c];
-      qs[c] = qs1[c];
-    }
-    gs1 = gs2;
-    ds = ds1;
-    vr0 = vr1;
-  }
-}
-
 // The band's input rows staged in shared memory (k_transport): logical row
 // k holds ring i0-2+k on the window's columns (L + 1 of them: v_theta is
 // also read one column to the right); dens and v_theta rings i0-2 ..
@@ -1784,8 +1707,13 @@ __device__ __forceinline__ RadRow<nq> rad_row_s(const TrView& V, const float* sI
   return R;
 }
 
-// rad_march on the staged rows of the band starting at ring i0 (ia = i0):
-// window column p, global column g.
+// Radial half of Transport (VanLeerRadialKernel, Kernels.cu:1137-1154) for
+// rings ia .. ib-1 at column g, marching outwards: each ring loads one new
+// row, one new slope and one new interface.  out[k][c] at stride ostride.
+// lost0 (may be null): receives the density's varq at ring 0, the mass that
+// leaves through the inner edge (LostByDisk, Kernels.cu:941-944).
+// The rows come from the band's staged rows (ia = i0): window column p,
+// global column g.
 template <int nq>
 __device__ __forceinline__ void rad_march_s(const TrView& V, const float* sIn, int ia, int ib, int p, int g,
                                             float dt, float Om, float dtheta, float* out, int ostride_c,
@@ -2163,7 +2091,7 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
       // window point x is source sector g0 + x - 4, stored at output sector
       // jb + x - 4 (jb < nsec and x - 4 < S <= nsec: one wrap at most)
       float* dsts[6] = {D.vri, D.vti, D.trr, D.tpp, D.a1, D.a0};
-      const long long row = (long long)i * nsec;
+      const int row = i * nsec;
       const int jb = s_jb[r] - 4;
       for (int x = 4 + lane; x < L - 4; x += 32) {
         int j = jb + x;
@@ -2593,7 +2521,7 @@ __global__ void __launch_bounds__(kThreads) k_init_velocities(BatchDev B, int di
   const long long base = 0;
   const DiskCtl* C = D.ctl;
   const int nsec = D.nsec, nrad = D.nrad;
-  const int loc = (int)(c - base), i = loc / nsec, j = loc - i * nsec;
+  const int loc = (int)(c - base), i = loc / nsec;
   const long long l = loc;
   float omega, r, ri;
   if (i == nrad) {
