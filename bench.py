@@ -14,7 +14,10 @@ Workloads (--workload):
 Output: one JSON line (rank 0).  `value` is device-resident throughput
 (CUDA events on the library's stream); `e2e` goes through the C ABI with
 page-locked host buffers: every step uploads every disk's state, advances
-one DT and downloads the state.  `--impl reference` times the reference's
+one DT and downloads the state.  The batched workloads split their disks
+over --groups batches (LPT on cell counts) advanced concurrently on their
+own streams: one batch's last substeps, when few of its disks are still
+inside their DT, and its host copies overlap the other batches' work.  `--impl reference` times the reference's
 own CUDA build (oracle/_ref/fargo_ref, from the reference sources) on a
 bounded sample of the same disks, with its own AlgoGas timer.
 
@@ -171,11 +174,11 @@ def materialise_all(disks, tmp):
     return P, L
 
 
-def noisy_init(batch, P, seed0):
+def noisy_init(batch, P, seeds):
     from cudaprotoplanetarydisksfloat_b200 import noise
-    for d, p in enumerate(P):
+    for d, (p, seed) in enumerate(zip(P, seeds)):
         f = batch.fields(d)
-        dens = noise.perturb_density(f["dens"].reshape(-1), p.NRAD, p.NSEC, seed0 + d)
+        dens = noise.perturb_density(f["dens"].reshape(-1), p.NRAD, p.NSEC, seed)
         batch.init_state(d, dens=dens)
 
 
@@ -191,10 +194,21 @@ def ours(args, world, rank, local, pg):
     P, L = materialise_all(disks, tmp)
     cells = np.array([p.NRAD * p.NSEC for p in P], dtype=np.int64)
     plain = args.workload == "c4plain"
-    groups = [[d] for d in range(len(P))] if plain else [list(range(len(P)))]
+    # batched workloads: the disks in --groups batches (LPT on cell counts),
+    # advanced concurrently on their own streams, so that one batch's last
+    # substeps (few disks still inside their DT) overlap another's
+    G = 1 if plain else max(1, min(args.groups, len(P)))
+    if plain:
+        groups = [[d] for d in range(len(P))]
+    elif G == 1:
+        groups = [list(range(len(P)))]
+    else:
+        from cudaprotoplanetarydisksfloat_b200 import shard
+        groups = [sorted(g) for g in shard.lpt_partition([int(c) for c in cells], G)]
+    gcells = np.array([cells[d] for g in groups for d in g], dtype=np.int64)  # nsub_total() order
     batches = [Batch([P[d] for d in g], [L[d] for d in g], device=local) for g in groups]
     for b, g in zip(batches, groups):
-        noisy_init(b, [P[d] for d in g], 20261203 + 1000 * rank + g[0])
+        noisy_init(b, [P[d] for d in g], [20261203 + 1000 * rank + d for d in g])
         if args.no_graph:
             b.set_graph_mode(False)
     streams = [torch.cuda.ExternalStream(lib.fargo_batch_stream(b.b), device=local) for b in batches]
@@ -233,73 +247,102 @@ def ours(args, world, rank, local, pg):
             b.sync()
         ms = ev0[0].elapsed_time(ev1[-1])
     else:
+        # every batch's stream starts after ev0 on stream 0; stream 0 waits for
+        # the others' ends before the closing event
         ev0[0].record(streams[0])
+        for st in streams[1:]:
+            st.wait_event(ev0[0])
         run(args.steps)
-        ev1[0].record(streams[0])
-        batches[0].sync()
-        ms = ev0[0].elapsed_time(ev1[0])
+        for st, ev in zip(streams, ev1):
+            ev.record(st)
+        end = torch.cuda.Event(enable_timing=True)
+        for ev in ev1[1:]:
+            streams[0].wait_event(ev)
+        end.record(streams[0])
+        for b in batches:
+            b.sync()
+        ms = ev0[0].elapsed_time(end)
     torch.cuda.synchronize()
     t_wall = time.time() - t_wall
     clocks = clk.stop()
     barrier(pg)
     n1 = nsub_total()
     l1 = sum(lib.fargo_batch_count_launches(b.b) for b in batches)
-    upd = float(np.sum(cells * (n1 - n0)))
+    upd = float(np.sum(gcells * (n1 - n0)))
     ms_max = allmax(pg, ms)
     upd_all = allsum(pg, upd)
     value = upd_all / (ms_max * 1e-3)
 
-    # end to end through the C ABI with page-locked host buffers
+    # end to end through the C ABI with page-locked host buffers: every step
+    # uploads every disk's state, advances one DT and downloads the state.  Each
+    # batch does so in order on its own stream; with several batches one
+    # batch's copies overlap another's DT.
+    ebatches, egroups = batches, groups
+    estreams = streams
     pinned = []
-    for b, g in zip(batches, groups):
+    for eb, g in zip(ebatches, egroups):
         for k, d in enumerate(g):
             n = (P[d].NRAD + 1) * P[d].NSEC
             arrs = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(3)]
-            f = b.fields(k)
-            for a, key in zip(arrs, ("dens", "vrad", "vtheta")):
-                a.numpy()[:] = f[key].reshape(-1)
-            pinned.append((b, k, arrs))
+            f = eb.fields(k)
+            for a_, key in zip(arrs, ("dens", "vrad", "vtheta")):
+                a_.numpy()[:] = f[key].reshape(-1)
+            pinned.append((eb, k, arrs))
     fp = C.POINTER(C.c_float)
+
+    def e_nsub():
+        return np.array([b.scalars(k)["nsub_total"] for b, g in zip(ebatches, egroups) for k in range(len(g))],
+                        dtype=np.int64)
+
+    ecells = np.array([P[d].NRAD * P[d].NSEC for g in egroups for d in g], dtype=np.int64)
 
     def e2e_step():
         if plain:
             # one disk after another: upload, one DT, download, then the next disk
             for b, k, arrs in pinned:
-                ptrs = [C.cast(a.data_ptr(), fp) for a in arrs]
+                ptrs = [C.cast(a_.data_ptr(), fp) for a_ in arrs]
                 lib.fargo_batch_upload_async(b.b, k, ptrs[0], ptrs[1], ptrs[2], None)
                 lib.fargo_batch_advance_async(b.b, 1)
                 lib.fargo_batch_download_async(b.b, k, ptrs[0], ptrs[1], ptrs[2], None)
                 b.sync()
             return
-        for b, k, arrs in pinned:
-            ptrs = [C.cast(a.data_ptr(), fp) for a in arrs]
-            lib.fargo_batch_upload_async(b.b, k, ptrs[0], ptrs[1], ptrs[2], None)
-        for b in batches:
-            lib.fargo_batch_advance_async(b.b, 1)
-        for b, k, arrs in pinned:
-            ptrs = [C.cast(a.data_ptr(), fp) for a in arrs]
-            lib.fargo_batch_download_async(b.b, k, ptrs[0], ptrs[1], ptrs[2], None)
+        for eb in ebatches:
+            mine = [(k, arrs) for b, k, arrs in pinned if b is eb]
+            for k, arrs in mine:
+                ptrs = [C.cast(a_.data_ptr(), fp) for a_ in arrs]
+                lib.fargo_batch_upload_async(eb.b, k, ptrs[0], ptrs[1], ptrs[2], None)
+            lib.fargo_batch_advance_async(eb.b, 1)
+            for k, arrs in mine:
+                ptrs = [C.cast(a_.data_ptr(), fp) for a_ in arrs]
+                lib.fargo_batch_download_async(eb.b, k, ptrs[0], ptrs[1], ptrs[2], None)
 
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
     for _ in range(2):
         e2e_step()
-    for b in batches:
+    for b in ebatches:
         b.sync()
-    n0 = nsub_total()
+    n0 = e_nsub()
     barrier(pg)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(streams[0])
+    ends = [torch.cuda.Event() for _ in estreams]
+    e0.record(estreams[0])
+    for st in estreams[1:]:
+        st.wait_event(e0)
     for _ in range(e2e_steps):
         e2e_step()
-    e1.record(streams[-1])
-    for b in batches:
+    for st, ev in zip(estreams, ends):
+        ev.record(st)
+    for ev in ends[1:]:
+        estreams[0].wait_event(ev)
+    e1.record(estreams[0])
+    for b in ebatches:
         b.sync()
     torch.cuda.synchronize()
     e_ms = e0.elapsed_time(e1)
-    n1 = nsub_total()
-    e_upd = allsum(pg, float(np.sum(cells * (n1 - n0))))
+    n1 = e_nsub()
+    e_upd = allsum(pg, float(np.sum(ecells * (n1 - n0))))
     e_ms = allmax(pg, e_ms)
     bytes_io = sum(4 * 3 * (P[d].NRAD + 1) * P[d].NSEC for d in range(len(P)))
     e2e = {"value": e_upd / (e_ms * 1e-3), "unit": "cell-updates/s", "h2d_bytes_per_step": bytes_io * world,
@@ -318,12 +361,16 @@ def ours(args, world, rank, local, pg):
             if st == 0:
                 ms_k += np.array(arr[:nk])
         n1 = nsub_total()
-        upd_prof = float(np.sum(cells * (n1 - n0)))
+        upd_prof = float(np.sum(gcells * (n1 - n0)))
         names = [lib.fargo_profile_kernel_name(k).decode() for k in range(nk)]
         top = int(np.argmax(ms_k[:nk - 1]))
         name = names[top]
         adi = int(P[0].Adiabatic)
-        launches = int(np.sum(n1 - n0)) if plain else int(max(1, (n1 - n0).max()))
+        # launches of each kernel: every batch's graph loops until its last
+        # disk ends its DT
+        dn = n1 - n0
+        off = np.cumsum([0] + [len(g) for g in groups])
+        launches = int(max(1, sum(int(dn[off[k]:off[k + 1]].max()) for k in range(len(groups)))))
         cells_per_launch = upd_prof / launches
         peak, kind = load_peaks()
         # algorithmic bytes per cell-update: the state read once and written once
@@ -354,7 +401,7 @@ def ours(args, world, rank, local, pg):
         "value": value, "ms_per_step": ms_max / args.steps, "e2e": e2e, "roofline": roof,
         "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(l1 - l0) * world,
         "wall_s": t_wall, "cells": int(cells.sum()) * world, "disks": len(P) * world,
-        "seg_out": sorted(set(seg_out)),
+        "seg_out": sorted(set(seg_out)), "batches": len(batches),
     }
 
 
@@ -444,6 +491,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c4", choices=["c4", "c4plain", "c4q", "c1", "c2", "c3", "c5"])
     ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--groups", type=int, default=4,
+                    help="concurrent batches the disks of a batched workload are split over")
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--ref-disks", type=int, default=6)
     ap.add_argument("--ref-steps", type=int, default=3)
@@ -463,7 +512,8 @@ def main():
                "c1": "isothermal 128x384, 1 planet", "c2": "adiabatic 256x768, alpha viscosity, 2 live planets",
                "c3": "self-gravitating 512x1024, 1 planet", "c5": "adiabatic+SG 2048x6144, 3 live planets"}
     config = {"workload": args.workload, "description": wl_desc[args.workload],
-              "parallelism": "disk-parallel, one batch of disks per GPU" if args.workload.startswith("c4") else
+              "parallelism": "disk-parallel: the GPU's disks in concurrent batches on their own streams"
+              if args.workload.startswith("c4") else
               "single disk per GPU", "l2": "working set larger than L2" if args.workload in ("c4", "c4plain", "c4q", "c5")
               else "working set L2-resident (launch-bound)"}
     metric = "cell-updates/s"
@@ -493,7 +543,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                 "higher_is_better": True, "scaling": "strong" if args.strong else "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic (seeded parameters and density noise)",
-                "config": dict(config, disks=r["disks"], cells=r["cells"],
+                "config": dict(config, disks=r["disks"], cells=r["cells"], batches=r["batches"],
                                tile={"transport_segment": r["seg_out"], "band_rings": 8, "autotuned": True}),
                 "e2e": r["e2e"], "roofline": r["roofline"], "cpu_baseline": r["cpu_baseline"],
                 "clocks": r["clocks"], "gpu_launches": r["gpu_launches"]}

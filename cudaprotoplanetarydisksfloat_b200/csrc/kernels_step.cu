@@ -814,6 +814,14 @@ __device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const d
 // NB >= every disk's body count (star + FeelDisk planets): the per-thread
 // FP64 force accumulators are sized for it.
 constexpr int kCflCells = FARGO_CFL_TILE / kThreads;
+// The per-cell limit CFLSECURITY / s (s = sqrtf(...), a float) is a double
+// division rounded to float.  For CFLSECURITY = 2^-1 it equals 0.5f times the
+// correctly rounded float reciprocal of s: scaling by a power of two commutes
+// with rounding (normal range), and rounding the double quotient 1/s to float
+// gives the correctly rounded float quotient, since 53 >= 2*24 + 2 makes the
+// double rounding innocuous for a quotient of two floats (Figueroa, "When is
+// double rounding innocuous?", SIGNUM 1995).
+static_assert(CFLSEC == 0.5, "the CFL limit's reciprocal form needs CFLSECURITY = 0.5");
 static_assert(kCflCells * kThreads == FARGO_CFL_TILE, "CFL tile = whole cells per thread");
 template <int NB>
 __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDev B) {
@@ -940,7 +948,10 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
               dvt = -dvt;
             float invdt4 = max2(dvr / dxrad, dvt / dxt);
             invdt4 *= 4.0 * CVNR * CVNR;
-            float dt2d = CFLSEC / sqrtf(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 + invdt4 * invdt4);
+            // CFLSECURITY / sqrtf(..) divides in double; with CFLSECURITY = 0.5
+            // that is 0.5 * the float IEEE reciprocal, bit for bit (see below)
+            float dt2d =
+                0.5f * __frcp_rn(sqrtf(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 + invdt4 * invdt4));
             if (dt2d < lmin) lmin = dt2d;
           }
           const float Rm = D.Rmed[ic];
