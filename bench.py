@@ -376,16 +376,20 @@ def ours(args, world, rank, local, pg):
         # algorithmic bytes per cell-update: the state read once and written once
         b_alg = B_ALG[args.workload]
         achieved = b_alg * cells_per_launch / (ms_k[top] * 1e-3 / launches) / 1e9
-        traffic = None
+        # the kernel's DRAM bytes per cell and issue utilisation from one ncu
+        # capture (profiles/dram_traffic_c4q_first_substep.md)
+        traffic = issue = None
         try:
             with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
                 tj = json.load(f)
             if name in tj:
                 traffic = round(float(tj[name]["dram_bytes_per_cell"]) * cells_per_launch)
+                issue = tj[name].get("issue_active_pct")
         except (OSError, ValueError, KeyError):
             pass
         roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                 "peak_kind": kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                "issue_active_pct_ncu": issue,
                 "alg_bytes_per_cell": b_alg, "alg_bytes_per_launch": round(b_alg * cells_per_launch),
                 "launch_ms": round(float(ms_k[top]) / launches, 4),
                 "step_frac": round(value * b_alg / (peak * 1e9), 4),
