@@ -483,7 +483,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   std::vector<long long> cell_off(n + 1, 0);
   std::vector<int> ring_off(n + 1, 0);
   std::vector<int4> theta_iso, theta_adi;
-  int seg_max = 0, any_bc = 0, max_body = 1;
+  int seg_max = 0, any_bc = 0, max_body = 1, src1_classes = 0;
   for (int d = 0; d < n; d++) {
     fargo_status st = check_params(b, &params[d], &planets[d]);
     if (st) return st;
@@ -502,6 +502,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     b->any_adiabatic |= h.p.Adiabatic;
     b->n_sg += h.p.SelfGravity ? 1 : 0;
     any_bc |= (h.p.OpenInner || h.p.NonReflecting || h.p.Evanescent) ? 1 : 0;
+    src1_classes |= 1 << (2 * (h.p.Adiabatic ? 1 : 0) + (h.p.SelfGravity ? 1 : 0));
     max_body = std::max(max_body, body_count(&planets[d]));
   }
   seg_max = build_items(b, FARGO_SEG_OUT, theta_iso, theta_adi);
@@ -533,6 +534,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   BatchDev& bd = b->bd;
   bd.ndisk = n;
   bd.any_bc = any_bc;
+  bd.src1_classes = src1_classes;
   bd.max_body = max_body;
   bd.ncell = cell_off[n];
   bd.nring = ring_off[n];

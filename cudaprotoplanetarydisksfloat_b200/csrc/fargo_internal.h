@@ -171,9 +171,10 @@ struct BatchDev {
   int* act_vtile_off;        // [ndisk+1] prefix of viscosity tiles (8 x 64 cells) of active disks
   int cell_grid, ring_grid, item_grid, grp_grid;  // fixed grid sizes of the grid-stride kernels
   int any_bc;                // some disk has an OPEN, NONREFLECTING or EVANESCENT boundary
+  int src1_classes;          // bit 2*Adiabatic + SelfGravity set for every kind of disk present
   int max_body;              // largest body count of the force sums (star + FeelDisk planets)
   // one-wave grids of the substep kernels (fargo_size_grids)
-  int g_cfl, g_source1, g_potential, g_viscosity, g_source2, g_energy, g_velocities, g_transport;
+  int g_cfl, g_source1[4], g_potential, g_viscosity, g_source2, g_energy, g_velocities, g_transport;
 };
 
 // kernel entry points (kernels_step.cu), launched by fargo_api.cu

@@ -391,10 +391,11 @@ struct Quad {
 // tiles, so it meets few disks; on entering a disk the block copies its
 // DiskDev to shared memory.  A thread's quad advances by FARGO_QTILE cells
 // from one tile to the next (no division after the disk's first tile); the
-// tiles of one disk form an inner loop without barriers.  adi_only: skip
-// isothermal disks (energy kernel).
+// tiles of one disk form an inner loop without barriers.  kAdi, kSg (0 or 1;
+// -1: any): only the disks whose Adiabatic / SelfGravity flags match (the
+// energy kernel takes adiabatic disks, the Substep1 instances one kind each).
 static_assert(FARGO_QTILE == 4 * kThreads, "four cells per thread");
-template <bool adi_only, class Body>
+template <int kAdi, int kSg, class Body>
 __device__ __forceinline__ void for_active_quads(const BatchDev& B, Body body) {
   __shared__ DiskDev sD;
   const int na = B.act[0];
@@ -409,7 +410,8 @@ __device__ __forceinline__ void for_active_quads(const BatchDev& B, Body body) {
     __syncthreads();
     copy_words(&sD, B.disks + B.act_disk[a], sizeof(DiskDev));
     __syncthreads();
-    if (!sD.IsDisk || (adi_only && !sD.Adiabatic)) {  // nothing to do on this disk
+    if (!sD.IsDisk || (kAdi >= 0 && (sD.Adiabatic != 0) != (kAdi == 1)) ||
+        (kSg >= 0 && (sD.SelfGravity != 0) != (kSg == 1))) {  // nothing to do on this disk
       t = te;
       continue;
     }
@@ -537,14 +539,14 @@ __device__ __forceinline__ void qst(float* p, const Quad<V>& q, const float (&v)
   }
 }
 
-#define QUAD_BEGIN_T(adi_only)                                                                         \
-  for_active_quads<adi_only>(B, [&](const DiskDev& D, const DiskCtl* C, const auto& q) {               \
+#define QUAD_BEGIN_T(kAdi, kSg)                                                                         \
+  for_active_quads<kAdi, kSg>(B, [&](const DiskDev& D, const DiskCtl* C, const auto& q) {              \
     constexpr bool V = std::decay_t<decltype(q)>::vec;                                                 \
     (void)V;                                                                                           \
     const int nsec = D.nsec, nrad = D.nrad;                                                            \
     (void)nsec;                                                                                        \
     (void)nrad;
-#define QUAD_BEGIN QUAD_BEGIN_T(false)
+#define QUAD_BEGIN QUAD_BEGIN_T(-1, -1)
 #define QUAD_END \
   });
 
@@ -1072,14 +1074,18 @@ __global__ void __launch_bounds__(kThreads) k_potential(BatchDev B) {
 // Substep1KernelVrad / Substep1KernelVtheta (Kernels.cu:52-88), with
 // CorrectVthetaKernel (Kernels.cu:1352-1359) applied on the fly, and the
 // self-gravity kick of Update_sgvelocityKernel (Kernels.cu:1024-1041).
-__global__ void __launch_bounds__(kThreads, 2) k_source1(BatchDev B) {
-  QUAD_BEGIN
+// One instance per kind of disk (kAdi: adiabatic, kSg: self-gravity), so
+// that the isothermal form without self-gravity holds no energy or
+// acceleration samples and runs with more warps per SM.
+template <int kAdi, int kSg>
+__global__ void __launch_bounds__(kThreads, (kAdi == 0 && kSg == 0) ? 3 : 2) k_source1(BatchDev B) {
+  QUAD_BEGIN_T(kAdi, kSg)
   const float dt = C->dtf;
   const float OmegaFrame = C->OmegaFrame;
   // CorrectVtheta (SideEuler.cu:184-188) on the fly; evanescent disks had it
   // applied in place by the boundary pass that precedes this kernel
   const float dom = D.Evanescent ? 0.0f : C->domega;
-  const bool adi = D.Adiabatic, sg = D.SelfGravity;
+  constexpr bool adi = kAdi == 1, sg = kSg == 1;
   auto vth = [&](float v, int r) -> float { return dom != 0.0f ? v - dom * D.Rmed[r] : v; };
   // (i, j), (i-1, j) and (i, j-1) samples; v_theta also at (i, j+1), (i-1, j+1)
   float Dn0[4], Dnm[4], Dna[4], E0[4], Em[4], Ea[4], Ph0[4], Phm[4], Pha[4];
@@ -1541,7 +1547,7 @@ __device__ __forceinline__ float qplus_at(const DiskDev& D, int i, int j, int ns
 }
 
 __global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
-  QUAD_BEGIN_T(true)
+  QUAD_BEGIN_T(1, -1)
   const float dt = C->dtf;
   float qv[4], ev[4];
 #pragma unroll
@@ -2711,7 +2717,10 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
     k_bc_disk<<<b.ndisk, kThreads, 0, s>>>(b);
   }
   REC();
-  k_source1<<<b.g_source1, kThreads, 0, s>>>(b);
+  if (b.src1_classes & 1) k_source1<0, 0><<<b.g_source1[0], kThreads, 0, s>>>(b);
+  if (b.src1_classes & 2) k_source1<0, 1><<<b.g_source1[1], kThreads, 0, s>>>(b);
+  if (b.src1_classes & 4) k_source1<1, 0><<<b.g_source1[2], kThreads, 0, s>>>(b);
+  if (b.src1_classes & 8) k_source1<1, 1><<<b.g_source1[3], kThreads, 0, s>>>(b);
   REC();
   k_viscosity<<<b.g_viscosity, kThreads, kViscSmem, s>>>(b);
   REC();
@@ -2775,7 +2784,10 @@ cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int ni
   };
   cudaError_t e;
   if ((e = wave(fargo_cfl_kernel(b.max_body), kThreads, 0, b.ncfl, &b.g_cfl))) return e;
-  if ((e = wave((const void*)k_source1, kThreads, 0, ncell_tiles, &b.g_source1))) return e;
+  if ((e = wave((const void*)k_source1<0, 0>, kThreads, 0, ncell_tiles, &b.g_source1[0]))) return e;
+  if ((e = wave((const void*)k_source1<0, 1>, kThreads, 0, ncell_tiles, &b.g_source1[1]))) return e;
+  if ((e = wave((const void*)k_source1<1, 0>, kThreads, 0, ncell_tiles, &b.g_source1[2]))) return e;
+  if ((e = wave((const void*)k_source1<1, 1>, kThreads, 0, ncell_tiles, &b.g_source1[3]))) return e;
   if ((e = wave((const void*)k_potential, kThreads, 0, ncell_tiles, &b.g_potential))) return e;
   if ((e = wave((const void*)k_viscosity, kThreads, kViscSmem, ncell_tiles, &b.g_viscosity))) return e;
   if ((e = wave((const void*)k_source2, kThreads, 0, ncell_tiles, &b.g_source2))) return e;
@@ -2784,11 +2796,13 @@ cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int ni
   return wave((const void*)k_transport<6>, kTT, fargo_transport_smem_bytes(1), nitems, &b.g_transport);
 }
 
-// Launches of one substep: 10 kernels, the energy kernel when a disk is
-// adiabatic, both transport forms in a batch of isothermal and adiabatic
-// disks, two per boundary call when a disk has a non-rigid boundary.
+// Launches of one substep: 9 kernels, one Substep1 instance per kind of disk
+// present, the energy kernel when a disk is adiabatic, both transport forms
+// in a batch of isothermal and adiabatic disks, two per boundary call when a
+// disk has a non-rigid boundary.
 int fargo_substep_launches(const BatchDev& b) {
-  return 10 + (b.ntheta_adi ? 1 : 0) + ((b.ntheta_iso && b.ntheta_adi) ? 1 : 0) + (b.any_bc ? 6 : 0);
+  return 9 + __builtin_popcount((unsigned)b.src1_classes) + (b.ntheta_adi ? 1 : 0) +
+         ((b.ntheta_iso && b.ntheta_adi) ? 1 : 0) + (b.any_bc ? 6 : 0);
 }
 
 void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s) {
