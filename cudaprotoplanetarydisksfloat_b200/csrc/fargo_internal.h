@@ -174,7 +174,7 @@ struct BatchDev {
   int src1_classes;          // bit 2*Adiabatic + SelfGravity set for every kind of disk present
   int max_body;              // largest body count of the force sums (star + FeelDisk planets)
   // one-wave grids of the substep kernels (fargo_size_grids)
-  int g_cfl, g_source1[4], g_potential, g_viscosity, g_source2, g_energy, g_velocities, g_transport;
+  int g_cfl, g_source1[4], g_potential, g_viscosity, g_source2[2], g_energy, g_velocities[2], g_transport;
 };
 
 // kernel entry points (kernels_step.cu), launched by fargo_api.cu

@@ -1481,10 +1481,13 @@ __device__ __forceinline__ float qvisc(float dv, float dens) {
   return 0.0f;
 }
 
-__global__ void __launch_bounds__(kThreads, 3) k_source2(BatchDev B) {
-  QUAD_BEGIN
+// One instance per kind of disk (kAdi: adiabatic): the isothermal form holds
+// no energy samples.
+template <int kAdi>
+__global__ void __launch_bounds__(kThreads, kAdi ? 3 : 4) k_source2(BatchDev B) {
+  QUAD_BEGIN_T(kAdi, -1)
   const float dt = C->dtf;
-  const bool adi = D.Adiabatic;
+  constexpr bool adi = kAdi == 1;
   // viscosity-updated VradInt / VthetaInt (k_viscosity) and the density
   float R0[4], Ru[4], Rd[4], T0[4], Tp[4], Tm[4], N0[4], Nd[4], Nm[4], E0[4];
   qld(R0, D.trr, q);
@@ -2125,8 +2128,11 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
 // ComputeVelocitiesKernel, Kernels.cu:1292-1306, from the transported
 // momenta (vri, vti, trr, tpp) and density (a0); then the transported
 // density (and energy, a1) become the state.
-__global__ void __launch_bounds__(kThreads, 4) k_velocities(BatchDev B) {
-  QUAD_BEGIN
+// One instance per kind of disk (kAdi: adiabatic, which also moves the
+// transported energy into the state).
+template <int kAdi>
+__global__ void __launch_bounds__(kThreads, kAdi ? 4 : 5) k_velocities(BatchDev B) {
+  QUAD_BEGIN_T(kAdi, -1)
   const float Om = C->OmegaFrame;
   float A0[4], Ad[4], Am[4], Rd[4], T0[4], P0[4], Pm[4], S0[4], E1[4];
   qld(A0, D.a0, q);  // transported density
@@ -2137,7 +2143,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_velocities(BatchDev B) {
   qld(P0, D.trr, q);
   qld_jm(Pm, P0, D.trr, q, nsec);
   qld(S0, D.tpp, q);
-  if (D.Adiabatic) qld(E1, D.a1, q);
+  if (kAdi == 1) qld(E1, D.a1, q);
   float vr[4], vt[4];
 #pragma unroll
   for (int u = 0; u < 4; u++) {
@@ -2151,7 +2157,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_velocities(BatchDev B) {
   qst(D.vrad, q, vr);
   qst(D.vtheta, q, vt);
   qst(D.dens, q, A0);
-  if (D.Adiabatic) qst(D.energy, q, E1);
+  if (kAdi == 1) qst(D.energy, q, E1);
   QUAD_END
 }
 
@@ -2724,7 +2730,8 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   REC();
   k_viscosity<<<b.g_viscosity, kThreads, kViscSmem, s>>>(b);
   REC();
-  k_source2<<<b.g_source2, kThreads, 0, s>>>(b);
+  if (b.ntheta_iso) k_source2<0><<<b.g_source2[0], kThreads, 0, s>>>(b);
+  if (b.ntheta_adi) k_source2<1><<<b.g_source2[1], kThreads, 0, s>>>(b);
   REC();
   if (b.any_bc) {
     k_bc_rings<1><<<b.ring_grid, kThreads, 0, s>>>(b);
@@ -2740,7 +2747,8 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   if (b.ntheta_adi)
     k_transport<6><<<std::min(b.g_transport, b.ntheta_adi), kTT, fargo_transport_smem_bytes(1), s>>>(b, b.theta_adi);
   REC();
-  k_velocities<<<b.g_velocities, kThreads, 0, s>>>(b);
+  if (b.ntheta_iso) k_velocities<0><<<b.g_velocities[0], kThreads, 0, s>>>(b);
+  if (b.ntheta_adi) k_velocities<1><<<b.g_velocities[1], kThreads, 0, s>>>(b);
   REC();
   if (b.any_bc) {
     k_bc_rings<2><<<b.ring_grid, kThreads, 0, s>>>(b);
@@ -2790,19 +2798,22 @@ cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int ni
   if ((e = wave((const void*)k_source1<1, 1>, kThreads, 0, ncell_tiles, &b.g_source1[3]))) return e;
   if ((e = wave((const void*)k_potential, kThreads, 0, ncell_tiles, &b.g_potential))) return e;
   if ((e = wave((const void*)k_viscosity, kThreads, kViscSmem, ncell_tiles, &b.g_viscosity))) return e;
-  if ((e = wave((const void*)k_source2, kThreads, 0, ncell_tiles, &b.g_source2))) return e;
+  if ((e = wave((const void*)k_source2<0>, kThreads, 0, ncell_tiles, &b.g_source2[0]))) return e;
+  if ((e = wave((const void*)k_source2<1>, kThreads, 0, ncell_tiles, &b.g_source2[1]))) return e;
   if ((e = wave((const void*)k_energy, kThreads, 0, ncell_tiles, &b.g_energy))) return e;
-  if ((e = wave((const void*)k_velocities, kThreads, 0, ncell_tiles, &b.g_velocities))) return e;
+  if ((e = wave((const void*)k_velocities<0>, kThreads, 0, ncell_tiles, &b.g_velocities[0]))) return e;
+  if ((e = wave((const void*)k_velocities<1>, kThreads, 0, ncell_tiles, &b.g_velocities[1]))) return e;
   return wave((const void*)k_transport<6>, kTT, fargo_transport_smem_bytes(1), nitems, &b.g_transport);
 }
 
-// Launches of one substep: 9 kernels, one Substep1 instance per kind of disk
-// present, the energy kernel when a disk is adiabatic, both transport forms
-// in a batch of isothermal and adiabatic disks, two per boundary call when a
-// disk has a non-rigid boundary.
+// Launches of one substep: 6 kernels, one Substep1 instance per kind of disk
+// present, the energy kernel when a disk is adiabatic, the isothermal and the
+// adiabatic forms of Substep2, transport and the velocity update when the
+// batch holds both, two per boundary call when a disk has a non-rigid
+// boundary.
 int fargo_substep_launches(const BatchDev& b) {
-  return 9 + __builtin_popcount((unsigned)b.src1_classes) + (b.ntheta_adi ? 1 : 0) +
-         ((b.ntheta_iso && b.ntheta_adi) ? 1 : 0) + (b.any_bc ? 6 : 0);
+  return 6 + __builtin_popcount((unsigned)b.src1_classes) + (b.ntheta_adi ? 1 : 0) +
+         3 * ((b.ntheta_iso && b.ntheta_adi) ? 2 : 1) + (b.any_bc ? 6 : 0);
 }
 
 void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s) {
