@@ -1234,6 +1234,8 @@ constexpr int kSO = 4;                                  // staged columns left o
 constexpr int kSR = kVR + 4, kSC = kVC + 2 * kSO;       // staged rows, columns (whole 16-byte chunks)
 constexpr int kTR = kVR + 2, kTC = kVC + 2;             // stress rows, columns
 constexpr int kTQ = (kTC + 3) / 4;                      // stress quads per row
+constexpr int kRuns = 14;                               // stress runs per row: 12 of 5 columns, 2 of 3
+static_assert(12 * 5 + 2 * 3 == kTC && kTR * kRuns <= kThreads, "stress runs cover a tile's rows in one pass");
 constexpr int kTCp = 4 * kTQ;                           // stress row length in shared memory
 static_assert(kVR * kVC == 4 * kThreads, "one quad of the tile per thread in the update");
 __device__ __forceinline__ int vtiles_of(const DiskDev& D) {
@@ -1351,50 +1353,55 @@ __global__ void __launch_bounds__(kThreads, 3) k_viscosity(BatchDev B) {
     const float invdphi = D.invdphi, onethird = D.onethird;
     if (D.IsDisk) {
       // stresses at rows i0-1 .. i0+kVR, columns j0-1 .. j0+kVC (viscous_terms),
-      // four consecutive columns of one row per thread: the row's tables are
-      // read once and neighbouring samples are shared in registers
-      for (int it = tid; it < kTR * kTQ; it += kThreads) {
-        const int r = it / kTQ, c0 = 4 * (it - r * kTQ);
+      // one run of consecutive columns of one row per thread (each row in 12
+      // runs of 5 and 2 of 3: all 18 rows in one pass of the block): the
+      // row's tables are read once and neighbouring samples are shared in
+      // registers
+      if (tid < kTR * kRuns) {
+        const int r = tid / kRuns, m = tid - r * kRuns;
+        const int c0 = m < 12 ? 5 * m : 60 + 3 * (m - 12);
+        const int len = m < 12 ? 5 : 3;
         const int i = i0 - 1 + r;
-        if (i < 0 || i >= nrad) continue;
-        const int rr = r + 1, cc = c0 + kSO - 1;  // staged indices of (i, j) for the first column
-        const float nu = D.visc[i];
-        const float iRm = D.invRmed[i];
-        const float idRs = D.invdiffRsup[i], Rs = D.Rsup[i], Ri = D.Rinf[i];
-        float vr[5], vr1[4], va[5], vam[4], dn[4], dnm[5];
+        if (i >= 0 && i < nrad) {
+          const int rr = r + 1, cc = c0 + kSO - 1;  // staged indices of (i, j) for the first column
+          const float nu = D.visc[i];
+          const float iRm = D.invRmed[i];
+          const float idRs = D.invdiffRsup[i], Rs = D.Rsup[i], Ri = D.Rinf[i];
+          float vr[6], vr1[5], va[6], vam[5], dn[5], dnm[6];
 #pragma unroll
-        for (int u = 0; u < 5; u++) {
-          vr[u] = sVr[rr][cc - 1 + u];   // columns c0-1 .. c0+3
-          va[u] = sVa[rr][cc + u];       // columns c0 .. c0+4
-          dnm[u] = sDn[rr - 1][cc - 1 + u];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          vr1[u] = sVr[rr + 1][cc + u];
-          vam[u] = sVa[rr - 1][cc + u];
-          dn[u] = sDn[rr][cc + u];
-        }
-        const float d0 = sD0[rr];
-        const float iRm1 = i > 0 ? D.invRmed[i - 1] : 0.0f;
-        const float idRm = D.invdiffRmed[i], iRi = D.invRinf[i];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const int c = c0 + u;
-          if (c >= kTC) break;
-          const float v0 = vr[u + 1], vp = vr1[u], a0 = va[u], ap = va[u + 1];
-          float DRR = (vp - v0) * idRs;
-          float DPP = (ap - a0) * invdphi * iRm + 0.5f * (vp + v0) * iRm;
-          float divV = (vp * Rs - v0 * Ri) * idRs * iRm;
-          divV += (ap - a0) * invdphi * iRm;
-          sTrr[r][c] = 2.0f * dn[u] * nu * (DRR - onethird * divV);
-          sTpp[r][c] = 2.0f * dn[u] * nu * (DPP - onethird * divV);
-          float rp = 0.0f;  // TAURP's ring 0 is never written: zero
-          if (i > 0) {
-            float DRP = 0.5f * (Ri * (a0 * iRm - vam[u] * iRm1) * idRm + (v0 - vr[u]) * invdphi * iRi);
-            // TAURP's third density sample is dens[i*nsec] (Kernels.cu:876)
-            rp = 0.5f * (dn[u] + dnm[u + 1] + d0 + dnm[u]) * nu * DRP;
+          for (int u = 0; u < 6; u++) {
+            vr[u] = sVr[rr][cc - 1 + u];   // columns c0-1 .. c0+4
+            va[u] = sVa[rr][cc + u];       // columns c0 .. c0+5
+            dnm[u] = sDn[rr - 1][cc - 1 + u];
           }
-          sTrp[r][c] = rp;
+#pragma unroll
+          for (int u = 0; u < 5; u++) {
+            vr1[u] = sVr[rr + 1][cc + u];
+            vam[u] = sVa[rr - 1][cc + u];
+            dn[u] = sDn[rr][cc + u];
+          }
+          const float d0 = sD0[rr];
+          const float iRm1 = i > 0 ? D.invRmed[i - 1] : 0.0f;
+          const float idRm = D.invdiffRmed[i], iRi = D.invRinf[i];
+#pragma unroll
+          for (int u = 0; u < 5; u++) {
+            if (u >= len) break;
+            const int c = c0 + u;
+            const float v0 = vr[u + 1], vp = vr1[u], a0 = va[u], ap = va[u + 1];
+            float DRR = (vp - v0) * idRs;
+            float DPP = (ap - a0) * invdphi * iRm + 0.5f * (vp + v0) * iRm;
+            float divV = (vp * Rs - v0 * Ri) * idRs * iRm;
+            divV += (ap - a0) * invdphi * iRm;
+            sTrr[r][c] = 2.0f * dn[u] * nu * (DRR - onethird * divV);
+            sTpp[r][c] = 2.0f * dn[u] * nu * (DPP - onethird * divV);
+            float rp = 0.0f;  // TAURP's ring 0 is never written: zero
+            if (i > 0) {
+              float DRP = 0.5f * (Ri * (a0 * iRm - vam[u] * iRm1) * idRm + (v0 - vr[u]) * invdphi * iRi);
+              // TAURP's third density sample is dens[i*nsec] (Kernels.cu:876)
+              rp = 0.5f * (dn[u] + dnm[u + 1] + d0 + dnm[u]) * nu * DRP;
+            }
+            sTrp[r][c] = rp;
+          }
         }
       }
     }
