@@ -142,8 +142,10 @@ def test_disk_force_matches_oracle(gpu):
 
 
 def test_batched_equals_single(gpu):
-    """A batch of uneven disks gives the same bits as each disk alone."""
-    cases = [("iso", 32, 96), ("iso", 48, 144), ("adi", 40, 120)]
+    """A batch of uneven disks of every kind (isothermal, adiabatic, each with
+    and without self-gravity: one Substep1 instance per kind) gives the same
+    bits as each disk alone."""
+    cases = [("iso", 32, 96), ("iso", 48, 144), ("adi", 40, 120), ("sg", 32, 64), ("adisg", 32, 64)]
     built = [small(k, nr, ns) for k, nr, ns in cases]
     P = [b[0] for b in built]
     L = [b[1] for b in built]
