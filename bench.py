@@ -22,7 +22,7 @@ own CUDA build (oracle/_ref/fargo_ref, from the reference sources) on a
 bounded sample of the same disks, with its own AlgoGas timer.
 
 Multi-GPU: `torchrun --nproc-per-node N bench.py --gpus N`; every rank
-advances its own 64-disk batch (disjoint seeds), no collective in the data
+advances its own 64 disks (disjoint seeds), no collective in the data
 path (weak scaling); the timed region is bracketed by barriers and the max
 over ranks is taken.
 """
