@@ -3,27 +3,32 @@
 // The reference runs ~120 single-purpose kernels, ~50 host-side reductions
 // (each with cudaMalloc/cudaFree) and ~15 full-grid device copies per
 // substep, with a device synchronisation after every launch
-// (SourceEuler.cu:230-299).  Here one substep is 11-12 launches that read
-// and write only the disk state and a few scratch fields, with the CFL
-// count, the disk forces and the planet integrator kept on the device:
+// (SourceEuler.cu:230-299).  Here one substep of an isothermal batch is 10
+// launches that read and write only the disk state and a few scratch fields,
+// with the CFL count, the disk forces and the planet integrator kept on the
+// device:
 //
 //   k_ring_mean<0>   serial FP32 ring means of v_theta for the CFL
-//   k_cfl_force      CFL minimum, disk-on-body forces; the last
-//                    block of each disk finishes the substep's scalar work
-//                    (dt, mass taper, potential parameters, planet kicks,
+//   k_cfl_force      CFL minimum, disk-on-body forces on 4096-cell tiles; the
+//                    last block of each disk finishes the substep's scalar
+//                    work (dt, mass taper, potential parameters, planet kicks,
 //                    FP64 RK5, frame rotation, per-ring viscosity)
-//   k_source1        Substep1 (pressure + potential + centrifugal kick),
-//                    potential evaluated on the fly, + self-gravity kick
+//   k_potential      star and planet potential of every cell
+//   k_source1        Substep1 (pressure + potential + centrifugal kick) +
+//                    self-gravity kick; one instance per kind of disk
 //   k_viscosity      viscous stress tensor + velocity update + sub-Keplerian
-//                    boundary on 8x64 tiles with halos in shared memory
+//                    boundary on 16x64 tiles staged in shared memory
 //   k_source2        artificial viscosity (Substep2) + energy predictor
 //   k_energy         viscous heating and implicit energy update (Substep3)
 //   k_ring_mean<1>   ring means of v_theta for FARGO: Nshift, residual
-//   k_transport      one azimuthal segment per CTA: momenta + radial van
-//                    Leer in registers, residual and constant azimuthal van
-//                    Leer sweeps in shared memory, shift fused into the load
+//   k_transport      a band of 8 rings x one segment of source sectors per
+//                    CTA: momenta + radial van Leer from staged rows, residual
+//                    and constant azimuthal van Leer sweeps in registers,
+//                    shift applied on the store
 //   k_velocities     velocities from the transported momenta
 //   k_substep_end    disks still inside their DT -> graph loop condition
+//
+// The cell kernels take four consecutive cells per thread (quads).
 //
 // Arithmetic per cell follows the reference kernels expression by expression
 // (a float meeting a double literal is promoted and rounded back on
