@@ -164,6 +164,21 @@ def workload_disks(name, seed_shift=0, rank=0, world=1, strong=False):
     return [fn()]
 
 
+def batch_groups(cells, groups, plain):
+    """The disks of one rank as batches: one per disk for the plain form;
+    otherwise `groups` batches balanced by LPT on cell counts, advanced
+    concurrently on their own streams, so that one batch's last substeps (few
+    disks still inside their DT) overlap another's work."""
+    n = len(cells)
+    if plain:
+        return [[d] for d in range(n)]
+    G = max(1, min(groups, n))
+    if G == 1:
+        return [list(range(n))]
+    from cudaprotoplanetarydisksfloat_b200 import shard
+    return [sorted(g) for g in shard.lpt_partition([int(c) for c in cells], G)]
+
+
 def materialise_all(disks, tmp):
     from cudaprotoplanetarydisksfloat_b200 import configs, read_params, read_planets
     P, L = [], []
@@ -194,17 +209,7 @@ def ours(args, world, rank, local, pg):
     P, L = materialise_all(disks, tmp)
     cells = np.array([p.NRAD * p.NSEC for p in P], dtype=np.int64)
     plain = args.workload == "c4plain"
-    # batched workloads: the disks in --groups batches (LPT on cell counts),
-    # advanced concurrently on their own streams, so that one batch's last
-    # substeps (few disks still inside their DT) overlap another's
-    G = 1 if plain else max(1, min(args.groups, len(P)))
-    if plain:
-        groups = [[d] for d in range(len(P))]
-    elif G == 1:
-        groups = [list(range(len(P)))]
-    else:
-        from cudaprotoplanetarydisksfloat_b200 import shard
-        groups = [sorted(g) for g in shard.lpt_partition([int(c) for c in cells], G)]
+    groups = batch_groups(cells, args.groups, plain)
     gcells = np.array([cells[d] for g in groups for d in g], dtype=np.int64)  # nsub_total() order
     batches = [Batch([P[d] for d in g], [L[d] for d in g], device=local) for g in groups]
     for b, g in zip(batches, groups):

@@ -102,3 +102,17 @@ def test_two_rank_sweep_matches_one_rank():
         g = got["res"][str(k)]
         for key in ("nsub_total", "physical_time", "mass", "angular_momentum"):
             assert np.float64(g[key]) == np.float64(s[key]), (k, key)
+
+
+def test_bench_batch_groups_cover_and_balance():
+    import bench
+    cells = [int(p["Nrad"]) * int(p["Nsec"]) for p, _ in __import__(
+        "cudaprotoplanetarydisksfloat_b200").configs.c4(64, seed=42)]
+    assert bench.batch_groups(cells, 4, plain=True) == [[d] for d in range(64)]
+    assert bench.batch_groups(cells, 1, plain=False) == [list(range(64))]
+    for g in (2, 4, 8):
+        parts = bench.batch_groups(cells, g, plain=False)
+        assert len(parts) == g
+        assert sorted(d for p in parts for d in p) == list(range(64))
+        loads = [sum(cells[d] for d in p) for p in parts]
+        assert max(loads) <= sum(cells) / g + max(cells)
