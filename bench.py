@@ -17,14 +17,25 @@ page-locked host buffers: every step uploads every disk's state, advances
 one DT and downloads the state.  The batched workloads split their disks
 over --groups batches (LPT on cell counts) advanced concurrently on their
 own streams: one batch's last substeps, when few of its disks are still
-inside their DT, and its host copies overlap the other batches' work.  `--impl reference` times the reference's
-own CUDA build (oracle/_ref/fargo_ref, from the reference sources) on a
-bounded sample of the same disks, with its own AlgoGas timer.
+inside their DT, and its host copies overlap the other batches' work.  The
+C4 line also carries the plain form (the same disks advanced one after
+another) measured in the same run, as `plain`.
 
-Multi-GPU: `torchrun --nproc-per-node N bench.py --gpus N`; every rank
-advances its own 64 disks (disjoint seeds), no collective in the data
-path (weak scaling); the timed region is bracketed by barriers and the max
-over ranks is taken.
+`--impl reference` times the reference's own CUDA build
+(oracle/_ref/fargo_ref, compiled from the reference sources) on a bounded
+sample of the same workload: one disk of every grid size of the sweep, the
+K timed steps shared out over them (one step = one DT of one sampled disk),
+each disk first run for its share of the W warm-up DTs.  Its AlgoGas wall
+time and substep count come from the timing hook (no device copies or file
+writes inside the timed call).  That arm loads nothing of this package: the
+workload definitions are read from configs.py by file path.
+
+Multi-GPU: `bench.py --gpus N` with N > 1 relaunches itself under
+torch.distributed.run with N ranks (or runs as one rank of an outside
+torchrun).  Every rank advances its own 64 disks (disjoint seeds), no
+collective in the data path (weak scaling); the timed region is bracketed
+by barriers and the max over ranks is taken.  `--plumbing` runs only the
+rank set-up, sharding and max/sum reductions on CPU (gloo), for tests.
 """
 import argparse
 import ctypes as C
@@ -42,10 +53,25 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic HBM bytes per cell-update of the whole substep: the state read
-# once and written once in FP32 (Sigma, v_r, v_theta [, e]); with self-gravity
-# four padded complex FFT passes add 128 B.
-B_ALG = {"c1": 24, "c2": 32, "c3": 152, "c4": 24, "c4plain": 24, "c4q": 24, "c5": 160}
+# Algorithmic HBM bytes per cell-update: the state read once and written once
+# in FP32 (Sigma, v_r, v_theta [, e]).  These are the bytes charged to the
+# dominant substep kernel (transport: it reads and rewrites the whole state);
+# with self-gravity the four padded complex FFT passes add 128 B per cell to
+# the substep, reported separately as `sg_alg_bytes_per_cell` and never
+# charged to a substep kernel.
+B_STATE = {"c1": 24, "c2": 32, "c3": 24, "c4": 24, "c4plain": 24, "c4q": 24, "c5": 32}
+B_SG = {"c3": 128, "c5": 128}
+
+
+def load_module(name):
+    """A module of the package loaded by file path, without importing the
+    package (whose __init__ loads the CUDA library)."""
+    import importlib.util
+    path = os.path.join(ROOT, "cudaprotoplanetarydisksfloat_b200", name + ".py")
+    spec = importlib.util.spec_from_file_location("fargo_bench_" + name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def load_peaks():
@@ -116,25 +142,35 @@ def dist_setup(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     pg = None
     if world > 1:
-        import torch
-
-        from cudaprotoplanetarydisksfloat_b200 import shard
-        torch.cuda.set_device(local)
-        pg = shard.init_process_group("nccl", timeout_s=120)
+        shard = load_module("shard")
+        if args.plumbing:
+            pg = shard.init_process_group("gloo", timeout_s=60)
+        else:
+            import torch
+            torch.cuda.set_device(local)
+            pg = shard.init_process_group("nccl", timeout_s=120)
     return world, rank, local, pg
+
+
+def _dev(pg):
+    import torch
+    return "cpu" if pg.get_backend() == "gloo" else "cuda"
 
 
 def barrier(pg):
     if pg is not None:
         import torch
-        pg.barrier(device_ids=[torch.cuda.current_device()])
+        if _dev(pg) == "cpu":
+            pg.barrier()
+        else:
+            pg.barrier(device_ids=[torch.cuda.current_device()])
 
 
 def allmax(pg, x):
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_dev(pg))
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -143,16 +179,16 @@ def allsum(pg, x):
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_dev(pg))
     pg.all_reduce(t, op=pg.ReduceOp.SUM)
     return float(t.item())
 
 
 def workload_disks(name, seed_shift=0, rank=0, world=1, strong=False):
-    from cudaprotoplanetarydisksfloat_b200 import configs
+    configs = load_module("configs")
     if strong and name in ("c4", "c4plain"):
         # one fixed 64-disk sweep, split over the ranks by LPT on cell counts
-        from cudaprotoplanetarydisksfloat_b200 import shard
+        shard = load_module("shard")
         sweep = configs.c4(64, seed=42)
         cells = [int(p["Nrad"]) * int(p["Nsec"]) for p, _ in sweep]
         return [sweep[i] for i in shard.lpt_partition(cells, world)[rank]]
@@ -162,6 +198,35 @@ def workload_disks(name, seed_shift=0, rank=0, world=1, strong=False):
         return configs.c4(64, seed=42 + seed_shift)[::4]
     fn = {"c1": configs.c1, "c2": configs.c2, "c3": configs.c3, "c5": configs.c5}[name]
     return [fn()]
+
+
+WL_DESC = {"c4": "64 isothermal disks (Nrad in {128..512}, Nsec=3*Nrad), batched, one DT each",
+           "c4plain": "64 isothermal disks (Nrad in {128..512}, Nsec=3*Nrad), one after another",
+           "c4q": "every 4th disk of the 64-disk sweep (16 disks, 6.1M cells), batched",
+           "c1": "isothermal 128x384, 1 planet", "c2": "adiabatic 256x768, alpha viscosity, 2 live planets",
+           "c3": "self-gravitating 512x1024, 1 planet", "c5": "adiabatic+SG 2048x6144, 3 live planets"}
+
+
+def workload_config(args, world):
+    """The `config` object of the JSON line: the same for both arms, computed
+    from the workload definition alone (nothing measured in it)."""
+    disks = workload_disks(args.workload)
+    n = len(disks)
+    per_rank = -(-n // world) if args.strong else n
+    if args.strong:
+        cells = sum(int(p["Nrad"]) * int(p["Nsec"]) for p, _ in disks)
+    else:
+        # every rank advances its own draw of the workload (seed shifted by rank)
+        cells = sum(int(p["Nrad"]) * int(p["Nsec"]) for r in range(world)
+                    for p, _ in workload_disks(args.workload, seed_shift=r))
+        n *= world
+    batches = per_rank if args.workload == "c4plain" else max(1, min(args.groups, per_rank))
+    return {"workload": args.workload, "description": WL_DESC[args.workload],
+            "parallelism": "disk-parallel: the GPU's disks in concurrent batches on their own streams"
+            if args.workload.startswith("c4") else "single disk per GPU",
+            "l2": "working set larger than L2" if args.workload in ("c4", "c4plain", "c4q", "c5")
+            else "working set L2-resident (launch-bound)",
+            "disks": n, "cells": cells, "batches_per_gpu": batches}
 
 
 def batch_groups(cells, groups, plain):
@@ -378,8 +443,10 @@ def ours(args, world, rank, local, pg):
         launches = int(max(1, sum(int(dn[off[k]:off[k + 1]].max()) for k in range(len(groups)))))
         cells_per_launch = upd_prof / launches
         peak, kind = load_peaks()
-        # algorithmic bytes per cell-update: the state read once and written once
-        b_alg = B_ALG[args.workload]
+        # algorithmic bytes per cell-update of the dominant kernel: the state
+        # read once and written once (self-gravity's FFT bytes excluded)
+        b_alg = B_STATE[args.workload]
+        b_sub = b_alg + B_SG.get(args.workload, 0)
         achieved = b_alg * cells_per_launch / (ms_k[top] * 1e-3 / launches) / 1e9
         # the kernel's DRAM bytes per cell and issue utilisation from one ncu
         # capture (profiles/dram_traffic_c4q_first_substep.md)
@@ -397,26 +464,75 @@ def ours(args, world, rank, local, pg):
                 "issue_active_pct_ncu": issue,
                 "alg_bytes_per_cell": b_alg, "alg_bytes_per_launch": round(b_alg * cells_per_launch),
                 "launch_ms": round(float(ms_k[top]) / launches, 4),
-                "step_frac": round(value * b_alg / (peak * 1e9), 4),
+                "step_frac": round(value * b_sub / (peak * 1e9), 4),
+                "substep_alg_bytes_per_cell": b_sub, "sg_alg_bytes_per_cell": B_SG.get(args.workload, 0),
                 "kernel_ms_share": {names[k]: round(float(ms_k[k] / ms_k.sum()), 4) for k in range(nk)
                                     if ms_k[k] > 0}}
 
+    for b in batches:
+        b.close()
+    plain_line = None
+    if args.workload == "c4" and args.plain_steps > 0:
+        plain_line = plain_form(args, P, L, rank, local, pg, world)
+        if plain_line is not None:
+            plain_line["batched_over_plain"] = round(value / plain_line["value"], 3)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args, disks)
-    for b in batches:
-        b.close()
     return {
         "value": value, "ms_per_step": ms_max / args.steps, "e2e": e2e, "roofline": roof,
         "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(l1 - l0) * world,
         "wall_s": t_wall, "cells": int(cells.sum()) * world, "disks": len(P) * world,
-        "seg_out": sorted(set(seg_out)), "batches": len(batches),
+        "seg_out": sorted(set(seg_out)), "batches": len(batches), "plain": plain_line,
     }
 
 
+def plain_form(args, P, L, rank, local, pg, world):
+    """The plain form on the same disks: each disk a context of its own,
+    advanced one after another (device-resident, CUDA events), after one
+    warm-up DT.  Measured beside the batched form so that the ratio of the
+    two is in the same line."""
+    import torch
+
+    from cudaprotoplanetarydisksfloat_b200 import Batch
+    from cudaprotoplanetarydisksfloat_b200._abi import lib
+    singles = [Batch([P[d]], [L[d]], device=local) for d in range(len(P))]
+    try:
+        for d, b in enumerate(singles):
+            noisy_init(b, [P[d]], [20261203 + 1000 * rank + d])
+            b.advance_async(1)
+        for b in singles:
+            b.sync()
+        streams = [torch.cuda.ExternalStream(lib.fargo_batch_stream(b.b), device=local) for b in singles]
+        n0 = np.array([b.scalars(0)["nsub_total"] for b in singles], dtype=np.int64)
+        barrier(pg)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        ends = [torch.cuda.Event(enable_timing=True) for _ in singles]
+        e0.record(streams[0])
+        for i, b in enumerate(singles):
+            streams[i].wait_event(e0 if i == 0 else ends[i - 1])
+            b.advance_async(args.plain_steps)
+            ends[i].record(streams[i])
+        for b in singles:
+            b.sync()
+        ms = e0.elapsed_time(ends[-1])
+        n1 = np.array([b.scalars(0)["nsub_total"] for b in singles], dtype=np.int64)
+        upd = float(np.sum(np.array([p.NRAD * p.NSEC for p in P], dtype=np.int64) * (n1 - n0)))
+        ms = allmax(pg, ms)
+        upd = allsum(pg, upd)
+    finally:
+        for b in singles:
+            b.close()
+    return {"value": upd / (ms * 1e-3), "ms_per_step": ms / args.plain_steps, "steps": args.plain_steps,
+            "unit": "cell-updates/s", "form": "each disk its own context, advanced one after another"}
+
+
 def cpu_baseline(args, disks):
-    """The oracle (CPU restatement, OpenMP, all host cores) on one disk of the
-    workload for a bounded number of DTs."""
+    """The oracle (the CPU restatement of the reference's algorithm, OpenMP
+    over all host cores) on the median-size disk of the workload, built in
+    FP64 (the baseline) and in FP32 (the reference's typing, reported as
+    `f32_value`), each for a bounded number of DTs."""
     from cudaprotoplanetarydisksfloat_b200 import noise
     from oracle.oracle import Oracle, set_threads
     tmp = tempfile.mkdtemp(prefix="fargo_cpu_")
@@ -424,72 +540,107 @@ def cpu_baseline(args, disks):
     k = int(np.argsort(sizes)[len(sizes) // 2])
     P, L = materialise_all([disks[k]], tmp)
     cores = os.cpu_count() or 1
-    set_threads(cores)
-    o = Oracle(P[0], L[0])
-    f = o.fields()
-    o.set_fields(dens=noise.perturb_density(f["dens"].reshape(-1), P[0].NRAD, P[0].NSEC, 7))
-    o.advance_dt()
-    t0 = time.time()
-    nsub = 0
-    ndt = 0
-    while ndt < args.cpu_max_dt and time.time() - t0 < args.cpu_seconds:
-        nsub += o.advance_dt()
-        ndt += 1
-    dt = time.time() - t0
+    o32 = Oracle(P[0], L[0], "f32")
+    f = o32.fields()
+    o32.init_state(dens=noise.perturb_density(f["dens"].reshape(-1), P[0].NRAD, P[0].NSEC, 7))
+    g = o32.fields()
     cells = P[0].NRAD * P[0].NSEC
-    return {"value": cells * nsub / dt, "unit": "cell-updates/s", "cores": cores, "kind": "port",
-            "sample": "oracle f32, disk %d of the workload (%dx%d), %d DTs, %d substeps, %.1f s"
-                      % (k, P[0].NRAD, P[0].NSEC, ndt, nsub, dt)}
+    out = {}
+    for prec, secs in (("f64", args.cpu_seconds), ("f32", 0.5 * args.cpu_seconds)):
+        set_threads(cores, prec)
+        o = o32 if prec == "f32" else Oracle(P[0], L[0], "f64")
+        if prec == "f64":
+            o.set_fields(dens=g["dens"], vrad=g["vrad"], vtheta=g["vtheta"], energy=g["energy"])
+        o.advance_dt()
+        t0 = time.time()
+        nsub = ndt = 0
+        while ndt < args.cpu_max_dt and time.time() - t0 < secs:
+            nsub += o.advance_dt()
+            ndt += 1
+        dt = time.time() - t0
+        out[prec] = (cells * nsub / dt, ndt, nsub, dt)
+        o.close()
+    v, ndt, nsub, dt = out["f64"]
+    return {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+            "sample": "oracle FP64 (OpenMP, %d threads), disk %d of the workload (%dx%d), %d DTs, %d substeps, "
+                      "%.1f s" % (cores, k, P[0].NRAD, P[0].NSEC, ndt, nsub, dt),
+            "f32_value": out["f32"][0]}
+
+
+def reference_sample(disks, K, W):
+    """The reference arm's sample of a workload: one disk of every grid size
+    (the first of each size in sweep order), with the K timed DTs and the W
+    warm-up DTs shared out over them (every disk takes at least one warm-up
+    DT, which pays the reference's first-call set-up)."""
+    firsts = {}
+    for k, (p, _) in enumerate(disks):
+        firsts.setdefault(int(p["Nrad"]), k)
+    pick = [firsts[n] for n in sorted(firsts)]
+    m = len(pick)
+    timed = [K // m + (1 if i < K % m else 0) for i in range(m)]
+    warm = [max(1, W // m + (1 if i < W % m else 0)) for i in range(m)]
+    return [(k, t, w) for k, t, w in zip(pick, timed, warm) if t > 0]
 
 
 def reference(args, world, rank):
-    """The reference's own CUDA build on a sample of the workload's disks."""
+    """The reference's own CUDA build (its only implementation of the path)
+    on a bounded sample of the workload, timed by its own AlgoGas calls."""
     exe = os.path.join(ROOT, "oracle", "_ref", "fargo_ref")
     if not os.path.exists(exe):
         return {"unavailable": "oracle/_ref/fargo_ref is not built (needs the reference sources at build time)"}
-    from cudaprotoplanetarydisksfloat_b200 import configs
+    configs = load_module("configs")
     disks = workload_disks(args.workload)
-    if args.workload in ("c4", "c4plain"):
-        sizes = np.array([int(p["Nrad"]) * int(p["Nsec"]) for p, _ in disks])
-        order = np.argsort(sizes)
-        pick = [int(order[int(q * (len(order) - 1))]) for q in np.linspace(0, 1, args.ref_disks)]
-    else:
-        pick = [0]
     tmp = tempfile.mkdtemp(prefix="fargo_ref_")
     tot_upd, tot_s, tot_dt, samples = 0.0, 0.0, 0, []
-    for k in pick:
+    for k, ntimed, nwarm in reference_sample(disks, args.steps, args.warmup):
         p, pl = disks[k]
-        ndt = args.warmup + args.ref_steps
-        p = dict(p, Ntot=str(ndt - 1), Ninterm="100000")
+        ndt = nwarm + ntimed
+        # Main.cu runs AlgoGas for i = 0 .. NTOT-1 (output only at i = 0)
+        p = dict(p, Ntot=str(ndt), Ninterm="100000")
         d = os.path.join(tmp, "disk%02d" % k)
-        par, cfg, out = configs.materialise(p, pl, d, "run", relative=True)
-        env = dict(os.environ, FARGO_REF_DUMP="dump_", FARGO_REF_NOISE_SEED=str(20261203 + k))
+        configs.materialise(p, pl, d, "run", relative=True)
+        times = os.path.join(d, "algogas_times.txt")
+        env = dict(os.environ, FARGO_REF_TIMES=times, FARGO_REF_NOISE_SEED=str(20261203 + k))
+        env.pop("FARGO_REF_DUMP", None)
         r = subprocess.run([exe, "run.par"], cwd=d, env=env, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
                            timeout=1200)
         if r.returncode != 0:
             return {"unavailable": "reference run failed with exit code %d" % r.returncode}
-        alg = np.loadtxt(os.path.join(d, "dump_algogas.txt"), ndmin=2)
+        alg = np.loadtxt(times, ndmin=2)
+        if alg.shape[0] < ndt or alg.shape[1] < 3:
+            return {"unavailable": "reference run wrote %d AlgoGas lines, expected %d" % (alg.shape[0], ndt)}
+        sel = alg[nwarm:ndt]
         nrad, nsec = int(p["Nrad"]), int(p["Nsec"])
-        raw = np.fromfile(os.path.join(d, "dump_nshift.bin"), dtype=np.uint8)
-        rec = 8 + 4 * nrad
-        dts = raw[: (raw.size // rec) * rec].reshape(-1, rec)[:, :8].copy().view(np.float64).reshape(-1)
-        # substeps per DT from the dt sequence (each DT sums to DT)
-        DT = float(p["DT"])
-        per_dt, acc, cnt = [], 0.0, 0
-        for x in dts:
-            acc += x
-            cnt += 1
-            if acc >= 0.999999999 * np.float32(DT):
-                per_dt.append(cnt)
-                acc, cnt = 0.0, 0
-        per_dt = np.array(per_dt[: alg.shape[0]])
-        sel = slice(args.warmup, alg.shape[0])
-        tot_upd += float(np.sum(per_dt[sel])) * nrad * nsec
-        tot_s += float(np.sum(alg[sel, 1]))
-        tot_dt += alg.shape[0] - args.warmup
-        samples.append("%dx%d" % (nrad, nsec))
-    value = tot_upd / tot_s
-    return {"value": value, "ms_per_step": 1e3 * tot_s / max(1, tot_dt), "sample": samples, "dts": tot_dt}
+        tot_upd += float(np.sum(sel[:, 2])) * nrad * nsec
+        tot_s += float(np.sum(sel[:, 1]))
+        tot_dt += sel.shape[0]
+        samples.append("%dx%d:%d" % (nrad, nsec, sel.shape[0]))
+    return {"value": tot_upd / tot_s, "ms_per_step": 1e3 * tot_s / max(1, tot_dt), "sample": samples,
+            "dts": tot_dt}
+
+
+def relaunch(args):
+    """`--gpus N` (N > 1) outside a launcher: run this script under
+    torch.distributed.run with N ranks on this node and return its status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def plumbing(args, world, rank, pg):
+    """Rank set-up, sharding and the max/sum reductions without a GPU: each
+    rank takes its disks as the timed run does and reports their cells."""
+    disks = workload_disks(args.workload, seed_shift=rank, rank=rank, world=world, strong=args.strong)
+    cells = float(sum(int(p["Nrad"]) * int(p["Nsec"]) for p, _ in disks))
+    barrier(pg)
+    t0 = time.perf_counter()
+    barrier(pg)
+    ms = allmax(pg, 1e3 * (time.perf_counter() - t0))
+    return {"cells": allsum(pg, cells), "ranks_reporting": allsum(pg, 1.0), "ms_max": ms}
 
 
 def main():
@@ -503,59 +654,66 @@ def main():
     ap.add_argument("--groups", type=int, default=4,
                     help="concurrent batches the disks of a batched workload are split over")
     ap.add_argument("--profile-steps", type=int, default=2)
-    ap.add_argument("--ref-disks", type=int, default=6)
-    ap.add_argument("--ref-steps", type=int, default=3)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--plain-steps", type=int, default=3,
+                    help="DTs of the plain form measured beside the batched C4 line (0: skip)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--cpu-max-dt", type=int, default=400)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--strong", action="store_true",
                     help="split one fixed 64-disk sweep over the ranks instead of one sweep per rank")
     ap.add_argument("--no-graph", action="store_true",
                     help="host loop instead of the CUDA graph (for per-launch profilers)")
+    ap.add_argument("--plumbing", action="store_true",
+                    help="ranks, sharding and reductions only, on CPU (gloo): no GPU work")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
-    world, rank, local, pg = dist_setup(args)
-    wl_desc = {"c4": "64 isothermal disks (Nrad in {128..512}, Nsec=3*Nrad), batched, one DT each",
-               "c4plain": "64 isothermal disks (Nrad in {128..512}, Nsec=3*Nrad), one after another",
-               "c4q": "every 4th disk of the 64-disk sweep (16 disks, 6.1M cells), batched",
-               "c1": "isothermal 128x384, 1 planet", "c2": "adiabatic 256x768, alpha viscosity, 2 live planets",
-               "c3": "self-gravitating 512x1024, 1 planet", "c5": "adiabatic+SG 2048x6144, 3 live planets"}
-    config = {"workload": args.workload, "description": wl_desc[args.workload],
-              "parallelism": "disk-parallel: the GPU's disks in concurrent batches on their own streams"
-              if args.workload.startswith("c4") else
-              "single disk per GPU", "l2": "working set larger than L2" if args.workload in ("c4", "c4plain", "c4q", "c5")
-              else "working set L2-resident (launch-bound)"}
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch(args)
+    if args.impl == "reference":
+        # no process group: rank 0 alone runs the reference, the others exit
+        world, rank, local, pg = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0, None
+    else:
+        world, rank, local, pg = dist_setup(args)
+    config = workload_config(args, world)
     metric = "cell-updates/s"
+    head = {"metric": metric, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "strong" if args.strong else "weak",
+            "vs_baseline": None, "dtype": "f32"}
+    if args.plumbing:
+        r = plumbing(args, world, rank, pg)
+        if rank == 0:
+            print(json.dumps(dict(head, value=None, data="none (plumbing check)", config=config, plumbing=r)),
+                  flush=True)
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
     if args.impl == "reference":
         if rank != 0:
             return 0
         r = reference(args, world, rank)
-        line = {"metric": metric, "impl": "reference", "unit": "cell-updates/s", "n_gpus": 1,
-                "steps": args.ref_steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded noise)", "config": config}
         if "unavailable" in r:
             line = {"impl": "reference", "unavailable": r["unavailable"]}
         else:
-            line.update({"value": r["value"], "ms_per_step": r["ms_per_step"],
-                         "e2e": {"value": r["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
-                                 "d2h_bytes_per_step": 0},
-                         "cpu_baseline": {"value": r["value"], "unit": "cell-updates/s", "cores": 1,
-                                          "kind": "reference",
-                                          "sample": "the reference's own CUDA build on the B200 (its only "
-                                                    "implementation), disks %s, %d DTs, AlgoGas wall time"
-                                                    % (",".join(r["sample"]), r["dts"])}})
+            sample = ("the reference's own CUDA build (its only implementation) on the B200, one disk of each "
+                      "grid size of the workload (%s, grid:DTs), %d timed DTs after warm-up, AlgoGas wall time"
+                      % (", ".join(r["sample"]), r["dts"]))
+            line = dict(head, impl="reference", n_gpus=world, data="synthetic (seeded parameters and density noise)",
+                        config=config, value=r["value"], ms_per_step=r["ms_per_step"],
+                        e2e={"value": r["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0},
+                        cpu_baseline={"value": r["value"], "unit": "cell-updates/s", "cores": 1,
+                                      "kind": "reference", "sample": sample})
         print(json.dumps(line), flush=True)
         return 0
     r = ours(args, world, rank, local, pg)
     if rank == 0:
-        line = {"metric": metric, "value": r["value"], "unit": "cell-updates/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
-                "higher_is_better": True, "scaling": "strong" if args.strong else "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic (seeded parameters and density noise)",
-                "config": dict(config, disks=r["disks"], cells=r["cells"], batches=r["batches"],
-                               tile={"transport_segment": r["seg_out"], "band_rings": 8, "autotuned": True}),
-                "e2e": r["e2e"], "roofline": r["roofline"], "cpu_baseline": r["cpu_baseline"],
-                "clocks": r["clocks"], "gpu_launches": r["gpu_launches"]}
+        line = dict(head, value=r["value"], ms_per_step=r["ms_per_step"],
+                    data="synthetic (seeded parameters and density noise)", config=config,
+                    tiles={"transport_segment": r["seg_out"], "band_rings": 8, "autotuned": True},
+                    e2e=r["e2e"], roofline=r["roofline"], cpu_baseline=r["cpu_baseline"], clocks=r["clocks"],
+                    gpu_launches=r["gpu_launches"])
+        if r.get("plain"):
+            line["plain"] = r["plain"]
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()

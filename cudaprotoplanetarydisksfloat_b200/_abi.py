@@ -14,6 +14,9 @@ FARGO_MAXPLANETS = 100
 FARGO_DIMFXY = 11
 FARGO_NOALLOC_MAXRAD = 4096
 FARGO_STRLEN = 512
+FARGO_MAX_SUBSTEPS = 100000
+FARGO_PRECISION_REFERENCE = 0
+FARGO_PRECISION_ACCURATE = 1
 
 STATUS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ECUFFT", 4: "ENONFINITE", 5: "ETIMEOUT", 6: "EOOM",
           7: "EIO", 8: "ENODEV"}
@@ -79,12 +82,14 @@ EXPORTS = [
     "fargo_params_default", "fargo_params_read", "fargo_params_derive", "fargo_planets_read",
     "fargo_grid_radii", "fargo_create", "fargo_destroy", "fargo_last_error", "fargo_init_state",
     "fargo_upload", "fargo_download", "fargo_get_planets", "fargo_set_planets", "fargo_advance_dt",
-    "fargo_advance", "fargo_advance_async", "fargo_sync", "fargo_disk_force", "fargo_disk_force_noalloc", "fargo_get_scalars",
+    "fargo_advance", "fargo_advance_async", "fargo_sync", "fargo_disk_force", "fargo_disk_force_noalloc",
+    "fargo_sg_accelerations", "fargo_get_scalars",
     "fargo_get_substep_log", "fargo_batch_create", "fargo_batch_destroy", "fargo_batch_last_error",
     "fargo_batch_init_state", "fargo_batch_upload", "fargo_batch_download", "fargo_batch_advance",
     "fargo_batch_advance_async", "fargo_batch_sync", "fargo_batch_get_scalars",
     "fargo_batch_get_planets", "fargo_batch_count_launches", "fargo_batch_kernel_launches", "fargo_abi_version",
-    "fargo_kernel_launches", "fargo_set_graph_mode", "fargo_batch_set_graph_mode", "fargo_batch_autotune", "fargo_autotune", "fargo_checkpoint_bytes", "fargo_checkpoint_save",
+    "fargo_kernel_launches", "fargo_set_graph_mode", "fargo_batch_set_graph_mode",
+    "fargo_set_max_substeps", "fargo_batch_set_max_substeps", "fargo_set_precision", "fargo_batch_set_precision", "fargo_batch_autotune", "fargo_autotune", "fargo_checkpoint_bytes", "fargo_checkpoint_save",
     "fargo_checkpoint_load", "fargo_stream", "fargo_batch_stream",
     "fargo_ctx_batch", "fargo_batch_upload_async", "fargo_batch_download_async", "fargo_batch_profile",
     "fargo_profile_kernel_name", "fargo_profile_kernel_count",
@@ -126,6 +131,7 @@ def _load():
         "fargo_disk_force": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, dp]),
         "fargo_disk_force_noalloc": (C.c_int, [vp, vp, vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_double,
                                                C.c_double, C.c_double, C.c_int, dp, vp, C.c_char_p, C.c_int]),
+        "fargo_sg_accelerations": (C.c_int, [vp, fp, fp]),
         "fargo_get_scalars": (C.c_int, [vp, P(FargoScalars)]),
         "fargo_get_substep_log": (C.c_int, [vp, C.c_int, P(C.c_int), dp, P(C.c_int)]),
         "fargo_batch_create": (C.c_int, [C.c_int, P(FargoParams), P(FargoPlanets), C.c_int, P(vp)]),
@@ -145,6 +151,10 @@ def _load():
         "fargo_kernel_launches": (C.c_longlong, [vp]),
         "fargo_set_graph_mode": (C.c_int, [vp, C.c_int]),
         "fargo_batch_set_graph_mode": (C.c_int, [vp, C.c_int]),
+        "fargo_set_max_substeps": (C.c_int, [vp, C.c_int]),
+        "fargo_batch_set_max_substeps": (C.c_int, [vp, C.c_int]),
+        "fargo_set_precision": (C.c_int, [vp, C.c_int]),
+        "fargo_batch_set_precision": (C.c_int, [vp, C.c_int]),
         "fargo_batch_autotune": (C.c_int, [vp, C.c_int, P(C.c_int)]),
         "fargo_autotune": (C.c_int, [vp, C.c_int, P(C.c_int)]),
         "fargo_checkpoint_bytes": (C.c_size_t, [vp]),

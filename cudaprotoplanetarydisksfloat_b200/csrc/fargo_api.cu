@@ -187,6 +187,8 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   D.ev_DRMAX = (float)(h.t.Rmed[p->NRAD - 1] * 0.84);
   D.SloppyCFL = p->SloppyCFL;
   D.IsDisk = p->IsDisk;
+  D.max_sub = FARGO_MAX_SUBSTEPS;
+  D.accurate = 0;
   D.invdphi = h.t.invdphi;
   D.onethird = h.t.onethird;
   size_t ng = (size_t)(p->NRAD + 1) * p->NSEC;
@@ -228,7 +230,7 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   U(D.invSurf, h.t.invSurf) U(D.invRmed, h.t.invRmed) U(D.invdiffRsup, h.t.invdiffRsup)
   U(D.invdiffRmed, h.t.invdiffRmed) U(D.dxtheta, h.t.dxtheta) U(D.supp_torque, h.t.supp_torque)
   U(D.SigmaMed, h.t.SigmaMed) U(D.SigmaInf, h.t.SigmaInf) U(D.EnergyMed, h.t.EnergyMed)
-  U(D.CoolingTimeMed, h.t.CoolingTimeMed) U(D.pow15, h.t.pow15)
+  U(D.CoolingTimeMed, h.t.CoolingTimeMed) U(D.pow15, h.t.pow15) U(D.star_grad, h.t.star_grad)
 #undef U
   // QplusMed is filled at initialisation (it needs the viscosity)
   float* qpm;
@@ -639,7 +641,9 @@ fargo_status finish_dts(fargo_batch* b) {
     DiskCtl c = ctl_header(b, d, &e);
     if (e != cudaSuccess) return set_err(b, FARGO_ECUDA, "ctl read: %s", cudaGetErrorString(e));
     if (c.error == 1) return set_err(b, FARGO_ENONFINITE, "disk %d: non-finite or non-positive CFL time step", d);
-    if (c.error == 2) return set_err(b, FARGO_ETIMEOUT, "disk %d: more than 1e5 substeps in one DT", d);
+    if (c.error == 2)
+      return set_err(b, FARGO_ETIMEOUT, "disk %d: the DT needs more than %d substeps (the substep limit)", d,
+                     b->disks[d].dev.max_sub);
   }
   return FARGO_OK;
 }
@@ -934,6 +938,21 @@ fargo_status fargo_disk_force(fargo_ctx* ctx, double x, double y, double rsmooth
   return disk_force_impl(&ctx->b, 0, x, y, rsmoothing, mass, dimfxy, globalforce);
 }
 
+fargo_status fargo_sg_accelerations(fargo_ctx* ctx, float* accr, float* acct) {
+  if (!ctx || !accr || !acct) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  DiskHost& h = b->disks[0];
+  if (!h.sg) return set_err(b, FARGO_EINVAL, "fargo_sg_accelerations: the run has no self-gravity");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  fargo_status st = sg_accelerations(h.sg, b->bd, 0, &h.dev, b->stream, b->err);
+  if (st) return st;
+  size_t n = (size_t)h.dev.nrad * h.dev.nsec;
+  CK(cudaMemcpy(accr, h.dev.sg_accr, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(acct, h.dev.sg_acct, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  return FARGO_OK;
+}
+
 static fargo_status scalars_impl(fargo_batch* b, int d, fargo_scalars* out) {
   if (!b || !out || d < 0 || d >= (int)b->disks.size()) return FARGO_EINVAL;
   CK(cudaSetDevice(b->device));
@@ -1203,6 +1222,44 @@ fargo_status fargo_batch_autotune(fargo_batch* b, int reps, int* seg_out) { retu
 fargo_status fargo_autotune(fargo_ctx* ctx, int reps, int* seg_out) {
   if (!ctx) return FARGO_EINVAL;
   return batch_autotune(&ctx->b, reps, seg_out);
+}
+
+fargo_status fargo_batch_set_max_substeps(fargo_batch* b, int n) {
+  if (!b || n < 1) return FARGO_EINVAL;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  for (int d = 0; d < (int)b->disks.size(); d++) {
+    b->disks[d].dev.max_sub = n;
+    CK(cudaMemcpy(&b->d_disks[d].max_sub, &n, sizeof(int), cudaMemcpyHostToDevice));
+  }
+  return FARGO_OK;
+}
+
+fargo_status fargo_batch_set_precision(fargo_batch* b, int mode) {
+  if (!b || (mode != FARGO_PRECISION_REFERENCE && mode != FARGO_PRECISION_ACCURATE)) return FARGO_EINVAL;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  const int acc = mode == FARGO_PRECISION_ACCURATE;
+  for (int d = 0; d < (int)b->disks.size(); d++) {
+    DiskHost& h = b->disks[d];
+    h.dev.accurate = acc;
+    CK(cudaMemcpy(&b->d_disks[d].accurate, &acc, sizeof(int), cudaMemcpyHostToDevice));
+    if (h.sg) {
+      fargo_status st = sg_tabulate(h.sg, h.t, acc, b->stream, b->err);
+      if (st) return st;
+    }
+  }
+  return FARGO_OK;
+}
+
+fargo_status fargo_set_precision(fargo_ctx* ctx, int mode) {
+  if (!ctx) return FARGO_EINVAL;
+  return fargo_batch_set_precision(&ctx->b, mode);
+}
+
+fargo_status fargo_set_max_substeps(fargo_ctx* ctx, int n) {
+  if (!ctx) return FARGO_EINVAL;
+  return fargo_batch_set_max_substeps(&ctx->b, n);
 }
 
 fargo_status fargo_batch_set_graph_mode(fargo_batch* b, int use_graph) {

@@ -95,6 +95,8 @@ struct DiskDev {
   int Adiabatic, Cooling, ViscosityAlpha, FastTransport, Indirect_Term, ExcludeHill;
   int ForcedCircular, Corotating, GuidingCenter, RocheSmoothing, SelfGravity, Evanescent;
   int OpenInner, NonReflecting, SloppyCFL, IsDisk;
+  int max_sub;  // substeps one DT may take before it stops with FARGO_ETIMEOUT
+  int accurate;  // precision mode: 0 the reference's arithmetic, 1 accurate (FARGO_PRECISION_*)
   // boundary constants computed on the host as the reference does:
   // pow(Rinf[1], -1.5), pow(Rinf[NRAD-2], -1.5) of NonReflectingBoundary;
   // damping zones and orbital periods of EvanescentBoundary (SideEuler.cu:127-132)
@@ -120,6 +122,7 @@ struct DiskDev {
   const float *Rinf, *Rsup, *Rmed, *Surf, *invRinf, *invSurf, *invRmed, *invdiffRsup, *invdiffRmed;
   const float *dxtheta, *supp_torque, *SigmaMed, *SigmaInf, *EnergyMed, *CoolingTimeMed, *QplusMed;
   const double* pow15;   // pow(Rmed[i], 1.5) from the host (FViscosity)
+  const float* star_grad;  // accurate mode: G / (Rmed[i] Rmed[i-1]) (FP64 radii)
   float* visc;           // viscosity_array of this substep
   float* cs_ring;        // isothermal sound speed per ring
   float* csmean;         // GLOBAL_bufarray: ring-mean sound speed

@@ -12,6 +12,10 @@ struct HostTables {
   std::vector<float> Radii, Rinf, Rsup, Rmed, Surf, invRinf, invSurf, invRmed, invdiffRsup, invdiffRmed;
   std::vector<float> powRmed, dxtheta, supp_torque, SigmaMed, SigmaInf, EnergyMed, CoolingTimeMed, QplusMed;
   std::vector<double> pow15;  // pow(Rmed[i], 1.5) as FViscosity evaluates it
+  // accurate mode: the star potential's radial difference quotient
+  // (-G/Rmed[i] + G/Rmed[i-1]) / (Rmed[i] - Rmed[i-1]) = G / (Rmed[i] Rmed[i-1]),
+  // from the FP64 radii, rounded once
+  std::vector<float> star_grad;
   float invdphi = 0, onethird = 0;
 };
 

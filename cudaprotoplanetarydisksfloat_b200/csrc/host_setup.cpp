@@ -38,6 +38,7 @@ void host_build_tables(const fargo_params* p, const double* radii_in, HostTables
                               &t->EnergyMed, &t->CoolingTimeMed, &t->QplusMed};
   for (auto* v : f1) v->assign(NRAD + 1, 0.0f);  // entries the reference leaves unset are 0
   t->pow15.assign(NRAD + 1, 0.0);
+  t->star_grad.assign(NRAD + 1, 0.0f);
   const std::vector<double>& R2 = t->Radii2;
   const std::vector<double>& M2 = t->Rmed2;
   for (int i = 0; i <= NRAD; i++) t->Radii[i] = (float)R2[i];
@@ -54,6 +55,7 @@ void host_build_tables(const fargo_params* p, const double* radii_in, HostTables
   t->Rinf[NRAD] = R2[NRAD];
   for (int i = 0; i < NRAD; i++) {
     if (i > 0) t->invdiffRmed[i] = 1.0 / (M2[i] - M2[i - 1]);
+    if (i > 0) t->star_grad[i] = (float)(1.0 / (M2[i] * M2[i - 1]));
     t->powRmed[i] = std::pow(M2[i], -2.5 + p->SIGMASLOPE);
     t->pow15[i] = std::pow((double)t->Rmed[i], 1.5);
   }

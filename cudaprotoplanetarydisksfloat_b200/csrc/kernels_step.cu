@@ -81,6 +81,19 @@ __device__ __forceinline__ int jwrap_p(int j, int nsec) { return j + 1 == nsec ?
 
 // max2 / min2, Kernels.cu:1459-1470
 __device__ __forceinline__ float max2(float a, float b) { return (b > a) ? b : a; }
+
+// Kahan-compensated FP32 sum (accurate mode's ring means): the same order as
+// the plain sum, with the rounding error of every addition carried into the
+// next one.  No multiplications, so no contraction into fused multiply-adds.
+struct KahanSum {
+  float s = 0.0f, c = 0.0f;
+  __device__ __forceinline__ void add(float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+};
 __device__ __forceinline__ float min2(float a, float b) { return (b < a) ? b : a; }
 
 // AspectRatioDevice, Kernels.cu:1473-1488
@@ -801,7 +814,7 @@ __device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const d
   C->nsub++;
   C->nsub_total++;
   C->more = (C->dtemp < 0.999999999 * DTd) ? 1 : 0;
-  if (C->nsub >= 100000) {
+  if (C->more && C->nsub >= D.max_sub) {
     C->error = 2;
     C->more = 0;
   }
@@ -1063,10 +1076,13 @@ __global__ void __launch_bounds__(kThreads) k_potential(BatchDev B) {
     }
     if (k == 0) {  // the star
       const float itx = C->itx, ity = C->ity;
+      // accurate mode: the star's -G/r enters Substep1 as its exact radial
+      // difference quotient (star_grad) instead of a difference of FP32 values
+      const bool star = !D.accurate;
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         float InvDistance = __fdiv_rn(1.0f, D.Rmed[q.i[u]]);
-        float pot = -InvDistance;
+        float pot = star ? -InvDistance : 0.0f;
         pot -= itx * x[u] + ity * y[u];
         P[u] += pot;
       }
@@ -1142,6 +1158,7 @@ __global__ void __launch_bounds__(kThreads, (kAdi == 0 && kSg == 0) ? 3 : 2) k_s
       const float Pm = adi ? (D.ADIABATICINDEX - 1.0f) * Em[u] : Dnm[u] * csm * csm;
       float gradp = (P0 - Pm) * 2.0f / (Dn0[u] + Dnm[u]) * D.invdiffRmed[i];
       float gradphi = (Ph0[u] - Phm[u]) * D.invdiffRmed[i];
+      if (D.accurate && C->nb > 0) gradphi += D.star_grad[i];
       float vt2 = vth(Vt0[u], i) + vth(Vtp[u], i) + vth(Vtm[u], i - 1) + vth(Vtmp[u], i - 1);
       vt2 = vt2 * 0.25f + D.Rinf[i] * OmegaFrame;
       vt2 = vt2 * vt2;
@@ -1838,6 +1855,8 @@ __global__ void __launch_bounds__(kRMT) k_ring_mean(BatchDev B) {
       for (int k = 0; k < 32; k++) buf[k * (kRMW + 1) + tid] = r[k];
     };
     float moy = 0.0f;
+    KahanSum ks;  // accurate mode
+    const bool acc = D.accurate;
     __syncthreads();
     load(0);
     store(0);
@@ -1847,7 +1866,9 @@ __global__ void __launch_bounds__(kRMT) k_ring_mean(BatchDev B) {
       if (tid < 32) {
         const float* row = rm_sm + (c & 1) * 32 * (kRMW + 1) + lane * (kRMW + 1);
         const int w = min(kRMW, nsec - c * kRMW);
-        if (w == kRMW) {
+        if (acc) {
+          for (int k = 0; k < w; k++) ks.add(row[k]);
+        } else if (w == kRMW) {
 #pragma unroll 32
           for (int k = 0; k < kRMW; k++) moy += row[k];
         } else {
@@ -1858,6 +1879,7 @@ __global__ void __launch_bounds__(kRMT) k_ring_mean(BatchDev B) {
       __syncthreads();
     }
     const int i = i0 + lane;
+    if (acc) moy = ks.s;
     if (tid < 32 && lane < nr) {
       if (mode == 0) {
         D.vmoy[i] = moy / (float)nsec;
@@ -2294,6 +2316,7 @@ __global__ void k_dt_begin(BatchDev B) {
     DiskCtl* C = D.ctl;
     C->dtemp = 0.0;
     C->nsub = 0;
+    C->error = 0;  // an error is reported at the end of the DT it stopped
     C->active = 1;
     C->more = 1;
     C->counter = 0;
@@ -2342,13 +2365,23 @@ __global__ void k_cs_ringmean(BatchDev B, int only_disk) {
   if (lane != 0) return;
   const int i = r - D.ring0, nsec = D.nsec;
   float sum = 0.0f;
+  KahanSum ks;  // accurate mode
   if (D.Adiabatic) {
     const float* f = D.cs + (size_t)i * nsec;
-    for (int j = 0; j < nsec; j++) sum += f[j];
+    if (D.accurate) {
+      for (int j = 0; j < nsec; j++) ks.add(f[j]);
+    } else {
+      for (int j = 0; j < nsec; j++) sum += f[j];
+    }
   } else {
     const float v = D.cs_ring[i];
-    for (int j = 0; j < nsec; j++) sum += v;
+    if (D.accurate) {
+      for (int j = 0; j < nsec; j++) ks.add(v);
+    } else {
+      for (int j = 0; j < nsec; j++) sum += v;
+    }
   }
+  if (D.accurate) sum = ks.s;
   D.csmean[i] = sum / (float)nsec;
 }
 
@@ -2395,7 +2428,13 @@ __global__ void __launch_bounds__(kThreads) k_bc_rings(BatchDev B) {
         __syncthreads();
         if (tid == 0) {
           float sum = 0.0f;  // Make1DprofileKernel: sectors in order
-          for (int j = 0; j < nsec; j++) sum += D.cs[r0 + j];
+          if (D.accurate) {
+            KahanSum ks;
+            for (int j = 0; j < nsec; j++) ks.add(D.cs[r0 + j]);
+            sum = ks.s;
+          } else {
+            for (int j = 0; j < nsec; j++) sum += D.cs[r0 + j];
+          }
           D.csmean[i] = sum / (float)nsec;
           D.visc[i] = fviscosity_ring(D, i, C->time_start, C->PhysicalTimeInitial);
         }
@@ -2608,7 +2647,7 @@ __global__ void __launch_bounds__(kThreads) k_disk_force(BatchDev B, int disk, f
     float d2 = dx * dx + dy * dy;
     float dist2 = d2 + rs * rs;
     float distance = sqrtf(dist2);
-    float InvDist3 = 1.0 / ((double)dist2 * (double)distance);
+    float InvDist3 = 1.0 / dist2 / distance;  // two FP64 divisions, as Kernels.cu:821
     bool inner = D.Rmed[i] < a;
     for (int k = 0; k < FARGO_DIMFXY; k++) {
       float hillcutfactor = (float)k / (float)(FARGO_DIMFXY - 1);

@@ -39,7 +39,9 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // ComputeForceKernel (Kernels.cu:804-839) for every Hill-cut level k at once,
 // one block per ring; the block's FP64 sums of the FP32 per-cell forces go to
-// part[i * kNQ + q].  The same arithmetic as the library's context-based
+// part[i * kNQ + q].  Each thread keeps all 44 FP64 sums, more than fit in
+// registers beside the rest (ptxas spills part of them to local memory):
+// acceptable for a diagnostic call made once per output, not per substep.  The same arithmetic as the library's context-based
 // disk force, reading the cell coordinates from the caller's
 // CellAbscissa/CellOrdinate arrays.
 __global__ void __launch_bounds__(kThreads) k_disk_force_rings(const float* __restrict__ dens,
@@ -64,7 +66,7 @@ __global__ void __launch_bounds__(kThreads) k_disk_force_rings(const float* __re
       float d2 = dx * dx + dy * dy;
       float dist2 = d2 + rs * rs;
       float distance = sqrtf(dist2);
-      float InvDist3 = 1.0 / ((double)dist2 * (double)distance);
+      float InvDist3 = 1.0 / dist2 / distance;  // two FP64 divisions, as Kernels.cu:821
 #pragma unroll
       for (int k = 0; k < FARGO_DIMFXY; k++) {
         float hillcutfactor = (float)k / (float)(FARGO_DIMFXY - 1);
@@ -167,6 +169,12 @@ extern "C" fargo_status fargo_disk_force_noalloc(const float* dens, const float*
   const double a = std::sqrt(x * x + y * y);
   const double rh = std::pow(mass / 3., 1. / 3.) * a + 1e-15;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // an error left pending by the caller's own launches is reported as such
+  // and left in place (peek), so it is neither blamed on this call nor lost
+  e = cudaPeekAtLastError();
+  if (e != cudaSuccess)
+    return fail(err, errlen, FARGO_ECUDA, "fargo_disk_force_noalloc: an earlier CUDA error is pending: %s",
+                cudaGetErrorString(e));
   double* totals = scratch + (size_t)FARGO_NOALLOC_MAXRAD * kNQ;
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

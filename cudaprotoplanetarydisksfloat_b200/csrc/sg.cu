@@ -179,10 +179,33 @@ fargo_status sg_create(SelfGravity** out, const fargo_params* p, const HostTable
   sg->plans = true;
   cufftSetStream(sg->fwd, s);
   cufftSetStream(sg->inv, s);
-  // compute_kernel (SgMain.cu:49-81), host float math as in the reference
+  return sg_tabulate(sg, t, 0, s, err);
+}
+
+// compute_kernel (SgMain.cu:49-81): the kernels K^r, K^t on the padded
+// (2 NRAD) x NSEC grid, tabulated with the reference's host float math
+// (accurate = 0) or in FP64 from the FP64 radii (accurate = 1), then
+// transformed once in FP64 (D2Z) and kept as FP32 spectra.
+fargo_status sg_tabulate(SelfGravity* sg, const HostTables& t, int accurate, cudaStream_t s, std::string& err) {
+  const int NRAD = sg->nrad, NSEC = sg->nsec;
+  long long nr = (long long)sg->nx * NSEC, nh = (long long)sg->nx * sg->nyh;
+  int n[2] = {sg->nx, NSEC};
+  cudaError_t e;
+  cufftResult r;
   std::vector<double> K(2 * (size_t)nr);
   float eps = sg->eps;
   for (int i = 0; i < 2 * NRAD; i++) {
+    if (accurate) {
+      const double ed = eps;
+      const double u = i < NRAD ? std::log(t.Radii2[i] / t.Radii2[0]) : -std::log(t.Radii2[2 * NRAD - i] / t.Radii2[0]);
+      for (int j = 0; j < NSEC; j++) {
+        const double th = 2.0 * PI_D * (double)j / (double)NSEC;
+        const double base = ed * ed * std::exp(u) + 2.0 * (std::cosh(u) - std::cos(th));
+        K[(size_t)i * NSEC + j] = (1.0 + ed * ed - std::cos(th) * std::exp(-u)) * std::pow(base, -1.5);
+        K[nr + (size_t)i * NSEC + j] = std::sin(th) * std::pow(base, -1.5);
+      }
+      continue;
+    }
     float u;
     if (i < NRAD)
       u = logf(t.Radii[i] / t.Radii[0]);

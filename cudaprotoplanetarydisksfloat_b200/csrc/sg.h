@@ -11,6 +11,9 @@ struct SelfGravity;
 fargo_status sg_create(SelfGravity** out, const fargo_params* p, const HostTables& t, cudaStream_t s, DiskDev* D,
                        std::string& err);
 void sg_destroy(SelfGravity* sg);
+// compute_kernel (SgMain.cu:49-81) tabulated in the reference's float math
+// (accurate = 0) or in FP64 (accurate = 1), transformed once in FP64
+fargo_status sg_tabulate(SelfGravity* sg, const HostTables& t, int accurate, cudaStream_t s, std::string& err);
 // pad -> R2C -> kernel-spectrum multiply -> C2R -> accelerations (SG_Accr/SG_Acct)
 fargo_status sg_accelerations(SelfGravity* sg, const BatchDev& b, int d, DiskDev* D, cudaStream_t s,
                               std::string& err);

@@ -140,8 +140,25 @@ class Disk:
                                        gf.ctypes.data_as(C.POINTER(C.c_double))), "fargo_disk_force")
         return gf
 
+    def sg_accelerations(self):
+        """(accr, acct), each (NRAD, NSEC) float32: the self-gravity
+        accelerations of the current density (between DTs)."""
+        n = self.nrad * self.nsec
+        ar, at = np.empty(n, np.float32), np.empty(n, np.float32)
+        self._chk(lib.fargo_sg_accelerations(self.ctx, _ptr(ar), _ptr(at)), "fargo_sg_accelerations")
+        return ar.reshape(self.nrad, self.nsec), at.reshape(self.nrad, self.nsec)
+
     def set_graph_mode(self, on):
         self._chk(lib.fargo_set_graph_mode(self.ctx, 1 if on else 0), "fargo_set_graph_mode")
+
+    def set_max_substeps(self, n):
+        """Substeps one DT may take before it stops with FARGO_ETIMEOUT."""
+        self._chk(lib.fargo_set_max_substeps(self.ctx, n), "fargo_set_max_substeps")
+
+    def set_precision(self, mode):
+        """0 (FARGO_PRECISION_REFERENCE): the reference's arithmetic;
+        1 (FARGO_PRECISION_ACCURATE): closer to FP64 (see the header)."""
+        self._chk(lib.fargo_set_precision(self.ctx, int(mode)), "fargo_set_precision")
 
     def autotune(self, reps=3):
         """Pick the transport segment width by timing (between DTs); returns it."""
@@ -221,6 +238,9 @@ class Batch:
 
     def set_graph_mode(self, on):
         self._chk(lib.fargo_batch_set_graph_mode(self.b, 1 if on else 0), "fargo_batch_set_graph_mode")
+
+    def set_precision(self, mode):
+        self._chk(lib.fargo_batch_set_precision(self.b, int(mode)), "fargo_batch_set_precision")
 
     def autotune(self, reps=3):
         """Pick the transport segment width by timing (between DTs); returns it."""

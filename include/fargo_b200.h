@@ -31,6 +31,7 @@ extern "C" {
 #define FARGO_DIMFXY 11        /* Main.cu:71 dimfxy: Hill-cut levels of ComputeForce */
 #define FARGO_NOALLOC_MAXRAD 4096 /* largest NRAD of fargo_disk_force_noalloc */
 #define FARGO_STRLEN 512
+#define FARGO_MAX_SUBSTEPS 100000 /* default substep limit of one DT */
 
 typedef enum fargo_status {
   FARGO_OK = 0,
@@ -185,6 +186,12 @@ fargo_status fargo_sync(fargo_ctx* ctx);
 fargo_status fargo_disk_force(fargo_ctx* ctx, double x, double y, double rsmoothing,
                               double mass, int dimfxy, double* globalforce);
 
+/* compute_selfgravity (SgMain.cu:23-45) on the current density, between
+   DTs: the radial and azimuthal self-gravity accelerations SG_Accr, SG_Acct
+   (NRAD*NSEC each, host memory), as the next substep would use them.
+   FARGO_EINVAL when the run has no self-gravity. */
+fargo_status fargo_sg_accelerations(fargo_ctx* ctx, float* accr, float* acct);
+
 /* No counterpart in the reference: fargo_disk_force for callers that keep
    their disk in their own device arrays and must not allocate device memory
    (they manage it themselves, or cannot afford cudaMalloc's device-wide
@@ -195,11 +202,13 @@ fargo_status fargo_disk_force(fargo_ctx* ctx, double x, double y, double rsmooth
    pointers in the reference's layout: dens, cell_x, cell_y [NRAD*NSEC]
    (Dens, CellAbscissa, CellOrdinate), surf, rmed [NRAD]; globalforce is
    host memory, filled as by fargo_disk_force.  Runs on `stream` (a
-   cudaStream_t, NULL for the default stream) on the current device and
-   waits for it.  The first call on a device looks up the scratch address
-   there: make it before any stream capture.  Calls share the scratch, so
-   calls that overlap on the GPU race.  err/errlen (may be NULL/0) receive a
-   message on failure. */
+   cudaStream_t, NULL for the default stream) on the current device, copies
+   the result to globalforce and synchronises that stream before returning.
+   The first call on a device looks up the scratch address there: make it
+   before any stream capture.  Calls share the scratch, so calls that
+   overlap on the GPU race.  A CUDA error already pending when the call
+   starts is reported (FARGO_ECUDA) and left pending.  err/errlen (may be
+   NULL/0) receive a message on failure. */
 fargo_status fargo_disk_force_noalloc(const float* dens, const float* cell_x, const float* cell_y,
                                       const float* surf, const float* rmed, int nrad, int nsec,
                                       double x, double y, double rsmoothing, double mass,
@@ -277,6 +286,34 @@ const char* fargo_profile_kernel_name(int k);
    over the substeps; 0: host loop with one wait per substep. */
 fargo_status fargo_set_graph_mode(fargo_ctx* ctx, int use_graph);
 fargo_status fargo_batch_set_graph_mode(fargo_batch* b, int use_graph);
+/* (new) Largest number of CFL substeps one DT may take (default
+   FARGO_MAX_SUBSTEPS).  A DT that needs more stops after that many substeps
+   and fargo_advance* return FARGO_ETIMEOUT; the context stays usable (upload
+   a state and advance again).  A CFL step that is not a positive finite
+   number (a NaN or Inf in the state) stops the DT with FARGO_ENONFINITE in
+   the same way.  Call between DTs. */
+fargo_status fargo_set_max_substeps(fargo_ctx* ctx, int n);
+fargo_status fargo_batch_set_max_substeps(fargo_batch* b, int n);
+/* (new) Precision mode of every disk of the context / batch.
+   FARGO_PRECISION_REFERENCE (default): the reference's FP32 arithmetic, so
+   that substep counts, every dt and every FARGO shift match its build bit
+   for bit.  FARGO_PRECISION_ACCURATE: closer to an FP64 run of the same
+   algorithm, at the same FP32 storage:
+   - the star's potential -G/r is left out of the stored potential and its
+     radial difference quotient enters Substep1 (SourceEuler.cu:305-335,
+     Kernels.cu:52-70) as G/(Rmed[i] Rmed[i-1]) from the FP64 radii: the
+     reference differences two FP32 values of -G/r ~ 1 across a ring
+     spacing of ~1%, which costs ~1e-5 of the radial gravity each substep;
+   - ring means (FARGO VMed, CFL mean, alpha-viscosity sound speed) are
+     Kahan-compensated FP32 sums in the same order;
+   - the self-gravity kernel is tabulated in FP64 (the reference's float
+     table is not exactly antisymmetric in azimuth).
+   Integer outcomes may then differ from the reference's build.  Call
+   between DTs, before the first one for a reproducible run. */
+#define FARGO_PRECISION_REFERENCE 0
+#define FARGO_PRECISION_ACCURATE 1
+fargo_status fargo_set_precision(fargo_ctx* ctx, int mode);
+fargo_status fargo_batch_set_precision(fargo_batch* b, int mode);
 /* (new) Tile autotuner: times the transport kernels on the current state for
    azimuthal segment widths 96..248 sectors and keeps the fastest (*seg_out).
    Call between DTs; the state is not advanced. */

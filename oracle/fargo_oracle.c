@@ -99,6 +99,11 @@ struct orc {
   int bc_angle[2];                   /* NonReflectingBoundary's i_angle, i_angle2 (last call) */
   fargo_planets sys, sys0;
   pairr DiskOnPrimaryAcceleration, IndirectTerm;
+  /* precision mode (orc_set_precision): 0 the reference's arithmetic,
+     1 accurate (FP64 star-potential gradient, compensated ring means, FP64
+     self-gravity kernel table) */
+  int accurate;
+  real* star_grad; /* G / (Rmed[i] Rmed[i-1]) from the FP64 radii, accurate mode */
   /* substep log */
   int nsub;
   int* log_nshift;
@@ -204,7 +209,18 @@ static void ring_mean(const orc* o, const real* f, real* out) {
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < o->nrad; i++) {
     real moy = 0.0;
-    for (int j = 0; j < nsec; j++) moy += f[i * nsec + j];
+    if (o->accurate) {
+      /* accurate mode: Kahan-compensated sum in the same order */
+      real comp = 0.0;
+      for (int j = 0; j < nsec; j++) {
+        real y = f[i * nsec + j] - comp;
+        real t = moy + y;
+        comp = (t - moy) - y;
+        moy = t;
+      }
+    } else {
+      for (int j = 0; j < nsec; j++) moy += f[i * nsec + j];
+    }
     out[i] = moy / (real)nsec;
   }
 }
@@ -415,10 +431,15 @@ static void dft_1d(double* a, int n, int s, int sign, double* tmp) {
    cufftExecC2C as Main.cu:186-196 and SgMain.cu:115-162 use them). */
 static void fft2d(orc* o, double* a, int sign) {
   int nx = 2 * o->nrad, ny = o->nsec;
-  double* tmp = (double*)malloc(sizeof(double) * 2 * (nx > ny ? nx : ny));
-  for (int i = 0; i < nx; i++) dft_1d(a + 2 * (size_t)i * ny, ny, 1, sign, tmp);
-  for (int j = 0; j < ny; j++) dft_1d(a + 2 * j, nx, ny, sign, tmp);
-  free(tmp);
+#pragma omp parallel
+  {
+    double* tmp = (double*)malloc(sizeof(double) * 2 * (nx > ny ? nx : ny));
+#pragma omp for schedule(static)
+    for (int i = 0; i < nx; i++) dft_1d(a + 2 * (size_t)i * ny, ny, 1, sign, tmp);
+#pragma omp for schedule(static)
+    for (int j = 0; j < ny; j++) dft_1d(a + 2 * j, nx, ny, sign, tmp);
+    free(tmp);
+  }
 }
 
 /* compute_kernel, SgMain.cu:49-81 (host float math), then the forward FFTs
@@ -448,6 +469,20 @@ static void sg_init_kernel(orc* o) {
     o->Kr_hat[2 * l + 1] = 0;
     o->Kt_hat[2 * l] = o->Kt_aux[l];
     o->Kt_hat[2 * l + 1] = 0;
+  }
+  if (o->accurate) {
+    /* accurate mode: the same kernel tabulated in FP64 from the FP64 radii */
+    double eps = o->SGP_eps;
+    for (int i = 0; i < 2 * NRAD; i++) {
+      double ud = i < NRAD ? log(o->Radii2[i] / o->Radii2[0]) : -log(o->Radii2[2 * NRAD - i] / o->Radii2[0]);
+      for (int j = 0; j < NSEC; j++) {
+        double th = 2.0 * PI * (double)j / (double)NSEC;
+        double b = eps * eps * exp(ud) + 2.0 * (cosh(ud) - cos(th));
+        size_t l = (size_t)i * NSEC + j;
+        o->Kr_hat[2 * l] = (1.0 + eps * eps - cos(th) * exp(-ud)) * pow(b, -1.5);
+        o->Kt_hat[2 * l] = sin(th) * pow(b, -1.5);
+      }
+    }
   }
   fft2d(o, o->Kr_hat, -1);
   fft2d(o, o->Kt_hat, -1);
@@ -867,7 +902,9 @@ static void fill_forces_arrays(orc* o) {
         if (p->Indirect_Term) pot += G * mp * ipd3 * (x * xp + y * yp);
         o->Potential[i * nsec + j] += pot;
         if (k == 0) {
-          pot = -G * 1.0 * InvDistance;
+          /* accurate mode: the star's -G/r enters Substep1 as its exact
+             radial difference (star_grad) instead */
+          pot = o->accurate ? 0.0 : -G * 1.0 * InvDistance;
           pot -= itx * x + ity * y;
           o->Potential[i * nsec + j] += pot;
         }
@@ -965,6 +1002,7 @@ static void substep1_kernels(orc* o, real dt) {
       if (i > 0) {
         gradp = (P[l] - P[l - nsec]) * 2.0 / (D[l] + D[l - nsec]) * o->invdiffRmed[i];
         gradphi = (Phi[l] - Phi[l - nsec]) * o->invdiffRmed[i];
+        if (o->accurate && o->sys.nb > 0) gradphi += o->star_grad[i];
         vt2 = Vt[l] + Vt[jp] + Vt[l - nsec] + Vt[jp - nsec];
         vt2 = vt2 / 4.0 + o->Rinf[i] * o->OmegaFrame;
         vt2 = vt2 * vt2;
@@ -1818,6 +1856,7 @@ void orc_destroy(orc* o) {
   free(o->Kr_hat);
   free(o->Kt_hat);
   free(o->cbuf0);
+  free(o->star_grad);
   free(o->cbuf1);
   free(o);
 }
@@ -1869,6 +1908,29 @@ void orc_get_fields_f32(const orc* o, float* dens, float* vrad, float* vtheta, f
   cp_out(energy, o->Energy, n);
   cp_out(temperature, o->Temperature, n);
   cp_out(qplus, o->Qplus, n);
+}
+
+/* The self-gravity accelerations (SG_Accr, SG_Acct; NRAD*NSEC each) of the
+   current density, as compute_selfgravity leaves them (SgMain.cu:23-45).
+   Returns -1 when the run has no self-gravity. */
+int orc_sg_accelerations(orc* o, double* accr, double* acct) {
+  if (!o->p.SelfGravity) return -1;
+  sg_accelerations(o);
+  size_t n = (size_t)o->nrad * o->nsec;
+  for (size_t l = 0; l < n; l++) {
+    accr[l] = o->SG_Accr[l];
+    acct[l] = o->SG_Acct[l];
+  }
+  return 0;
+}
+
+/* Precision mode: 0 the reference's arithmetic (default), 1 accurate.  Call
+   before the first DT (re-tabulates the self-gravity kernel). */
+void orc_set_precision(orc* o, int mode) {
+  o->accurate = mode == 1;
+  if (!o->star_grad) o->star_grad = zr(o->nrad + 1);
+  for (int i = 1; i < o->nrad; i++) o->star_grad[i] = (real)(G / (o->Rmed2[i] * o->Rmed2[i - 1]));
+  if (o->p.SelfGravity) sg_init_kernel(o);
 }
 
 void orc_get_planets(const orc* o, fargo_planets* out) { *out = o->sys; }

@@ -48,6 +48,12 @@ void orc_set_fields_f32(orc* o, const float* dens, const float* vrad, const floa
 void orc_get_fields_f32(const orc* o, float* dens, float* vrad, float* vtheta, float* energy,
                         float* temperature, float* qplus);
 
+/* SG_Accr / SG_Acct of the current density (NRAD*NSEC each, in the
+   build's precision widened to double); -1 without self-gravity. */
+int orc_sg_accelerations(orc* o, double* accr, double* acct);
+/* 0: the reference's arithmetic (default); 1: accurate mode (FP64 star
+   potential gradient, Kahan ring means, FP64 self-gravity kernel table). */
+void orc_set_precision(orc* o, int mode);
 void orc_get_planets(const orc* o, fargo_planets* out);
 void orc_set_planets(orc* o, const fargo_planets* in);
 

@@ -52,6 +52,9 @@ def _lib(prec):
     lib.orc_set_planets.argtypes = [vp, vp]
     lib.orc_get_table.argtypes = [vp, C.c_int, dp]
     lib.orc_set_threads.argtypes = [C.c_int]
+    lib.orc_set_precision.argtypes = [vp, C.c_int]
+    lib.orc_sg_accelerations.restype = C.c_int
+    lib.orc_sg_accelerations.argtypes = [vp, dp, dp]
     lib.orc_real_size.restype = C.c_int
     _libs[prec] = lib
     return lib
@@ -140,6 +143,20 @@ class Oracle:
         gf = np.zeros(4 * dimfxy, np.float64)
         self.lib.orc_disk_force(self.h, x, y, rs, mass, dimfxy, gf.ctypes.data_as(C.POINTER(C.c_double)))
         return gf
+
+    def set_precision(self, mode):
+        """0: the reference's arithmetic; 1: accurate mode."""
+        self.lib.orc_set_precision(self.h, int(mode))
+
+    def sg_accelerations(self):
+        """(accr, acct) of the current density, each (NRAD, NSEC) float64."""
+        n = self.nrad * self.nsec
+        ar, at = np.zeros(n), np.zeros(n)
+        st = self.lib.orc_sg_accelerations(self.h, ar.ctypes.data_as(C.POINTER(C.c_double)),
+                                           at.ctypes.data_as(C.POINTER(C.c_double)))
+        if st != 0:
+            raise RuntimeError("no self-gravity in this run")
+        return ar.reshape(self.nrad, self.nsec), at.reshape(self.nrad, self.nsec)
 
     def table(self, which):
         out = np.zeros(self.nrad + 1, np.float64)

@@ -14,8 +14,16 @@
  *   FARGO_REF_NOISE_AMP   noise amplitude (default 1e-3).
  *   FARGO_REF_DUMP        path prefix: <prefix>nshift.bin gets, per hydro
  *                         substep, the substep dt (double) and Nshift[NRAD]
- *                         (int32) right after Transport; <prefix>algogas.txt
- *                         gets the wall time of every AlgoGas call.
+ *                         (int32) right after Transport (a device-to-host
+ *                         copy and a file write per substep: golden data
+ *                         only, never in a timed run); <prefix>algogas.txt
+ *                         gets the line of every AlgoGas call (below).
+ *   FARGO_REF_TIMES       file that gets, for every AlgoGas call, the line
+ *                         "<iteration> <wall seconds> <substeps>".  The
+ *                         substep count is a host counter that the Transport
+ *                         hook increments (one Transport call per substep):
+ *                         no device copy and no I/O inside AlgoGas, so the
+ *                         timed call is the reference's own.
  */
 #include "Main.cuh"
 #include <time.h>
@@ -61,9 +69,12 @@ static FILE* dump_file(const char* suffix, const char* mode) {
   return fopen(name, mode);
 }
 
+static long transport_calls = 0;
+
 __host__ void fargo_hook_Transport(float* Dens, float* Vrad, float* Vtheta, float* Energy, float* Label,
                                    float dt) {
   Transport(Dens, Vrad, Vtheta, Energy, Label, dt);
+  transport_calls++;
   static FILE* f = NULL;
   static int opened = 0;
   if (!opened) {
@@ -85,9 +96,11 @@ __host__ void fargo_hook_AlgoGas(Force* force, float* Dens, float* Vrad, float* 
   static FILE* f = NULL;
   static int opened = 0;
   if (!opened) {
-    f = dump_file("algogas.txt", "w");
+    const char* times = getenv("FARGO_REF_TIMES");
+    f = times ? fopen(times, "w") : dump_file("algogas.txt", "w");
     opened = 1;
   }
+  long calls0 = transport_calls;
   cudaDeviceSynchronize();
   struct timespec t0, t1;
   clock_gettime(CLOCK_MONOTONIC, &t0);
@@ -96,7 +109,7 @@ __host__ void fargo_hook_AlgoGas(Force* force, float* Dens, float* Vrad, float* 
   clock_gettime(CLOCK_MONOTONIC, &t1);
   double s = (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
   if (f) {
-    fprintf(f, "%d %.9f\n", iteracion, s);
+    fprintf(f, "%d %.9f %ld\n", iteracion, s, transport_calls - calls0);
     fflush(f);
   }
 }

@@ -10,8 +10,9 @@ see oracle/ref/ref_hooks.cu).  This script runs it and packs the outputs:
 
 `collect` writes tests/golden/<case>.npz with the reference's output fields
 after 0 and NDT time steps (dens/vrad/vtheta/energy/temperature dumps,
-Output.cu:104-170), the per-substep dt and Nshift, the bigplanet and tqwk
-log lines (Output.cu:70-88, Force.cu:76-138) and used_rad.dat.
+Output.cu:104-170; only after NDT steps for grids of BIG cells or more), the
+per-substep dt and Nshift, the bigplanet and tqwk log lines
+(Output.cu:70-88, Force.cu:76-138) and used_rad.dat.
 """
 import os
 import subprocess
@@ -47,7 +48,30 @@ def cases():
     p, pl = configs.small("iso", 128, 256)
     p = dict(p, InnerBoundary="OPEN")
     out["ref_open_iso_128x256"] = (p, pl, SEED + 4, NDT)
+    # the benchmark configurations at their own size: C2 (adiabatic, alpha
+    # viscosity, two live planets) and the largest disk size of the C4 sweep
+    # (the sweep's first 512-ring disk, with the noise seed the sweep gives it)
+    p, pl = configs.c2()
+    p = dict(p, WriteEnergy="YES")
+    out["ref_c2_256x768"] = (p, pl, SEED + 5, NDT)
+    k, (p, pl) = c4_disk(512)
+    out["ref_c4d%02d_512x1536" % k] = (p, pl, SEED + k, NDT)
     return out
+
+
+def c4_disk(nrad):
+    """(index, (params, planets)) of the first disk of the 64-disk sweep with
+    `nrad` rings."""
+    for k, d in enumerate(configs.c4(64, seed=42)):
+        if int(d[0]["Nrad"]) == nrad:
+            return k, d
+    raise ValueError(nrad)
+
+
+# fixtures of this many cells or more store only the fields after NDT DTs
+# (the initial fields are rebuilt from the parameters and the seed, and the
+# small cases already pin that initialisation to the reference's)
+BIG = 150000
 
 
 def _selected(names):
@@ -68,7 +92,7 @@ def run(rawdir, names=()):
         if seed is not None:
             env["FARGO_REF_NOISE_SEED"] = str(seed)
         with open(os.path.join(d, "stdout.txt"), "w") as f:
-            r = subprocess.run([exe, "run.par"], cwd=d, env=env, stdout=f, stderr=subprocess.STDOUT, timeout=600)
+            r = subprocess.run([exe, "run.par"], cwd=d, env=env, stdout=f, stderr=subprocess.STDOUT, timeout=1200)
         print(name, "exit", r.returncode)
         status |= r.returncode
     return status
@@ -85,8 +109,11 @@ def collect(rawdir, names=()):
         out = os.path.join(d, "run_out")
         nrad, nsec = int(p["Nrad"]), int(p["Nsec"])
         z = {"nrad": nrad, "nsec": nsec, "ndt": ndt, "seed": -1 if seed is None else seed}
+        big = nrad * nsec >= BIG
         for fld in ("dens", "vrad", "vtheta", "energy", "temperature"):
-            for k in (0, 1):
+            if big and fld == "temperature":
+                continue
+            for k in ((1,) if big else (0, 1)):
                 f = os.path.join(out, fld, "%s%d.dat" % (fld, k))
                 if os.path.exists(f):
                     z["%s%d" % (fld, k)] = _read_field(f, nrad, nsec)
@@ -96,11 +123,11 @@ def collect(rawdir, names=()):
         raw = raw[:nrec * rec].reshape(nrec, rec)
         z["sub_dt"] = raw[:, :8].copy().view(np.float64).reshape(-1)
         z["sub_nshift"] = raw[:, 8:].copy().view(np.int32).reshape(nrec, nrad)
-        big = []
+        rows = []
         for k in range(len(pl)):
             f = os.path.join(out, "bigplanet%d.dat" % k)
-            big.append(np.loadtxt(f, ndmin=2))
-        z["bigplanet"] = np.stack(big)
+            rows.append(np.loadtxt(f, ndmin=2))
+        z["bigplanet"] = np.stack(rows)
         tq = []
         for k in range(len(pl)):
             f = os.path.join(out, "tqwk%d.dat" % k)

@@ -65,3 +65,45 @@ def test_checkpoint_restore_api(gpu):
         assert np.array_equal(a[k], b[k]), k
     pa, pb = d1.planets(), d2.planets()
     assert pa.x[0] == pb.x[0] and pa.y[0] == pb.y[0]
+
+
+def test_driver_output_files_match_reference(gpu, tmp_path):
+    """The drop-in driver on C1 (128x384, no noise) for 10 DTs against the
+    reference's own run of the same .par (tests/golden/ref_c1_128x384.npz):
+    used_rad.dat (SourceEuler.cu:159-171) identical; bigplanet0.dat
+    (Output.cu:70-88) line by line: planet to 1e-6 of its scale, mass,
+    PhysicalTime and OmegaFrame exact, CircumPlanetaryMass to 1e-4;
+    tqwk0.dat (UpdateLog, Force.cu:76-138) torques and powers within 1e-4 of
+    each column's largest value (FP64 force sums here, FP32 tree sums in the
+    reference, of fields within FIELD_TOL); the fields after 10 DTs within
+    FIELD_TOL."""
+    from tests.golden import make_ref_golden as G
+    from tests.helpers import FIELD_TOL, rel_l2
+    z = np.load(os.path.join(HERE, "golden", "ref_c1_128x384.npz"))
+    p, pl, seed, ndt = G.cases()["ref_c1_128x384"]
+    assert seed is None
+    d = str(tmp_path / "c1")
+    p = dict(p, Ntot=str(ndt), Ninterm=str(ndt))
+    configs.materialise(p, pl, d, "run", relative=True)
+    _run(["run.par"], d)
+    out = os.path.join(d, "run_out")
+    used = np.loadtxt(os.path.join(out, "used_rad.dat"))
+    assert np.array_equal(used, z["used_rad"])
+    big = np.loadtxt(os.path.join(out, "bigplanet0.dat"), ndmin=2)
+    ref = z["bigplanet"][0]
+    assert big.shape == ref.shape
+    for c in (1, 2, 3, 4):
+        assert np.abs(big[:, c] - ref[:, c]).max() <= 1e-6 * np.abs(ref[:, c]).max(), c
+    for c in (0, 5, 6, 7, 8):
+        assert np.array_equal(big[:, c], ref[:, c]), c
+    assert np.allclose(big[:, 9], ref[:, 9], rtol=1e-4, atol=0)
+    tq = np.loadtxt(os.path.join(out, "tqwk0.dat"), ndmin=2)
+    rq = z["tqwk"][0]
+    assert tq.shape == rq.shape
+    assert np.array_equal(tq[:, 0], rq[:, 0]) and np.array_equal(tq[:, 9], rq[:, 9])
+    for c in range(1, 9):
+        assert np.abs(tq[:, c] - rq[:, c]).max() <= 1e-4 * np.abs(rq[:, c]).max(), c
+    nrad, nsec = int(z["nrad"]), int(z["nsec"])
+    for fld in ("dens", "vrad", "vtheta"):
+        a = np.fromfile(os.path.join(out, fld, "%s1.dat" % fld), np.float32).reshape(nrad, nsec)
+        assert rel_l2(a, z[fld + "1"]) <= FIELD_TOL[fld], fld

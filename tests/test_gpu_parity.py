@@ -49,6 +49,10 @@ def _compare(P, d, o, ndt, fields=("dens", "vrad", "vtheta"), tol=TOL, scale=1.0
     pa, pb = planets_dict(d.planets()), planets_dict(o.planets())
     for k in ("x", "y", "vx", "vy"):
         assert planet_err(pa[k], pb[k]) <= planet_rtol, (k, pa[k], pb[k])
+    # CircumPlanetaryMass of planet 0 (SourceEuler.cu:539-553), both summed in FP64
+    if pa["x"].size:
+        m1, m2 = d.scalars()["mdcp1"], o.scalars()["mdcp1"]
+        assert abs(m1 - m2) <= 1e-4 * abs(m2) + 1e-30, (m1, m2)
     return errs
 
 
@@ -199,3 +203,22 @@ def test_autotune_keeps_results(gpu):
     a, b = d1.fields(), d2.fields()
     for k in ("dens", "vrad", "vtheta", "energy"):
         assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("kind,nrad,nsec", [("iso", 64, 192), ("adi", 48, 160), ("sg", 32, 64)])
+def test_accurate_mode_parity(gpu, kind, nrad, nsec):
+    """The accurate precision mode against the oracle's accurate mode (the
+    same restatement with the FP64 star-potential gradient, Kahan ring means
+    and the FP64 self-gravity kernel): integer outcomes exact, fields within
+    FIELD_TOL."""
+    P, L, _ = small(kind, nrad, nsec)
+    d = Disk(P, L)
+    d.set_precision(1)
+    f0 = d.fields()
+    d.init_state(dens=noise.perturb_density(f0["dens"].reshape(-1), P.NRAD, P.NSEC, SEED))
+    g = d.fields()
+    o = Oracle(P, L)
+    o.set_precision(1)
+    o.set_fields(dens=g["dens"], vrad=g["vrad"], vtheta=g["vtheta"], energy=g["energy"])
+    fields = ("dens", "vrad", "vtheta", "energy") if kind == "adi" else ("dens", "vrad", "vtheta")
+    _compare(P, d, o, 5, fields=fields, planet_rtol=1e-5 if kind != "iso" else 1e-9)

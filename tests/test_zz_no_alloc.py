@@ -6,9 +6,10 @@ Surf, Rmed) and may not allocate device memory in the middle of a step,
 because they manage device memory themselves or cannot afford cudaMalloc's
 device-wide synchronisation.  It takes no context and uses only a fixed
 static scratch array.  Two calls in a row must each agree with the
-context-based entry point within the disk-force tolerance of the parity
-tests, leave free device memory unchanged, and an NRAD beyond the scratch
-must be refused with a clear message.
+context-based entry point and with the CPU oracle within the disk-force
+tolerance of the parity tests; the second call must leave free device
+memory unchanged, and an NRAD beyond the scratch must be refused with a
+clear message.
 
 The file name makes pytest collect it last."""
 import ctypes as C
@@ -19,6 +20,7 @@ import torch
 
 from cudaprotoplanetarydisksfloat_b200 import Disk, grid_radii, noise
 from cudaprotoplanetarydisksfloat_b200._abi import FARGO_DIMFXY, FARGO_NOALLOC_MAXRAD, lib
+from oracle.oracle import Oracle
 from tests.helpers import SEED, rel_l2, small
 
 pytestmark = pytest.mark.gpu
@@ -60,18 +62,23 @@ def test_noalloc_disk_force_matches_context_entry_point(gpu):
     d.init_state(dens=noise.perturb_density(f0["dens"].reshape(-1), P.NRAD, P.NSEC, SEED))
     d.advance(2)
     T = _device_arrays(d, P)
+    # the CPU oracle on the same density (the checker of every disk force)
+    o = Oracle(P, L)
+    o.set_fields(dens=d.fields()["dens"])
     torch.cuda.synchronize()
     bodies = [(1.0, 0.0, 0.03, 1e-3), (0.3, -0.9, 0.05, 3e-4)]
-    free = []
-    for x, y, rs, m in bodies:
+    for n, (x, y, rs, m) in enumerate(bodies):
+        before = torch.cuda.mem_get_info(0)[0]
         st, got, msg = _noalloc(T, P.NRAD, P.NSEC, x, y, rs, m)
+        after = torch.cuda.mem_get_info(0)[0]
         assert st == 0, msg
-        free.append(torch.cuda.mem_get_info(0)[0])
+        if n == 1:
+            # the second call (set-up done by the first) allocates nothing
+            assert after == before
         want = d.disk_force(x, y, rs, m)
         assert rel_l2(got, want) <= 1e-6
         assert np.allclose(got, want, rtol=1e-5, atol=1e-6 * np.abs(want).max())
-    # the second call (set-up done by the first) left free device memory as it was
-    assert free[1] == free[0]
+        assert rel_l2(got, o.disk_force(x, y, rs, m)) <= 1e-6
     d.close()
 
 
