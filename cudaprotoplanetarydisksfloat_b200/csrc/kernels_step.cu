@@ -1918,6 +1918,82 @@ size_t fargo_transport_smem_bytes(int adiabatic) {
 }
 static_assert((kPad * 4) % 16 == 0 && (kRow * 4) % 16 == 0, "staged rows 16-byte aligned");
 
+// One van Leer pass of OneWindTheta on the window (see sweep_ring).  kind 0:
+// every point's own velocity v[k] (the residual sweep); kind 1 / 2: one
+// velocity vu for the whole ring (the constant-residual sweep), whose
+// interfaces all take their upwind value from the left (1: vu dt > 0) or
+// from the right (2), at the same distance h: no per-point selects.
+template <int nq, int kind>
+__device__ __forceinline__ void sweep_pass(float (&q)[nq][8], const float (&v)[8], float vu, float dt,
+                                           float dxtheta, float invdxtheta, float invsurf, float dxrad) {
+  auto slope = [&](float wm, float w0, float wp) -> float {
+    float dqm = (w0 - wm);
+    float dqp = (wp - w0);
+    if (fm(dqp, dqm) > 0.0f) return fm(__fdividef(fm(dqp, dqm), dqp + dqm), invdxtheta);
+    return 0.0f;
+  };
+  // upwind side of each point's left interface and the distance to it:
+  // ksi > 0 takes point k-1 at dxtheta - ksi, else point k at -(dxtheta + ksi)
+  float vv[8], rr[8], S[8], GS[8], sD[8], h[8];
+  unsigned up = 0;
+  const float ksu = fm(vu, dt);
+  const float hu = (kind == 1) ? dxtheta - ksu : dxtheta + ksu;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    vv[k] = (kind == 0) ? v[k] : vu;
+    S[k] = q[nq - 1][k];
+    rr[k] = __fdividef(1.0f, S[k] + 1e-20f);
+    if (kind == 0) {
+      const float ksi = fm(vv[k], dt);
+      if (ksi > 0.0f) up |= 1u << k;
+      h[k] = (ksi > 0.0f) ? dxtheta - ksi : dxtheta + ksi;
+    } else {
+      h[k] = hu;
+    }
+  }
+  auto is_left = [&](int k) -> bool { return kind == 0 ? ((up >> k) & 1u) != 0 : kind == 1; };
+  const float Sl = __shfl_up_sync(0xffffffffu, S[7], 1);
+  const float Sr = __shfl_down_sync(0xffffffffu, S[0], 1);
+#pragma unroll
+  for (int k = 0; k < 8; k++) GS[k] = slope(k ? S[k - 1] : Sl, S[k], k < 7 ? S[k + 1] : Sr);
+  const float GSl = (kind == 2) ? 0.0f : __shfl_up_sync(0xffffffffu, GS[7], 1);
+  // DensStar (StarThetaKernel2 on the density); a - fm(h, g) = a + fm(h, -g)
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const bool u = is_left(k);
+    const float su = u ? (k ? S[k - 1] : Sl) : S[k];
+    const float gu = u ? (k ? GS[k - 1] : GSl) : -GS[k];
+    sD[k] = su + fm(h[k], gu);
+  }
+  // every quantity, density last; all quotients use the pre-sweep density
+#pragma unroll
+  for (int c = 0; c < nq; c++) {
+    float W[8], G[8], F[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) W[k] = fm(q[c][k], rr[k]);
+    const float Wl = __shfl_up_sync(0xffffffffu, W[7], 1);
+    const float Wr = __shfl_down_sync(0xffffffffu, W[0], 1);
+#pragma unroll
+    for (int k = 0; k < 8; k++) G[k] = slope(k ? W[k - 1] : Wl, W[k], k < 7 ? W[k + 1] : Wr);
+    const float Gl = (kind == 2) ? 0.0f : __shfl_up_sync(0xffffffffu, G[7], 1);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const bool u = is_left(k);
+      const float wu = u ? (k ? W[k - 1] : Wl) : W[k];
+      const float gu = u ? (k ? G[k - 1] : Gl) : -G[k];
+      const float qr = wu + fm(h[k], gu);
+      F[k] = fm(fm(fm(dxrad, qr), sD[k]), vv[k]);  // flux through the left interface of point k
+    }
+    const float Fr = __shfl_down_sync(0xffffffffu, F[0], 1);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      float varq = F[k];
+      varq -= (k < 7 ? F[k + 1] : Fr);
+      q[c][k] += fm(varq, invsurf);
+    }
+  }
+}
+
 // The residual and constant-residual van Leer sweeps of OneWindTheta
 // (StarThetaKernel, StarThetaKernel2, VanLeerThetaKernel, Kernels.cu:1157-1273)
 // on one ring's window of 256 points, by one warp: lane l holds points
@@ -1928,6 +2004,10 @@ static_assert((kPad * 4) % 16 == 0 && (kRow * 4) % 16 == 0, "staged rows 16-byte
 // a point depends on the points within two of it, so after the two sweeps
 // the values at 4 .. L-5 do not depend on anything outside the window and
 // the edges need no special case (their values are never stored).
+// The second sweep's velocity is the ring's constant residual: one upwind
+// side for the whole ring (a warp-uniform branch), and none of it when that
+// residual is exactly zero (every flux is then zero: the quantities are
+// unchanged, as the reference's q + 0 leaves them).
 template <int nq>
 __device__ __forceinline__ void sweep_ring(float* sRr, float VMed, float vconst, bool fast, float dt,
                                            float dxtheta, float invdxtheta, float invsurf, float dxrad) {
@@ -1943,67 +2023,11 @@ __device__ __forceinline__ void sweep_ring(float* sRr, float VMed, float vconst,
     v[k] = vres;
   }
   if (!fast) vconst = 0.0f;
-  auto slope = [&](float wm, float w0, float wp) -> float {
-    float dqm = (w0 - wm);
-    float dqp = (wp - w0);
-    if (fm(dqp, dqm) > 0.0f) return fm(__fdividef(fm(dqp, dqm), dqp + dqm), invdxtheta);
-    return 0.0f;
-  };
-  for (int sweep = 0; sweep < 2; sweep++) {
-    // upwind side of each point's left interface and the distance to it:
-    // ksi > 0 takes point k-1 at dxtheta - ksi, else point k at -(dxtheta + ksi)
-    float vv[8], rr[8], S[8], GS[8], sD[8], h[8];
-    unsigned up = 0;
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      vv[k] = (sweep == 1) ? vconst : v[k];
-      S[k] = q[nq - 1][k];
-      rr[k] = __fdividef(1.0f, S[k] + 1e-20f);
-      const float ksi = fm(vv[k], dt);
-      if (ksi > 0.0f) up |= 1u << k;
-      h[k] = (ksi > 0.0f) ? dxtheta - ksi : dxtheta + ksi;
-    }
-    const float Sl = __shfl_up_sync(0xffffffffu, S[7], 1);
-    const float Sr = __shfl_down_sync(0xffffffffu, S[0], 1);
-#pragma unroll
-    for (int k = 0; k < 8; k++) GS[k] = slope(k ? S[k - 1] : Sl, S[k], k < 7 ? S[k + 1] : Sr);
-    const float GSl = __shfl_up_sync(0xffffffffu, GS[7], 1);
-    // DensStar (StarThetaKernel2 on the density); a - fm(h, g) = a + fm(h, -g)
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const bool u = (up >> k) & 1u;
-      const float su = u ? (k ? S[k - 1] : Sl) : S[k];
-      const float gu = u ? (k ? GS[k - 1] : GSl) : -GS[k];
-      sD[k] = su + fm(h[k], gu);
-    }
-    // every quantity, density last; all quotients use the pre-sweep density
-#pragma unroll
-    for (int c = 0; c < nq; c++) {
-      float W[8], G[8], F[8];
-#pragma unroll
-      for (int k = 0; k < 8; k++) W[k] = fm(q[c][k], rr[k]);
-      const float Wl = __shfl_up_sync(0xffffffffu, W[7], 1);
-      const float Wr = __shfl_down_sync(0xffffffffu, W[0], 1);
-#pragma unroll
-      for (int k = 0; k < 8; k++) G[k] = slope(k ? W[k - 1] : Wl, W[k], k < 7 ? W[k + 1] : Wr);
-      const float Gl = __shfl_up_sync(0xffffffffu, G[7], 1);
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        const bool u = (up >> k) & 1u;
-        const float wu = u ? (k ? W[k - 1] : Wl) : W[k];
-        const float gu = u ? (k ? G[k - 1] : Gl) : -G[k];
-        const float qr = wu + fm(h[k], gu);
-        F[k] = fm(fm(fm(dxrad, qr), sD[k]), vv[k]);  // flux through the left interface of point k
-      }
-      const float Fr = __shfl_down_sync(0xffffffffu, F[0], 1);
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        float varq = F[k];
-        varq -= (k < 7 ? F[k + 1] : Fr);
-        q[c][k] += fm(varq, invsurf);
-      }
-    }
-  }
+  sweep_pass<nq, 0>(q, v, 0.0f, dt, dxtheta, invdxtheta, invsurf, dxrad);
+  if (fm(vconst, dt) > 0.0f)
+    sweep_pass<nq, 1>(q, v, vconst, dt, dxtheta, invdxtheta, invsurf, dxrad);
+  else if (vconst != 0.0f)
+    sweep_pass<nq, 2>(q, v, vconst, dt, dxtheta, invdxtheta, invsurf, dxrad);
   __syncwarp();
 #pragma unroll
   for (int k = 0; k < 8; k++)
