@@ -6,12 +6,15 @@
 //   WHILE(any disk inside its DT) { one substep }  -> one CUDA graph launch
 // The WHILE node's condition is written by the last kernel of the substep
 // (cudaGraphSetConditional), so the host never waits inside a DT.
+#include <cuda.h>  // CUtensorMap (encoded through the runtime's driver entry point; no libcuda link)
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -135,6 +138,28 @@ fargo_status check_params(fargo_batch* b, const fargo_params* p, const fargo_pla
 }
 
 // Device memory and constant tables of one disk.
+// cuTensorMapEncodeTiled, looked up once through the runtime (null when the
+// driver does not provide it: the transport then stages by cp.async).
+PFN_cuTensorMapEncodeTiled_v12000 tensormap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+// The transport's three tensor maps of one disk (Sigma, v_r, v_theta):
+// 2-D, NSEC columns x rows (NRAD for Sigma and v_theta, NRAD + 1 for v_r
+// with its ghost row), boxes of FARGO_TR_ROW columns x the band's staged
+// rows, FP32, no swizzle, zero fill outside.  Needs NSEC a multiple of 4
+// (16-byte row pitch) and >= 64; D.tmap stays null otherwise.
+fargo_status make_tensor_maps(fargo_batch* b, DiskHost& h, DiskDev& D);
+
 fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   const fargo_params* p = &h.p;
   host_build_tables(p, radii, &h.t);
@@ -223,6 +248,7 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   D.sin_pot = sp;
   D.cos_cell = cc;
   D.sin_cell = sc;
+  if ((st = make_tensor_maps(b, h, D))) return st;
 #define U(ptr, vec)                            \
   if ((st = dupload(b, h, &(ptr), (vec)))) \
     return st;
@@ -240,6 +266,35 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
     st = sg_create(&h.sg, p, h.t, b->stream, &D, b->err);
     if (st) return st;
   }
+  return FARGO_OK;
+}
+
+fargo_status make_tensor_maps(fargo_batch* b, DiskHost& h, DiskDev& D) {
+  D.tmap = nullptr;
+  const int nrad = h.p.NRAD, nsec = h.p.NSEC;
+  if ((nsec & 3) != 0 || nsec < 64) return FARGO_OK;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensormap_encoder();
+  if (!enc) return FARGO_OK;
+  static_assert(sizeof(CUtensorMap) == 128, "three maps at 128-byte strides");
+  CUtensorMap m[3];
+  const float* base[3] = {D.dens, D.vrad, D.vtheta};
+  const int rows[3] = {nrad, nrad + 1, nrad};
+  const int box_rows[3] = {FARGO_TR_ROWS_D, FARGO_TR_ROWS_R, FARGO_TR_ROWS_T};
+  for (int k = 0; k < 3; k++) {
+    cuuint64_t dim[2] = {(cuuint64_t)nsec, (cuuint64_t)rows[k]};
+    cuuint64_t stride[1] = {(cuuint64_t)nsec * sizeof(float)};
+    cuuint32_t box[2] = {FARGO_TR_ROW, (cuuint32_t)box_rows[k]};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(&m[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base[k]), dim, stride, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return FARGO_OK;  // staged by cp.async instead
+  }
+  CUtensorMap* dm = nullptr;
+  fargo_status st = dalloc(b, h, &dm, 3);
+  if (st) return st;
+  CK(cudaMemcpy(dm, m, sizeof(m), cudaMemcpyHostToDevice));
+  D.tmap = dm;
   return FARGO_OK;
 }
 
@@ -641,6 +696,8 @@ fargo_status finish_dts(fargo_batch* b) {
     DiskCtl c = ctl_header(b, d, &e);
     if (e != cudaSuccess) return set_err(b, FARGO_ECUDA, "ctl read: %s", cudaGetErrorString(e));
     if (c.error == 1) return set_err(b, FARGO_ENONFINITE, "disk %d: non-finite or non-positive CFL time step", d);
+    if (c.error == 3)
+      return set_err(b, FARGO_ETIMEOUT, "disk %d: a transport block gave up waiting for its staged rows", d);
     if (c.error == 2)
       return set_err(b, FARGO_ETIMEOUT, "disk %d: the DT needs more than %d substeps (the substep limit)", d,
                      b->disks[d].dev.max_sub);
@@ -1184,7 +1241,7 @@ fargo_status batch_autotune(fargo_batch* b, int reps, int* chosen) {
   if (!b || reps < 1) return FARGO_EINVAL;
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
-  static const int cand[] = {96, 128, 160, 192, 224, 248};
+  static const int cand[] = {96, 128, 160, 192, 224, FARGO_SEG_MAX};
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));

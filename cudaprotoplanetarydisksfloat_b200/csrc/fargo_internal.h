@@ -97,6 +97,10 @@ struct DiskDev {
   int OpenInner, NonReflecting, SloppyCFL, IsDisk;
   int max_sub;  // substeps one DT may take before it stops with FARGO_ETIMEOUT
   int accurate;  // precision mode: 0 the reference's arithmetic, 1 accurate (FARGO_PRECISION_*)
+  // three CUtensorMap (Sigma, v_r, v_theta; 2-D, FARGO_TR_ROW-column boxes)
+  // for the transport's TMA staging, or null (NSEC not a multiple of 4, or
+  // below 64): then the rows are staged by 16- or 4-byte cp.async copies
+  const void* tmap;
   // boundary constants computed on the host as the reference does:
   // pow(Rinf[1], -1.5), pow(Rinf[NRAD-2], -1.5) of NonReflectingBoundary;
   // damping zones and orbital periods of EvanescentBoundary (SideEuler.cu:127-132)
@@ -184,6 +188,15 @@ struct BatchDev {
 #define FARGO_NKERNELS 14  // profiled slots per substep (boundary slots empty for rigid boundaries)
 #define FARGO_SEG_OUT 192  // largest azimuthal transport segment (output sectors per CTA)
 #define FARGO_BAND 8       // rings per transport CTA
+#define FARGO_SEG_MAX 244  // widest segment the autotuner may pick: window + 1 = 253 <= FARGO_TR_ROW
+// Transport staging: each band's input rows are copied into shared memory as
+// rows of FARGO_TR_ROW columns (one TMA box of a 2-D tensor map per field):
+// Sigma and v_theta rings i0-2 .. i0+FARGO_BAND+1, v_r rings i0-2 ..
+// i0+FARGO_BAND+2.
+#define FARGO_TR_ROW 256
+#define FARGO_TR_ROWS_D (FARGO_BAND + 4)
+#define FARGO_TR_ROWS_R (FARGO_BAND + 5)
+#define FARGO_TR_ROWS_T (FARGO_BAND + 4)
 cudaError_t fargo_kernel_attributes(int max_nsec);
 void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s);
 // only_disk >= 0: that disk; -1: every disk still inside its DT

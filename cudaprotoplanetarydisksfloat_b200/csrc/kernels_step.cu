@@ -1730,11 +1730,15 @@ __device__ __forceinline__ void rad_face(const TrView& V, int b, float vr, float
 // i0+kBR+1, v_r rings i0-2 .. i0+kBR+2 (its ghost row NRAD included).
 // Rings outside the disk are zero-filled: they only feed zero slopes and
 // zero interface fluxes, whose values do not depend on them.
-constexpr int kRow = 264;                    // staged row length (>= window + 1, 16-byte multiple)
+constexpr int kRow = FARGO_TR_ROW;           // staged row length (>= window + 1; one TMA box)
 constexpr int kInD = 0, kInR = 12, kInT = 25;  // first staged row of dens, v_r, v_theta
 constexpr int kInRows = 37;
-static_assert(kInR - kInD == FARGO_BAND + 4 && kInT - kInR == FARGO_BAND + 5 &&
-                  kInRows - kInT == FARGO_BAND + 4, "staged rows of one band");
+static_assert(kInR - kInD == FARGO_TR_ROWS_D && kInT - kInR == FARGO_TR_ROWS_R &&
+                  kInRows - kInT == FARGO_TR_ROWS_T, "staged rows of one band");
+static_assert(FARGO_SEG_MAX + 9 <= kRow && (FARGO_SEG_MAX & 3) == 0, "a window fits one staged row");
+static_assert((kInR * kRow * 4) % 128 == 0 && (kInT * kRow * 4) % 128 == 0, "TMA destinations 128-byte aligned");
+// bytes one band's three TMA boxes deliver (zero-filled parts included)
+constexpr unsigned kTmaBytes = 4u * kRow * kInRows;
 
 template <int nq>
 __device__ __forceinline__ RadRow<nq> rad_row_s(const TrView& V, const float* sIn, int r, int k, int p, int g,
@@ -1914,7 +1918,8 @@ __device__ __forceinline__ int pidx(int t) { return t + (t >> 3); }
 
 size_t fargo_transport_smem_bytes(int adiabatic) {
   const int nq = adiabatic ? 6 : 5;
-  return sizeof(float) * ((size_t)kPad * (size_t)(kBR * (nq + 1) + 1) + (size_t)kInRows * kRow);
+  // + 128: the staged rows start on a 128-byte boundary
+  return sizeof(float) * ((size_t)kPad * (size_t)(kBR * (nq + 1) + 1) + (size_t)kInRows * kRow) + 128;
 }
 static_assert((kPad * 4) % 16 == 0 && (kRow * 4) % 16 == 0, "staged rows 16-byte aligned");
 
@@ -2036,11 +2041,58 @@ __device__ __forceinline__ void sweep_ring(float* sRr, float VMed, float vconst,
   __syncwarp();
 }
 
+// ---- TMA staging: mbarrier and bulk tensor copy (one CTA, no cluster) ----
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase of the given parity, polling at most kSpin times (each
+// poll itself blocks for a bounded, hardware-defined time): false when the
+// wait gave up, so that a copy that never lands cannot hang the GPU.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+  constexpr int kSpin = 1 << 20;
+  for (int k = 0; k < kSpin; k++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// 2-D tiled TMA load of one box at coordinates (x, y) of the tensor map
+// (global memory of this GPU) into shared memory, completing on `bar`.
+// x is a column index (multiple of 4: 16 bytes); x and y may be negative or
+// beyond the tensor: those elements are zero-filled.
+__device__ __forceinline__ void tma_load_2d(float* dst, const void* tmap, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // Issue the asynchronous staging of transport item t's input rows (see
-// kRow): 16-byte copies when NSEC and the segment start are multiples of 4
-// (every 4-column chunk then lies inside the ring), else 4-byte copies.
+// kRow).  With the disk's tensor maps (NSEC a multiple of 4, >= 64) one
+// thread issues three TMA box loads (Sigma, v_r, v_theta rows; rings outside
+// the disk come zero-filled) that complete on `bar`, and the call returns
+// true; columns of the window that wrap around the ring are then filled in
+// by tr_fixup once the copies have landed.  Otherwise every thread issues
+// cp.async copies (16-byte when NSEC and the segment start are multiples of
+// 4, so that every 4-column chunk lies inside the ring, else 4-byte), which
+// follow the azimuthal wrap themselves, and the call returns false.  The
+// choice depends only on the item and the disk: it is block-uniform.
 template <int nq>
-__device__ __forceinline__ void tr_stage(const BatchDev& B, const int4* __restrict__ items, int t, float* sIn) {
+__device__ __forceinline__ bool tr_stage(const BatchDev& B, const int4* __restrict__ items, int t, float* sIn,
+                                         uint64_t* bar) {
   const int nak = (nq == 5) ? B.act[1] : B.act[2];
   const int* aoff = (nq == 5) ? B.act_iso_off : B.act_adi_off;
   const int* adisk = (nq == 5) ? B.act_iso_disk : B.act_adi_disk;
@@ -2049,6 +2101,19 @@ __device__ __forceinline__ void tr_stage(const BatchDev& B, const int4* __restri
   const int4 it = items[D.item0 + (t - aoff[a])];
   const int i0 = it.y, g0 = it.z, W = it.w + 9;  // window + 1 columns
   const int nsec = D.nsec, nrad = D.nrad;
+  if (D.tmap && (nsec & 3) == 0 && nsec >= 64 && (g0 & 3) == 0 && (smem_u32(sIn) & 127) == 0) {
+    if (threadIdx.x == 0) {
+      const char* tm = static_cast<const char*>(D.tmap);
+      // the previous item's reads of sIn (generic proxy) are complete (the
+      // block passed a barrier): order them before the copies' writes
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      mbar_expect_tx(bar, kTmaBytes);
+      tma_load_2d(sIn + kInD * kRow, tm, g0 - 4, i0 - 2, bar);
+      tma_load_2d(sIn + kInR * kRow, tm + 128, g0 - 4, i0 - 2, bar);
+      tma_load_2d(sIn + kInT * kRow, tm + 256, g0 - 4, i0 - 2, bar);
+    }
+    return true;
+  }
   const float *dens = D.dens, *vrad = D.vrad, *vth = D.vtheta;
   auto src = [&](int row, int& r, int& lim) -> const float* {
     if (row < kInR) {
@@ -2089,6 +2154,42 @@ __device__ __forceinline__ void tr_stage(const BatchDev& B, const int4* __restri
     }
   }
   cp_async_commit();
+  return false;
+}
+
+// After a TMA staging has landed: the window's columns left of sector 0 or
+// right of sector NSEC-1 were zero-filled by the copy (the tensor map does
+// not wrap); fill them from the other end of the ring, as the reference's
+// periodic azimuth reads them.  At most 4 columns on the left and 5 on the
+// right (the segment lies inside the ring).
+__device__ __forceinline__ void tr_fixup(const DiskDev& D, int4 it, float* sIn) {
+  const int i0 = it.y, g0 = it.z, W = it.w + 9;
+  const int nsec = D.nsec, nrad = D.nrad;
+  const int nl = g0 < 4 ? 4 - g0 : 0;
+  const int nr = max(0, g0 - 4 + W - nsec);
+  const int nw = nl + nr;
+  for (int q = threadIdx.x; q < kInRows * nw; q += kTT) {
+    const int row = q / nw, k = q - row * nw;
+    const int c = k < nl ? k : W - nr + (k - nl);
+    int g = g0 - 4 + c;
+    g = g < 0 ? g + nsec : (g >= nsec ? g - nsec : g);
+    const float* base;
+    int r, lim;
+    if (row < kInR) {
+      r = i0 - 2 + row - kInD;
+      lim = nrad - 1;
+      base = D.dens;
+    } else if (row < kInT) {
+      r = i0 - 2 + row - kInR;
+      lim = nrad;  // the ghost row
+      base = D.vrad;
+    } else {
+      r = i0 - 2 + row - kInT;
+      lim = nrad - 1;
+      base = D.vtheta;
+    }
+    sIn[row * kRow + c] = (r >= 0 && r <= lim) ? __ldg(base + r * nsec + g) : 0.0f;
+  }
 }
 
 // Transport (TransportEuler.cu:24-35) of a band of up to kBR rings i0 ..
@@ -2111,26 +2212,53 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
   extern __shared__ __align__(16) float tr_sm[];
   float* sR = tr_sm;                         // [kBR][nq + 1][kPad] radial results + v_theta
   float* sL = sR + kBR * (nq + 1) * kPad;    // [kPad] mass through the inner edge (OPEN)
-  float* sIn = sL + kPad;                    // [kInRows][kRow] staged input rows
+  // [kInRows][kRow] staged input rows, 128-byte aligned (TMA destination)
+  float* sIn = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sL + kPad) + 127) & ~uintptr_t(127));
   __shared__ int s_jb[kBR];
   __shared__ float s_vmed[kBR], s_vc[kBR];
+  __shared__ __align__(8) uint64_t s_bar;  // completion of the TMA staging
+  __shared__ int s_gaveup;
   const int nak = (nq == 5) ? B.act[1] : B.act[2];
   const int* aoff = (nq == 5) ? B.act_iso_off : B.act_adi_off;
   const int* adisk = (nq == 5) ? B.act_iso_disk : B.act_adi_disk;
   const int nai = nak > 0 ? aoff[nak] : 0;
   const int p = threadIdx.x, warp = p >> 5, lane = p & 31;
-  if ((int)blockIdx.x < nai) tr_stage<nq>(B, items, blockIdx.x, sIn);
+  if (p == 0) {
+    mbar_init(&s_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_gaveup = 0;
+  }
+  __syncthreads();
+  unsigned phase = 0;  // parity of the staging barrier's next phase
+  bool pend = false;   // a TMA staging is in flight
+  if ((int)blockIdx.x < nai) pend = tr_stage<nq>(B, items, blockIdx.x, sIn, &s_bar);
   for (int t = blockIdx.x; t < nai; t += gridDim.x) {
     const int tn = t + gridDim.x;  // this block's next item
     const int a = find_range(aoff, nak, t);
     const DiskDev& D = B.disks[adisk[a]];
+    const int4 it = items[D.item0 + (t - aoff[a])];
+    if (pend) {
+      if (mbar_wait_bounded(&s_bar, phase)) {
+        tr_fixup(D, it, sIn);
+      } else {
+        s_gaveup = 1;
+      }
+    }
     cp_async_wait<0>();
     __syncthreads();  // staged rows visible; the previous item's sweeps are done
+    if (s_gaveup) {
+      // the staged rows never arrived: report it on the disk (the host maps
+      // it to FARGO_ETIMEOUT), wait once more for the copies, and stop
+      if (p == 0) const_cast<DiskCtl*>(D.ctl)->error = 3;
+      mbar_wait_bounded(&s_bar, phase);
+      return;
+    }
+    if (pend) phase ^= 1;
+    pend = false;
     if (!D.IsDisk) {
-      if (tn < nai) tr_stage<nq>(B, items, tn, sIn);
+      if (tn < nai) pend = tr_stage<nq>(B, items, tn, sIn, &s_bar);
       continue;
     }
-    const int4 it = items[D.item0 + (t - aoff[a])];
     const DiskCtl* C = D.ctl;
     const int i0 = it.y, g0 = it.z, S = it.w;
     const int nsec = D.nsec, nrad = D.nrad;
@@ -2157,7 +2285,7 @@ __global__ void __launch_bounds__(kTT, 2) k_transport(BatchDev B, const int4* __
       for (int r = 0; r < nb; r++) o[(r * (nq + 1) + nq) * kPad] = sIn[(kInT + r + 2) * kRow + p];
     }
     __syncthreads();  // radial results complete; the staged rows are free
-    if (tn < nai) tr_stage<nq>(B, items, tn, sIn);
+    if (tn < nai) pend = tr_stage<nq>(B, items, tn, sIn, &s_bar);
     const int r = warp;
     if (r < nb) {
       const int i = i0 + r;

@@ -315,7 +315,7 @@ fargo_status fargo_batch_set_max_substeps(fargo_batch* b, int n);
 fargo_status fargo_set_precision(fargo_ctx* ctx, int mode);
 fargo_status fargo_batch_set_precision(fargo_batch* b, int mode);
 /* (new) Tile autotuner: times the transport kernels on the current state for
-   azimuthal segment widths 96..248 sectors and keeps the fastest (*seg_out).
+   azimuthal segment widths 96..244 sectors and keeps the fastest (*seg_out).
    Call between DTs; the state is not advanced. */
 fargo_status fargo_batch_autotune(fargo_batch* b, int reps, int* seg_out);
 fargo_status fargo_autotune(fargo_ctx* ctx, int reps, int* seg_out);
