@@ -948,6 +948,11 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
         for (int u = 0; u < kG; u++) {
           if (!ok[u]) continue;
           const int ic = ci[u];
+          // a NaN or Inf in the state: a NaN dt2d would be skipped by the
+          // minimum below (as the reference's is) and the step would go on
+          // with it; mark the tile instead, so that the DT stops with
+          // FARGO_ENONFINITE (finite values leave lmin as it is)
+          if (!(fabsf(v0[u]) + fabsf(vr0[u]) + fabsf(dn[u]) + fabsf(csv[u]) <= 3.4028235e38f)) lmin = -1.0f;
           if (ic > 0) {
             const float dxrad = D.Rsup[ic] - D.Rinf[ic];
             const float dxt = D.dxtheta[ic];
@@ -1655,23 +1660,48 @@ __global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
 // van Leer slope of StarRadKernel (Kernels.cu:917-927)
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
 
+// Paired FP32 arithmetic (Blackwell's two-lane FADD2 / FMUL2): each lane
+// rounds to nearest as the scalar operation does, so a pair of quantities
+// goes through one instruction with the same results bit for bit.
+__device__ __forceinline__ float2 bc2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 m2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 a2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 s2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 sel2(bool c, float2 a, float2 b) { return c ? a : b; }
+
 __device__ __forceinline__ float vl_rad_slope(float qm, float q0, float qp, float invdm, float invdp) {
   float dqm = fm(q0 - qm, invdm);
   float dqp = fm(qp - q0, invdp);
   if (fm(dqp, dqm) > 0.0f) return __fdividef(fm(fm(2.0f, dqp), dqm), dqp + dqm);
   return 0.0f;
 }
+// the same for two quantities at once
+__device__ __forceinline__ float2 vl_rad_slope2(float2 qm, float2 q0, float2 qp, float invdm, float invdp) {
+  const float2 dqm = m2(s2(q0, qm), bc2(invdm));
+  const float2 dqp = m2(s2(qp, q0), bc2(invdp));
+  const float2 t = m2(dqp, dqm);
+  const float2 num = m2(m2(bc2(2.0f), dqp), dqm);
+  const float2 den = a2(dqp, dqm);
+  return make_float2(t.x > 0.0f ? __fdividef(num.x, den.x) : 0.0f, t.y > 0.0f ? __fdividef(num.y, den.y) : 0.0f);
+}
 
 // One row sample of the radial half of Transport at column g: the
 // LRMomentaKernel quantities (Kernels.cu:883-896) RadMomP, RadMomM,
 // ThetaMomP, ThetaMomM, [energy], density, and their DivisePolarGridKernel
-// quotients by the density (Kernels.cu:1127-1134).
+// quotients by the density (Kernels.cu:1127-1134).  Quantity c is lane
+// c % 2 of pair c / 2; with an odd count the last pair's second lane is a
+// zero that no result reads.
 template <int nq>
 struct RadRow {
-  float S;      // density
-  float Q[nq];  // quantities, Q[nq-1] = S
-  float W[nq];  // quotients Q / (S + 1e-20)
+  static constexpr int np = (nq + 1) / 2;
+  float S;         // density
+  float2 Q[np];    // quantities, quantity nq-1 = S
+  float2 W[np];    // quotients Q / (S + 1e-20)
 };
+template <int nq>
+__device__ __forceinline__ float lane_of(const float2 (&v)[(nq + 1) / 2], int c) {
+  return (c & 1) ? v[c >> 1].y : v[c >> 1].x;
+}
 
 // The disk fields and ring tables the radial half reads, loaded once per
 // band into registers (the band's shared-memory stores then cannot force
@@ -1683,19 +1713,20 @@ struct TrView {
 };
 
 // van Leer slopes at row r from rows r-1, r, r+1 (StarRadKernel; zero on the
-// first and last ring): g[c] for the quotients, gs for the density.
+// first and last ring): g[] for the quotients, gs for the density.
 template <int nq>
 __device__ __forceinline__ void rad_slopes(const TrView& V, int r, const RadRow<nq>& A, const RadRow<nq>& Bm,
-                                           const RadRow<nq>& Cp, float* g, float& gs) {
+                                           const RadRow<nq>& Cp, float2* g, float& gs) {
+  constexpr int np = RadRow<nq>::np;
   if (r <= 0 || r >= V.nrad - 1) {
 #pragma unroll
-    for (int c = 0; c < nq; c++) g[c] = 0.0f;
+    for (int c = 0; c < np; c++) g[c] = bc2(0.0f);
     gs = 0.0f;
     return;
   }
   const float im = __ldg(V.invdiffRmed + r), ip = __ldg(V.invdiffRmed + r + 1);
 #pragma unroll
-  for (int c = 0; c < nq; c++) g[c] = vl_rad_slope(A.W[c], Bm.W[c], Cp.W[c], im, ip);
+  for (int c = 0; c < np; c++) g[c] = vl_rad_slope2(A.W[c], Bm.W[c], Cp.W[c], im, ip);
   gs = vl_rad_slope(A.S, Bm.S, Cp.S, im, ip);
 }
 
@@ -1704,24 +1735,26 @@ __device__ __forceinline__ void rad_slopes(const TrView& V, int r, const RadRow<
 // the inner edge and beyond the outer ring.
 template <int nq>
 __device__ __forceinline__ void rad_face(const TrView& V, int b, float vr, float dt, const RadRow<nq>& lo,
-                                         const RadRow<nq>& hi, const float* glo, float gslo, const float* ghi,
-                                         float gshi, float* qs, float& ds) {
+                                         const RadRow<nq>& hi, const float2* glo, float gslo, const float2* ghi,
+                                         float gshi, float2* qs, float& ds) {
+  constexpr int np = RadRow<nq>::np;
   const int nrad = V.nrad;
   if (b <= 0 || b >= nrad) {
 #pragma unroll
-    for (int c = 0; c < nq; c++) qs[c] = 0.0f;
+    for (int c = 0; c < np; c++) qs[c] = bc2(0.0f);
     ds = 0.0f;
     return;
   }
   // upwind side by selection (columns differ in sign): vr > 0 takes row b-1
-  // at + h, else row b at -h; a - fm(h, g) = a + fm(h, -g)
+  // at + h, else row b at -h; a - fm(h, g) = a + fm(-h, g)
   const bool pos = vr > 0.0f;
   const float rm = __ldg(V.Rmed + b), rl = __ldg(V.Rmed + b - 1);
   const float rp = (b + 1 <= nrad - 1) ? __ldg(V.Rmed + b + 1) : 0.0f;  // only meets a zero slope
   const float h = pos ? fm(rm - rl - fm(vr, dt), 0.5f) : fm(rp - rm + fm(vr, dt), 0.5f);
+  const float hs = pos ? h : -h;
 #pragma unroll
-  for (int c = 0; c < nq; c++) qs[c] = (pos ? lo.W[c] : hi.W[c]) + fm(h, pos ? glo[c] : -ghi[c]);
-  ds = (pos ? lo.S : hi.S) + fm(h, pos ? gslo : -gshi);
+  for (int c = 0; c < np; c++) qs[c] = a2(sel2(pos, lo.W[c], hi.W[c]), m2(bc2(hs), sel2(pos, glo[c], ghi[c])));
+  ds = (pos ? lo.S : hi.S) + fm(hs, pos ? gslo : gshi);
 }
 
 // The band's input rows staged in shared memory (k_transport): logical row
@@ -1743,20 +1776,24 @@ constexpr unsigned kTmaBytes = 4u * kRow * kInRows;
 template <int nq>
 __device__ __forceinline__ RadRow<nq> rad_row_s(const TrView& V, const float* sIn, int r, int k, int p, int g,
                                                 float Om) {
+  constexpr int np = RadRow<nq>::np;
   const int rc = r < 0 ? 0 : (r > V.nrad - 1 ? V.nrad - 1 : r);
   RadRow<nq> R;
   const float sg = sIn[(kInD + k) * kRow + p];
   const float rm = __ldg(V.Rmed + rc);
   R.S = sg;
-  R.Q[0] = fm(sg, sIn[(kInR + k + 1) * kRow + p]);
-  R.Q[1] = fm(sg, sIn[(kInR + k) * kRow + p]);
-  R.Q[2] = fm(fm(sg, sIn[(kInT + k) * kRow + p + 1] + fm(rm, Om)), rm);
-  R.Q[3] = fm(fm(sg, sIn[(kInT + k) * kRow + p] + fm(rm, Om)), rm);
-  if (nq == 6) R.Q[4] = __ldg(V.energy + rc * V.nsec + g);
-  R.Q[nq - 1] = sg;
+  // RadMomP, RadMomM = Sigma v_r(i+1), Sigma v_r(i)
+  R.Q[0] = m2(bc2(sg), make_float2(sIn[(kInR + k + 1) * kRow + p], sIn[(kInR + k) * kRow + p]));
+  // ThetaMomP, ThetaMomM = Sigma (v_theta(j+1) + r Omega) r, Sigma (v_theta(j) + r Omega) r
+  const float2 vt = make_float2(sIn[(kInT + k) * kRow + p + 1], sIn[(kInT + k) * kRow + p]);
+  R.Q[1] = m2(m2(bc2(sg), a2(vt, bc2(fm(rm, Om)))), bc2(rm));
+  if (nq == 6)
+    R.Q[2] = make_float2(__ldg(V.energy + rc * V.nsec + g), sg);
+  else
+    R.Q[2] = make_float2(sg, 0.0f);
   const float rden = __fdividef(1.0f, sg + 1e-20f);
 #pragma unroll
-  for (int c = 0; c < nq; c++) R.W[c] = fm(R.Q[c], rden);
+  for (int c = 0; c < np; c++) R.W[c] = m2(R.Q[c], bc2(rden));
   return R;
 }
 
@@ -1771,10 +1808,12 @@ template <int nq>
 __device__ __forceinline__ void rad_march_s(const TrView& V, const float* sIn, int ia, int ib, int p, int g,
                                             float dt, float Om, float dtheta, float* out, int ostride_c,
                                             int ostride_r, float* lost0) {
+  constexpr int np = RadRow<nq>::np;
   RadRow<nq> R0 = rad_row_s<nq>(V, sIn, ia - 1, 1, p, g, Om);  // row i-1 for the first slope
   RadRow<nq> R1 = rad_row_s<nq>(V, sIn, ia, 2, p, g, Om);      // row i
   RadRow<nq> R2 = rad_row_s<nq>(V, sIn, ia + 1, 3, p, g, Om);  // row i+1
-  float G0[nq], G1[nq], gs0, gs1, qs[nq], ds;
+  float2 G0[np], G1[np], qs[np];
+  float gs0, gs1, ds;
   {
     RadRow<nq> Rm = rad_row_s<nq>(V, sIn, ia - 2, 0, p, g, Om);
     rad_slopes<nq>(V, ia - 1, Rm, R0, R1, G0, gs0);  // slope at row i-1
@@ -1788,25 +1827,28 @@ __device__ __forceinline__ void rad_march_s(const TrView& V, const float* sIn, i
     const int i = ia + k;
     if (i >= ib) break;
     RadRow<nq> R3 = rad_row_s<nq>(V, sIn, i + 2, k + 4, p, g, Om);
-    float G2[nq], gs2;
+    float2 G2[np], qs1[np];
+    float gs2, ds1;
     rad_slopes<nq>(V, i + 1, R1, R2, R3, G2, gs2);  // slope at row i+1
     const float vr1 = sIn[(kInR + k + 3) * kRow + p];  // row nrad is the zero ghost row
-    float qs1[nq], ds1;
     rad_face<nq>(V, i + 1, vr1, dt, R1, R2, G1, gs1, G2, gs2, qs1, ds1);
     const float Ri = __ldg(V.Rinf + i), Rs = __ldg(V.Rsup + i), iS = __ldg(V.invSurf + i);
     const float fi = fm(dtdth, Ri), fs = fm(dtdth, Rs);
     float* o = out + k * ostride_r;
+    float2 varq[np];
 #pragma unroll
-    for (int c = 0; c < nq; c++) {
-      float varq = fm(fm(fm(fi, qs[c]), ds), vr0);
-      varq -= fm(fm(fm(fs, qs1[c]), ds1), vr1);
-      o[c * ostride_c] = R1.Q[c] + fm(varq, iS);
-      if (c == nq - 1 && i == 0 && lost0) *lost0 = varq;
+    for (int c = 0; c < np; c++) {
+      varq[c] = m2(m2(m2(bc2(fi), qs[c]), bc2(ds)), bc2(vr0));
+      varq[c] = s2(varq[c], m2(m2(m2(bc2(fs), qs1[c]), bc2(ds1)), bc2(vr1)));
+      const float2 r = a2(R1.Q[c], m2(varq[c], bc2(iS)));
+      o[(2 * c) * ostride_c] = r.x;
+      if (2 * c + 1 < nq) o[(2 * c + 1) * ostride_c] = r.y;
     }
+    if (i == 0 && lost0) *lost0 = lane_of<nq>(varq, nq - 1);
     R1 = R2;
     R2 = R3;
 #pragma unroll
-    for (int c = 0; c < nq; c++) {
+    for (int c = 0; c < np; c++) {
       G1[c] = G2[c];
       qs[c] = qs1[c];
     }

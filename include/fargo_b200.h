@@ -289,9 +289,10 @@ fargo_status fargo_batch_set_graph_mode(fargo_batch* b, int use_graph);
 /* (new) Largest number of CFL substeps one DT may take (default
    FARGO_MAX_SUBSTEPS).  A DT that needs more stops after that many substeps
    and fargo_advance* return FARGO_ETIMEOUT; the context stays usable (upload
-   a state and advance again).  A CFL step that is not a positive finite
-   number (a NaN or Inf in the state) stops the DT with FARGO_ENONFINITE in
-   the same way.  Call between DTs. */
+   a state and advance again).  A NaN or Inf in the density, velocities or
+   sound speed (checked on every cell by the CFL kernel at the start of each
+   substep), or a CFL step that is not positive, stops the DT in the same
+   way with FARGO_ENONFINITE.  Call between DTs. */
 fargo_status fargo_set_max_substeps(fargo_ctx* ctx, int n);
 fargo_status fargo_batch_set_max_substeps(fargo_batch* b, int n);
 /* (new) Precision mode of every disk of the context / batch.

@@ -65,7 +65,9 @@ def set_threads(n, prec="f32"):
 
 
 class Oracle:
-    """CPU restatement of one disk; prec 'f32' (reference typing) or 'f64'."""
+    """CPU restatement of one disk; prec 'f32' (reference typing), 'f64', or
+    'f32fma' (the float build with a*b+c fused: a second FP32 build whose
+    distance from 'f32' is the rounding-order floor)."""
 
     def __init__(self, params, planets, prec="f32", radii=None):
         self.lib = _lib(prec)
@@ -97,14 +99,14 @@ class Oracle:
         self.lib.orc_set_fields_f32(self.h, *[None if a is None else a.ctypes.data_as(fp) for a in arrs])
 
     def set_fields_native(self, dens=None, vrad=None, vtheta=None, energy=None):
-        dt = np.float32 if self.prec == "f32" else np.float64
+        dt = np.float32 if self.prec in ("f32", "f32fma") else np.float64
         arrs = [None if a is None else np.ascontiguousarray(a, dt).reshape(-1) for a in
                 (dens, vrad, vtheta, energy)]
         self.lib.orc_set_fields(self.h, *[None if a is None else a.ctypes.data for a in arrs])
 
     def fields(self, native=False):
         n = self.size_grid
-        dt = (np.float32 if self.prec == "f32" else np.float64) if native else np.float32
+        dt = (np.float32 if self.prec in ("f32", "f32fma") else np.float64) if native else np.float32
         out = {k: np.empty(n, dt) for k in ("dens", "vrad", "vtheta", "energy", "temperature", "qplus")}
         if native:
             self.lib.orc_get_fields(self.h, *[out[k].ctypes.data for k in

@@ -49,3 +49,29 @@ def small(kind, nrad=32, nsec=96, **over):
     p, pl = configs.small(kind, nrad, nsec)
     p = dict(p, **over)
     return make(p, pl, kind)
+
+
+def floor_tol(P, L, start, ndt, f32_after, keys=("dens", "vrad", "vtheta", "energy"), precision=0):
+    """Field tolerances of one case, scaled by its own rounding-order floor.
+
+    FIELD_TOL was measured on the small grids; on other physics (the C4
+    sweep's thin, low-alpha disks, C5's first substeps, where v_r is still
+    near zero) two FP32 builds of the same algorithm drift further apart.
+    The floor is measured live: the oracle's FMA-contracted build advanced
+    `ndt` DTs from the same `start` fields as the plain float build, whose
+    result is `f32_after`.  tol[k] = max(FIELD_TOL[k], 2 * rel_l2(fma, f32))."""
+    from oracle.oracle import Oracle
+    o = Oracle(P, L, "f32fma")
+    if precision:
+        o.set_precision(precision)
+    o.set_fields(dens=start["dens"], vrad=start["vrad"], vtheta=start["vtheta"], energy=start["energy"])
+    for _ in range(ndt):
+        o.advance_dt()
+    g = o.fields()
+    o.close()
+    nrad = P.NRAD
+    tol = {}
+    for k in keys:
+        fl = rel_l2(g[k][:nrad], f32_after[k][:nrad]) if np.any(f32_after[k][:nrad]) else 0.0
+        tol[k] = max(FIELD_TOL[k], 2.0 * fl)
+    return tol

@@ -5,11 +5,11 @@ from its unmodified sources (oracle/ref/Makefile.ref) and run on a B200 by
 tests/golden/make_ref_golden.py, on seeded noisy initial conditions.  The
 oracle (float build) restarted from the same parameters must reproduce the
 reference's initial fields, every substep's dt and every ring's FARGO shift
-count exactly, and the fields after 10 DTs within TOL.
-
-TOL is the rounding-order floor between two FP32 builds (FIELD_TOL,
-tests/helpers.py): nvcc contracts a*b+c into fused multiply-adds, the
-oracle's gcc build does not."""
+count exactly, and the fields after 10 DTs within the rounding-order floor
+between two FP32 builds: nvcc contracts a*b+c into fused multiply-adds, the
+oracle's gcc build does not.  The bound is FIELD_TOL (tests/helpers.py) or,
+where this case's own floor is wider (the larger grids), twice the measured
+distance between the oracle's plain and FMA-contracted builds (floor_tol)."""
 import glob
 import os
 
@@ -19,7 +19,7 @@ import pytest
 from cudaprotoplanetarydisksfloat_b200 import noise
 from oracle.oracle import Oracle, set_threads
 from tests.golden import make_ref_golden as G
-from tests.helpers import FIELD_TOL, make, rel_l2
+from tests.helpers import FIELD_TOL, floor_tol, make, rel_l2
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_*.npz")))
@@ -51,6 +51,7 @@ def test_oracle_matches_reference(path):
     for k in ("dens", "vrad", "vtheta"):
         if k + "0" in z:
             assert rel_l2(f0[k][:nrad], z[k + "0"]) <= 1e-7, k
+    start = {k: v.copy() for k, v in f0.items()}
     sub_ns = z["sub_nshift"]
     sub_dt = z["sub_dt"]
     s = 0
@@ -61,7 +62,11 @@ def test_oracle_matches_reference(path):
         assert np.allclose(dt.astype(np.float32), sub_dt[s:s + n].astype(np.float32), rtol=0, atol=0)
         s += n
     f1 = o.fields()
+    # the reference's build fuses multiply-adds, the oracle's float build does
+    # not: bound by this case's floor between the two (floor_tol)
+    tol = floor_tol(P, L, start, ndt, f1, keys=("dens", "vrad", "vtheta", "energy"))
+    tol["temperature"] = max(TOL["temperature"], tol["dens"])
     for k in ("dens", "vrad", "vtheta", "energy", "temperature"):
         if k + "1" in z:
             e = rel_l2(f1[k][:nrad], z[k + "1"])
-            assert e <= TOL[k], (k, e)
+            assert e <= tol[k], (k, e, tol[k])
