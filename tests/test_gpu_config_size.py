@@ -81,8 +81,10 @@ def test_c3_sg_accelerations_vs_fp64(gpu, mode):
     # with the reference's float kernel table part of the axisymmetric
     # density leaks into it (5% at this size); the FP64 table of the
     # accurate mode removes that part, leaving the FP32 FFT's rounding.
-    assert er <= 3e-5
-    assert et <= (0.1 if mode == 0 else 0.02)
+    # measured: reference mode g_r 7.3e-6, g_phi 5.0e-2; accurate mode g_r
+    # 2.0e-7, g_phi 1.4e-4
+    assert er <= (3e-5 if mode == 0 else 1e-6)
+    assert et <= (0.1 if mode == 0 else 1e-3)
     d.close()
 
 
