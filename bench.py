@@ -7,7 +7,9 @@ workload (each disk takes its own CFL substeps inside the DT).
 
 Workloads (--workload):
   c4  (default) 64 isothermal disks of uneven size and physics, batched: one
-      launch per kernel advances all of them (the "batched" form)
+      launch per kernel advances all of them (the "batched" form); the disks
+      are grouped into --groups batches of similar CFL substep counts
+      (measured by one probe DT) and balanced work
   c4plain  the same 64 disks advanced one after another (the "plain" form)
   c1, c2, c3, c5  single disks of the other configurations
 
@@ -244,6 +246,22 @@ def batch_groups(cells, groups, plain):
     return [sorted(g) for g in shard.lpt_partition([int(c) for c in cells], G)]
 
 
+def substep_groups(P, L, cells, probe_groups, G, rank, local):
+    """Batches of disks with similar CFL substep counts (shard.group_by_substeps):
+    one probe DT of every disk, in the cell-balanced batches, gives the counts
+    (outside the timed region; the timed batches start afresh)."""
+    from cudaprotoplanetarydisksfloat_b200 import Batch, shard
+    nsub = np.zeros(len(P), dtype=np.int64)
+    for g in probe_groups:
+        b = Batch([P[d] for d in g], [L[d] for d in g], device=local)
+        noisy_init(b, [P[d] for d in g], [20261203 + 1000 * rank + d for d in g])
+        b.advance(1)
+        for k, d in enumerate(g):
+            nsub[d] = b.scalars(k)["nsub_last_dt"]
+        b.close()
+    return shard.group_by_substeps(cells, nsub, G)
+
+
 def materialise_all(disks, tmp):
     from cudaprotoplanetarydisksfloat_b200 import configs, read_params, read_planets
     P, L = [], []
@@ -275,6 +293,8 @@ def ours(args, world, rank, local, pg):
     cells = np.array([p.NRAD * p.NSEC for p in P], dtype=np.int64)
     plain = args.workload == "c4plain"
     groups = batch_groups(cells, args.groups, plain)
+    if not plain and len(groups) > 1 and args.group_by == "substeps":
+        groups = substep_groups(P, L, cells, groups, args.groups, rank, local)
     gcells = np.array([cells[d] for g in groups for d in g], dtype=np.int64)  # nsub_total() order
     batches = [Batch([P[d] for d in g], [L[d] for d in g], device=local) for g in groups]
     for b, g in zip(batches, groups):
@@ -484,6 +504,8 @@ def ours(args, world, rank, local, pg):
         "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(l1 - l0) * world,
         "wall_s": t_wall, "cells": int(cells.sum()) * world, "disks": len(P) * world,
         "seg_out": sorted(set(seg_out)), "batches": len(batches), "plain": plain_line,
+        "batching": {"by": "one disk per context" if plain else args.group_by,
+                     "disks_per_batch": [len(g) for g in groups]},
     }
 
 
@@ -653,6 +675,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--groups", type=int, default=4,
                     help="concurrent batches the disks of a batched workload are split over")
+    ap.add_argument("--group-by", default="substeps", choices=["substeps", "cells"],
+                    help="batch the disks by similar CFL substep counts (one probe DT) or by cells (LPT)")
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--plain-steps", type=int, default=3,
                     help="DTs of the plain form measured beside the batched C4 line (0: skip)")
@@ -710,6 +734,7 @@ def main():
         line = dict(head, value=r["value"], ms_per_step=r["ms_per_step"],
                     data="synthetic (seeded parameters and density noise)", config=config,
                     tiles={"transport_segment": r["seg_out"], "band_rings": 8, "autotuned": True},
+                    batching=r["batching"],
                     e2e=r["e2e"], roofline=r["roofline"], cpu_baseline=r["cpu_baseline"], clocks=r["clocks"],
                     gpu_launches=r["gpu_launches"])
         if r.get("plain"):

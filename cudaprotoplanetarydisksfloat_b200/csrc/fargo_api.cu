@@ -625,7 +625,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     bd.cell_grid = (int)std::min<long long>(cg, (long long)nsm * 8);
     bd.ring_grid = std::min(bd.nring, nsm * 6);
     bd.item_grid = std::min((int)(theta_iso.size() + theta_adi.size()), nsm * 8);
-    bd.grp_grid = std::min((bd.nring + 31 * n + 31) / 32, nsm * 3);
+    bd.grp_grid = std::min((bd.nring + (FARGO_RM_RINGS - 1) * (n + 1)) / FARGO_RM_RINGS, nsm * 8);
   }
   CK(fargo_kernel_attributes(b->max_nsec));
   {

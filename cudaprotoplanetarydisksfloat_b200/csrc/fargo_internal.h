@@ -172,7 +172,7 @@ struct BatchDev {
   int* act_iso_off;          // [ndisk+1] prefix of their transport items
   int* act_adi_disk;
   int* act_adi_off;
-  int* act_grp_off;          // [ndisk+1] prefix of 32-ring groups of active disks
+  int* act_grp_off;          // [ndisk+1] prefix of FARGO_RM_RINGS-ring groups of active disks
   int* act_tile_off;         // [ndisk+1] prefix of cell tiles (FARGO_QTILE cells) of active disks
   int* act_ctile_off;        // [ndisk+1] prefix of CFL tiles (FARGO_CFL_TILE cells) of active disks
   int* act_vtile_off;        // [ndisk+1] prefix of viscosity tiles (8 x 64 cells) of active disks
@@ -188,6 +188,7 @@ struct BatchDev {
 #define FARGO_NKERNELS 14  // profiled slots per substep (boundary slots empty for rigid boundaries)
 #define FARGO_SEG_OUT 192  // largest azimuthal transport segment (output sectors per CTA)
 #define FARGO_BAND 8       // rings per transport CTA
+#define FARGO_RM_RINGS 8   // rings per ring-mean CTA (serial FP32 chain per ring)
 #define FARGO_SEG_MAX 244  // widest segment the autotuner may pick: window + 1 = 253 <= FARGO_TR_ROW
 // Transport staging: each band's input rows are copied into shared memory as
 // rows of FARGO_TR_ROW columns (one TMA box of a 2-D tensor map per field):

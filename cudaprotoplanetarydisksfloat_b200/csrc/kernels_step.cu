@@ -1864,41 +1864,46 @@ __device__ __forceinline__ void rad_march_s(const TrView& V, const float* sIn, i
 // of ConditionCFLKernel1D (Kernels.cu:352-356) and of
 // ComputeAverageThetaVelocitiesKernel (Kernels.cu:1184-1198) sum them: the
 // FARGO shift floor(Ntilde + 0.5) and the CFL dt depend on the last bit.
-// One CTA takes 32 rings of one disk.  All its threads stream the rings
-// through shared memory in chunks of kRMW sectors (coalesced, 32 loads in
+// One CTA takes kRMR rings of one disk.  All its threads stream the rings
+// through shared memory in chunks of kRMW sectors (coalesced, kRMR loads in
 // flight per thread) while warp 0, lane r owning ring i0 + r, adds the
-// previous chunk's row in order.
+// previous chunk's row in order.  The chain of one ring (NSEC dependent
+// additions) bounds the kernel, so a few rings per CTA spread the chains over
+// every SM in one wave.
 //   mode 0: vmoy[i] (CFL, substep start)
 //   mode 1: transport VMed, Nshift and constant residual (OneWindTheta,
 //           TransportEuler.cu:171-219 with ComputeConstantResidualKernel,
 //           Kernels.cu:1201-1232), and the Nshift log of the DT.
-constexpr int kRMT = 256;  // threads
-constexpr int kRMW = 256;  // sectors per chunk
-size_t fargo_ring_mean_smem_bytes() { return sizeof(float) * 2 * 32 * (kRMW + 1); }
+constexpr int kRMT = 256;             // threads
+constexpr int kRMW = 256;             // sectors per chunk
+constexpr int kRMR = FARGO_RM_RINGS;  // rings per CTA (one serial chain each)
+static_assert(kRMR <= 32, "one lane of warp 0 per ring");
+size_t fargo_ring_mean_smem_bytes() { return sizeof(float) * 2 * kRMR * (kRMW + 1); }
 template <int mode>
 __global__ void __launch_bounds__(kRMT) k_ring_mean(BatchDev B) {
-  extern __shared__ float rm_sm[];  // [2][32][kRMW + 1]
+  extern __shared__ float rm_sm[];  // [2][kRMR][kRMW + 1]
   const int na = B.act[0];
   const int ng = na > 0 ? B.act_grp_off[na] : 0;
   const int tid = threadIdx.x, lane = tid & 31;
   for (int g = blockIdx.x; g < ng; g += gridDim.x) {
     const int a = find_range(B.act_grp_off, na, g);
     const DiskDev& D = B.disks[B.act_disk[a]];
-    const int i0 = (g - B.act_grp_off[a]) * 32;
+    const int i0 = (g - B.act_grp_off[a]) * kRMR;
     const int nsec = D.nsec, nrad = D.nrad;
-    const int nr = min(32, nrad - i0);
+    const int nr = min(kRMR, nrad - i0);
     const float* base = D.vtheta + (size_t)i0 * nsec;
     const int nchunk = (nsec + kRMW - 1) / kRMW;
-    float r[32];
+    float r[kRMR];
     auto load = [&](int c) {
       const int col = c * kRMW + tid;
 #pragma unroll
-      for (int k = 0; k < 32; k++) r[k] = (c < nchunk && k < nr && col < nsec) ? __ldg(base + (size_t)k * nsec + col) : 0.0f;
+      for (int k = 0; k < kRMR; k++)
+        r[k] = (c < nchunk && k < nr && col < nsec) ? __ldg(base + (size_t)k * nsec + col) : 0.0f;
     };
     auto store = [&](int c) {
-      float* buf = rm_sm + (c & 1) * 32 * (kRMW + 1);
+      float* buf = rm_sm + (c & 1) * kRMR * (kRMW + 1);
 #pragma unroll
-      for (int k = 0; k < 32; k++) buf[k * (kRMW + 1) + tid] = r[k];
+      for (int k = 0; k < kRMR; k++) buf[k * (kRMW + 1) + tid] = r[k];
     };
     float moy = 0.0f;
     KahanSum ks;  // accurate mode
@@ -1909,8 +1914,8 @@ __global__ void __launch_bounds__(kRMT) k_ring_mean(BatchDev B) {
     __syncthreads();
     for (int c = 0; c < nchunk; c++) {
       load(c + 1);
-      if (tid < 32) {
-        const float* row = rm_sm + (c & 1) * 32 * (kRMW + 1) + lane * (kRMW + 1);
+      if (tid < kRMR) {
+        const float* row = rm_sm + (c & 1) * kRMR * (kRMW + 1) + lane * (kRMW + 1);
         const int w = min(kRMW, nsec - c * kRMW);
         if (acc) {
           for (int k = 0; k < w; k++) ks.add(row[k]);
@@ -2437,7 +2442,7 @@ __device__ void compact_active(const BatchDev& B) {
         B.act_vtile_off[na] = vt;
         cc += s_cells[k];
         rr += s_nrad[k];
-        gg += (s_nrad[k] + 31) / 32;
+        gg += (s_nrad[k] + FARGO_RM_RINGS - 1) / FARGO_RM_RINGS;
         tt += s_tiles[k];
         ct += s_ctiles[k];
         vt += s_vtiles[k];

@@ -36,6 +36,40 @@ def lpt_partition(weights, nparts):
     return [sorted(p) for p in parts]
 
 
+def group_by_substeps(cells, nsub, ngroups):
+    """Batches of disks with similar substep counts and balanced work.
+
+    A batch advances until its slowest disk ends its DT, so a disk that
+    needs few CFL substeps idles through the rest of its batch's DT.  Sorted
+    by substep count (ties by index) and cut into `ngroups` contiguous runs,
+    the disks of one batch need about as many substeps as each other; the
+    cut points are chosen greedily so that the runs' work (sum of cells x
+    substeps) is as even as possible (the batches advance concurrently on
+    their own streams).  Returns ngroups sorted lists of disk indices."""
+    cells = np.asarray(cells, dtype=np.float64)
+    nsub = np.asarray(nsub, dtype=np.float64)
+    n = len(cells)
+    if ngroups < 1:
+        raise ValueError("ngroups must be >= 1")
+    ngroups = min(ngroups, n)
+    order = sorted(range(n), key=lambda i: (nsub[i], i))
+    w = (cells * nsub)[order]
+    cum = np.concatenate([[0.0], np.cumsum(w)])
+    total = cum[-1]
+    cuts = [0]
+    for g in range(1, ngroups):
+        target = total * g / ngroups
+        k = int(np.searchsorted(cum, target))
+        # the nearer of the two candidate cut points, keeping every run non-empty
+        if k > 0 and abs(cum[k - 1] - target) <= abs(cum[min(k, n)] - target):
+            k -= 1
+        k = max(k, cuts[-1] + 1)
+        k = min(k, n - (ngroups - g))
+        cuts.append(k)
+    cuts.append(n)
+    return [sorted(order[cuts[g]:cuts[g + 1]]) for g in range(ngroups)]
+
+
 def disk_cells(params):
     return [int(p.NRAD) * int(p.NSEC) for p in params]
 

@@ -116,3 +116,24 @@ def test_bench_batch_groups_cover_and_balance():
         assert sorted(d for p in parts for d in p) == list(range(64))
         loads = [sum(cells[d] for d in p) for p in parts]
         assert max(loads) <= sum(cells) / g + max(cells)
+
+
+def test_group_by_substeps_cover_contiguous_balanced():
+    """Batches by substep count: every disk once, each batch a contiguous run
+    of the substep order, work (cells x substeps) evenly split."""
+    from cudaprotoplanetarydisksfloat_b200 import shard
+    rng = np.random.default_rng(3)
+    nrad = rng.choice([128, 192, 256, 384, 512], 64)
+    cells = nrad * 3 * nrad
+    nsub = rng.integers(7, 55, 64)
+    for G in (1, 2, 4, 6):
+        gs = shard.group_by_substeps(cells, nsub, G)
+        assert len(gs) == G and all(gs)
+        assert sorted(sum(gs, [])) == list(range(64))
+        # contiguous in substep order: no batch's range of counts overlaps another's interior
+        spans = sorted((min(nsub[g]), max(nsub[g])) for g in gs)
+        for (a0, a1), (b0, b1) in zip(spans, spans[1:]):
+            assert a1 <= b0
+        work = [float((cells[g] * nsub[g]).sum()) for g in gs]
+        # at most one disk's work above the even share
+        assert max(work) <= sum(work) / G + float((cells * nsub).max())
