@@ -487,7 +487,11 @@ def ours(args, world, rank, local, pg):
                 "step_frac": round(value * b_sub / (peak * 1e9), 4),
                 "substep_alg_bytes_per_cell": b_sub, "sg_alg_bytes_per_cell": B_SG.get(args.workload, 0),
                 "kernel_ms_share": {names[k]: round(float(ms_k[k] / ms_k.sum()), 4) for k in range(nk)
-                                    if ms_k[k] > 0}}
+                                    if ms_k[k] > 0},
+                # the batches' kernels one after another (host loop, one batch at a
+                # time): against ms_per_step it shows how much the concurrent
+                # batches overlap
+                "kernel_ms_per_step_serial": round(float(ms_k.sum()) / args.profile_steps, 3)}
 
     for b in batches:
         b.close()
