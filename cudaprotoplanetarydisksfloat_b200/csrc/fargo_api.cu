@@ -257,6 +257,7 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   U(D.invdiffRmed, h.t.invdiffRmed) U(D.dxtheta, h.t.dxtheta) U(D.supp_torque, h.t.supp_torque)
   U(D.SigmaMed, h.t.SigmaMed) U(D.SigmaInf, h.t.SigmaInf) U(D.EnergyMed, h.t.EnergyMed)
   U(D.CoolingTimeMed, h.t.CoolingTimeMed) U(D.pow15, h.t.pow15) U(D.star_grad, h.t.star_grad)
+  U(D.cfl_rdr, h.t.cfl_rdr) U(D.cfl_rdt, h.t.cfl_rdt) U(D.cfl_rmd, h.t.cfl_rmd)
 #undef U
   // QplusMed is filled at initialisation (it needs the viscosity)
   float* qpm;

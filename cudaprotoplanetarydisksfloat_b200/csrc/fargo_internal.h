@@ -127,6 +127,7 @@ struct DiskDev {
   const float *dxtheta, *supp_torque, *SigmaMed, *SigmaInf, *EnergyMed, *CoolingTimeMed, *QplusMed;
   const double* pow15;   // pow(Rmed[i], 1.5) from the host (FViscosity)
   const float* star_grad;  // accurate mode: G / (Rmed[i] Rmed[i-1]) (FP64 radii)
+  const float *cfl_rdr, *cfl_rdt, *cfl_rmd;  // RN(1/(Rsup-Rinf)), RN(1/dxtheta), RN(1/min of the two)
   float* visc;           // viscosity_array of this substep
   float* cs_ring;        // isothermal sound speed per ring
   float* csmean;         // GLOBAL_bufarray: ring-mean sound speed

@@ -16,6 +16,10 @@ struct HostTables {
   // (-G/Rmed[i] + G/Rmed[i-1]) / (Rmed[i] - Rmed[i-1]) = G / (Rmed[i] Rmed[i-1]),
   // from the FP64 radii, rounded once
   std::vector<float> star_grad;
+  // the CFL's per-ring divisors Rsup-Rinf, dxtheta and their minimum
+  // (ConditionCFLKernel2D1, Kernels.cu:1380-1400), as correctly rounded FP32
+  // reciprocals: the quotients are then formed by Markstein's method
+  std::vector<float> cfl_rdr, cfl_rdt, cfl_rmd;
   float invdphi = 0, onethird = 0;
 };
 

@@ -39,6 +39,9 @@ void host_build_tables(const fargo_params* p, const double* radii_in, HostTables
   for (auto* v : f1) v->assign(NRAD + 1, 0.0f);  // entries the reference leaves unset are 0
   t->pow15.assign(NRAD + 1, 0.0);
   t->star_grad.assign(NRAD + 1, 0.0f);
+  t->cfl_rdr.assign(NRAD + 1, 0.0f);
+  t->cfl_rdt.assign(NRAD + 1, 0.0f);
+  t->cfl_rmd.assign(NRAD + 1, 0.0f);
   const std::vector<double>& R2 = t->Radii2;
   const std::vector<double>& M2 = t->Rmed2;
   for (int i = 0; i <= NRAD; i++) t->Radii[i] = (float)R2[i];
@@ -66,6 +69,16 @@ void host_build_tables(const fargo_params* p, const double* radii_in, HostTables
   for (int i = 0; i < NRAD; i++) {
     t->supp_torque[i] = p->IMPOSEDDISKDRIFT * 0.5 * std::pow(t->Rmed[i], -2.5 + p->SIGMASLOPE);
     t->dxtheta[i] = 2.0 * PI / (float)NSEC * t->Rmed[i];
+  }
+  // RN(1/d) in FP32: the FP64 quotient rounded to float (double rounding is
+  // innocuous for a quotient of floats: 53 >= 2*24 + 2)
+  for (int i = 0; i < NRAD; i++) {
+    const float dxr = t->Rsup[i] - t->Rinf[i];  // the device's float subtraction
+    const float dxt = t->dxtheta[i];
+    const float md = (dxt < dxr) ? dxt : dxr;  // min2(dxrad, dxtheta)
+    t->cfl_rdr[i] = (float)(1.0 / (double)dxr);
+    t->cfl_rdt[i] = (float)(1.0 / (double)dxt);
+    t->cfl_rmd[i] = (float)(1.0 / (double)md);
   }
   // FillSigma / FillEnergy / FillCoolingTime (Theo.cu:23-61), Sigma(r)
   for (int i = 0; i < NRAD; i++) {

@@ -43,6 +43,7 @@
 #include <type_traits>
 
 #include "fargo_internal.h"
+#include "fast_div.cuh"
 
 #define PI_D FARGO_PI
 #define CVNR FARGO_CVNR
@@ -958,9 +959,12 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
             const float dxt = D.dxtheta[ic];
             float cs = csv[u];
             float vres = D.FastTransport ? v0[u] - D.vmoy[ic] : v0[u];  // vmoy: k_ring_mean<0>
-            float invdt1 = cs / (min2(dxrad, dxt));
-            float invdt2 = fabsf(vr0[u]) / dxrad;
-            float invdt3 = fabsf(vres) / dxt;
+            // the IEEE quotients by the ring's divisors, from their correctly
+            // rounded reciprocals (Markstein's method, fast_div.cuh)
+            const float rdr = D.cfl_rdr[ic], rdt = D.cfl_rdt[ic];
+            float invdt1 = div_by_recip(cs, min2(dxrad, dxt), D.cfl_rmd[ic]);
+            float invdt2 = div_by_recip(fabsf(vr0[u]), dxrad, rdr);
+            float invdt3 = div_by_recip(fabsf(vres), dxt, rdt);
             float dvr = vrp[u] - vr0[u];
             float dvt = vtp[u] - v0[u];
             if (dvr >= 0.0)
@@ -971,7 +975,7 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
               dvt = 1e-10;
             else
               dvt = -dvt;
-            float invdt4 = max2(dvr / dxrad, dvt / dxt);
+            float invdt4 = max2(div_by_recip(dvr, dxrad, rdr), div_by_recip(dvt, dxt, rdt));
             invdt4 *= 4.0 * CVNR * CVNR;
             // CFLSECURITY / sqrtf(..) divides in double; with CFLSECURITY = 0.5
             // that is 0.5 * the float IEEE reciprocal, bit for bit (see below)
