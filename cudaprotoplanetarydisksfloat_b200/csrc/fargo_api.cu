@@ -272,43 +272,30 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
 
 fargo_status make_tensor_maps(fargo_batch* b, DiskHost& h, DiskDev& D) {
   D.tmap = nullptr;
-  D.vtmap = nullptr;
   const int nrad = h.p.NRAD, nsec = h.p.NSEC;
   if ((nsec & 3) != 0 || nsec < 64) return FARGO_OK;
   PFN_cuTensorMapEncodeTiled_v12000 enc = tensormap_encoder();
   if (!enc) return FARGO_OK;
   static_assert(sizeof(CUtensorMap) == 128, "three maps at 128-byte strides");
-  // 2-D FP32 maps of NSEC columns x rows, no swizzle, zero fill outside
-  auto encode = [&](CUtensorMap* m, const float* base, int rows, int box_cols, int box_rows) {
-    cuuint64_t dim[2] = {(cuuint64_t)nsec, (cuuint64_t)rows};
-    cuuint64_t stride[1] = {(cuuint64_t)nsec * sizeof(float)};
-    cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
-    cuuint32_t es[2] = {1, 1};
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dim, stride, box, es,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-  };
-  // transport: Sigma and v_theta rings 0..NRAD-1, v_r with its ghost row
   CUtensorMap m[3];
-  if (encode(&m[0], D.dens, nrad, FARGO_TR_ROW, FARGO_TR_ROWS_D) &&
-      encode(&m[1], D.vrad, nrad + 1, FARGO_TR_ROW, FARGO_TR_ROWS_R) &&
-      encode(&m[2], D.vtheta, nrad, FARGO_TR_ROW, FARGO_TR_ROWS_T)) {
-    CUtensorMap* dm = nullptr;
-    fargo_status st = dalloc(b, h, &dm, 3);
-    if (st) return st;
-    CK(cudaMemcpy(dm, m, sizeof(m), cudaMemcpyHostToDevice));
-    D.tmap = dm;
+  const float* base[3] = {D.dens, D.vrad, D.vtheta};
+  const int rows[3] = {nrad, nrad + 1, nrad};
+  const int box_rows[3] = {FARGO_TR_ROWS_D, FARGO_TR_ROWS_R, FARGO_TR_ROWS_T};
+  for (int k = 0; k < 3; k++) {
+    cuuint64_t dim[2] = {(cuuint64_t)nsec, (cuuint64_t)rows[k]};
+    cuuint64_t stride[1] = {(cuuint64_t)nsec * sizeof(float)};
+    cuuint32_t box[2] = {FARGO_TR_ROW, (cuuint32_t)box_rows[k]};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(&m[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base[k]), dim, stride, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return FARGO_OK;  // staged by cp.async instead
   }
-  // viscosity: VradInt, VthetaInt, Sigma, rings 0..NRAD (the ghost row)
-  if (nsec >= FARGO_VISC_BOX_COLS && encode(&m[0], D.vri, nrad + 1, FARGO_VISC_BOX_COLS, FARGO_VISC_BOX_ROWS) &&
-      encode(&m[1], D.vti, nrad + 1, FARGO_VISC_BOX_COLS, FARGO_VISC_BOX_ROWS) &&
-      encode(&m[2], D.dens, nrad + 1, FARGO_VISC_BOX_COLS, FARGO_VISC_BOX_ROWS)) {
-    CUtensorMap* dm = nullptr;
-    fargo_status st = dalloc(b, h, &dm, 3);
-    if (st) return st;
-    CK(cudaMemcpy(dm, m, sizeof(m), cudaMemcpyHostToDevice));
-    D.vtmap = dm;
-  }
+  CUtensorMap* dm = nullptr;
+  fargo_status st = dalloc(b, h, &dm, 3);
+  if (st) return st;
+  CK(cudaMemcpy(dm, m, sizeof(m), cudaMemcpyHostToDevice));
+  D.tmap = dm;
   return FARGO_OK;
 }
 

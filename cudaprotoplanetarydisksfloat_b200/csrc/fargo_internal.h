@@ -101,9 +101,6 @@ struct DiskDev {
   // for the transport's TMA staging, or null (NSEC not a multiple of 4, or
   // below 64): then the rows are staged by 16- or 4-byte cp.async copies
   const void* tmap;
-  // three CUtensorMap (VradInt, VthetaInt, Sigma; boxes of one viscosity
-  // tile with its halo) for k_viscosity's TMA staging, or null (as tmap)
-  const void* vtmap;
   // boundary constants computed on the host as the reference does:
   // pow(Rinf[1], -1.5), pow(Rinf[NRAD-2], -1.5) of NonReflectingBoundary;
   // damping zones and orbital periods of EvanescentBoundary (SideEuler.cu:127-132)
@@ -202,10 +199,6 @@ struct BatchDev {
 #define FARGO_TR_ROWS_D (FARGO_BAND + 4)
 #define FARGO_TR_ROWS_R (FARGO_BAND + 5)
 #define FARGO_TR_ROWS_T (FARGO_BAND + 4)
-// Viscosity staging: one tile of 16 x 64 cells with its halo, 20 rings x 72
-// sectors per field (one TMA box)
-#define FARGO_VISC_BOX_ROWS 20
-#define FARGO_VISC_BOX_COLS 72
 cudaError_t fargo_kernel_attributes(int max_nsec);
 void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s);
 // only_disk >= 0: that disk; -1: every disk still inside its DT

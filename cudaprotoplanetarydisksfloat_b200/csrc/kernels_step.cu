@@ -1268,49 +1268,9 @@ constexpr int kTQ = (kTC + 3) / 4;                      // stress quads per row
 constexpr int kRuns = 14;                               // stress runs per row: 12 of 5 columns, 2 of 3
 static_assert(12 * 5 + 2 * 3 == kTC && kTR * kRuns <= kThreads, "stress runs cover a tile's rows in one pass");
 constexpr int kTCp = 4 * kTQ;                           // stress row length in shared memory
-static_assert(kSR == FARGO_VISC_BOX_ROWS && kSC == FARGO_VISC_BOX_COLS, "viscosity tensor-map boxes");
 static_assert(kVR * kVC == 4 * kThreads, "one quad of the tile per thread in the update");
 __device__ __forceinline__ int vtiles_of(const DiskDev& D) {
   return ((D.nrad + kVR - 1) / kVR) * ((D.nsec + kVC - 1) / kVC);
-}
-
-// ---- TMA staging: mbarrier and bulk tensor copy (one CTA, no cluster) ----
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Wait for the phase of the given parity, polling at most kSpin times (each
-// poll itself blocks for a bounded, hardware-defined time): false when the
-// wait gave up, so that a copy that never lands cannot hang the GPU.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
-  constexpr int kSpin = 1 << 20;
-  for (int k = 0; k < kSpin; k++)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-// 2-D tiled TMA load of one box at coordinates (x, y) of the tensor map
-// (global memory of this GPU) into shared memory, completing on `bar`.
-// x is a column index (multiple of 4: 16 bytes); x and y may be negative or
-// beyond the tensor: those elements are zero-filled.
-__device__ __forceinline__ void tma_load_2d(float* dst, const void* tmap, int x, int y, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
-          smem_u32(dst)),
-      "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
 }
 
 // 4-byte asynchronous global -> shared copy (zero-filled when !valid)
@@ -1332,33 +1292,16 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(n) : "memory");
 }
 
-// dynamic: the staged tiles, + 128 so that they start on a 128-byte boundary
-// (TMA destinations); each [kSR][kSC] tile is a multiple of 128 bytes
-constexpr size_t kViscSmem = sizeof(float) * 3 * 2 * kSR * kSC + 128;
-static_assert((sizeof(float) * kSR * kSC) % 128 == 0 && (kSC * 4) % 16 == 0 && kSC <= 256 && kSR <= 256,
-              "viscosity tiles as TMA boxes");
-constexpr unsigned kViscTmaBytes = 3u * sizeof(float) * kSR * kSC;
+constexpr size_t kViscSmem = sizeof(float) * 3 * 2 * kSR * kSC;  // dynamic: the staged tiles
 __global__ void __launch_bounds__(kThreads, 3) k_viscosity(BatchDev B) {
   __shared__ DiskDev sD;
   extern __shared__ __align__(16) float vs_sm[];
-  float* vs_base = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(vs_sm) + 127) & ~uintptr_t(127));
-  float(*sVrb)[kSR][kSC] = reinterpret_cast<float(*)[kSR][kSC]>(vs_base);  // [2][kSR][kSC] each
+  float(*sVrb)[kSR][kSC] = reinterpret_cast<float(*)[kSR][kSC]>(vs_sm);  // [2][kSR][kSC] each
   float(*sVab)[kSR][kSC] = sVrb + 2;
   float(*sDnb)[kSR][kSC] = sVab + 2;
   __shared__ float sD0b[2][kSR];
   __shared__ float sTrr[kTR][kTCp], sTpp[kTR][kTCp], sTrp[kTR][kTCp];
-  __shared__ __align__(8) uint64_t s_vbar[2];  // completion of each buffer's TMA staging
-  __shared__ int s_vgaveup;
   const int tid = threadIdx.x;
-  if (tid == 0) {
-    mbar_init(&s_vbar[0], 1);
-    mbar_init(&s_vbar[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    s_vgaveup = 0;
-  }
-  __syncthreads();
-  unsigned vphase[2] = {0u, 0u};  // parity of each buffer barrier's next phase
-  bool vtma[2] = {false, false};  // buffer staged by TMA (its wrapped columns still to fill)
   const int na = B.act[0];
   const int ntile = na > 0 ? B.act_vtile_off[na] : 0;
   const int per = (ntile + gridDim.x - 1) / gridDim.x;
@@ -1372,21 +1315,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_viscosity(BatchDev B) {
     const int nsec = sD.nsec, nrad = sD.nrad;
     const int ncol = (nsec + kVC - 1) / kVC;
     const int i0 = (lt / ncol) * kVR, j0 = (lt % ncol) * kVC;
-    vtma[bf] = false;
-    if (sD.vtmap && (nsec & 3) == 0 && nsec >= kSC && (smem_u32(vs_base) & 127) == 0) {
-      // one thread: three 2-D TMA boxes (VradInt, VthetaInt, Sigma; rows
-      // outside 0..NRAD and columns past the ring's end zero-filled; the
-      // wrapped columns are filled by visc_fixup once they have landed)
-      if (tid == 0) {
-        const char* tm = static_cast<const char*>(sD.vtmap);
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        mbar_expect_tx(&s_vbar[bf], kViscTmaBytes);
-        tma_load_2d(&sVrb[bf][0][0], tm, j0 - kSO, i0 - 2, &s_vbar[bf]);
-        tma_load_2d(&sVab[bf][0][0], tm + 128, j0 - kSO, i0 - 2, &s_vbar[bf]);
-        tma_load_2d(&sDnb[bf][0][0], tm + 256, j0 - kSO, i0 - 2, &s_vbar[bf]);
-      }
-      vtma[bf] = true;
-    } else if ((nsec & 3) == 0) {
+    if ((nsec & 3) == 0) {
       constexpr int kCh = kSC / 4;  // chunks per staged row
       for (int q = tid; q < kSR * kCh; q += kThreads) {
         const int r = q / kCh, c = 4 * (q - r * kCh);
@@ -1420,29 +1349,6 @@ __global__ void __launch_bounds__(kThreads, 3) k_viscosity(BatchDev B) {
     }
     cp_async_commit();
   };
-  // after a TMA staging of tile lt into buffer bf has landed: the window's
-  // columns left of sector 0 (j0 = 0) or right of sector NSEC-1 came
-  // zero-filled; fill them from the other end of the ring (periodic azimuth)
-  auto visc_fixup = [&](int lt, int bf) {
-    const int nsec = sD.nsec, nrad = sD.nrad;
-    const int ncol = (nsec + kVC - 1) / kVC;
-    const int i0 = (lt / ncol) * kVR, j0 = (lt % ncol) * kVC;
-    const int nl = j0 < kSO ? kSO - j0 : 0;
-    const int nr = max(0, j0 - kSO + kSC - nsec);
-    const int nw = nl + nr;
-    for (int q = tid; q < kSR * nw; q += kThreads) {
-      const int r = q / nw, k = q - r * nw;
-      const int c = k < nl ? k : kSC - nr + (k - nl);
-      int j = j0 - kSO + c;
-      j = j < 0 ? j + nsec : (j >= nsec ? j - nsec : j);
-      const int i = i0 - 2 + r;
-      const bool ok = i >= 0 && i <= nrad;
-      const int l = ok ? i * nsec + j : 0;
-      sVrb[bf][r][c] = ok ? __ldg(sD.vri + l) : 0.0f;
-      sVab[bf][r][c] = ok ? __ldg(sD.vti + l) : 0.0f;
-      sDnb[bf][r][c] = ok ? __ldg(sD.dens + l) : 0.0f;
-    }
-  };
   int lo = 0, hi = -1, bf = 0;
   bool have = false;  // tile t already staged (prefetched) in buffer bf
   for (int t = t0; t < t1; t++) {
@@ -1464,22 +1370,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_viscosity(BatchDev B) {
     } else {
       cp_async_wait<0>();
     }
-    if (vtma[bf]) {
-      if (mbar_wait_bounded(&s_vbar[bf], vphase[bf]))
-        visc_fixup(t - lo, bf);
-      else
-        s_vgaveup = 1;
-      vphase[bf] ^= 1u;
-      vtma[bf] = false;
-    }
     __syncthreads();
-    if (s_vgaveup) {
-      // the staged tile never arrived: report it on the disk (FARGO_ETIMEOUT
-      // on the host), wait once more for the other buffer's copies, and stop
-      if (tid == 0) const_cast<DiskCtl*>(sD.ctl)->error = 3;
-      if (vtma[bf ^ 1]) mbar_wait_bounded(&s_vbar[bf ^ 1], vphase[bf ^ 1]);
-      return;
-    }
     float(*sVr)[kSC] = sVrb[bf];
     float(*sVa)[kSC] = sVab[bf];
     float(*sDn)[kSC] = sDnb[bf];
@@ -2199,6 +2090,45 @@ __device__ __forceinline__ void sweep_ring(float* sRr, float VMed, float vconst,
 #pragma unroll
     for (int c = 0; c < nq; c++) sRr[c * kPad + b0 + k] = q[c][k];
   __syncwarp();
+}
+
+// ---- TMA staging: mbarrier and bulk tensor copy (one CTA, no cluster) ----
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase of the given parity, polling at most kSpin times (each
+// poll itself blocks for a bounded, hardware-defined time): false when the
+// wait gave up, so that a copy that never lands cannot hang the GPU.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+  constexpr int kSpin = 1 << 20;
+  for (int k = 0; k < kSpin; k++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// 2-D tiled TMA load of one box at coordinates (x, y) of the tensor map
+// (global memory of this GPU) into shared memory, completing on `bar`.
+// x is a column index (multiple of 4: 16 bytes); x and y may be negative or
+// beyond the tensor: those elements are zero-filled.
+__device__ __forceinline__ void tma_load_2d(float* dst, const void* tmap, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
 }
 
 // Issue the asynchronous staging of transport item t's input rows (see
