@@ -17,6 +17,10 @@ FARGO_STRLEN = 512
 FARGO_MAX_SUBSTEPS = 100000
 FARGO_PRECISION_REFERENCE = 0
 FARGO_PRECISION_ACCURATE = 1
+FARGO_STRIPE_GHOST = 8
+FARGO_STRIPE_MAX_GHOST = 64
+FARGO_STRIPE_HEAD = 3
+FARGO_CFL_TILE = 4096
 
 STATUS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ECUFFT", 4: "ENONFINITE", 5: "ETIMEOUT", 6: "EOOM",
           7: "EIO", 8: "ENODEV"}
@@ -71,6 +75,11 @@ class FargoPlanets(C.Structure):
                 ("name", (C.c_char * 64) * FARGO_MAXPLANETS)]
 
 
+class FargoStripeLayout(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("base", "nrad", "nsec", "own_lo", "own_hi", "ghost_lo", "ghost_hi",
+                                        "nfields", "halo_floats_lo", "halo_floats_hi", "block_doubles")]
+
+
 class FargoScalars(C.Structure):
     _fields_ = [("physical_time", C.c_float), ("omega_frame", C.c_float), ("mdcp1", C.c_float),
                 ("lost_mass", C.c_float), ("nsub_last_dt", C.c_int), ("nsub_total", C.c_int),
@@ -93,6 +102,8 @@ EXPORTS = [
     "fargo_checkpoint_load", "fargo_stream", "fargo_batch_stream",
     "fargo_ctx_batch", "fargo_batch_upload_async", "fargo_batch_download_async", "fargo_batch_profile",
     "fargo_profile_kernel_name", "fargo_profile_kernel_count",
+    "fargo_stripe_create", "fargo_stripe_info", "fargo_stripe_dt_begin", "fargo_stripe_forces",
+    "fargo_stripe_substep", "fargo_stripe_halo_pack", "fargo_stripe_halo_unpack", "fargo_stripe_more",
 ]
 
 
@@ -168,6 +179,15 @@ def _load():
         "fargo_batch_profile": (C.c_int, [vp, C.c_int, dp, P(C.c_int)]),
         "fargo_profile_kernel_name": (C.c_char_p, [C.c_int]),
         "fargo_profile_kernel_count": (C.c_int, []),
+        "fargo_stripe_create": (C.c_int, [P(FargoParams), P(FargoPlanets), dp, C.c_int, C.c_int, C.c_int,
+                                          C.c_int, P(vp)]),
+        "fargo_stripe_info": (C.c_int, [vp, P(FargoStripeLayout)]),
+        "fargo_stripe_dt_begin": (C.c_int, [vp]),
+        "fargo_stripe_forces": (C.c_int, [vp, vp]),
+        "fargo_stripe_substep": (C.c_int, [vp, vp, C.c_int, C.c_int]),
+        "fargo_stripe_halo_pack": (C.c_int, [vp, vp, vp]),
+        "fargo_stripe_halo_unpack": (C.c_int, [vp, vp, vp]),
+        "fargo_stripe_more": (C.c_int, [vp, P(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

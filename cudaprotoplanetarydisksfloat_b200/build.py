@@ -37,7 +37,7 @@ def _newer(target, deps):
 
 def build(verbose=False, force=False):
     srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
-    hdrs = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".h")]
+    hdrs = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
     hdrs.append(os.path.join(ROOT, "include", "fargo_b200.h"))
     nv = _nvcc()
     objdir = os.path.join(HERE, "_build")

@@ -61,6 +61,9 @@ struct fargo_batch {
   bool use_graph = true;
   long long launches = 0;
   long long ncell_ghost = 0;
+  // radial stripe (fargo_stripe_create): global ring of local ring 0, the
+  // whole disk's ring count, ghost rings below and above the own rings
+  int stripe = 0, stripe_base = 0, stripe_nrad = 0, ghost_lo = 0, ghost_hi = 0;
   std::string err;
 };
 
@@ -214,6 +217,9 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   D.IsDisk = p->IsDisk;
   D.max_sub = FARGO_MAX_SUBSTEPS;
   D.accurate = 0;
+  D.own_lo = 0;
+  D.own_hi = p->NRAD;
+  D.stripe = 0;
   D.invdphi = h.t.invdphi;
   D.onethird = h.t.onethird;
   size_t ng = (size_t)(p->NRAD + 1) * p->NSEC;
@@ -662,6 +668,7 @@ void batch_free(fargo_batch* b) {
 }
 
 fargo_status advance_dt_async(fargo_batch* b) {
+  if (b->stripe) return set_err(b, FARGO_EINVAL, "a radial stripe advances through fargo_stripe_*");
   CK(cudaSetDevice(b->device));
   fargo_launch_dt_begin(b->bd, b->stream);
   b->launches += 1;
@@ -1166,7 +1173,7 @@ fargo_status fargo_batch_download_async(fargo_batch* b, int d, float* dens, floa
 int fargo_profile_kernel_count(void) { return FARGO_NKERNELS + 1; }
 
 fargo_status fargo_batch_profile(fargo_batch* b, int ndt, double* ms, int* nsub) {
-  if (!b || !ms || ndt < 1) return FARGO_EINVAL;
+  if (!b || !ms || ndt < 1 || b->stripe) return FARGO_EINVAL;
   CK(cudaSetDevice(b->device));
   const int NK = FARGO_NKERNELS;
   cudaEvent_t ev[FARGO_NKERNELS + 1], sg0, sg1;
@@ -1229,8 +1236,7 @@ long long fargo_batch_count_launches(fargo_batch* b) {
 
 fargo_status fargo_set_graph_mode(fargo_ctx* ctx, int use_graph) {
   if (!ctx) return FARGO_EINVAL;
-  ctx->b.use_graph = use_graph != 0;
-  return build_graph(&ctx->b);
+  return fargo_batch_set_graph_mode(&ctx->b, use_graph);
 }
 
 // Autotuner of the transport tile: the azimuthal segment width (output
@@ -1322,8 +1328,175 @@ fargo_status fargo_set_max_substeps(fargo_ctx* ctx, int n) {
 
 fargo_status fargo_batch_set_graph_mode(fargo_batch* b, int use_graph) {
   if (!b) return FARGO_EINVAL;
+  if (b->stripe && use_graph) return set_err(b, FARGO_EINVAL, "a radial stripe runs its substeps from the host");
   b->use_graph = use_graph != 0;
   return build_graph(b);
+}
+
+// ------------------------------------------------------------ radial stripes
+// One stripe of a disk decomposed by rings over several contexts (usually
+// one per GPU): its own rings ring_lo .. ring_hi-1 plus `ghost` rings on
+// each side (fewer at the disk's edges), computed as a disk of its own on the
+// whole disk's radii.  After every substep the ghost rings are refreshed from
+// the neighbours' own rings (halo pack / unpack), so that the boundary
+// treatment at the stripe's cut edges, which is not the whole disk's, only
+// ever reaches ghost rings.  The substep's scalars come from every stripe's
+// partials (fargo_stripe_forces, gathered by the caller, then
+// fargo_stripe_substep), so all stripes take the same dt and planet update.
+
+static int stripe_nfields(const fargo_batch* b) { return b->disks[0].p.Adiabatic ? 4 : 3; }
+
+fargo_status fargo_stripe_create(const fargo_params* p, const fargo_planets* planets, const double* radii,
+                                 int ring_lo, int ring_hi, int ghost, int device, fargo_ctx** out) {
+  if (!p || !planets || !out) return FARGO_EINVAL;
+  *out = nullptr;
+  fargo_ctx* ctx = new fargo_ctx();
+  *out = ctx;  // returned even on failure so that fargo_last_error can explain
+  fargo_batch* b = &ctx->b;
+  const int NRAD = p->NRAD;
+  if (ring_lo < 0 || ring_hi > NRAD || ring_lo >= ring_hi)
+    return set_err(b, FARGO_EINVAL, "stripe rings [%d, %d) outside the disk's %d rings", ring_lo, ring_hi, NRAD);
+  if (ghost < 1 || ghost > FARGO_STRIPE_MAX_GHOST)
+    return set_err(b, FARGO_EINVAL, "ghost rings must be 1 .. %d", FARGO_STRIPE_MAX_GHOST);
+  if (ring_hi - ring_lo < ghost && !(ring_lo == 0 && ring_hi == NRAD))
+    return set_err(b, FARGO_EINVAL, "a stripe needs at least as many own rings (%d) as ghost rings (%d)",
+                   ring_hi - ring_lo, ghost);
+  if (p->SelfGravity)
+    return set_err(b, FARGO_EINVAL, "self-gravity couples every ring: a self-gravitating disk is not decomposed");
+  if (p->OpenInner || p->NonReflecting || p->Evanescent)
+    return set_err(b, FARGO_EINVAL, "radial stripes need RIGID inner and outer boundaries");
+  std::vector<double> R(NRAD + 1);
+  if (radii) {
+    std::memcpy(R.data(), radii, sizeof(double) * (NRAD + 1));
+  } else {
+    fargo_status st = fargo_grid_radii(p, R.data());
+    if (st) return set_err(b, st, "grid radii");
+  }
+  const int base = std::max(0, ring_lo - ghost), top = std::min(NRAD, ring_hi + ghost);
+  fargo_params q = *p;
+  q.NRAD = top - base;
+  q.RMIN = (float)R[base];
+  q.RMAX = (float)R[top];
+  const double* r[1] = {R.data() + base};
+  fargo_status st = batch_create(b, 1, &q, planets, r, device);
+  if (st) return st;
+  DiskDev& D = b->disks[0].dev;
+  D.own_lo = ring_lo - base;
+  D.own_hi = ring_hi - base;
+  D.stripe = 1;
+  b->stripe = 1;
+  b->stripe_base = base;
+  b->stripe_nrad = NRAD;
+  b->ghost_lo = ring_lo - base;
+  b->ghost_hi = top - ring_hi;
+  b->bd.ncfl = fargo_cfl_tiles_own(D);
+  CK(cudaMemcpy(b->d_disks, &D, sizeof(DiskDev), cudaMemcpyHostToDevice));
+  b->use_graph = false;
+  return build_graph(b);
+}
+
+fargo_status fargo_stripe_info(fargo_ctx* ctx, fargo_stripe_layout* out) {
+  if (!ctx || !out || !ctx->b.stripe) return FARGO_EINVAL;
+  const fargo_batch* b = &ctx->b;
+  const DiskDev& D = b->disks[0].dev;
+  out->base = b->stripe_base;
+  out->nrad = D.nrad;
+  out->nsec = D.nsec;
+  out->own_lo = D.own_lo;
+  out->own_hi = D.own_hi;
+  out->ghost_lo = b->ghost_lo;
+  out->ghost_hi = b->ghost_hi;
+  out->nfields = stripe_nfields(b);
+  out->halo_floats_lo = out->nfields * b->ghost_lo * D.nsec;
+  out->halo_floats_hi = out->nfields * b->ghost_hi * D.nsec;
+  out->block_doubles = FARGO_STRIPE_HEAD + 4 * FARGO_MAXBODY * fargo_cfl_tiles_own(D);
+  return FARGO_OK;
+}
+
+fargo_status fargo_stripe_dt_begin(fargo_ctx* ctx) {
+  if (!ctx || !ctx->b.stripe) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  CK(cudaSetDevice(b->device));
+  fargo_launch_dt_begin(b->bd, b->stream);
+  b->launches += 1;
+  if (b->any_adiabatic) {
+    fargo_launch_cs_refresh(b->bd, -1, b->stream);
+    b->launches += 2;
+  }
+  CK(cudaGetLastError());
+  return FARGO_OK;
+}
+
+fargo_status fargo_stripe_forces(fargo_ctx* ctx, double* block) {
+  if (!ctx || !ctx->b.stripe || !block) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  CK(cudaSetDevice(b->device));
+  fargo_launch_substep(b->bd, 0, 0, b->stream, b->max_nsec, &b->launches, nullptr, FARGO_PART_HEAD);
+  fargo_launch_stripe_block(b->bd, block, b->stream);
+  b->launches += 1;
+  CK(cudaGetLastError());
+  return FARGO_OK;
+}
+
+fargo_status fargo_stripe_substep(fargo_ctx* ctx, const double* blocks, int nstripe, int stride) {
+  if (!ctx || !ctx->b.stripe || !blocks || nstripe < 1 || stride < FARGO_STRIPE_HEAD) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  CK(cudaSetDevice(b->device));
+  if (fargo_launch_stripe_finish(b->bd, blocks, nstripe, stride, b->stream))
+    return set_err(b, FARGO_EINVAL, "stripe count %d out of range", nstripe);
+  b->launches += 1;
+  fargo_launch_substep(b->bd, 0, 0, b->stream, b->max_nsec, &b->launches, nullptr, FARGO_PART_TAIL);
+  CK(cudaGetLastError());
+  return FARGO_OK;
+}
+
+// ghost rows of one side: [field][rows][nsec], fields Sigma, v_r, v_theta (+ e)
+static fargo_status stripe_halo(fargo_batch* b, int row0, int rows, float* buf, bool pack) {
+  if (rows == 0) return FARGO_OK;
+  const DiskDev& D = b->disks[0].dev;
+  float* f[4] = {D.dens, D.vrad, D.vtheta, D.energy};
+  const size_t n = (size_t)rows * D.nsec;
+  for (int k = 0; k < stripe_nfields(b); k++) {
+    float* grid = f[k] + (size_t)row0 * D.nsec;
+    if (pack)
+      CK(cudaMemcpyAsync(buf + k * n, grid, sizeof(float) * n, cudaMemcpyDeviceToDevice, b->stream));
+    else
+      CK(cudaMemcpyAsync(grid, buf + k * n, sizeof(float) * n, cudaMemcpyDeviceToDevice, b->stream));
+  }
+  return FARGO_OK;
+}
+
+fargo_status fargo_stripe_halo_pack(fargo_ctx* ctx, float* lo, float* hi) {
+  if (!ctx || !ctx->b.stripe) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  if ((b->ghost_lo && !lo) || (b->ghost_hi && !hi)) return set_err(b, FARGO_EINVAL, "missing halo buffer");
+  CK(cudaSetDevice(b->device));
+  const DiskDev& D = b->disks[0].dev;
+  fargo_status st = stripe_halo(b, D.own_lo, b->ghost_lo, lo, true);
+  if (st) return st;
+  return stripe_halo(b, D.own_hi - b->ghost_hi, b->ghost_hi, hi, true);
+}
+
+fargo_status fargo_stripe_halo_unpack(fargo_ctx* ctx, const float* lo, const float* hi) {
+  if (!ctx || !ctx->b.stripe) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  if ((b->ghost_lo && !lo) || (b->ghost_hi && !hi)) return set_err(b, FARGO_EINVAL, "missing halo buffer");
+  CK(cudaSetDevice(b->device));
+  const DiskDev& D = b->disks[0].dev;
+  fargo_status st = stripe_halo(b, D.own_lo - b->ghost_lo, b->ghost_lo, const_cast<float*>(lo), false);
+  if (st) return st;
+  return stripe_halo(b, D.own_hi, b->ghost_hi, const_cast<float*>(hi), false);
+}
+
+fargo_status fargo_stripe_more(fargo_ctx* ctx, int* more) {
+  if (!ctx || !ctx->b.stripe || !more) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  CK(cudaSetDevice(b->device));
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, b->d_flags, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  *more = h;
+  return h ? FARGO_OK : finish_dts(b);
 }
 
 }  // extern "C"

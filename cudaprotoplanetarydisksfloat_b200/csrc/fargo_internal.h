@@ -78,6 +78,9 @@ inline __host__ __device__ int fargo_cfl_tiles(int nrad, int nsec) {
   return (int)(((long long)nrad * nsec + FARGO_CFL_TILE - 1) / FARGO_CFL_TILE);
 }
 
+// CFL tiles of a disk's own rings (every ring unless it is a radial stripe)
+#define fargo_cfl_tiles_own(D) fargo_cfl_tiles((D).own_hi - (D).own_lo, (D).nsec)
+
 // scratch of the device RK5 (q0, q1, k1..k6, distances): 33 doubles per planet
 #define FARGO_RK_WORK(nb) (33 * (nb))
 
@@ -96,6 +99,13 @@ struct DiskDev {
   int ForcedCircular, Corotating, GuidingCenter, RocheSmoothing, SelfGravity, Evanescent;
   int OpenInner, NonReflecting, SloppyCFL, IsDisk;
   int max_sub;  // substeps one DT may take before it stops with FARGO_ETIMEOUT
+  // Radial stripe of a decomposed disk: the rings own_lo .. own_hi-1 are this
+  // context's own, the others are ghost rings refreshed from the neighbouring
+  // stripes after every substep.  The CFL limit and the disk forces cover the
+  // own rings only, and with stripe = 1 the CFL kernel leaves the substep's
+  // scalar work to k_stripe_finish, which reads every stripe's partials.
+  // A whole disk: own_lo = 0, own_hi = nrad, stripe = 0.
+  int own_lo, own_hi, stripe;
   int accurate;  // precision mode: 0 the reference's arithmetic, 1 accurate (FARGO_PRECISION_*)
   // three CUtensorMap (Sigma, v_r, v_theta; 2-D, FARGO_TR_ROW-column boxes)
   // for the transport's TMA staging, or null (NSEC not a multiple of 4, or
@@ -204,9 +214,20 @@ void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s);
 // only_disk >= 0: that disk; -1: every disk still inside its DT
 void fargo_launch_cs_refresh(const BatchDev& b, int only_disk, cudaStream_t s);
 void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s);
-// ev (optional): FARGO_NKERNELS+1 events, before each kernel and after the last
+// ev (optional): FARGO_NKERNELS+1 events, before each kernel and after the last.
+// part: FARGO_PART_HEAD (ring means and CFL/forces), FARGO_PART_TAIL (the
+// rest: potential ... end of substep) or both.
+#define FARGO_PART_HEAD 1
+#define FARGO_PART_TAIL 2
 void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int use_handle, cudaStream_t s,
-                          int max_nsec, long long* launches, cudaEvent_t* ev = nullptr);
+                          int max_nsec, long long* launches, cudaEvent_t* ev = nullptr,
+                          int part = FARGO_PART_HEAD | FARGO_PART_TAIL);
+// radial stripes: the stripe's block for the gather (3 + 4 * bodies * own CFL
+// tiles doubles), and the substep scalars from the gathered blocks (nonzero
+// return: nstripe out of range)
+void fargo_launch_stripe_block(const BatchDev& b, double* out, cudaStream_t s);
+int fargo_launch_stripe_finish(const BatchDev& b, const double* blk, int nstripe, int stride, cudaStream_t s);
+#define FARGO_STRIPE_HEAD 3
 const char* fargo_substep_kernel_name(int k);
 void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s);
 void fargo_launch_init_velocities(const BatchDev& b, int disk, long long ncell_ghost, cudaStream_t s);

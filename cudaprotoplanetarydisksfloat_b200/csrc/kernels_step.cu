@@ -655,37 +655,91 @@ __device__ float block_min_f(float v, float* sh) {
 
 // -------------------------------------------------------------- CFL + forces
 
-// Last block of a disk: the scalar part of the substep (SourceEuler.cu:231-264).
-// Substep scalars of one disk, run by the block that completed the disk's
-// last CFL tile.  Tile minima and force partials were written by other SMs
-// in this launch: read through L2.  The serial part runs on a shared-memory
-// copy of the disk's control block (sC), written back at the end.
+// The scalar part of the substep (SourceEuler.cu:231-264), run by the block
+// that completed a disk's last CFL tile (or, for a radial stripe, by
+// k_stripe_finish once every stripe's partials are gathered).
 constexpr int kRkShared = 16;  // planets whose RK5 scratch fits in shared memory
 __device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const double* s_sum, double* work);
-template <int NB>
-__device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* Cg, DiskCtl* sC, float* shf, double* s_sum,
-                                       double* s_work) {
-  const int nrad = D.nrad, nsec = D.nsec, tid = threadIdx.x;
-  const int nct = fargo_cfl_tiles(nrad, nsec);
-  // ConditionCFL host part (SourceEuler.cu:513-535): minimum over the tile
-  // minima (cells of rings 1 .. NRAD-1), the shear limit DT1D
-  // (ConditionCFLKernel2D2, Kernels.cu:1425-1428) and DeltaT.
-  float m = 1e30f;
+
+// ConditionCFL host part (SourceEuler.cu:513-535): the shear limit DT1D
+// (ConditionCFLKernel2D2, Kernels.cu:1425-1428) of the ring pairs (i, i+1),
+// i in [i0, i1), folded into a thread's running minimum.
+__device__ __forceinline__ float dt1d_min(const DiskDev& D, int i0, int i1, int tid, int nt, float m) {
 #pragma unroll 4
-  for (int t = tid; t < nct; t += blockDim.x) {
-    float v = __ldcg(D.ringmin + t);
-    if (v < m) m = v;
-  }
-#pragma unroll 4
-  for (int i = tid; i < nrad - 1; i += blockDim.x) {
-    float dt1 = 2.0 * PI_D * CFLSEC / (float)nsec / fabsf(D.vmoy[i] * D.invRmed[i] - D.vmoy[i + 1] * D.invRmed[i + 1]);
+  for (int i = i0 + tid; i < i1; i += nt) {
+    float dt1 = 2.0 * PI_D * CFLSEC / (float)D.nsec / fabsf(D.vmoy[i] * D.invRmed[i] - D.vmoy[i + 1] * D.invRmed[i + 1]);
     if (dt1 < m) m = dt1;
   }
-  float newdt = block_min_f(m, shf);
+  return m;
+}
+
+// Inputs of the finishing sums of a whole disk: its CFL tiles' minima and
+// force partials ([sum][tile]), written by the blocks of this launch (read
+// through L2), and the shear limit of every ring pair.
+struct DiskTiles {
+  const DiskDev& D;
+  int nct;
+  __device__ float thread_min(int tid, int nt) const {
+    float m = 1e30f;
+#pragma unroll 4
+    for (int t = tid; t < nct; t += nt) {
+      float v = __ldcg(D.ringmin + t);
+      if (v < m) m = v;
+    }
+    return dt1d_min(D, 0, D.nrad - 1, tid, nt, m);
+  }
+  __device__ int ntiles() const { return nct; }
+  __device__ double partial(int q, int t) const { return __ldcg(D.partials + (size_t)q * nct + t); }
+};
+
+// Inputs of the finishing sums of a radially decomposed disk: one block per
+// stripe, gathered from every stripe in stripe order (k_stripe_block writes
+// them): [0] the minimum over the stripe's tiles and own ring pairs, [1] its
+// CFL tile count, [2] its body count, then its force partials [sum][tile].
+// The stripes' tiles, concatenated, are the whole disk's tiles (stripe
+// boundaries on tile boundaries), so the sums below add the same partials in
+// the same order as DiskTiles does.
+constexpr int kStripeHead = FARGO_STRIPE_HEAD;
+struct StripeBlocks {
+  const double* blk;
+  int nstripe, stride;
+  const int* t0;  // shared: first tile of each stripe, t0[nstripe] = all tiles
+  __device__ float thread_min(int tid, int nt) const {
+    float m = 1e30f;
+    for (int s = tid; s < nstripe; s += nt) {
+      float v = (float)blk[(size_t)s * stride];
+      if (v < m) m = v;
+    }
+    return m;
+  }
+  __device__ int ntiles() const { return t0[nstripe]; }
+  __device__ double partial(int q, int t) const {
+    int lo = 0, hi = nstripe - 1;  // the stripe s with t0[s] <= t < t0[s+1]
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (t0[mid] <= t)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const int n = t0[lo + 1] - t0[lo];
+    return blk[(size_t)lo * stride + kStripeHead + (size_t)q * n + (t - t0[lo])];
+  }
+};
+
+// Substep scalars of one disk, run by one block: the CFL minimum, the disk
+// forces summed over the tiles in a fixed order, the viscosity per ring and
+// the serial part (on a shared-memory copy of the disk's control block, sC,
+// written back at the end).
+template <int NB, class Src>
+__device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* Cg, DiskCtl* sC, float* shf, double* s_sum,
+                                       double* s_work, const Src& src) {
+  const int nrad = D.nrad, tid = threadIdx.x;
+  const int nct = src.ntiles();
+  float newdt = block_min_f(src.thread_min(tid, blockDim.x), shf);
   // disk-force sums over the tiles in a fixed order: every thread a strided
-  // share of the tiles for all sums at once (partials are [sum][tile]), the
-  // warps by shuffle, then the warps in order (s_work is free until the
-  // planet update)
+  // share of the tiles for all sums at once, the warps by shuffle, then the
+  // warps in order (s_work is free until the planet update)
   const int nbody = min(Cg->nbody, NB), nsum = 4 * nbody;
   const int w = tid >> 5, l = tid & 31, nw = blockDim.x >> 5;
   double acc[4 * NB];
@@ -695,7 +749,7 @@ __device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* Cg, DiskCtl* s
   for (int t = tid; t < nct; t += blockDim.x) {
 #pragma unroll
     for (int q = 0; q < 4 * NB; q++)
-      if (q < nsum) acc[q] += __ldcg(D.partials + (size_t)q * nct + t);
+      if (q < nsum) acc[q] += src.partial(q, t);
   }
 #pragma unroll
   for (int q = 0; q < 4 * NB; q++) {
@@ -864,8 +918,12 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
   // A run of tiles of one disk is done: count it on the disk's ticket; the
   // block that completes the disk's last tile finishes the substep.  Warp 0
   // wrote the run's results and fences them before the ticket.
+  // A radial stripe takes no ticket: k_stripe_finish finishes it.
   auto finish_run = [&]() {
-    if (run == 0) return;
+    if (run == 0 || sD.stripe) {  // block-uniform
+      run = 0;
+      return;
+    }
     DiskCtl* Cr = sD.ctl;
     if (w == 0) {
       __threadfence();
@@ -873,9 +931,10 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
       if (l == 0) s_ticket = atomicAdd(&Cr->counter, (unsigned)run);
     }
     __syncthreads();
-    if (s_ticket + (unsigned)run == (unsigned)fargo_cfl_tiles(sD.nrad, sD.nsec)) {
+    const int nct = fargo_cfl_tiles_own(sD);
+    if (s_ticket + (unsigned)run == (unsigned)nct) {
       __threadfence();
-      finish_cfl_and_planets<NB>(sD, Cr, &sC, s_min[0], s_sum, s_work);
+      finish_cfl_and_planets<NB>(sD, Cr, &sC, s_min[0], s_sum, s_work, DiskTiles{sD, nct});
     }
     run = 0;
     __syncthreads();
@@ -912,7 +971,9 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
     if (D.IsDisk) {
       const int kh = D.ExcludeHill ? FARGO_DIMFXY - 1 : 0;
       const float hillcutfactor = (float)kh / (float)(FARGO_DIMFXY - 1);
-      const int c0 = k * FARGO_CFL_TILE + tid;
+      // tiles start at the first own ring (ring 0 unless a radial stripe)
+      const int c0 = D.own_lo * nsec + k * FARGO_CFL_TILE + tid;
+      const int iend = D.own_hi;
       int i = c0 / nsec, j = c0 - i * nsec;
       // kG cells at a time: their loads are issued together (cells past
       // the disk's end read cell 0 and are skipped); fewer with more bodies,
@@ -923,7 +984,7 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
         bool ok[kG];
 #pragma unroll
         for (int u = 0; u < kG; u++) {
-          ok[u] = i < nrad;
+          ok[u] = i < iend;
           ci[u] = ok[u] ? i : 0;
           cj[u] = ok[u] ? j : 0;
           j += kThreads;
@@ -1041,7 +1102,7 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
           if (s_min[pb][u] < m) m = s_min[pb][u];
         D.ringmin[k] = m;
       }
-      const int nct = fargo_cfl_tiles(nrad, nsec);
+      const int nct = fargo_cfl_tiles_own(D);
       for (int u = l; u < 4 * nbody; u += 32) {
         double v = 0.0;
         for (int x = 0; x < kThreads / 32; x++) v += s_red[pb][u][x];
@@ -1051,6 +1112,61 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
     run++;
   }
   finish_run();
+}
+
+// ----------------------------------------------------------- radial stripes
+
+// A radial stripe's block for the gather across stripes (StripeBlocks): the
+// minimum over its CFL tiles and over the shear limits of its own ring pairs
+// (i, i+1) (the disk's last ring has none), its tile count, its body count
+// and its force partials [sum][tile].  One block; the stripe is disk 0 of
+// its batch.
+__global__ void __launch_bounds__(kThreads) k_stripe_block(BatchDev B, double* out) {
+  __shared__ float shf[32];
+  const DiskDev& D = B.disks[0];
+  const int tid = threadIdx.x;
+  const int nct = fargo_cfl_tiles_own(D);
+  float m = 1e30f;
+  for (int t = tid; t < nct; t += blockDim.x) {
+    const float v = D.ringmin[t];
+    if (v < m) m = v;
+  }
+  m = dt1d_min(D, D.own_lo, D.own_hi < D.nrad ? D.own_hi : D.nrad - 1, tid, blockDim.x, m);
+  m = block_min_f(m, shf);
+  const int nbody = D.ctl->nbody;
+  if (tid == 0) {
+    out[0] = m;
+    out[1] = nct;
+    out[2] = nbody;
+  }
+  for (int u = tid; u < 4 * nbody * nct; u += blockDim.x) out[kStripeHead + u] = D.partials[u];
+}
+
+// The substep scalars of a radial stripe from every stripe's block (the
+// same minimum and the same sums, in the same order, as the whole disk's
+// finishing block forms): every stripe runs it on the same blocks, so every
+// stripe takes the same dt, planet update and substep count.
+constexpr int kMaxStripes = 256;
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_stripe_finish(BatchDev B, const double* blk, int nstripe, int stride) {
+  __shared__ DiskDev sD;
+  __shared__ DiskCtl sC;
+  __shared__ float shf[32];
+  __shared__ double s_sum[4 * FARGO_MAXBODY];
+  __shared__ double s_work[FARGO_RK_WORK(kRkShared)];
+  __shared__ int s_t0[kMaxStripes + 1];
+  const int tid = threadIdx.x;
+  copy_words(&sD, B.disks, sizeof(DiskDev));
+  if (tid == 0) {
+    int t = 0;
+    for (int k = 0; k < nstripe; k++) {
+      s_t0[k] = t;
+      t += (int)blk[(size_t)k * stride + 1];
+    }
+    s_t0[nstripe] = t;
+  }
+  __syncthreads();
+  finish_cfl_and_planets<NB>(sD, sD.ctl, &sC, shf, s_sum, s_work, StripeBlocks{blk, nstripe, stride, s_t0});
 }
 
 // ----------------------------------------------------------- source terms
@@ -2425,7 +2541,7 @@ __device__ void compact_active(const BatchDev& B) {
       s_nrad[tid] = D.nrad;
       s_cells[tid] = cells;
       s_tiles[tid] = (int)((cells + FARGO_QTILE - 1) / FARGO_QTILE);
-      s_ctiles[tid] = fargo_cfl_tiles(D.nrad, D.nsec);
+      s_ctiles[tid] = fargo_cfl_tiles_own(D);
       s_vtiles[tid] = vtiles_of(D);
     }
     __syncthreads();
@@ -2950,7 +3066,7 @@ const char* fargo_substep_kernel_name(int k) {
 }
 
 void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int use_handle, cudaStream_t s,
-                          int max_nsec, long long* launches, cudaEvent_t* ev) {
+                          int max_nsec, long long* launches, cudaEvent_t* ev, int part) {
   (void)max_nsec;
   int k = 0;
 #define REC()                                  \
@@ -2958,17 +3074,25 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
     if (ev) cudaEventRecord(ev[k], s);         \
     k++;                                       \
   } while (0)
-  REC();
-  k_ring_mean<0><<<b.grp_grid, kRMT, fargo_ring_mean_smem_bytes(), s>>>(b);
-  REC();
-  if (b.max_body <= 1)
-    k_cfl_force<1><<<b.g_cfl, kThreads, 0, s>>>(b);
-  else if (b.max_body <= 2)
-    k_cfl_force<2><<<b.g_cfl, kThreads, 0, s>>>(b);
-  else if (b.max_body <= 4)
-    k_cfl_force<4><<<b.g_cfl, kThreads, 0, s>>>(b);
-  else
-    k_cfl_force<FARGO_MAXBODY><<<b.g_cfl, kThreads, 0, s>>>(b);
+  if (part & FARGO_PART_HEAD) {
+    REC();
+    k_ring_mean<0><<<b.grp_grid, kRMT, fargo_ring_mean_smem_bytes(), s>>>(b);
+    REC();
+    if (b.max_body <= 1)
+      k_cfl_force<1><<<b.g_cfl, kThreads, 0, s>>>(b);
+    else if (b.max_body <= 2)
+      k_cfl_force<2><<<b.g_cfl, kThreads, 0, s>>>(b);
+    else if (b.max_body <= 4)
+      k_cfl_force<4><<<b.g_cfl, kThreads, 0, s>>>(b);
+    else
+      k_cfl_force<FARGO_MAXBODY><<<b.g_cfl, kThreads, 0, s>>>(b);
+  } else {
+    k = 2;
+  }
+  if (!(part & FARGO_PART_TAIL)) {
+    if (launches) *launches += 2;
+    return;
+  }
   REC();
   k_potential<<<b.g_potential, kThreads, 0, s>>>(b);
   REC();
@@ -3012,7 +3136,24 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   k_substep_end<<<1, kThreads, 0, s>>>(b, h, use_handle);
   REC();
 #undef REC
-  if (launches) *launches += fargo_substep_launches(b);
+  if (launches) *launches += fargo_substep_launches(b) - ((part & FARGO_PART_HEAD) ? 0 : 2);
+}
+
+void fargo_launch_stripe_block(const BatchDev& b, double* out, cudaStream_t s) {
+  k_stripe_block<<<1, kThreads, 0, s>>>(b, out);
+}
+
+int fargo_launch_stripe_finish(const BatchDev& b, const double* blk, int nstripe, int stride, cudaStream_t s) {
+  if (nstripe < 1 || nstripe > kMaxStripes) return 1;
+  if (b.max_body <= 1)
+    k_stripe_finish<1><<<1, kThreads, 0, s>>>(b, blk, nstripe, stride);
+  else if (b.max_body <= 2)
+    k_stripe_finish<2><<<1, kThreads, 0, s>>>(b, blk, nstripe, stride);
+  else if (b.max_body <= 4)
+    k_stripe_finish<4><<<1, kThreads, 0, s>>>(b, blk, nstripe, stride);
+  else
+    k_stripe_finish<FARGO_MAXBODY><<<1, kThreads, 0, s>>>(b, blk, nstripe, stride);
+  return 0;
 }
 
 // The transport kernels alone (both forms), for the autotuner: they read the

@@ -321,6 +321,63 @@ fargo_status fargo_batch_set_precision(fargo_batch* b, int mode);
 fargo_status fargo_batch_autotune(fargo_batch* b, int reps, int* seg_out);
 fargo_status fargo_autotune(fargo_ctx* ctx, int reps, int* seg_out);
 
+/* (new) Radial decomposition of one disk over several contexts, usually one
+   per GPU (the loop of AlgoGas, SourceEuler.cu:208-301, split by rings).
+   A stripe owns the rings [ring_lo, ring_hi) of the whole disk (p->NRAD
+   rings on `radii`, NRAD+1 values, or on fargo_grid_radii(p) when null) and
+   computes `ghost` more rings on each side (fewer at the disk's edges) as a
+   disk of its own.  One DT, driven by the caller:
+     fargo_stripe_dt_begin
+     do {
+       fargo_stripe_forces(block)       CFL minimum and force partials of the
+                                        own rings -> this stripe's block
+       gather every stripe's block, in stripe order, each `stride` doubles
+       fargo_stripe_substep(blocks)     the substep's scalars from all blocks
+                                        (the same on every stripe), then the
+                                        rest of the substep
+       fargo_stripe_halo_pack(lo, hi)   own edge rings -> send buffers
+       fargo_stripe_more(&more)         waits; more = another substep follows
+       send lo to the stripe below, hi to the stripe above, receive theirs
+       fargo_stripe_halo_unpack(lo, hi) received rings -> ghost rings
+     } while (more)
+   With every stripe boundary a multiple of 4096 / gcd(NSEC, 4096) rings
+   (whole CFL tiles) and ghost >= FARGO_STRIPE_GHOST, the own rings end
+   every substep with the bits of the undecomposed disk: the tiles and the
+   finishing sums are the same, and the cut edges' boundary treatment
+   reaches fewer than FARGO_STRIPE_GHOST rings into the ghosts in one
+   substep (4 to 5 rings, measured).  Stripes need RIGID boundaries and no
+   self-gravity (FARGO_EINVAL otherwise), at least `ghost` own rings each,
+   and the same parameters, radii and planets.
+   Upload the initial state of the stripe's rings base .. base+nrad (the
+   local grid, ghost row included) with fargo_init_state or fargo_upload,
+   then exchange halos once before the first DT.  fargo_advance* and the
+   CUDA graph are not available on a stripe. */
+#define FARGO_STRIPE_GHOST 8
+#define FARGO_STRIPE_MAX_GHOST 64
+typedef struct {
+  int base;        /* whole-disk ring of the stripe's local ring 0 */
+  int nrad, nsec;  /* local grid: nrad rings (ghosts included) */
+  int own_lo, own_hi;      /* own rings, local indices */
+  int ghost_lo, ghost_hi;  /* ghost rings below / above (0 at the disk's edges) */
+  int nfields;             /* fields in a halo: Sigma, v_r, v_theta (+ energy) */
+  int halo_floats_lo, halo_floats_hi;  /* floats of each side's halo buffer */
+  int block_doubles;       /* doubles of this stripe's block (the stride must
+                              be at least the largest over the stripes) */
+} fargo_stripe_layout;
+fargo_status fargo_stripe_create(const fargo_params* p, const fargo_planets* planets, const double* radii,
+                                 int ring_lo, int ring_hi, int ghost, int device, fargo_ctx** out);
+fargo_status fargo_stripe_info(fargo_ctx* ctx, fargo_stripe_layout* out);
+fargo_status fargo_stripe_dt_begin(fargo_ctx* ctx);
+/* device pointers; the calls are asynchronous on the context's stream
+   (fargo_stream) except fargo_stripe_more */
+fargo_status fargo_stripe_forces(fargo_ctx* ctx, double* block);
+fargo_status fargo_stripe_substep(fargo_ctx* ctx, const double* blocks, int nstripe, int stride);
+fargo_status fargo_stripe_halo_pack(fargo_ctx* ctx, float* lo, float* hi);
+fargo_status fargo_stripe_halo_unpack(fargo_ctx* ctx, const float* lo, const float* hi);
+/* waits for the stripe's stream; at the end of the DT (more = 0) reports
+   its errors as fargo_advance_dt does */
+fargo_status fargo_stripe_more(fargo_ctx* ctx, int* more);
+
 #ifdef __cplusplus
 }
 #endif
