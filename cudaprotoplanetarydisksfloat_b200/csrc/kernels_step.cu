@@ -1997,11 +1997,15 @@ __device__ __forceinline__ void rad_march_s(const TrView& V, const float* sIn, i
 constexpr int kRMT = 256;             // threads
 constexpr int kRMW = 256;             // sectors per chunk
 constexpr int kRMR = FARGO_RM_RINGS;  // rings per CTA (one serial chain each)
-static_assert(kRMR <= 32, "one lane of warp 0 per ring");
-size_t fargo_ring_mean_smem_bytes() { return sizeof(float) * 2 * kRMR * (kRMW + 1); }
+// shared row stride: 16-byte aligned rows, and the kRMR lanes' 16-byte reads
+// at the same offset fall on disjoint banks (260 = 4 mod 32)
+constexpr int kRMS = kRMW + 4;
+static_assert(kRMR <= 32 && kRMR * 4 <= 32, "one lane of warp 0 per ring, conflict-free 16-byte reads");
+static_assert(kRMW % 32 == 0 && kRMS % 4 == 0, "chunks of whole 32-sector blocks, 16-byte rows");
+size_t fargo_ring_mean_smem_bytes() { return sizeof(float) * 2 * kRMR * kRMS; }
 template <int mode>
 __global__ void __launch_bounds__(kRMT) k_ring_mean(BatchDev B) {
-  extern __shared__ float rm_sm[];  // [2][kRMR][kRMW + 1]
+  extern __shared__ __align__(16) float rm_sm[];  // [2][kRMR][kRMS]
   const int na = B.act[0];
   const int ng = na > 0 ? B.act_grp_off[na] : 0;
   const int tid = threadIdx.x, lane = tid & 31;
@@ -2021,9 +2025,9 @@ __global__ void __launch_bounds__(kRMT) k_ring_mean(BatchDev B) {
         r[k] = (c < nchunk && k < nr && col < nsec) ? __ldg(base + (size_t)k * nsec + col) : 0.0f;
     };
     auto store = [&](int c) {
-      float* buf = rm_sm + (c & 1) * kRMR * (kRMW + 1);
+      float* buf = rm_sm + (c & 1) * kRMR * kRMS;
 #pragma unroll
-      for (int k = 0; k < kRMR; k++) buf[k * (kRMW + 1) + tid] = r[k];
+      for (int k = 0; k < kRMR; k++) buf[k * kRMS + tid] = r[k];
     };
     float moy = 0.0f;
     KahanSum ks;  // accurate mode
@@ -2035,13 +2039,33 @@ __global__ void __launch_bounds__(kRMT) k_ring_mean(BatchDev B) {
     for (int c = 0; c < nchunk; c++) {
       load(c + 1);
       if (tid < kRMR) {
-        const float* row = rm_sm + (c & 1) * kRMR * (kRMW + 1) + lane * (kRMW + 1);
+        const float* row = rm_sm + (c & 1) * kRMR * kRMS + lane * kRMS;
         const int w = min(kRMW, nsec - c * kRMW);
         if (acc) {
           for (int k = 0; k < w; k++) ks.add(row[k]);
         } else if (w == kRMW) {
-#pragma unroll 32
-          for (int k = 0; k < kRMW; k++) moy += row[k];
+          // the chain in sector order, its operands read 32 ahead as 16-byte
+          // words, so that the shared-memory latency stays off the chain
+          const float4* r4 = reinterpret_cast<const float4*>(row);
+          float4 a[8], b[8];
+#pragma unroll
+          for (int k = 0; k < 8; k++) a[k] = r4[k];
+#pragma unroll
+          for (int blk = 0; blk < kRMW / 32; blk++) {
+            if (blk + 1 < kRMW / 32) {
+#pragma unroll
+              for (int k = 0; k < 8; k++) b[k] = r4[(blk + 1) * 8 + k];
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+              moy += a[k].x;
+              moy += a[k].y;
+              moy += a[k].z;
+              moy += a[k].w;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k++) a[k] = b[k];
+          }
         } else {
           for (int k = 0; k < w; k++) moy += row[k];
         }
