@@ -971,110 +971,159 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
     if (D.IsDisk) {
       const int kh = D.ExcludeHill ? FARGO_DIMFXY - 1 : 0;
       const float hillcutfactor = (float)kh / (float)(FARGO_DIMFXY - 1);
-      // tiles start at the first own ring (ring 0 unless a radial stripe)
-      const int c0 = D.own_lo * nsec + k * FARGO_CFL_TILE + tid;
       const int iend = D.own_hi;
-      int i = c0 / nsec, j = c0 - i * nsec;
-      // kG cells at a time: their loads are issued together (cells past
-      // the disk's end read cell 0 and are skipped); fewer with more bodies,
-      // whose accumulators take the registers
-      constexpr int kG = NB <= 2 ? 4 : (NB <= 4 ? 2 : 1);
-      for (int g = 0; g < kCflCells; g += kG) {
-        int ci[kG], cj[kG];
-        bool ok[kG];
+      // One cell (ring ic, sector cj): its CFL limit (rings > 0) and its
+      // force on every body.  Ring constants come in rt (dxrad, dxtheta,
+      // their three reciprocals, the ring-mean velocity, Rmed, Surf).
+      auto cell = [&](int ic, int cj, float v0, float vr0, float dn, float vrp, float vtp, float csv, float cth,
+                      float sth, const float (&rt)[8]) {
+        // a NaN or Inf in the state: a NaN dt2d would be skipped by the
+        // minimum below (as the reference's is) and the step would go on
+        // with it; mark the tile instead, so that the DT stops with
+        // FARGO_ENONFINITE (finite values leave lmin as it is)
+        if (!(fabsf(v0) + fabsf(vr0) + fabsf(dn) + fabsf(csv) <= 3.4028235e38f)) lmin = -1.0f;
+        if (ic > 0) {
+          const float dxrad = rt[0], dxt = rt[1];
+          float cs = csv;
+          float vres = D.FastTransport ? v0 - rt[5] : v0;  // vmoy: k_ring_mean<0>
+          // the IEEE quotients by the ring's divisors, from their correctly
+          // rounded reciprocals (Markstein's method, fast_div.cuh)
+          const float rdr = rt[2], rdt = rt[3];
+          float invdt1 = div_by_recip(cs, min2(dxrad, dxt), rt[4]);
+          float invdt2 = div_by_recip(fabsf(vr0), dxrad, rdr);
+          float invdt3 = div_by_recip(fabsf(vres), dxt, rdt);
+          float dvr = vrp - vr0;
+          float dvt = vtp - v0;
+          if (dvr >= 0.0)
+            dvr = 1e-10;
+          else
+            dvr = -dvr;
+          if (dvt >= 0.0)
+            dvt = 1e-10;
+          else
+            dvt = -dvt;
+          float invdt4 = max2(div_by_recip(dvr, dxrad, rdr), div_by_recip(dvt, dxt, rdt));
+          invdt4 *= 4.0 * CVNR * CVNR;
+          // CFLSECURITY / sqrtf(..) divides in double; with CFLSECURITY = 0.5
+          // that is 0.5 * the float IEEE reciprocal, bit for bit (see below)
+          float dt2d =
+              0.5f * __frcp_rn(sqrtf(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 + invdt4 * invdt4));
+          if (dt2d < lmin) lmin = dt2d;
+        }
+        const float Rm = rt[6];
+        float cellmass = rt[7] * dn;
+        float cx = Rm * cth;
+        float cy = Rm * sth;
 #pragma unroll
-        for (int u = 0; u < kG; u++) {
-          ok[u] = i < iend;
-          ci[u] = ok[u] ? i : 0;
-          cj[u] = ok[u] ? j : 0;
-          j += kThreads;
+        for (int b = 0; b < NB; b++) {
+          if (b < nbody) {
+            float dx = cx - s_b[0][b];
+            float dy = cy - s_b[1][b];
+            float rs = s_b[2][b];
+            float d2 = dx * dx + dy * dy;
+            float dist2 = d2 + rs * rs;
+            float distance = sqrtf(dist2);
+            // 1.0/dist2/distance, as one float reciprocal
+            float InvDist3 = __frcp_rn(dist2 * distance);
+            float hill_cut;
+            if (kh != 0) {
+              float rh = s_b[3][b] * hillcutfactor;
+              hill_cut = 1. - expf(-d2 / (rh * rh));
+            } else
+              hill_cut = 1.;
+            const double fx = cellmass * dx * InvDist3 * hill_cut;
+            const double fy = cellmass * dy * InvDist3 * hill_cut;
+            if (Rm < s_b[4][b]) {  // f*_inner (constant indices: the sums stay in registers)
+              acc[b][0] += fx;
+              acc[b][2] += fy;
+            } else {  // f*_outer
+              acc[b][1] += fx;
+              acc[b][3] += fy;
+            }
+          }
+        }
+      };
+      auto ring_consts = [&](int ic, float (&rt)[8]) {
+        rt[0] = D.Rsup[ic] - D.Rinf[ic];
+        rt[1] = D.dxtheta[ic];
+        rt[2] = D.cfl_rdr[ic];
+        rt[3] = D.cfl_rdt[ic];
+        rt[4] = D.cfl_rmd[ic];
+        rt[5] = D.FastTransport ? D.vmoy[ic] : 0.0f;
+        rt[6] = D.Rmed[ic];
+        rt[7] = D.Surf[ic];
+      };
+      if ((nsec & 3) == 0) {
+        // four consecutive cells of one ring per thread and step (16-byte
+        // loads; the ring's constants once per four cells): the tile's 1024
+        // quads, thread tid takes quads tid, tid + 256, ...
+        const int c0 = D.own_lo * nsec + k * FARGO_CFL_TILE + 4 * tid;
+        int i = c0 / nsec, j = c0 - i * nsec;
+#pragma unroll 1
+        for (int g = 0; g < kCflCells / 4; g++) {
+          if (i >= iend) break;
+          const int q = i * nsec + j;
+          const float4 V0 = __ldg(reinterpret_cast<const float4*>(D.vtheta + q));
+          const float4 VR0 = __ldg(reinterpret_cast<const float4*>(D.vrad + q));
+          const float4 DN = __ldg(reinterpret_cast<const float4*>(D.dens + q));
+          const float4 VRP = __ldg(reinterpret_cast<const float4*>(D.vrad + q + nsec));
+          const float vt4 = __ldg(D.vtheta + q - j + (j + 4 == nsec ? 0 : j + 4));
+          const float4 CS = D.Adiabatic ? __ldg(reinterpret_cast<const float4*>(D.cs + q))
+                                        : make_float4(D.cs_ring[i], D.cs_ring[i], D.cs_ring[i], D.cs_ring[i]);
+          const float4 CT = __ldg(reinterpret_cast<const float4*>(D.cos_cell + j));
+          const float4 ST = __ldg(reinterpret_cast<const float4*>(D.sin_cell + j));
+          float rt[8];
+          ring_consts(i, rt);
+          cell(i, j, V0.x, VR0.x, DN.x, VRP.x, V0.y, CS.x, CT.x, ST.x, rt);
+          cell(i, j + 1, V0.y, VR0.y, DN.y, VRP.y, V0.z, CS.y, CT.y, ST.y, rt);
+          cell(i, j + 2, V0.z, VR0.z, DN.z, VRP.z, V0.w, CS.z, CT.z, ST.z, rt);
+          cell(i, j + 3, V0.w, VR0.w, DN.w, VRP.w, vt4, CS.w, CT.w, ST.w, rt);
+          j += 4 * kThreads;
           while (j >= nsec) {
             j -= nsec;
             i++;
           }
         }
-        float v0[kG], vr0[kG], dn[kG], vrp[kG], vtp[kG], csv[kG], cth[kG], sth[kG];
+      } else {
+        const int c0 = D.own_lo * nsec + k * FARGO_CFL_TILE + tid;
+        int i = c0 / nsec, j = c0 - i * nsec;
+        // kG cells at a time: their loads are issued together (cells past
+        // the disk's end read cell 0 and are skipped); fewer with more bodies,
+        // whose accumulators take the registers
+        constexpr int kG = NB <= 2 ? 4 : (NB <= 4 ? 2 : 1);
+        for (int g = 0; g < kCflCells; g += kG) {
+          int ci[kG], cj[kG];
+          bool ok[kG];
 #pragma unroll
-        for (int u = 0; u < kG; u++) {
-          const int q = ci[u] * nsec + cj[u];
-          v0[u] = D.vtheta[q];
-          vr0[u] = D.vrad[q];
-          dn[u] = D.dens[q];
-          vrp[u] = D.vrad[q + nsec];
-          vtp[u] = D.vtheta[q - cj[u] + jwrap_p(cj[u], nsec)];
-          csv[u] = D.Adiabatic ? D.cs[q] : D.cs_ring[ci[u]];
-          cth[u] = D.cos_cell[cj[u]];
-          sth[u] = D.sin_cell[cj[u]];
-        }
-#pragma unroll
-        for (int u = 0; u < kG; u++) {
-          if (!ok[u]) continue;
-          const int ic = ci[u];
-          // a NaN or Inf in the state: a NaN dt2d would be skipped by the
-          // minimum below (as the reference's is) and the step would go on
-          // with it; mark the tile instead, so that the DT stops with
-          // FARGO_ENONFINITE (finite values leave lmin as it is)
-          if (!(fabsf(v0[u]) + fabsf(vr0[u]) + fabsf(dn[u]) + fabsf(csv[u]) <= 3.4028235e38f)) lmin = -1.0f;
-          if (ic > 0) {
-            const float dxrad = D.Rsup[ic] - D.Rinf[ic];
-            const float dxt = D.dxtheta[ic];
-            float cs = csv[u];
-            float vres = D.FastTransport ? v0[u] - D.vmoy[ic] : v0[u];  // vmoy: k_ring_mean<0>
-            // the IEEE quotients by the ring's divisors, from their correctly
-            // rounded reciprocals (Markstein's method, fast_div.cuh)
-            const float rdr = D.cfl_rdr[ic], rdt = D.cfl_rdt[ic];
-            float invdt1 = div_by_recip(cs, min2(dxrad, dxt), D.cfl_rmd[ic]);
-            float invdt2 = div_by_recip(fabsf(vr0[u]), dxrad, rdr);
-            float invdt3 = div_by_recip(fabsf(vres), dxt, rdt);
-            float dvr = vrp[u] - vr0[u];
-            float dvt = vtp[u] - v0[u];
-            if (dvr >= 0.0)
-              dvr = 1e-10;
-            else
-              dvr = -dvr;
-            if (dvt >= 0.0)
-              dvt = 1e-10;
-            else
-              dvt = -dvt;
-            float invdt4 = max2(div_by_recip(dvr, dxrad, rdr), div_by_recip(dvt, dxt, rdt));
-            invdt4 *= 4.0 * CVNR * CVNR;
-            // CFLSECURITY / sqrtf(..) divides in double; with CFLSECURITY = 0.5
-            // that is 0.5 * the float IEEE reciprocal, bit for bit (see below)
-            float dt2d =
-                0.5f * __frcp_rn(sqrtf(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 + invdt4 * invdt4));
-            if (dt2d < lmin) lmin = dt2d;
-          }
-          const float Rm = D.Rmed[ic];
-          float cellmass = D.Surf[ic] * dn[u];
-          float cx = Rm * cth[u];
-          float cy = Rm * sth[u];
-#pragma unroll
-          for (int b = 0; b < NB; b++) {
-            if (b < nbody) {
-              float dx = cx - s_b[0][b];
-              float dy = cy - s_b[1][b];
-              float rs = s_b[2][b];
-              float d2 = dx * dx + dy * dy;
-              float dist2 = d2 + rs * rs;
-              float distance = sqrtf(dist2);
-              // 1.0/dist2/distance, as one float reciprocal
-              float InvDist3 = __frcp_rn(dist2 * distance);
-              float hill_cut;
-              if (kh != 0) {
-                float rh = s_b[3][b] * hillcutfactor;
-                hill_cut = 1. - expf(-d2 / (rh * rh));
-              } else
-                hill_cut = 1.;
-              const double fx = cellmass * dx * InvDist3 * hill_cut;
-              const double fy = cellmass * dy * InvDist3 * hill_cut;
-              if (Rm < s_b[4][b]) {  // f*_inner (constant indices: the sums stay in registers)
-                acc[b][0] += fx;
-                acc[b][2] += fy;
-              } else {  // f*_outer
-                acc[b][1] += fx;
-                acc[b][3] += fy;
-              }
+          for (int u = 0; u < kG; u++) {
+            ok[u] = i < iend;
+            ci[u] = ok[u] ? i : 0;
+            cj[u] = ok[u] ? j : 0;
+            j += kThreads;
+            while (j >= nsec) {
+              j -= nsec;
+              i++;
             }
+          }
+          float v0[kG], vr0[kG], dn[kG], vrp[kG], vtp[kG], csv[kG], cth[kG], sth[kG];
+#pragma unroll
+          for (int u = 0; u < kG; u++) {
+            const int q = ci[u] * nsec + cj[u];
+            v0[u] = D.vtheta[q];
+            vr0[u] = D.vrad[q];
+            dn[u] = D.dens[q];
+            vrp[u] = D.vrad[q + nsec];
+            vtp[u] = D.vtheta[q - cj[u] + jwrap_p(cj[u], nsec)];
+            csv[u] = D.Adiabatic ? D.cs[q] : D.cs_ring[ci[u]];
+            cth[u] = D.cos_cell[cj[u]];
+            sth[u] = D.sin_cell[cj[u]];
+          }
+#pragma unroll
+          for (int u = 0; u < kG; u++) {
+            if (!ok[u]) continue;
+            float rt[8];
+            ring_consts(ci[u], rt);
+            cell(ci[u], cj[u], v0[u], vr0[u], dn[u], vrp[u], vtp[u], csv[u], cth[u], sth[u], rt);
           }
         }
       }
