@@ -34,7 +34,10 @@
 // (a float meeting a double literal is promoted and rounded back on
 // assignment); where the reference computes one IEEE operation in double on
 // two float operands and rounds to float, the float operation is used, which
-// gives the same bits.
+// gives the same bits.  Per-cell quotients by sums of densities (Substep1,
+// Substep2, the viscous update, the velocities) use div_refined
+// (fast_div.cuh): the IEEE quotient but within ~2^-22 ulp of a rounding
+// boundary, one ulp from it there.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -1330,7 +1333,7 @@ __global__ void __launch_bounds__(kThreads, (kAdi == 0 && kSg == 0) ? 3 : 2) k_s
     if (i > 0) {
       const float csm = adi ? 0.0f : D.cs_ring[i - 1];
       const float Pm = adi ? (D.ADIABATICINDEX - 1.0f) * Em[u] : Dnm[u] * csm * csm;
-      float gradp = (P0 - Pm) * 2.0f / (Dn0[u] + Dnm[u]) * D.invdiffRmed[i];
+      float gradp = div_refined((P0 - Pm) * 2.0f, Dn0[u] + Dnm[u]) * D.invdiffRmed[i];
       float gradphi = (Ph0[u] - Phm[u]) * D.invdiffRmed[i];
       if (D.accurate && C->nb > 0) gradphi += D.star_grad[i];
       float vt2 = vth(Vt0[u], i) + vth(Vtp[u], i) + vth(Vtm[u], i - 1) + vth(Vtmp[u], i - 1);
@@ -1346,7 +1349,7 @@ __global__ void __launch_bounds__(kThreads, (kAdi == 0 && kSg == 0) ? 3 : 2) k_s
     float dxtheta = 2.0f * (float)PI_D / (float)nsec * D.Rmed[i];
     float invdxtheta = 1.0f / dxtheta;
     const float Pa = adi ? (D.ADIABATICINDEX - 1.0f) * Ea[u] : Dna[u] * cs * cs;
-    float gradp = (P0 - Pa) * 2.0f / (Dn0[u] + Dna[u]) * invdxtheta;
+    float gradp = div_refined((P0 - Pa) * 2.0f, Dn0[u] + Dna[u]) * invdxtheta;
     float gradphi = (Ph0[u] - Pha[u]) * invdxtheta;
     float v = vth(Vt0[u], i) - dt * (gradp + gradphi);
     v += dt * D.supp_torque[i];
@@ -1641,16 +1644,16 @@ __global__ void __launch_bounds__(kThreads, 3) k_viscosity(BatchDev B) {
 #pragma unroll
           for (int u = 0; u < 4; u++) {
             if (i > 0 && i < nrad - 1) {
-              vti[u] += DeltaT * iRm *
-                        ((Rs * trp1[u] - Ri * trp0[u]) * idRs + (tpp0[u + 1] - tpp0[u]) * invdphi +
-                         0.5f * (trp0[u] + trp1[u])) /
-                        (0.5f * (dn[u + 1] + dn[u]));
+              vti[u] += div_refined(DeltaT * iRm *
+                                        ((Rs * trp1[u] - Ri * trp0[u]) * idRs + (tpp0[u + 1] - tpp0[u]) * invdphi +
+                                         0.5f * (trp0[u] + trp1[u])),
+                                    0.5f * (dn[u + 1] + dn[u]));
             }
             if (i > 0) {
-              vri[u] += DeltaT * iRi *
-                        ((Rm * trr0[u] - Rm1 * trr1[u]) * idRm + (trp0[u + 1] - trp0[u]) * invdphi -
-                         0.5f * (tpp0[u + 1] + tpp1[u])) /
-                        (0.5f * (dn[u + 1] + dnm[u]));
+              vri[u] += div_refined(DeltaT * iRi *
+                                        ((Rm * trr0[u] - Rm1 * trr1[u]) * idRm + (trp0[u + 1] - trp0[u]) * invdphi -
+                                         0.5f * (tpp0[u + 1] + tpp1[u])),
+                                    0.5f * (dn[u + 1] + dnm[u]));
             }
             if (kep && i == 0) vti[u] = vin - D.Rmed[0] * C->OmegaFrame;
             if (kep && i == nrad - 1) vti[u] = vout - D.Rmed[nrad - 1] * C->OmegaFrame;
@@ -1712,12 +1715,12 @@ __global__ void __launch_bounds__(kThreads, kAdi ? 3 : 4) k_source2(BatchDev B) 
     float vr_new = 0.0f;
     if (i > 0) {
       float qrm = qvisc(R0[u] - Rd[u], Nd[u]);
-      vr_new = R0[u] - dt * 2.0f / (N0[u] + Nd[u]) * (qr - qrm) * D.invdiffRmed[i];
+      vr_new = R0[u] - div_refined(dt * 2.0f, N0[u] + Nd[u]) * (qr - qrm) * D.invdiffRmed[i];
     }
     float qtm = qvisc(T0[u] - Tm[u], Nm[u]);
     float dxtheta = 2.0f * (float)PI_D / (float)nsec * D.Rmed[i];
     float invdxtheta = 1.0f / dxtheta;
-    vtn[u] = T0[u] - dt * 2.0f / (N0[u] + Nm[u]) * (qt - qtm) * invdxtheta;
+    vtn[u] = T0[u] - div_refined(dt * 2.0f, N0[u] + Nm[u]) * (qt - qtm) * invdxtheta;
     vrn[u] = vr_new;
     // EnergyInt goes to scratch: the boundary pass before Substep3 still sees the state energy
     if (adi) ein[u] = E0[u] - dt * qr * (Ru[u] - R0[u]) * D.invdiffRsup[i] - dt * qt * (Tp[u] - T0[u]) * invdxtheta;
@@ -2577,8 +2580,8 @@ __global__ void __launch_bounds__(kThreads, kAdi ? 4 : 5) k_velocities(BatchDev 
     if (i == 0)
       vr[u] = 0.0;
     else
-      vr[u] = (Rd[u] + T0[u]) / (A0[u] + Ad[u] + 1e-20f);
-    vt[u] = (Pm[u] + S0[u]) / (A0[u] + Am[u] + 1e-15f) / D.Rmed[i] - D.Rmed[i] * Om;
+      vr[u] = div_refined(Rd[u] + T0[u], A0[u] + Ad[u] + 1e-20f);
+    vt[u] = div_refined(div_refined(Pm[u] + S0[u], A0[u] + Am[u] + 1e-15f), D.Rmed[i]) - D.Rmed[i] * Om;
   }
   qst(D.vrad, q, vr);
   qst(D.vtheta, q, vt);

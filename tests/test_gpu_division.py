@@ -1,4 +1,4 @@
-"""Markstein's division (csrc/fast_div.cuh) against CUDA's IEEE division.
+"""The divisions of csrc/fast_div.cuh against CUDA's IEEE division.
 
 The CFL kernel divides by three per-ring constants (Rsup - Rinf, dxtheta and
 their minimum) through their correctly rounded reciprocals: q0 = RN(x r),
@@ -70,6 +70,41 @@ __global__ void k_check_all(unsigned lo, unsigned hi, unsigned long long* bad, u
   }
 }
 
+// div_refined against the IEEE division: x over the 2^23 significands of
+// [1, 2), d over the given values; counts quotients that differ and those
+// more than one ulp away.
+__global__ void k_check_refined(const float* ds, int nd, unsigned long long* bad) {
+  const int di = blockIdx.y;
+  if (di >= nd) return;
+  const float d = ds[di];
+  unsigned long long n1 = 0, n2 = 0;
+  for (unsigned m = blockIdx.x * blockDim.x + threadIdx.x; m < (1u << 23); m += gridDim.x * blockDim.x) {
+    const float x = __uint_as_float(0x3f800000u | m);
+    const int a = (int)__float_as_uint(__fdiv_rn(x, d)), b = (int)__float_as_uint(div_refined(x, d));
+    if (a != b) n1++;
+    if (a - b > 1 || b - a > 1) n2++;
+  }
+  if (n1) atomicAdd(bad, n1);
+  if (n2) atomicAdd(bad + 1, n2);
+}
+
+extern "C" int check_refined(const float* hd, int nd, unsigned long long* bad_out) {
+  float* d = nullptr;
+  unsigned long long* bad = nullptr;
+  if (cudaMalloc(&d, sizeof(float) * nd) || cudaMalloc(&bad, 16)) return 1;
+  cudaMemcpy(d, hd, sizeof(float) * nd, cudaMemcpyHostToDevice);
+  cudaMemset(bad, 0, 16);
+  for (int o = 0; o < nd; o += 65535) {
+    const int n = nd - o < 65535 ? nd - o : 65535;
+    k_check_refined<<<dim3(64, n), 256>>>(d + o, n, bad);
+  }
+  cudaError_t e = cudaDeviceSynchronize();
+  cudaMemcpy(bad_out, bad, 16, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  cudaFree(bad);
+  return e != cudaSuccess;
+}
+
 extern "C" int check_values(const float* hd, int nd, unsigned long long* bad_out, unsigned* first_out) {
   float* d = nullptr;
   unsigned long long* bad = nullptr;
@@ -123,6 +158,7 @@ def divlib(gpu, tmp_path_factory):
     lib = C.CDLL(str(so))
     lib.check_values.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     lib.check_all.argtypes = [C.c_void_p, C.c_void_p]
+    lib.check_refined.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
     return lib
 
 
@@ -163,3 +199,19 @@ def test_markstein_division_benchmark_denominators(divlib):
 def test_markstein_division_all_significand_pairs(divlib):
     nbad, _, first = _run(divlib, divlib.check_all)
     assert nbad == 0, ("quotient differs from the IEEE division", first)
+
+
+def test_refined_division_within_one_ulp(divlib):
+    """div_refined (the per-cell quotients by density sums): against the IEEE
+    division for every numerator significand and 4096 denominators spread
+    over 2^-40 .. 2^40, no quotient more than one ulp away and fewer than
+    1e-5 of them different at all."""
+    rng = np.random.default_rng(7)
+    ds = (rng.uniform(1.0, 2.0, 4096) * np.exp2(rng.integers(-40, 41, 4096))).astype(np.float32)
+    bad = np.zeros(2, np.uint64)
+    assert divlib.check_refined(ds.ctypes.data, len(ds), bad.ctypes.data) == 0
+    total = len(ds) * (1 << 23)
+    print("\ndiv_refined: %d of %d quotients differ from IEEE (%.2e), %d by more than one ulp"
+          % (int(bad[0]), total, int(bad[0]) / total, int(bad[1])))
+    assert int(bad[1]) == 0
+    assert int(bad[0]) < 1e-5 * total
