@@ -1027,7 +1027,7 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
             float dist2 = d2 + rs * rs;
             float distance = sqrtf(dist2);
             // 1.0/dist2/distance, as one float reciprocal
-            float InvDist3 = __frcp_rn(dist2 * distance);
+            float InvDist3 = div_refined(1.0f, dist2 * distance);
             float hill_cut;
             if (kh != 0) {
               float rh = s_b[3][b] * hillcutfactor;
@@ -1247,7 +1247,7 @@ __global__ void __launch_bounds__(kThreads) k_potential(BatchDev B) {
     for (int u = 0; u < 4; u++) {
       float distance = (x[u] - xp) * (x[u] - xp) + (y[u] - yp) * (y[u] - yp);
       float distancesmooth = sqrtf(distance + sm);
-      float pot = __fdiv_rn(-mp, distancesmooth);  // -G*mplanet/distancesmooth
+      float pot = div_refined(-mp, distancesmooth);  // -G*mplanet/distancesmooth
       if (ind) pot += mp * ip3 * (x[u] * xp + y[u] * yp);
       P[u] += pot;
     }
