@@ -64,6 +64,13 @@ struct fargo_batch {
   // radial stripe (fargo_stripe_create): global ring of local ring 0, the
   // whole disk's ring count, ghost rings below and above the own rings
   int stripe = 0, stripe_base = 0, stripe_nrad = 0, ghost_lo = 0, ghost_hi = 0;
+  // self-gravity of a self-gravitating stripe: the whole disk's convolution
+  // (gsg) on a view gv of the whole grid, whose density is gathered from
+  // every stripe's own rings before each substep; gt: the whole disk's tables
+  SelfGravity* gsg = nullptr;
+  DiskDev gv{};
+  HostTables gt;
+  std::vector<void*> gallocs;
   std::string err;
 };
 
@@ -271,6 +278,8 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   D.QplusMed = qpm;
   if (p->SelfGravity) {
     st = sg_create(&h.sg, p, h.t, b->stream, &D, b->err);
+    if (D.sg_accr) h.allocs.push_back(D.sg_accr);
+    if (D.sg_acct) h.allocs.push_back(D.sg_acct);
     if (st) return st;
   }
   return FARGO_OK;
@@ -378,11 +387,18 @@ fargo_status init_disk_state(fargo_batch* b, int d, const float* dens, const flo
   if ((st = put_ctl_header(b, d, c))) return st;
   CK(cudaMemcpy(b->d_disks + d, &D, sizeof(DiskDev), cudaMemcpyHostToDevice));
   if (p->SelfGravity) {
-    // compute_selfgravity(init) + Init_planetarysys_withSG (Main.cu:302-329)
-    st = sg_accelerations(h.sg, b->bd, d, &D, b->stream, b->err);
+    // compute_selfgravity(init) + Init_planetarysys_withSG (Main.cu:302-329);
+    // a radial stripe takes the whole disk's convolution on the whole
+    // density (gathered into gv.dens by fargo_stripe_init_state), its
+    // tables, and the profile's values at its own rings
+    SelfGravity* sg = b->gsg ? b->gsg : h.sg;
+    DiskDev* G = b->gsg ? &b->gv : &D;
+    const HostTables& T = b->gsg ? b->gt : h.t;
+    const int base = b->gsg ? b->stripe_base : 0;
+    st = sg_accelerations(sg, b->bd, d, G, b->stream, b->err);
     if (st) return st;
-    std::vector<float> axi(nrad);
-    st = sg_axisymmetric(h.sg, &D, axi.data(), b->stream, b->err);
+    std::vector<float> axi(G->nrad);
+    st = sg_axisymmetric(sg, G, axi.data(), b->stream, b->err);
     if (st) return st;
     for (int k = 0; k < pl.nb; k++) {
       float r, dist, ri, rip1, dr, sgacc;
@@ -390,9 +406,9 @@ fargo_status init_disk_state(fargo_batch* b, int d, const float* dens, const flo
       r = pl.x[k];
       dist = (float)(r / (1. + p->ECCENTRICITY));
       ipl = 0;
-      while (h.t.Rmed[ipl] <= dist) ipl++;
-      ri = h.t.Rmed[ipl];
-      rip1 = h.t.Rmed[ipl + 1];
+      while (T.Rmed[ipl] <= dist) ipl++;
+      ri = T.Rmed[ipl];
+      rip1 = T.Rmed[ipl + 1];
       dr = rip1 - ri;
       sgacc = (dist - ri) * axi[ipl + 1] + (rip1 - dist) * axi[ipl];
       sgacc /= dr;
@@ -400,7 +416,7 @@ fargo_status init_disk_state(fargo_batch* b, int d, const float* dens, const flo
     }
     planets_to_ctl(&pl, &c);
     // Init_azimutalvelocity_withSG (SourceEuler.cu:428-437)
-    st = sg_init_vtheta(h.sg, &D, axi.data(), b->stream, b->err);
+    st = sg_init_vtheta(sg, &D, axi.data() + base, b->stream, b->err);
     if (st) return st;
   }
   // OmegaFrame (Main.cu:332-333)
@@ -660,6 +676,8 @@ void batch_free(fargo_batch* b) {
     if (h.sg) sg_destroy(h.sg);
     for (void* p : h.allocs) cudaFree(p);
   }
+  if (b->gsg) sg_destroy(b->gsg);
+  for (void* p : b->gallocs) cudaFree(p);
   void* ps[] = {b->d_disks, b->d_ctl, b->d_cell_off, b->d_ring_off, b->d_theta, b->d_flags, b->d_red,
                 b->d_act, b->d_act_cell};
   for (void* p : ps)
@@ -743,6 +761,8 @@ const char* fargo_last_error(const fargo_ctx* ctx) { return ctx ? ctx->b.err.c_s
 fargo_status fargo_init_state(fargo_ctx* ctx, const float* dens, const float* energy) {
   if (!ctx) return FARGO_EINVAL;
   fargo_batch* b = &ctx->b;
+  if (b->gsg)
+    return set_err(b, FARGO_EINVAL, "a self-gravitating stripe starts from the whole density: fargo_stripe_init_state");
   CK(cudaSetDevice(b->device));
   return init_disk_state(b, 0, dens, energy);
 }
@@ -1008,6 +1028,7 @@ fargo_status fargo_sg_accelerations(fargo_ctx* ctx, float* accr, float* acct) {
   fargo_batch* b = &ctx->b;
   DiskHost& h = b->disks[0];
   if (!h.sg) return set_err(b, FARGO_EINVAL, "fargo_sg_accelerations: the run has no self-gravity");
+  if (b->stripe) return set_err(b, FARGO_EINVAL, "fargo_sg_accelerations: not on a radial stripe");
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
   fargo_status st = sg_accelerations(h.sg, b->bd, 0, &h.dev, b->stream, b->err);
@@ -1313,6 +1334,11 @@ fargo_status fargo_batch_set_precision(fargo_batch* b, int mode) {
       if (st) return st;
     }
   }
+  if (b->gsg) {
+    b->gv.accurate = acc;
+    fargo_status st = sg_tabulate(b->gsg, b->gt, acc, b->stream, b->err);
+    if (st) return st;
+  }
   return FARGO_OK;
 }
 
@@ -1361,8 +1387,6 @@ fargo_status fargo_stripe_create(const fargo_params* p, const fargo_planets* pla
   if (ring_hi - ring_lo < ghost && !(ring_lo == 0 && ring_hi == NRAD))
     return set_err(b, FARGO_EINVAL, "a stripe needs at least as many own rings (%d) as ghost rings (%d)",
                    ring_hi - ring_lo, ghost);
-  if (p->SelfGravity)
-    return set_err(b, FARGO_EINVAL, "self-gravity couples every ring: a self-gravitating disk is not decomposed");
   if (p->OpenInner || p->NonReflecting || p->Evanescent)
     return set_err(b, FARGO_EINVAL, "radial stripes need RIGID inner and outer boundaries");
   std::vector<double> R(NRAD + 1);
@@ -1391,8 +1415,89 @@ fargo_status fargo_stripe_create(const fargo_params* p, const fargo_planets* pla
   b->ghost_hi = top - ring_hi;
   b->bd.ncfl = fargo_cfl_tiles_own(D);
   CK(cudaMemcpy(b->d_disks, &D, sizeof(DiskDev), cudaMemcpyHostToDevice));
+  if (p->SelfGravity) {
+    // the whole disk's convolution: a view of the whole grid with its own
+    // density buffer and ring tables, this stripe's control block
+    host_build_tables(p, R.data(), &b->gt);
+    DiskDev& G = b->gv;
+    G = D;
+    G.nrad = NRAD;
+    G.own_lo = 0;
+    G.own_hi = NRAD;
+    G.sg_accr = G.sg_acct = nullptr;
+    float *gd = nullptr, *gr = nullptr;
+    CK(cudaMalloc(&gd, sizeof(float) * (size_t)NRAD * p->NSEC));
+    b->gallocs.push_back(gd);
+    CK(cudaMalloc(&gr, sizeof(float) * (NRAD + 1)));
+    b->gallocs.push_back(gr);
+    CK(cudaMemcpy(gr, b->gt.Rmed.data(), sizeof(float) * (NRAD + 1), cudaMemcpyHostToDevice));
+    G.dens = gd;
+    G.Rmed = gr;
+    fargo_status sst = sg_create(&b->gsg, p, b->gt, b->stream, &G, b->err);
+    if (G.sg_accr) b->gallocs.push_back(G.sg_accr);
+    if (G.sg_acct) b->gallocs.push_back(G.sg_acct);
+    if (sst) return sst;
+  }
   b->use_graph = false;
   return build_graph(b);
+}
+
+fargo_status fargo_stripe_init_state(fargo_ctx* ctx, const float* dens, const float* energy) {
+  if (!ctx || !ctx->b.stripe) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  CK(cudaSetDevice(b->device));
+  const DiskDev& D = b->disks[0].dev;
+  const int nsec = D.nsec, NRAD = b->stripe_nrad;
+  const size_t off = (size_t)b->stripe_base * nsec;
+  if (b->gsg) {
+    // the whole density, for the initial convolution (the profile by default)
+    std::vector<float> S;
+    const float* src = dens;
+    if (!src) {
+      S.resize((size_t)NRAD * nsec);
+      for (int i = 0; i < NRAD; i++)
+        for (int j = 0; j < nsec; j++) S[(size_t)i * nsec + j] = b->gt.SigmaMed[i];
+      src = S.data();
+    }
+    CK(cudaMemcpy(b->gv.dens, src, sizeof(float) * (size_t)NRAD * nsec, cudaMemcpyHostToDevice));
+  }
+  return init_disk_state(b, 0, dens ? dens + off : nullptr, energy ? energy + off : nullptr);
+}
+
+fargo_status fargo_stripe_sg_rows(fargo_ctx* ctx, float* out) {
+  if (!ctx || !ctx->b.stripe || !out) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  if (!b->gsg) return set_err(b, FARGO_EINVAL, "the stripe has no self-gravity");
+  CK(cudaSetDevice(b->device));
+  const DiskDev& D = b->disks[0].dev;
+  CK(cudaMemcpyAsync(out, D.dens + (size_t)D.own_lo * D.nsec, sizeof(float) * (size_t)(D.own_hi - D.own_lo) * D.nsec,
+                     cudaMemcpyDeviceToDevice, b->stream));
+  return FARGO_OK;
+}
+
+fargo_status fargo_stripe_sg_apply(fargo_ctx* ctx, const float* gathered, int nstripe, int stride,
+                                   const int* cuts) {
+  if (!ctx || !ctx->b.stripe || !gathered || !cuts || nstripe < 1) return FARGO_EINVAL;
+  fargo_batch* b = &ctx->b;
+  if (!b->gsg) return set_err(b, FARGO_EINVAL, "the stripe has no self-gravity");
+  const DiskDev& D = b->disks[0].dev;
+  const int nsec = D.nsec, NRAD = b->stripe_nrad;
+  if (cuts[0] != 0 || cuts[nstripe] != NRAD) return set_err(b, FARGO_EINVAL, "stripe cuts must span 0 .. NRAD");
+  for (int k = 0; k < nstripe; k++)
+    if (cuts[k + 1] <= cuts[k] || (long long)(cuts[k + 1] - cuts[k]) * nsec > stride)
+      return set_err(b, FARGO_EINVAL, "stripe %d: rows %d .. %d do not fit a stride of %d floats", k, cuts[k],
+                     cuts[k + 1], stride);
+  CK(cudaSetDevice(b->device));
+  for (int k = 0; k < nstripe; k++)
+    CK(cudaMemcpyAsync(b->gv.dens + (size_t)cuts[k] * nsec, gathered + (size_t)k * stride,
+                       sizeof(float) * (size_t)(cuts[k + 1] - cuts[k]) * nsec, cudaMemcpyDeviceToDevice, b->stream));
+  sg_capture_substep(b->gsg, b->bd, 0, &b->gv, b->stream);
+  const size_t n = (size_t)D.nrad * nsec, o = (size_t)b->stripe_base * nsec;
+  CK(cudaMemcpyAsync(D.sg_accr, b->gv.sg_accr + o, sizeof(float) * n, cudaMemcpyDeviceToDevice, b->stream));
+  CK(cudaMemcpyAsync(D.sg_acct, b->gv.sg_acct + o, sizeof(float) * n, cudaMemcpyDeviceToDevice, b->stream));
+  b->launches += 6;
+  CK(cudaGetLastError());
+  return FARGO_OK;
 }
 
 fargo_status fargo_stripe_info(fargo_ctx* ctx, fargo_stripe_layout* out) {

@@ -300,11 +300,12 @@ fargo_status sg_axisymmetric(SelfGravity* sg, DiskDev* D, float* axi, cudaStream
 }
 
 fargo_status sg_init_vtheta(SelfGravity* sg, DiskDev* D, const float* axi, cudaStream_t s, std::string& err) {
+  (void)sg;
   float* dax = nullptr;
-  cudaError_t e = cudaMalloc(&dax, sizeof(float) * sg->nrad);
+  cudaError_t e = cudaMalloc(&dax, sizeof(float) * D->nrad);
   if (e) return fail(err, FARGO_EOOM, "cudaMalloc", e);
-  cudaMemcpyAsync(dax, axi, sizeof(float) * sg->nrad, cudaMemcpyHostToDevice, s);
-  k_sg_vtheta<<<blocks((long long)sg->nrad * sg->nsec), 256, 0, s>>>(*D, dax);
+  cudaMemcpyAsync(dax, axi, sizeof(float) * D->nrad, cudaMemcpyHostToDevice, s);
+  k_sg_vtheta<<<blocks((long long)D->nrad * D->nsec), 256, 0, s>>>(*D, dax);
   e = cudaStreamSynchronize(s);
   cudaFree(dax);
   if (e) return fail(err, FARGO_ECUDA, "vtheta init", e);

@@ -19,7 +19,8 @@ fargo_status sg_accelerations(SelfGravity* sg, const BatchDev& b, int d, DiskDev
                               std::string& err);
 // Make1Dprofile(2): ring means of SG_Accr, copied to the host (nrad values)
 fargo_status sg_axisymmetric(SelfGravity* sg, DiskDev* D, float* axi, cudaStream_t s, std::string& err);
-// Init_azimutalvelocity_withSG (SourceEuler.cu:428-437)
+// Init_azimutalvelocity_withSG (SourceEuler.cu:428-437) on the rings of D,
+// axi[i] the axisymmetric acceleration at ring i of D (D->nrad values)
 fargo_status sg_init_vtheta(SelfGravity* sg, DiskDev* D, const float* axi, cudaStream_t s, std::string& err);
 // enqueue the per-substep pipeline (capturable)
 void sg_capture_substep(SelfGravity* sg, const BatchDev& b, int d, DiskDev* D, cudaStream_t s);

@@ -12,6 +12,9 @@ substep:
      (fargo_stripe_substep), then runs the rest of the substep;
   3. the own rings next to each cut are sent to the neighbouring stripe,
      whose ghost rings they replace (halo exchange).
+A self-gravitating disk first gathers every stripe's own density rings
+(all-gather): each stripe runs the whole disk's convolution on the whole
+density and keeps its own rings' accelerations (fargo_stripe_sg_*).
 
 With the cuts on whole CFL tiles and ghost >= FARGO_STRIPE_GHOST the own
 rings carry, after every substep, the bits of the same disk advanced whole.
@@ -87,6 +90,8 @@ class Stripe:
         self.stream = torch.cuda.ExternalStream(lib.fargo_stream(self.ctx), device=self.device)
         self.block_doubles = L.block_doubles
         self.block = None  # allocated by set_stride
+        self.sg = bool(params.SelfGravity)
+        self.sg_send = None  # allocated by set_sg_stride
         f32 = dict(dtype=torch.float32, device=self.device)
         self.send_lo = torch.zeros(max(1, L.halo_floats_lo), **f32)
         self.recv_lo = torch.zeros(max(1, L.halo_floats_lo), **f32)
@@ -100,6 +105,9 @@ class Stripe:
         self.stride = stride
         self.block = torch.zeros(stride, dtype=torch.float64, device=self.device)
 
+    def set_sg_stride(self, stride):
+        self.sg_send = torch.zeros(stride, dtype=torch.float32, device=self.device)
+
     # rows of the whole grid this stripe holds, and the ones it owns (the
     # outer stripe also owns the v_r row at NRAD)
     def local_rows(self):
@@ -112,10 +120,10 @@ class Stripe:
         return b + L["own_lo"], b + top
 
     def init_state(self, dens=None, energy=None):
-        a, b = self.local_rows()
-        d = None if dens is None else np.ascontiguousarray(np.asarray(dens, np.float32)[a:b]).reshape(-1)
-        e = None if energy is None else np.ascontiguousarray(np.asarray(energy, np.float32)[a:b]).reshape(-1)
-        self._chk(lib.fargo_init_state(self.ctx, _fptr(d), _fptr(e)), "fargo_init_state")
+        """Whole-grid (NRAD+1, NSEC) arrays, or None for the profiles."""
+        d = None if dens is None else np.ascontiguousarray(dens, np.float32).reshape(-1)
+        e = None if energy is None else np.ascontiguousarray(energy, np.float32).reshape(-1)
+        self._chk(lib.fargo_stripe_init_state(self.ctx, _fptr(d), _fptr(e)), "fargo_stripe_init_state")
 
     def upload(self, dens=None, vrad=None, vtheta=None, energy=None):
         a, b = self.local_rows()
@@ -136,6 +144,13 @@ class Stripe:
     # the per-substep operations (asynchronous on the stripe's stream, but more)
     def dt_begin(self):
         self._chk(lib.fargo_stripe_dt_begin(self.ctx), "fargo_stripe_dt_begin")
+
+    def sg_rows(self):
+        self._chk(lib.fargo_stripe_sg_rows(self.ctx, _vp(self.sg_send)), "fargo_stripe_sg_rows")
+
+    def sg_apply(self, gathered, nstripe, stride, cuts):
+        c = (C.c_int * len(cuts))(*cuts)
+        self._chk(lib.fargo_stripe_sg_apply(self.ctx, _vp(gathered), nstripe, stride, c), "fargo_stripe_sg_apply")
 
     def forces(self):
         self._chk(lib.fargo_stripe_forces(self.ctx, _vp(self.block)), "fargo_stripe_forces")
@@ -190,7 +205,10 @@ def drive_dt(stripes, xfer):
     for s in stripes:
         s.dt_begin()
     nsub = 0
+    sg = getattr(stripes[0], "sg", False)
     while True:
+        if sg:
+            xfer.sg(stripes)
         for s in stripes:
             s.forces()
         blocks = xfer.gather(stripes)
@@ -219,6 +237,26 @@ class LocalExchange:
         self.stride = max(s.block_doubles for s in stripes)
         for s in stripes:
             s.set_stride(self.stride)
+        if getattr(stripes[0], "sg", False):
+            nsec = stripes[0].params.NSEC
+            self.cuts = [s.lo for s in stripes] + [stripes[-1].hi]
+            self.sg_stride = max(s.hi - s.lo for s in stripes) * nsec
+            for s in stripes:
+                s.set_sg_stride(self.sg_stride)
+
+    def sg(self, stripes):
+        for s in stripes:
+            s.sg_rows()
+        self._drain(stripes)
+        out, cache = [], {}
+        for s in stripes:
+            if s.device not in cache:
+                cache[s.device] = torch.cat([t.sg_send.to(s.device) for t in stripes])
+            out.append(cache[s.device])
+        self._sync(stripes)
+        for s, g in zip(stripes, out):
+            s.sg_apply(g, self.nstripe, self.sg_stride, self.cuts)
+        self._sg = out  # alive until the stripes' streams are drained
 
     @staticmethod
     def _drain(stripes):
@@ -257,7 +295,7 @@ class DistExchange:
     are issued on the stripe's own stream (torch.cuda.ExternalStream), so
     that they follow its kernels and precede its next ones."""
 
-    def __init__(self, stripes, group=None):
+    def __init__(self, stripes, group=None, parts=None):
         import torch.distributed as dist
         (s,) = stripes
         self.dist, self.group = dist, group
@@ -269,6 +307,19 @@ class DistExchange:
         self.stride = int(m.item())
         s.set_stride(self.stride)
         self.out = torch.zeros(self.nstripe * self.stride, dtype=torch.float64, device=s.block.device)
+        if getattr(s, "sg", False):
+            nsec = s.params.NSEC
+            self.cuts = [lo for lo, _ in parts] + [parts[-1][1]]
+            self.sg_stride = max(hi - lo for lo, hi in parts) * nsec
+            s.set_sg_stride(self.sg_stride)
+            self.sg_out = torch.zeros(self.nstripe * self.sg_stride, dtype=torch.float32, device=s.sg_send.device)
+
+    def sg(self, stripes):
+        (s,) = stripes
+        s.sg_rows()
+        with self._on(s):
+            self.dist.all_gather(list(self.sg_out.split(self.sg_stride)), s.sg_send, group=self.group)
+        s.sg_apply(self.sg_out, self.nstripe, self.sg_stride, self.cuts)
 
     def _on(self, s):
         return torch.cuda.stream(s.stream) if s.stream is not None else _Null()
@@ -380,7 +431,7 @@ class DistStripes(_StripedDisk):
         if device is None:
             device = torch.cuda.current_device()
         self.stripes = [Stripe(params, planets, lo, hi, ghost, device, radii, r, n)]
-        self.xfer = DistExchange(self.stripes, group)
+        self.xfer = DistExchange(self.stripes, group, self.parts)
 
     def fields(self):
         """Whole-grid {field: (NRAD+1, NSEC)} on every rank (all-gather of

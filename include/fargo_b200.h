@@ -329,6 +329,9 @@ fargo_status fargo_autotune(fargo_ctx* ctx, int reps, int* seg_out);
    disk of its own.  One DT, driven by the caller:
      fargo_stripe_dt_begin
      do {
+       [self-gravity: fargo_stripe_sg_rows(rows) -> gather every stripe's
+        rows in stripe order -> fargo_stripe_sg_apply(gathered): the whole
+        disk's convolution on the whole density, this stripe's rings of it]
        fargo_stripe_forces(block)       CFL minimum and force partials of the
                                         own rings -> this stripe's block
        gather every stripe's block, in stripe order, each `stride` doubles
@@ -345,13 +348,18 @@ fargo_status fargo_autotune(fargo_ctx* ctx, int reps, int* seg_out);
    every substep with the bits of the undecomposed disk: the tiles and the
    finishing sums are the same, and the cut edges' boundary treatment
    reaches fewer than FARGO_STRIPE_GHOST rings into the ghosts in one
-   substep (4 to 5 rings, measured).  Stripes need RIGID boundaries and no
-   self-gravity (FARGO_EINVAL otherwise), at least `ghost` own rings each,
-   and the same parameters, radii and planets.
-   Upload the initial state of the stripe's rings base .. base+nrad (the
-   local grid, ghost row included) with fargo_init_state or fargo_upload,
-   then exchange halos once before the first DT.  fargo_advance* and the
-   CUDA graph are not available on a stripe. */
+   substep (4 to 5 rings, measured).  Stripes need RIGID boundaries
+   (FARGO_EINVAL otherwise), at least `ghost` own rings each, and the same
+   parameters, radii and planets.  Self-gravity couples every ring: each
+   stripe runs the whole disk's log-polar convolution on the whole density,
+   gathered from the stripes' own rings before every substep, and keeps its
+   own rings' accelerations; the result stays bit-identical to the whole
+   disk's.  Start with fargo_stripe_init_state (the whole grid's arrays; the
+   stripe takes its rings, a self-gravitating one the whole density too) or
+   upload the stripe's rings base .. base+nrad (the local grid, ghost row
+   included) with fargo_upload, then exchange halos once before the first
+   DT.  fargo_advance*, the CUDA graph and fargo_sg_accelerations are not
+   available on a stripe. */
 #define FARGO_STRIPE_GHOST 8
 #define FARGO_STRIPE_MAX_GHOST 64
 typedef struct {
@@ -367,6 +375,17 @@ typedef struct {
 fargo_status fargo_stripe_create(const fargo_params* p, const fargo_planets* planets, const double* radii,
                                  int ring_lo, int ring_hi, int ghost, int device, fargo_ctx** out);
 fargo_status fargo_stripe_info(fargo_ctx* ctx, fargo_stripe_layout* out);
+/* dens / energy: (NRAD+1)*NSEC host arrays of the whole grid, or NULL for
+   the reference's profiles (as fargo_init_state) */
+fargo_status fargo_stripe_init_state(fargo_ctx* ctx, const float* dens, const float* energy);
+/* self-gravity: the density of the own rings -> out ((own_hi-own_lo)*NSEC
+   floats, device); the gathered rows of every stripe (stripe k's at
+   gathered + k*stride, its rings cuts[k] .. cuts[k+1]-1; cuts: host array of
+   nstripe+1 rings) -> the whole disk's convolution, this stripe's rings of
+   it.  Asynchronous on the stripe's stream. */
+fargo_status fargo_stripe_sg_rows(fargo_ctx* ctx, float* out);
+fargo_status fargo_stripe_sg_apply(fargo_ctx* ctx, const float* gathered, int nstripe, int stride,
+                                   const int* cuts);
 fargo_status fargo_stripe_dt_begin(fargo_ctx* ctx);
 /* device pointers; the calls are asynchronous on the context's stream
    (fargo_stream) except fargo_stripe_more */

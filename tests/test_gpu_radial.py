@@ -8,6 +8,10 @@ row of every field and the planets.
   circular orbit) in 2 and 3 stripes;
 - C2 (256x768, adiabatic, alpha viscosity, two live planets that feel the
   disk) in 2 and 4 stripes.
+- C3 (512x1024, self-gravity) in 2 and 4 stripes, and C5's grid and physics
+  (2048x6144, adiabatic, self-gravity, three live planets; DT shortened to
+  0.004, a few substeps) in 2 stripes: every stripe gathers the whole
+  density before each substep and runs the whole disk's convolution.
 Cuts off the CFL tile grid group the force sums differently: the result
 then stays within the FP32 rounding floor of the whole disk (FIELD_TOL).
 A NaN in one stripe's own rings stops every stripe's DT with
@@ -68,6 +72,26 @@ def test_c1_stripes_bit_identical(gpu, nstripes):
 @pytest.mark.parametrize("nstripes", [2, 4])
 def test_c2_stripes_bit_identical(gpu, nstripes):
     P, nw, ns, a, b, pa, pb, sa, sb = _run_pair(configs.c2(), "rad_c2", nstripes, 3)
+    assert nw == ns
+    for k in KEYS:
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(pa, pb)
+
+
+@pytest.mark.parametrize("nstripes", [2, 4])
+def test_c3_self_gravity_stripes_bit_identical(gpu, nstripes):
+    P, nw, ns, a, b, pa, pb, _, _ = _run_pair(configs.c3(), "rad_c3", nstripes, 2)
+    assert nw == ns
+    for k in KEYS:
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(pa, pb)
+
+
+def test_c5_stripes_bit_identical(gpu):
+    p, pl = configs.c5()
+    p = dict(p, DT="0.004")
+    P, nw, ns, a, b, pa, pb, _, _ = _run_pair((p, pl), "rad_c5", 2, 1)
+    print("\nC5 in 2 stripes: %d substeps" % ns[0])
     assert nw == ns
     for k in KEYS:
         assert np.array_equal(a[k], b[k]), k

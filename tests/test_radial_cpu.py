@@ -8,7 +8,9 @@
   stand-in run undecomposed.  The stand-in's update has a radial reach per
   substep and a boundary rule at its local edges, so a ghost zone narrower
   than the reach, a halo sent the wrong way or blocks gathered out of order
-  all change the result.
+  all change the result.  Its self-gravitating form also takes a term from
+  every ring of the whole grid (the gathered own rows), as the library's
+  stripes take the whole disk's convolution.
 - fargo_stripe_create's argument checks (no GPU needed: they run first).
 """
 import ctypes as C
@@ -16,6 +18,8 @@ import multiprocessing as mp
 import os
 import socket
 import tempfile
+
+import types
 
 import numpy as np
 import pytest
@@ -40,8 +44,10 @@ class FakeStripe:
     passes of a 3-row stencil plus the gathered total, with a boundary rule
     on the local edge rows (the cut edges' rule is not the disk's)."""
 
-    def __init__(self, lo, hi, ghost, u0):
-        self.lo, self.hi = lo, hi
+    def __init__(self, lo, hi, ghost, u0, sg=False):
+        self.lo, self.hi, self.sg = lo, hi, sg
+        self.params = types.SimpleNamespace(NSEC=NSEC)
+        self.gterm = 0.0
         self.base = max(0, lo - ghost)
         top = min(NRAD, hi + ghost)
         self.own_lo, self.own_hi = lo - self.base, hi - self.base
@@ -59,6 +65,20 @@ class FakeStripe:
     def set_stride(self, stride):
         self.stride = stride
         self.block = torch.zeros(stride, dtype=torch.float64)
+
+    def set_sg_stride(self, stride):
+        self.sg_send = torch.zeros(stride, dtype=torch.float32)
+
+    def sg_rows(self):
+        own = self.u[self.own_lo:self.own_hi].reshape(-1)
+        self.sg_send[:own.size].copy_(torch.from_numpy(own.copy()))
+
+    def sg_apply(self, gathered, nstripe, stride, cuts):
+        g = gathered.numpy()
+        whole = np.concatenate([g[k * stride:k * stride + (cuts[k + 1] - cuts[k]) * NSEC] for k in range(nstripe)])
+        ring = whole.reshape(NRAD, NSEC).astype(np.float64).mean(axis=1)
+        ring = np.append(ring, 0.0)  # the row at NRAD
+        self.gterm = (1e-4 * ring[self.base:self.base + self.u.shape[0]]).astype(np.float32)[:, None]
 
     def dt_begin(self):
         self.dtemp = 0.0
@@ -87,6 +107,7 @@ class FakeStripe:
         for _ in range(REACH):
             v = u.copy()
             v[1:-1] = u[1:-1] + np.float32(0.2) * (u[:-2] - 2 * u[1:-1] + u[2:]) + np.float32(1e-6 * total)
+            v = v + self.gterm
             v[0] = np.float32(0.5) * u[1]  # boundary rule at the local edges
             v[-1] = np.float32(0.5) * u[-2]
             u = np.roll(v, 1, axis=1)
@@ -113,8 +134,8 @@ class FakeStripe:
         return self.u[self.own_lo:top]
 
 
-def _whole(ndt):
-    s = FakeStripe(0, NRAD, 1, _init())
+def _whole(ndt, sg=False):
+    s = FakeStripe(0, NRAD, 1, _init(), sg)
     x = radial.LocalExchange([s])
     n = [radial.drive_dt([s], x) for _ in range(ndt)]
     return s.own(), n, s.history
@@ -144,10 +165,11 @@ def test_partition_cuts_on_whole_tiles():
         radial.partition(64, 384, 8)  # 32-ring granule: stripes of 0 or 32 rings
 
 
-def test_local_exchange_matches_whole():
-    want, nsub, hist = _whole(3)
+@pytest.mark.parametrize("sg", [False, True], ids=["plain", "self-gravity"])
+def test_local_exchange_matches_whole(sg):
+    want, nsub, hist = _whole(3, sg)
     for parts, ghost in ([[(0, 20), (20, 40), (40, 60)], 10], [[(0, 24), (24, 60)], 12]):
-        ss = [FakeStripe(lo, hi, ghost, _init()) for lo, hi in parts]
+        ss = [FakeStripe(lo, hi, ghost, _init(), sg) for lo, hi in parts]
         x = radial.LocalExchange(ss)
         got = [radial.drive_dt(ss, x) for _ in range(3)]
         assert got == nsub
@@ -166,7 +188,7 @@ def test_narrow_ghost_zone_is_detected():
     assert not np.array_equal(_assemble(ss), want)
 
 
-def _rank_main(rank, world, port, out):
+def _rank_main(rank, world, port, out, sg):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
     import datetime
     import torch.distributed as dist
@@ -174,8 +196,8 @@ def _rank_main(rank, world, port, out):
     try:
         parts = radial.partition(NRAD, NSEC, world, ghost=REACH + 1, aligned=False)
         lo, hi = parts[rank]
-        s = FakeStripe(lo, hi, REACH + 1, _init())
-        x = radial.DistExchange([s])
+        s = FakeStripe(lo, hi, REACH + 1, _init(), sg)
+        x = radial.DistExchange([s], parts=parts)
         nsub = [radial.drive_dt([s], x) for _ in range(3)]
         np.savez(out % rank, own=s.own(), lo=lo, nsub=nsub, hist=np.array(s.history))
         dist.barrier()
@@ -189,13 +211,13 @@ def _free_port():
         return s.getsockname()[1]
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_gloo_ranks_match_whole(world):
-    want, nsub, hist = _whole(3)
+@pytest.mark.parametrize("world,sg", [(2, False), (3, False), (3, True)])
+def test_gloo_ranks_match_whole(world, sg):
+    want, nsub, hist = _whole(3, sg)
     out = os.path.join(tempfile.mkdtemp(prefix="fargo_radial_"), "rank%d.npz")
     ctx = mp.get_context("spawn")
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, out)) for r in range(world)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, out, sg)) for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
@@ -221,9 +243,9 @@ def test_stripe_create_checks_arguments():
         assert st == 1, (lo, hi, ghost)  # FARGO_EINVAL
         assert lib.fargo_last_error(ctx)
         lib.fargo_destroy(ctx)
-    sg = type(P).from_buffer_copy(P)
-    sg.SelfGravity = 1
+    op = type(P).from_buffer_copy(P)
+    op.OpenInner = 1
     ctx = C.c_void_p()
-    assert lib.fargo_stripe_create(C.byref(sg), C.byref(FargoPlanets()), None, 0, 32, 8, 0, C.byref(ctx)) == 1
-    assert b"self-gravity" in lib.fargo_last_error(ctx)
+    assert lib.fargo_stripe_create(C.byref(op), C.byref(FargoPlanets()), None, 0, 32, 8, 0, C.byref(ctx)) == 1
+    assert b"RIGID" in lib.fargo_last_error(ctx)
     lib.fargo_destroy(ctx)
