@@ -8,7 +8,14 @@
 //     every call (SgMain.cu:124,138);
 //   - the density transforms are real-to-complex and the inverse
 //     complex-to-real (the inputs are real, so the reference's C2C result
-//     is the same Hermitian spectrum), batched two at a time;
+//     is the same Hermitian spectrum);
+//   - the 2-D transforms are done as their row and column passes, pruned:
+//     the density occupies rows 0 .. NRAD-1 of the zero-padded 2 NRAD rows,
+//     so the forward azimuthal (row) transforms run on those rows only, into
+//     a spectrum buffer whose rows NRAD .. 2 NRAD-1 stay zero, and the
+//     inverse ones only on the rows the accelerations use; the radial
+//     (column) transforms take all 2 NRAD rows, strided, one column per
+//     transform of the batch;
 //   - the velocity kick (Update_sgvelocityKernel) is fused into the
 //     Substep1 kernel, so the accelerations are stored once and read once.
 #include <cufft.h>
@@ -23,49 +30,46 @@
 
 struct SelfGravity {
   int nrad = 0, nsec = 0, nx = 0, nyh = 0;
-  cufftHandle fwd = 0, inv = 0;
-  float* real2 = nullptr;     // [2][2*nrad][nsec]: Sr, St, then Gr, Gphi
-  float2* spec2 = nullptr;    // [2][2*nrad][nsec/2+1]
-  float2* khat = nullptr;     // [2][2*nrad][nsec/2+1]: K^r, K^t spectra
+  cufftHandle rowf = 0, rowi = 0, col = 0;  // row R2C / C2R on nrad rows, column C2C on 2 nrad rows
+  // the two fields (Sr, St; then Gr, Gphi) interleaved by row, so that one
+  // transform call takes both: element (row i, field f, column j)
+  float* real2 = nullptr;     // [nrad][2][nsec]
+  float2* rows2 = nullptr;    // [2*nrad][2][nsec/2+1]: row spectra, rows nrad.. zero
+  float2* spec2 = nullptr;    // [2*nrad][2][nsec/2+1]: 2-D spectra
+  float2* khat = nullptr;     // [2*nrad][2][nsec/2+1]: K^r, K^t spectra
   float eps = 0, rstep = 0, tstep = 0;
   bool plans = false;
 };
 
 namespace {
 
-// ComputeFFTKernel's density part (Kernels.cu:957-976) as real arrays.
-__global__ void k_sg_pad(DiskDev D, float* real2, float eps) {
+// ComputeFFTKernel's density part (Kernels.cu:957-976) as real arrays, on
+// the rows that hold the density (the padding rows are the zero rows of the
+// row-spectrum buffer).
+__global__ void k_sg_pad(DiskDev D, float* real2) {
   const int nrad = D.nrad, nsec = D.nsec;
-  long long n = 2LL * nrad * nsec;
+  long long n = (long long)nrad * nsec;
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   if (!D.ctl->active) return;
-  int i = (int)(c / nsec);
-  float sr = 0.0f, st = 0.0f;
-  if (i < nrad) {
-    float var = D.dens[c] * sqrtf(D.Rmed[i] / D.Rmed[0]);
-    sr = var;
-    st = var * D.Rmed[i] / D.Rmed[0];
-  }
-  real2[c] = sr;
-  real2[n + c] = st;
-  (void)eps;
+  int i = (int)(c / nsec), j = (int)(c - (long long)i * nsec);
+  float var = D.dens[c] * sqrtf(D.Rmed[i] / D.Rmed[0]);
+  float* row = real2 + 2LL * i * nsec + j;
+  row[0] = var;
+  row[nsec] = var * D.Rmed[i] / D.Rmed[0];
 }
 
-// ComputeConvolutionKernel, Kernels.cu:980-999 (half spectrum)
-__global__ void k_sg_mul(const DiskCtl* C, float2* spec2, const float2* khat, long long nh) {
+// ComputeConvolutionKernel, Kernels.cu:980-999 (half spectrum): G = -K S
+// for both fields, element by element (spectra and kernels share a layout)
+__global__ void k_sg_mul(const DiskCtl* C, float2* spec2, const float2* khat, long long n) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nh) return;
+  if (c >= n) return;
   if (!C->active) return;
-  float2 sr = spec2[c], st = spec2[nh + c];
-  float2 kr = khat[c], kt = khat[nh + c];
-  float2 gr, gp;
-  gp.x = -1.0 * (kt.x * st.x - kt.y * st.y);
-  gp.y = -1.0 * (kt.x * st.y + kt.y * st.x);
-  gr.x = -1.0 * (kr.x * sr.x - kr.y * sr.y);
-  gr.y = -1.0 * (kr.x * sr.y + kr.y * sr.x);
-  spec2[c] = gr;
-  spec2[nh + c] = gp;
+  const float2 sv = spec2[c], k = khat[c];
+  float2 g;
+  g.x = -1.0 * (k.x * sv.x - k.y * sv.y);
+  g.y = -1.0 * (k.x * sv.y + k.y * sv.x);
+  spec2[c] = g;
 }
 
 // ComputeSgAccKernel, Kernels.cu:1002-1021 (the C2R output is unnormalised,
@@ -76,16 +80,16 @@ __global__ void k_sg_acc(DiskDev D, const float* real2, float rstep, float tstep
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   if (!D.ctl->active) return;
-  int i = (int)(c / nsec);
-  long long n2 = 2LL * nrad * nsec;
+  int i = (int)(c / nsec), j = (int)(c - (long long)i * nsec);
+  const float* row = real2 + 2LL * i * nsec + j;  // Gr, then Gphi one row on
   float normaccr, normacct, divRmed;
   divRmed = D.Rmed[i] / D.Rmed[0];
   normaccr = rstep * tstep / ((float)(2 * nrad) * (float)nsec);
   normacct = normaccr;
   normaccr /= sqrtf(divRmed);
   normacct /= (divRmed * sqrtf(divRmed));
-  D.sg_acct[c] = real2[n2 + c] * normacct;
-  float a = real2[c] * normaccr;
+  D.sg_acct[c] = row[nsec] * normacct;
+  float a = row[0] * normaccr;
   a += 1.0 * D.dens[c] * rstep * tstep / eps;
   D.sg_accr[c] = a;
 }
@@ -132,9 +136,13 @@ __global__ void k_sg_vtheta(DiskDev D, const float* axi) {
   D.vtheta[c] = D.Rmed[i] * omega;
 }
 
-__global__ void k_to_complex_float(const double2* in, float2* out, long long n) {
+// [2][rows][nyh] FP64 spectra -> [rows][2][nyh] FP32 (fields interleaved by row)
+__global__ void k_to_complex_float(const double2* in, float2* out, long long rows, int nyh) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < n) out[c] = make_float2((float)in[c].x, (float)in[c].y);
+  if (c >= 2 * rows * nyh) return;
+  const long long nh = rows * nyh;
+  const long long f = c / nh, r = (c - f * nh) / nyh, m = c - f * nh - r * nyh;
+  out[(r * 2 + f) * nyh + m] = make_float2((float)in[c].x, (float)in[c].y);
 }
 
 inline unsigned blocks(long long n) { return (unsigned)((n + 255) / 256); }
@@ -161,24 +169,33 @@ fargo_status sg_create(SelfGravity** out, const fargo_params* p, const HostTable
   sg->eps = p->THICKNESSSMOOTHING * p->ASPECTRATIO;
   sg->rstep = logf(t.Radii[NRAD] / t.Radii[0]) / (float)NRAD;
   sg->tstep = 2.0 * PI_D / (float)NSEC;
-  long long nr = (long long)sg->nx * NSEC, nh = (long long)sg->nx * sg->nyh;
+  long long nr = (long long)NRAD * NSEC, nh = (long long)sg->nx * sg->nyh;
   cudaError_t e;
   if ((e = cudaMalloc(&sg->real2, sizeof(float) * 2 * nr))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  if ((e = cudaMalloc(&sg->rows2, sizeof(float2) * 2 * nh))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
   if ((e = cudaMalloc(&sg->spec2, sizeof(float2) * 2 * nh))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
   if ((e = cudaMalloc(&sg->khat, sizeof(float2) * 2 * nh))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
   if ((e = cudaMalloc(&D->sg_accr, sizeof(float) * (size_t)NRAD * NSEC))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
   if ((e = cudaMalloc(&D->sg_acct, sizeof(float) * (size_t)NRAD * NSEC))) return fail(err, FARGO_EOOM, "cudaMalloc", e);
+  cudaMemsetAsync(sg->rows2, 0, sizeof(float2) * 2 * nh, s);  // the padding rows stay zero
   cudaMemsetAsync(D->sg_accr, 0, sizeof(float) * (size_t)NRAD * NSEC, s);
   cudaMemsetAsync(D->sg_acct, 0, sizeof(float) * (size_t)NRAD * NSEC, s);
-  int n[2] = {sg->nx, NSEC};
+  // row transforms: the 2 NRAD rows (both fields) of the density;
+  // column transforms: the 2 nyh columns (both fields), 2 NRAD long
+  int nsec1[1] = {NSEC}, nx1[1] = {sg->nx};
+  int rin[1] = {NSEC}, rout[1] = {sg->nyh}, cemb[1] = {sg->nx};
+  const int ncol = 2 * sg->nyh;
   cufftResult r;
-  if ((r = cufftPlanMany(&sg->fwd, 2, n, nullptr, 1, (int)nr, nullptr, 1, (int)nh, CUFFT_R2C, 2)))
+  if ((r = cufftPlanMany(&sg->rowf, 1, nsec1, rin, 1, NSEC, rout, 1, sg->nyh, CUFFT_R2C, 2 * NRAD)))
     return fail(err, FARGO_ECUFFT, "cufftPlanMany R2C", r);
-  if ((r = cufftPlanMany(&sg->inv, 2, n, nullptr, 1, (int)nh, nullptr, 1, (int)nr, CUFFT_C2R, 2)))
+  if ((r = cufftPlanMany(&sg->rowi, 1, nsec1, rout, 1, sg->nyh, rin, 1, NSEC, CUFFT_C2R, 2 * NRAD)))
     return fail(err, FARGO_ECUFFT, "cufftPlanMany C2R", r);
+  if ((r = cufftPlanMany(&sg->col, 1, nx1, cemb, ncol, 1, cemb, ncol, 1, CUFFT_C2C, ncol)))
+    return fail(err, FARGO_ECUFFT, "cufftPlanMany C2C", r);
   sg->plans = true;
-  cufftSetStream(sg->fwd, s);
-  cufftSetStream(sg->inv, s);
+  cufftSetStream(sg->rowf, s);
+  cufftSetStream(sg->rowi, s);
+  cufftSetStream(sg->col, s);
   return sg_tabulate(sg, t, 0, s, err);
 }
 
@@ -239,7 +256,7 @@ fargo_status sg_tabulate(SelfGravity* sg, const HostTables& t, int accurate, cud
   }
   cufftSetStream(pd, s);
   r = cufftExecD2Z(pd, dK, dKh);
-  k_to_complex_float<<<blocks(2 * nh), 256, 0, s>>>(dKh, sg->khat, 2 * nh);
+  k_to_complex_float<<<blocks(2 * nh), 256, 0, s>>>(dKh, sg->khat, sg->nx, sg->nyh);
   cudaStreamSynchronize(s);
   cufftDestroy(pd);
   cudaFree(dK);
@@ -251,10 +268,12 @@ fargo_status sg_tabulate(SelfGravity* sg, const HostTables& t, int accurate, cud
 void sg_destroy(SelfGravity* sg) {
   if (!sg) return;
   if (sg->plans) {
-    cufftDestroy(sg->fwd);
-    cufftDestroy(sg->inv);
+    cufftDestroy(sg->rowf);
+    cufftDestroy(sg->rowi);
+    cufftDestroy(sg->col);
   }
   cudaFree(sg->real2);
+  cudaFree(sg->rows2);
   cudaFree(sg->spec2);
   cudaFree(sg->khat);
   delete sg;
@@ -263,14 +282,19 @@ void sg_destroy(SelfGravity* sg) {
 void sg_capture_substep(SelfGravity* sg, const BatchDev& b, int d, DiskDev* D, cudaStream_t s) {
   (void)b;
   (void)d;
-  long long nr = (long long)sg->nx * sg->nsec, nh = (long long)sg->nx * sg->nyh;
-  cufftSetStream(sg->fwd, s);
-  cufftSetStream(sg->inv, s);
-  k_sg_pad<<<blocks(nr), 256, 0, s>>>(*D, sg->real2, sg->eps);
-  cufftExecR2C(sg->fwd, sg->real2, (cufftComplex*)sg->spec2);
-  k_sg_mul<<<blocks(nh), 256, 0, s>>>(D->ctl, sg->spec2, sg->khat, nh);
-  cufftExecC2R(sg->inv, (cufftComplex*)sg->spec2, sg->real2);
-  k_sg_acc<<<blocks((long long)sg->nrad * sg->nsec), 256, 0, s>>>(*D, sg->real2, sg->rstep, sg->tstep, sg->eps);
+  const long long nr = (long long)sg->nrad * sg->nsec, nh = (long long)sg->nx * sg->nyh;
+  cufftSetStream(sg->rowf, s);
+  cufftSetStream(sg->rowi, s);
+  cufftSetStream(sg->col, s);
+  cufftComplex* rows = reinterpret_cast<cufftComplex*>(sg->rows2);
+  cufftComplex* spec = reinterpret_cast<cufftComplex*>(sg->spec2);
+  k_sg_pad<<<blocks(nr), 256, 0, s>>>(*D, sg->real2);
+  cufftExecR2C(sg->rowf, sg->real2, rows);                    // rows 0 .. nrad-1 of both fields
+  cufftExecC2C(sg->col, rows, spec, CUFFT_FORWARD);          // all 2 nrad rows
+  k_sg_mul<<<blocks(2 * nh), 256, 0, s>>>(D->ctl, sg->spec2, sg->khat, 2 * nh);
+  cufftExecC2C(sg->col, spec, spec, CUFFT_INVERSE);
+  cufftExecC2R(sg->rowi, spec, sg->real2);                    // rows 0 .. nrad-1 of both fields
+  k_sg_acc<<<blocks(nr), 256, 0, s>>>(*D, sg->real2, sg->rstep, sg->tstep, sg->eps);
   k_sg_axi_edges<<<1, 32, 0, s>>>(*D);
 }
 
