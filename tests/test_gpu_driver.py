@@ -75,10 +75,10 @@ def test_driver_output_files_match_reference(gpu, tmp_path):
     PhysicalTime and OmegaFrame exact, CircumPlanetaryMass to 1e-4;
     tqwk0.dat (UpdateLog, Force.cu:76-138) torques and powers within 1e-4 of
     each column's largest value (FP64 force sums here, FP32 tree sums in the
-    reference, of fields within FIELD_TOL); the fields after 10 DTs within
-    FIELD_TOL."""
+    reference, of fields within REF_TOL); the fields after 10 DTs within
+    REF_TOL (tests/helpers.py)."""
     from tests.golden import make_ref_golden as G
-    from tests.helpers import FIELD_TOL, rel_l2
+    from tests.helpers import REF_TOL, rel_l2
     z = np.load(os.path.join(HERE, "golden", "ref_c1_128x384.npz"))
     p, pl, seed, ndt = G.cases()["ref_c1_128x384"]
     assert seed is None
@@ -106,4 +106,4 @@ def test_driver_output_files_match_reference(gpu, tmp_path):
     nrad, nsec = int(z["nrad"]), int(z["nsec"])
     for fld in ("dens", "vrad", "vtheta"):
         a = np.fromfile(os.path.join(out, fld, "%s1.dat" % fld), np.float32).reshape(nrad, nsec)
-        assert rel_l2(a, z[fld + "1"]) <= FIELD_TOL[fld], fld
+        assert rel_l2(a, z[fld + "1"]) <= REF_TOL[fld], fld

@@ -44,6 +44,8 @@ def _compare(P, d, o, ndt, fields=("dens", "vrad", "vtheta"), tol=TOL, scale=1.0
         assert np.array_equal(dt1, dt2), "substep dt differ"
     a, b = d.fields(), o.fields()
     errs = {k: rel_l2(a[k][:P.NRAD], b[k][:P.NRAD]) for k in fields}
+    print("\nCUDA vs oracle %dx%d after %d DTs: %s" % (P.NRAD, P.NSEC, ndt,
+                                                      {k: "%.2e" % e for k, e in errs.items()}))
     for k, e in errs.items():
         assert e <= tol[k] * scale, (k, e, errs)
     pa, pb = planets_dict(d.planets()), planets_dict(o.planets())

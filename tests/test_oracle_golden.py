@@ -7,7 +7,7 @@ oracle (float build) restarted from the same parameters must reproduce the
 reference's initial fields, every substep's dt and every ring's FARGO shift
 count exactly, and the fields after 10 DTs within the rounding-order floor
 between two FP32 builds: nvcc contracts a*b+c into fused multiply-adds, the
-oracle's gcc build does not.  The bound is FIELD_TOL (tests/helpers.py) or,
+oracle's gcc build does not.  The bound is REF_TOL (tests/helpers.py) or,
 where this case's own floor is wider (the larger grids), twice the measured
 distance between the oracle's plain and FMA-contracted builds (floor_tol)."""
 import glob
@@ -19,11 +19,11 @@ import pytest
 from cudaprotoplanetarydisksfloat_b200 import noise
 from oracle.oracle import Oracle, set_threads
 from tests.golden import make_ref_golden as G
-from tests.helpers import FIELD_TOL, floor_tol, make, rel_l2
+from tests.helpers import REF_TOL, floor_tol, make, rel_l2
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_*.npz")))
-TOL = FIELD_TOL
+TOL = REF_TOL
 
 
 def _setup(name):
