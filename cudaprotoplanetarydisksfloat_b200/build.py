@@ -20,7 +20,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
            "-diag-suppress", "177", "-I" + os.path.join(ROOT, "include")]
 
-LIB_SOURCES = ["kernels_step.cu", "fargo_api.cu", "sg.cu", "noalloc.cu", "host_params.cpp", "host_setup.cpp"]
+LIB_SOURCES = ["kernels_step.cu", "kernels_dispatch.cu", "fargo_api.cu", "sg.cu", "noalloc.cu", "host_params.cpp",
+               "host_setup.cpp"]
+# the step kernels a second time, without contraction of a*b+c into fused
+# multiply-adds: the accurate precision mode's kernel set
+VARIANTS = [("kernels_step.cu", "kernels_step_nofma.cu.o", ["-DFARGO_NOFMA", "-fmad=false"])]
 
 
 def _nvcc():
@@ -44,12 +48,14 @@ def build(verbose=False, force=False):
     os.makedirs(objdir, exist_ok=True)
     objs = []
     procs = []
-    for s in srcs:
-        o = os.path.join(objdir, os.path.basename(s) + ".o")
+    jobs = [(s, os.path.basename(s) + ".o", []) for s in srcs]
+    jobs += [(os.path.join(CSRC, s), o, f) for s, o, f in VARIANTS]
+    for s, oname, extra in jobs:
+        o = os.path.join(objdir, oname)
         objs.append(o)
         if force or _newer(o, [s] + hdrs):
             lang = [] if s.endswith(".cu") else ["-x", "cu"]
-            cmd = [nv] + NVFLAGS + ARCH + lang + ["-c", s, "-o", o]
+            cmd = [nv] + NVFLAGS + extra + ARCH + lang + ["-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd))
             procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))

@@ -1339,7 +1339,8 @@ fargo_status fargo_batch_set_precision(fargo_batch* b, int mode) {
     fargo_status st = sg_tabulate(b->gsg, b->gt, acc, b->stream, b->err);
     if (st) return st;
   }
-  return FARGO_OK;
+  b->bd.accurate = acc;   // the accurate mode runs the kernel set without fused multiply-adds
+  return build_graph(b);  // whose launches the graph must capture
 }
 
 fargo_status fargo_set_precision(fargo_ctx* ctx, int mode) {

@@ -190,6 +190,7 @@ struct BatchDev {
   int cell_grid, ring_grid, item_grid, grp_grid;  // fixed grid sizes of the grid-stride kernels
   int any_bc;                // some disk has an OPEN, NONREFLECTING or EVANESCENT boundary
   int src1_classes;          // bit 2*Adiabatic + SelfGravity set for every kind of disk present
+  int accurate;              // precision mode of the batch's disks: which kernel set runs (FARGO_LAUNCHERS)
   int max_body;              // largest body count of the force sums (star + FeelDisk planets)
   // one-wave grids of the substep kernels (fargo_size_grids)
   int g_cfl, g_source1[4], g_potential, g_viscosity, g_source2[2], g_energy, g_velocities[2], g_transport;
@@ -209,32 +210,46 @@ struct BatchDev {
 #define FARGO_TR_ROWS_D (FARGO_BAND + 4)
 #define FARGO_TR_ROWS_R (FARGO_BAND + 5)
 #define FARGO_TR_ROWS_T (FARGO_BAND + 4)
-cudaError_t fargo_kernel_attributes(int max_nsec);
-void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s);
-// only_disk >= 0: that disk; -1: every disk still inside its DT
-void fargo_launch_cs_refresh(const BatchDev& b, int only_disk, cudaStream_t s);
-void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s);
 // ev (optional): FARGO_NKERNELS+1 events, before each kernel and after the last.
 // part: FARGO_PART_HEAD (ring means and CFL/forces), FARGO_PART_TAIL (the
 // rest: potential ... end of substep) or both.
 #define FARGO_PART_HEAD 1
 #define FARGO_PART_TAIL 2
-void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int use_handle, cudaStream_t s,
-                          int max_nsec, long long* launches, cudaEvent_t* ev = nullptr,
-                          int part = FARGO_PART_HEAD | FARGO_PART_TAIL);
-// radial stripes: the stripe's block for the gather (3 + 4 * bodies * own CFL
-// tiles doubles), and the substep scalars from the gathered blocks (nonzero
-// return: nstripe out of range)
-void fargo_launch_stripe_block(const BatchDev& b, double* out, cudaStream_t s);
-int fargo_launch_stripe_finish(const BatchDev& b, const double* blk, int nstripe, int stride, cudaStream_t s);
 #define FARGO_STRIPE_HEAD 3
-const char* fargo_substep_kernel_name(int k);
-void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s);
-void fargo_launch_init_velocities(const BatchDev& b, int disk, long long ncell_ghost, cudaStream_t s);
-void fargo_launch_disk_force(const BatchDev& b, int disk, float x, float y, float rs, float rh, float a,
-                             double* out44, int nblocks, cudaStream_t s);
-void fargo_launch_diagnostics(const BatchDev& b, int disk, double* out3, int nblocks, cudaStream_t s);
-int fargo_substep_launches(const BatchDev& b);
-cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int nitems);
-const void* fargo_cfl_kernel(int max_body);
-void fargo_launch_transport(const BatchDev& b, cudaStream_t s);
+// The kernels and their launchers are compiled twice (kernels_step.cu):
+// fargo_k with the compiler's contraction of a*b+c into fused multiply-adds
+// (the reference-arithmetic precision mode, as the reference's own build)
+// and fargo_k_nofma without it (the accurate mode: each product rounded
+// before it is added, as the FP64-checked restatement does).  The
+// unqualified launchers below pick the set by BatchDev::accurate
+// (kernels_dispatch.cu).
+#define FARGO_LAUNCHERS                                                                                        \
+  cudaError_t fargo_kernel_attributes(int max_nsec);                                                          \
+  void fargo_launch_dt_begin(const BatchDev& b, cudaStream_t s);                                              \
+  /* only_disk >= 0: that disk; -1: every disk still inside its DT */                                         \
+  void fargo_launch_cs_refresh(const BatchDev& b, int only_disk, cudaStream_t s);                             \
+  void fargo_launch_cs_isothermal(const BatchDev& b, int only_disk, cudaStream_t s);                          \
+  void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int use_handle, cudaStream_t s,   \
+                            int max_nsec, long long* launches, cudaEvent_t* ev = nullptr,                     \
+                            int part = FARGO_PART_HEAD | FARGO_PART_TAIL);                                     \
+  /* radial stripes: the stripe's block for the gather (3 + 4 * bodies * own CFL tiles doubles), and the     \
+     substep scalars from the gathered blocks (nonzero return: nstripe out of range) */                       \
+  void fargo_launch_stripe_block(const BatchDev& b, double* out, cudaStream_t s);                             \
+  int fargo_launch_stripe_finish(const BatchDev& b, const double* blk, int nstripe, int stride, cudaStream_t s); \
+  const char* fargo_substep_kernel_name(int k);                                                               \
+  void fargo_launch_sector_tables(const BatchDev& b, int max_nsec, cudaStream_t s);                           \
+  void fargo_launch_init_velocities(const BatchDev& b, int disk, long long ncell_ghost, cudaStream_t s);      \
+  void fargo_launch_disk_force(const BatchDev& b, int disk, float x, float y, float rs, float rh, float a,     \
+                               double* out44, int nblocks, cudaStream_t s);                                   \
+  void fargo_launch_diagnostics(const BatchDev& b, int disk, double* out3, int nblocks, cudaStream_t s);      \
+  int fargo_substep_launches(const BatchDev& b);                                                              \
+  cudaError_t fargo_size_grids(BatchDev& b, int nsm, long long ncell_tiles, int nitems);                      \
+  const void* fargo_cfl_kernel(int max_body);                                                                 \
+  void fargo_launch_transport(const BatchDev& b, cudaStream_t s);
+namespace fargo_k {
+FARGO_LAUNCHERS
+}
+namespace fargo_k_nofma {
+FARGO_LAUNCHERS
+}
+FARGO_LAUNCHERS

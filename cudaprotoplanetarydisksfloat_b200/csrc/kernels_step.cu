@@ -3117,6 +3117,15 @@ __global__ void __launch_bounds__(kThreads) k_diagnostics(BatchDev B, int disk, 
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
+// This file is compiled twice: with contraction of a*b+c into fused
+// multiply-adds (fargo_k) and, with FARGO_NOFMA defined, without
+// (fargo_k_nofma, nvcc -fmad=false); fargo_internal.h has the dispatch.
+#ifdef FARGO_NOFMA
+#define FARGO_KNS fargo_k_nofma
+#else
+#define FARGO_KNS fargo_k
+#endif
+namespace FARGO_KNS {
 
 static inline unsigned cell_blocks(long long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
@@ -3212,7 +3221,7 @@ void fargo_launch_substep(const BatchDev& b, cudaGraphConditionalHandle h, int u
   k_substep_end<<<1, kThreads, 0, s>>>(b, h, use_handle);
   REC();
 #undef REC
-  if (launches) *launches += fargo_substep_launches(b) - ((part & FARGO_PART_HEAD) ? 0 : 2);
+  if (launches) *launches += FARGO_KNS::fargo_substep_launches(b) - ((part & FARGO_PART_HEAD) ? 0 : 2);
 }
 
 void fargo_launch_stripe_block(const BatchDev& b, double* out, cudaStream_t s) {
@@ -3321,3 +3330,5 @@ cudaError_t fargo_kernel_attributes(int max_nsec) {
   return cudaFuncSetAttribute(k_transport<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)fargo_transport_smem_bytes(1));
 }
+
+}  // namespace FARGO_KNS

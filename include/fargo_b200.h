@@ -308,7 +308,9 @@ fargo_status fargo_batch_set_max_substeps(fargo_batch* b, int n);
    - ring means (FARGO VMed, CFL mean, alpha-viscosity sound speed) are
      Kahan-compensated FP32 sums in the same order;
    - the self-gravity kernel is tabulated in FP64 (the reference's float
-     table is not exactly antisymmetric in azimuth).
+     table is not exactly antisymmetric in azimuth);
+   - the step kernels run as a second build without contraction of a*b+c
+     into fused multiply-adds (every product rounded before it is added).
    Integer outcomes may then differ from the reference's build.  Call
    between DTs, before the first one for a reproducible run. */
 #define FARGO_PRECISION_REFERENCE 0

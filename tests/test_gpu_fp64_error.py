@@ -32,9 +32,10 @@ pytestmark = pytest.mark.gpu
 
 # loose bounds for every case: they catch a broken path, not rounding
 BOUND = {"dens": 1e-4, "vrad": 2e-3, "vtheta": 1e-5, "energy": 2e-4}
-# the accurate mode on C1 (isothermal, one fixed planet): at the FP32 storage
-# floor, 1.0e-5 measured on the B200 (10% margin)
-C1_ACCURATE_SIGMA = 1.1e-5
+# the accurate mode on C1 (isothermal, one fixed planet): the target of
+# 1e-5 after 10 DTs, at the FP32 storage floor (9.99e-6 measured on the B200,
+# with the accurate mode's kernels built without fused multiply-adds)
+C1_ACCURATE_SIGMA = 1e-5
 
 
 def _case(name):
