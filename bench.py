@@ -316,6 +316,9 @@ def ours(args, world, rank, local, pg):
     for b in batches:
         b.sync()
     seg_out = [b.autotune(reps=2) for b in batches]
+    # the widths the autotuner kept per class of disk (NSEC), batch by batch
+    seg_by_nsec = [{int(P[d].NSEC): s for d, s in sorted(zip(g, b.segments()), key=lambda x: P[x[0]].NSEC)}
+                   for b, g in zip(batches, groups)]
     n0 = nsub_total()
     l0 = sum(lib.fargo_batch_count_launches(b.b) for b in batches)
     barrier(pg)
@@ -507,7 +510,7 @@ def ours(args, world, rank, local, pg):
         "value": value, "ms_per_step": ms_max / args.steps, "e2e": e2e, "roofline": roof,
         "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(l1 - l0) * world,
         "wall_s": t_wall, "cells": int(cells.sum()) * world, "disks": len(P) * world,
-        "seg_out": sorted(set(seg_out)), "batches": len(batches), "plain": plain_line,
+        "seg_out": sorted(set(seg_out)), "seg_by_nsec": seg_by_nsec, "batches": len(batches), "plain": plain_line,
         "batching": {"by": "one disk per context" if plain else args.group_by,
                      "disks_per_batch": [len(g) for g in groups]},
     }
@@ -737,7 +740,8 @@ def main():
     if rank == 0:
         line = dict(head, value=r["value"], ms_per_step=r["ms_per_step"],
                     data="synthetic (seeded parameters and density noise)", config=config,
-                    tiles={"transport_segment": r["seg_out"], "band_rings": 8, "autotuned": True},
+                    tiles={"transport_segment": r["seg_out"], "segment_by_nsec": r["seg_by_nsec"], "band_rings": 8,
+                           "autotuned": True},
                     batching=r["batching"],
                     e2e=r["e2e"], roofline=r["roofline"], cpu_baseline=r["cpu_baseline"], clocks=r["clocks"],
                     gpu_launches=r["gpu_launches"])

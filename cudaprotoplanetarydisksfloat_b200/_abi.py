@@ -104,7 +104,7 @@ EXPORTS = [
     "fargo_profile_kernel_name", "fargo_profile_kernel_count",
     "fargo_stripe_create", "fargo_stripe_info", "fargo_stripe_dt_begin", "fargo_stripe_forces",
     "fargo_stripe_substep", "fargo_stripe_halo_pack", "fargo_stripe_halo_unpack", "fargo_stripe_more",
-    "fargo_stripe_init_state", "fargo_stripe_sg_rows", "fargo_stripe_sg_apply",
+    "fargo_stripe_init_state", "fargo_stripe_sg_rows", "fargo_stripe_sg_apply", "fargo_batch_segments",
 ]
 
 
@@ -190,6 +190,7 @@ def _load():
         "fargo_stripe_halo_unpack": (C.c_int, [vp, vp, vp]),
         "fargo_stripe_more": (C.c_int, [vp, P(C.c_int)]),
         "fargo_stripe_init_state": (C.c_int, [vp, fp, fp]),
+        "fargo_batch_segments": (C.c_int, [vp, C.c_int, P(C.c_int)]),
         "fargo_stripe_sg_rows": (C.c_int, [vp, vp]),
         "fargo_stripe_sg_apply": (C.c_int, [vp, vp, C.c_int, C.c_int, P(C.c_int)]),
     }

@@ -14,8 +14,11 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "fargo_internal.h"
@@ -26,6 +29,7 @@ namespace {
 
 
 struct DiskHost {
+  int seg_out = FARGO_SEG_OUT;  // transport segment width of this disk (autotuned per NSEC class)
   fargo_params p;
   fargo_planets planets0;
   HostTables t;
@@ -488,18 +492,35 @@ fargo_status build_graph(fargo_batch* b) {
   return FARGO_OK;
 }
 
+// Segment widths chosen by the autotuner, kept for the life of the process
+// per class of disk (NSEC, adiabatic, precision mode): a batch created later
+// with disks of a tuned class starts from the tuned width.  The transport's
+// results do not depend on the width (its arithmetic is contraction-free and
+// per cell), only its speed does.
+using SegKey = std::tuple<int, int, int>;
+std::mutex g_seg_mutex;
+std::map<SegKey, int> g_seg_cache;
+SegKey seg_key(const DiskHost& h) { return SegKey(h.p.NSEC, h.p.Adiabatic ? 1 : 0, h.dev.accurate); }
+void apply_seg_cache(fargo_batch* b) {
+  std::lock_guard<std::mutex> lock(g_seg_mutex);
+  for (auto& h : b->disks) {
+    auto it = g_seg_cache.find(seg_key(h));
+    if (it != g_seg_cache.end()) h.seg_out = it->second;
+  }
+}
+
 // Transport work items of every disk: bands of FARGO_BAND rings, each in
-// nseg near-equal azimuthal segments of at most seg_out source sectors (the
-// sectors a band reads; each ring stores them shifted by its Nshift); isothermal
-// and adiabatic disks in separate lists.  Sets each disk's item0 / nitems
-// (host copy) and returns the widest segment.
-int build_items(fargo_batch* b, int seg_out, std::vector<int4>& theta_iso, std::vector<int4>& theta_adi) {
+// nseg near-equal azimuthal segments of at most the disk's seg_out source
+// sectors (the sectors a band reads; each ring stores them shifted by its
+// Nshift); isothermal and adiabatic disks in separate lists.  Sets each
+// disk's item0 / nitems (host copy) and returns the widest segment.
+int build_items(fargo_batch* b, std::vector<int4>& theta_iso, std::vector<int4>& theta_adi) {
   int seg_max = 0;
   theta_iso.clear();
   theta_adi.clear();
   for (int d = 0; d < (int)b->disks.size(); d++) {
     DiskHost& h = b->disks[d];
-    const int nrad = h.p.NRAD, nsec = h.p.NSEC;
+    const int nrad = h.p.NRAD, nsec = h.p.NSEC, seg_out = h.seg_out;
     std::vector<int4>& theta = h.p.Adiabatic ? theta_adi : theta_iso;
     h.dev.item0 = (int)theta.size();
     const int nseg = (nsec + seg_out - 1) / seg_out;
@@ -516,15 +537,14 @@ int build_items(fargo_batch* b, int seg_out, std::vector<int4>& theta_iso, std::
     }
     h.dev.nitems = (int)theta.size() - h.dev.item0;
   }
-  b->seg_out = seg_out;
   return seg_max;
 }
 
 // Replace the batch's transport items (device list, per-disk item0/nitems,
-// grid) with those for seg_out.
-fargo_status install_items(fargo_batch* b, int seg_out) {
+// grid) with those of the disks' current segment widths.
+fargo_status install_items(fargo_batch* b) {
   std::vector<int4> theta_iso, theta_adi;
-  int seg_max = build_items(b, seg_out, theta_iso, theta_adi);
+  int seg_max = build_items(b, theta_iso, theta_adi);
   CK(cudaStreamSynchronize(b->stream));
   if (b->d_theta) CK(cudaFree(b->d_theta));
   b->d_theta = nullptr;
@@ -585,7 +605,8 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     src1_classes |= 1 << (2 * (h.p.Adiabatic ? 1 : 0) + (h.p.SelfGravity ? 1 : 0));
     max_body = std::max(max_body, body_count(&planets[d]));
   }
-  seg_max = build_items(b, FARGO_SEG_OUT, theta_iso, theta_adi);
+  apply_seg_cache(b);
+  seg_max = build_items(b, theta_iso, theta_adi);
   CK(cudaMalloc(&b->d_disks, sizeof(DiskDev) * n));
   CK(cudaMalloc(&b->d_ctl, sizeof(DiskCtl) * n));
   CK(cudaMemsetAsync(b->d_ctl, 0, sizeof(DiskCtl) * n, b->stream));
@@ -1273,13 +1294,12 @@ fargo_status batch_autotune(fargo_batch* b, int reps, int* chosen) {
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  float best_ms = 1e30f;
-  int best = b->seg_out;
-  for (int c : cand) {
-    fargo_status st = install_items(b, c);
+  // install the disks' current widths and time the transport kernels on the
+  // current state (every disk active, the compacted item prefixes rebuilt
+  // for these items, as the next DT starts; the kernels write only scratch)
+  auto timed = [&](float* ms) -> fargo_status {
+    fargo_status st = install_items(b);
     if (st) return st;
-    // every disk active, and the compacted item prefixes rebuilt for these
-    // items (the next DT starts the same way)
     fargo_launch_dt_begin(b->bd, b->stream);
     fargo_launch_transport(b->bd, b->stream);
     CK(cudaEventRecord(e0, b->stream));
@@ -1287,19 +1307,68 @@ fargo_status batch_autotune(fargo_batch* b, int reps, int* chosen) {
     CK(cudaEventRecord(e1, b->stream));
     CK(cudaEventSynchronize(e1));
     CK(cudaGetLastError());
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    return FARGO_OK;
+  };
+  // the classes of disk, largest share of cells first
+  std::map<SegKey, long long> cells;
+  for (auto& h : b->disks) cells[seg_key(h)] += (long long)h.p.NRAD * h.p.NSEC;
+  std::vector<std::pair<long long, SegKey>> classes;
+  for (auto& kv : cells) classes.push_back({kv.second, kv.first});
+  std::sort(classes.begin(), classes.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+  auto set_class = [&](const SegKey& k, int w) {
+    for (auto& h : b->disks)
+      if (seg_key(h) == k) h.seg_out = w;
+  };
+  // one width for every disk, then each class in turn with the others fixed
+  float best_ms = 1e30f;
+  int best = FARGO_SEG_OUT;
+  fargo_status st = FARGO_OK;
+  for (int c : cand) {
+    for (auto& h : b->disks) h.seg_out = c;
     float ms = 0.0f;
-    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if ((st = timed(&ms))) return st;
     if (ms < best_ms) {
       best_ms = ms;
       best = c;
     }
   }
+  for (auto& h : b->disks) h.seg_out = best;
+  if (classes.size() > 1) {
+    for (auto& cl : classes) {
+      int keep = best;
+      for (int c : cand) {
+        if (c == keep) continue;
+        set_class(cl.second, c);
+        float ms = 0.0f;
+        if ((st = timed(&ms))) return st;
+        if (ms < best_ms) {
+          best_ms = ms;
+          keep = c;
+        }
+      }
+      set_class(cl.second, keep);
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  fargo_status st = install_items(b, best);
-  if (st) return st;
-  if (chosen) *chosen = best;
+  if ((st = install_items(b))) return st;
+  {
+    std::lock_guard<std::mutex> lock(g_seg_mutex);
+    for (auto& h : b->disks) g_seg_cache[seg_key(h)] = h.seg_out;
+  }
+  b->seg_out = best;
+  if (chosen) {  // the width of the class with the most cells
+    for (auto& h : b->disks)
+      if (seg_key(h) == classes[0].second) *chosen = h.seg_out;
+  }
   return build_graph(b);
+}
+
+fargo_status fargo_batch_segments(fargo_batch* b, int cap, int* seg_per_disk) {
+  if (!b || cap < 0 || (cap && !seg_per_disk)) return FARGO_EINVAL;
+  for (int d = 0; d < (int)b->disks.size() && d < cap; d++) seg_per_disk[d] = b->disks[d].seg_out;
+  return FARGO_OK;
 }
 
 fargo_status fargo_batch_autotune(fargo_batch* b, int reps, int* seg_out) { return batch_autotune(b, reps, seg_out); }
@@ -1339,7 +1408,10 @@ fargo_status fargo_batch_set_precision(fargo_batch* b, int mode) {
     fargo_status st = sg_tabulate(b->gsg, b->gt, acc, b->stream, b->err);
     if (st) return st;
   }
-  b->bd.accurate = acc;   // the accurate mode runs the kernel set without fused multiply-adds
+  b->bd.accurate = acc;  // the accurate mode runs the kernel set without fused multiply-adds
+  apply_seg_cache(b);    // the segment widths tuned for this mode, if any
+  fargo_status st = install_items(b);
+  if (st) return st;
   return build_graph(b);  // whose launches the graph must capture
 }
 

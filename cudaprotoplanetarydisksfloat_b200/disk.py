@@ -248,6 +248,12 @@ class Batch:
         self._chk(lib.fargo_batch_autotune(self.b, reps, C.byref(seg)), "fargo_batch_autotune")
         return seg.value
 
+    def segments(self):
+        """The transport segment width of each disk (autotuned per class)."""
+        out = (C.c_int * self.n)()
+        self._chk(lib.fargo_batch_segments(self.b, self.n, out), "fargo_batch_segments")
+        return list(out)
+
     def sync(self):
         self._chk(lib.fargo_batch_sync(self.b), "fargo_batch_sync")
 

@@ -318,10 +318,17 @@ fargo_status fargo_batch_set_max_substeps(fargo_batch* b, int n);
 fargo_status fargo_set_precision(fargo_ctx* ctx, int mode);
 fargo_status fargo_batch_set_precision(fargo_batch* b, int mode);
 /* (new) Tile autotuner: times the transport kernels on the current state for
-   azimuthal segment widths 96..244 sectors and keeps the fastest (*seg_out).
-   Call between DTs; the state is not advanced. */
+   azimuthal segment widths 96..244 sectors, first one width for every disk,
+   then each class of disk (NSEC, adiabatic, precision mode; largest share of
+   cells first) in turn with the others fixed, and keeps the fastest.
+   *seg_out: the width of the class with the most cells.  The widths are kept
+   for the life of the process per class: batches created later (and a change
+   of precision mode) start from them.  Results do not depend on the widths.
+   Call between DTs; the state is not advanced.  fargo_batch_segments gives
+   each disk's width (cap entries). */
 fargo_status fargo_batch_autotune(fargo_batch* b, int reps, int* seg_out);
 fargo_status fargo_autotune(fargo_ctx* ctx, int reps, int* seg_out);
+fargo_status fargo_batch_segments(fargo_batch* b, int cap, int* seg_per_disk);
 
 /* (new) Radial decomposition of one disk over several contexts, usually one
    per GPU (the loop of AlgoGas, SourceEuler.cu:208-301, split by rings).
