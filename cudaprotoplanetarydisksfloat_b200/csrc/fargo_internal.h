@@ -81,8 +81,9 @@ inline __host__ __device__ int fargo_cfl_tiles(int nrad, int nsec) {
 // CFL tiles of a disk's own rings (every ring unless it is a radial stripe)
 #define fargo_cfl_tiles_own(D) fargo_cfl_tiles((D).own_hi - (D).own_lo, (D).nsec)
 
-// scratch of the device RK5 (q0, q1, k1..k6, distances): 33 doubles per planet
-#define FARGO_RK_WORK(nb) (33 * (nb))
+// scratch of the device RK5 (q0, q1, k1..k6, distances, perturber quotients):
+// 34 doubles per planet
+#define FARGO_RK_WORK(nb) (34 * (nb))
 
 struct DiskDev {
   int nrad, nsec;

@@ -162,7 +162,14 @@ __device__ void deriv_motion(const DiskDev& D, const DiskCtl* C, const double* q
                              float dt, double* Dist) {
   const double *x = q, *y = q + nb, *vx = q + 2 * nb, *vy = q + 3 * nb;
   double *dx = deriv, *dy = deriv + nb, *dvx = deriv + 2 * nb, *dvy = deriv + 3 * nb;
-  for (int i = 0; i < nb; i++) Dist[i] = sqrt(x[i] * x[i] + y[i] * y[i]);
+  // m_j / d_j / d_j / d_j depends on j alone: formed once per perturber (the
+  // same expression, so the same bits), not once per pair; Dist holds the
+  // distances in [0, nb) and these quotients in [nb, 2 nb)
+  double* mD3 = Dist + nb;
+  for (int i = 0; i < nb; i++) {
+    Dist[i] = sqrt(x[i] * x[i] + y[i] * y[i]);
+    mD3[i] = 1.0 * C->mass[i] / Dist[i] / Dist[i] / Dist[i];
+  }
   for (int i = 0; i < nb; i++) {
     dx[i] = vx[i];
     dy[i] = vy[i];
@@ -170,12 +177,12 @@ __device__ void deriv_motion(const DiskDev& D, const DiskCtl* C, const double* q
     dvy[i] = -1.0 * 1.0 / Dist[i] / Dist[i] / Dist[i] * y[i];
     for (int j = 0; j < nb; j++) {
       if (D.Indirect_Term) {
-        dvx[i] -= 1.0 * C->mass[j] / Dist[j] / Dist[j] / Dist[j] * x[j];
-        dvy[i] -= 1.0 * C->mass[j] / Dist[j] / Dist[j] / Dist[j] * y[j];
+        dvx[i] -= mD3[j] * x[j];
+        dvy[i] -= mD3[j] * y[j];
       }
       if ((j != i) && C->feelothers[i]) {
-        dvx[i] += 1.0 * C->mass[j] / Dist[j] / Dist[j] / Dist[j] * (x[j] - x[i]);
-        dvy[i] += 1.0 * C->mass[j] / Dist[j] / Dist[j] / Dist[j] * (y[j] - y[i]);
+        dvx[i] += mD3[j] * (x[j] - x[i]);
+        dvy[i] += mD3[j] * (y[j] - y[i]);
       }
     }
   }
