@@ -231,6 +231,7 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
   D.own_lo = 0;
   D.own_hi = p->NRAD;
   D.stripe = 0;
+  D.cfl_tile = FARGO_CFL_TILE;  // set per batch by set_cfl_tiles
   D.invdphi = h.t.invdphi;
   D.onethird = h.t.onethird;
   size_t ng = (size_t)(p->NRAD + 1) * p->NSEC;
@@ -248,7 +249,7 @@ fargo_status alloc_disk(fargo_batch* b, DiskHost& h, const double* radii) {
     D.a1 = D.a0;  // never written in isothermal runs
   }
   A(D.pres, ng) A(D.phi, ng)
-  size_t nct = std::max<size_t>(n1, (size_t)fargo_cfl_tiles(p->NRAD, p->NSEC));
+  size_t nct = std::max<size_t>(n1, (size_t)fargo_cfl_tiles(p->NRAD, p->NSEC, FARGO_CFL_TILE_SMALL));
   A(D.visc, n1) A(D.cs_ring, n1) A(D.csmean, n1) A(D.vmoy, n1) A(D.ringmin, nct) A(D.nshift, n1)
   A(D.tvmed, n1) A(D.tvconst, n1)
   A(D.log_nshift, (size_t)FARGO_MAXLOG * p->NRAD) A(D.partials, nct * 4 * FARGO_MAXBODY)
@@ -570,6 +571,21 @@ fargo_status install_items(fargo_batch* b) {
   return FARGO_OK;
 }
 
+// CFL/force tile size of every disk of the batch: the small tile when the
+// large one would give fewer than two tiles per SM over `cells` (the whole
+// disk's cells for a radial stripe, so that its tiles are the whole disk's),
+// and the batch's tile count.  Host copies only; the caller uploads.
+void set_cfl_tiles(fargo_batch* b, long long cells, int device) {
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  const int tile = cells < 2LL * nsm * FARGO_CFL_TILE ? FARGO_CFL_TILE_SMALL : FARGO_CFL_TILE;
+  b->bd.ncfl = 0;
+  for (auto& h : b->disks) {
+    h.dev.cfl_tile = tile;
+    b->bd.ncfl += fargo_cfl_tiles_own(h.dev);
+  }
+}
+
 fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, const fargo_planets* planets,
                           const double* const* radii, int device) {
   int ndev = 0;
@@ -630,6 +646,7 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
     CK(cudaMemcpyAsync(b->d_theta + theta_iso.size(), theta_adi.data(), sizeof(int4) * theta_adi.size(),
                        cudaMemcpyHostToDevice, b->stream));
   for (int d = 0; d < n; d++) b->disks[d].dev.ctl = b->d_ctl + d;
+  set_cfl_tiles(b, cell_off[n], device);  // sets bd.ncfl
   for (int d = 0; d < n; d++)
     CK(cudaMemcpyAsync(b->d_disks + d, &b->disks[d].dev, sizeof(DiskDev), cudaMemcpyHostToDevice, b->stream));
   BatchDev& bd = b->bd;
@@ -639,8 +656,6 @@ fargo_status batch_create(fargo_batch* b, int n, const fargo_params* params, con
   bd.max_body = max_body;
   bd.ncell = cell_off[n];
   bd.nring = ring_off[n];
-  bd.ncfl = 0;
-  for (int d = 0; d < n; d++) bd.ncfl += fargo_cfl_tiles(b->disks[d].dev.nrad, b->disks[d].dev.nsec);
   bd.cell_off = b->d_cell_off;
   bd.ring_off = b->d_ring_off;
   bd.disks = b->d_disks;
@@ -1486,7 +1501,7 @@ fargo_status fargo_stripe_create(const fargo_params* p, const fargo_planets* pla
   b->stripe_nrad = NRAD;
   b->ghost_lo = ring_lo - base;
   b->ghost_hi = top - ring_hi;
-  b->bd.ncfl = fargo_cfl_tiles_own(D);
+  set_cfl_tiles(b, (long long)NRAD * p->NSEC, b->device);  // the whole disk's tiles; sets bd.ncfl
   CK(cudaMemcpy(b->d_disks, &D, sizeof(DiskDev), cudaMemcpyHostToDevice));
   if (p->SelfGravity) {
     // the whole disk's convolution: a view of the whole grid with its own

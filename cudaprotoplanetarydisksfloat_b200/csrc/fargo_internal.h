@@ -71,15 +71,18 @@ struct DiskCtl {
 // four per thread
 #define FARGO_QTILE 1024
 
-// CFL/force tiles: FARGO_CFL_TILE consecutive cells of one disk, each with its
-// own minimum and force partials
+// CFL/force tiles: DiskDev::cfl_tile consecutive cells of one disk, each with
+// its own minimum and force partials: FARGO_CFL_TILE, or FARGO_CFL_TILE_SMALL
+// in a batch too small to give every SM two tiles of the large size (more
+// blocks share the per-cell work of a small disk)
 #define FARGO_CFL_TILE 4096
-inline __host__ __device__ int fargo_cfl_tiles(int nrad, int nsec) {
-  return (int)(((long long)nrad * nsec + FARGO_CFL_TILE - 1) / FARGO_CFL_TILE);
+#define FARGO_CFL_TILE_SMALL 1024
+inline __host__ __device__ int fargo_cfl_tiles(int nrad, int nsec, int tile) {
+  return (int)(((long long)nrad * nsec + tile - 1) / tile);
 }
 
 // CFL tiles of a disk's own rings (every ring unless it is a radial stripe)
-#define fargo_cfl_tiles_own(D) fargo_cfl_tiles((D).own_hi - (D).own_lo, (D).nsec)
+#define fargo_cfl_tiles_own(D) fargo_cfl_tiles((D).own_hi - (D).own_lo, (D).nsec, (D).cfl_tile)
 
 // scratch of the device RK5 (q0, q1, k1..k6, distances, perturber quotients):
 // 34 doubles per planet
@@ -107,6 +110,7 @@ struct DiskDev {
   // scalar work to k_stripe_finish, which reads every stripe's partials.
   // A whole disk: own_lo = 0, own_hi = nrad, stripe = 0.
   int own_lo, own_hi, stripe;
+  int cfl_tile;  // cells per CFL/force tile (FARGO_CFL_TILE or FARGO_CFL_TILE_SMALL)
   int accurate;  // precision mode: 0 the reference's arithmetic, 1 accurate (FARGO_PRECISION_*)
   // three CUtensorMap (Sigma, v_r, v_theta; 2-D, FARGO_TR_ROW-column boxes)
   // for the transport's TMA staging, or null (NSEC not a multiple of 4, or

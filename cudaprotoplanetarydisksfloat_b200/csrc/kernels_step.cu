@@ -890,15 +890,17 @@ __device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const d
 // ConditionCFLKernel1D + ConditionCFLKernel2D1 + the cell minimum of
 // ConditionCFLKernel2D2 (Kernels.cu:1363-1422), and the disk force of
 // ComputeForceKernel (Kernels.cu:804-839) for the star and every FeelDisk
-// planet, accumulated in double, on CFL tiles of FARGO_CFL_TILE consecutive
-// cells (kCflCells per thread, their loads issued together).  Each tile
+// planet, accumulated in double, on CFL tiles of D.cfl_tile consecutive
+// cells (four consecutive cells per thread and step, their loads issued
+// together).  Each tile
 // writes its minimum and its force partials (inner / outer by the ring of
 // each cell), so that the finishing sums run in a fixed order.  Each block
 // takes a contiguous run of tiles; the block that completes a disk's last
 // tile finishes the substep's scalar work.
 // NB >= every disk's body count (star + FeelDisk planets): the per-thread
 // FP64 force accumulators are sized for it.
-constexpr int kCflCells = FARGO_CFL_TILE / kThreads;
+static_assert(FARGO_CFL_TILE_SMALL == 4 * kThreads && FARGO_CFL_TILE % FARGO_CFL_TILE_SMALL == 0,
+              "a CFL tile is whole quads of every thread");
 // The per-cell limit CFLSECURITY / s (s = sqrtf(...), a float) is a double
 // division rounded to float.  For CFLSECURITY = 2^-1 it equals 0.5f times the
 // correctly rounded float reciprocal of s: scaling by a power of two commutes
@@ -907,7 +909,6 @@ constexpr int kCflCells = FARGO_CFL_TILE / kThreads;
 // double rounding innocuous for a quotient of two floats (Figueroa, "When is
 // double rounding innocuous?", SIGNUM 1995).
 static_assert(CFLSEC == 0.5, "the CFL limit's reciprocal form needs CFLSECURITY = 0.5");
-static_assert(kCflCells * kThreads == FARGO_CFL_TILE, "CFL tile = whole cells per thread");
 template <int NB>
 __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDev B) {
   __shared__ DiskDev sD;
@@ -1067,10 +1068,11 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
         // four consecutive cells of one ring per thread and step (16-byte
         // loads; the ring's constants once per four cells): the tile's 1024
         // quads, thread tid takes quads tid, tid + 256, ...
-        const int c0 = D.own_lo * nsec + k * FARGO_CFL_TILE + 4 * tid;
+        const int c0 = D.own_lo * nsec + k * D.cfl_tile + 4 * tid;
         int i = c0 / nsec, j = c0 - i * nsec;
+        const int nq = D.cfl_tile / (4 * kThreads);
 #pragma unroll 1
-        for (int g = 0; g < kCflCells / 4; g++) {
+        for (int g = 0; g < nq; g++) {
           if (i >= iend) break;
           const int q = i * nsec + j;
           const float4 V0 = __ldg(reinterpret_cast<const float4*>(D.vtheta + q));
@@ -1095,13 +1097,14 @@ __global__ void __launch_bounds__(kThreads, NB <= 1 ? 3 : 2) k_cfl_force(BatchDe
           }
         }
       } else {
-        const int c0 = D.own_lo * nsec + k * FARGO_CFL_TILE + tid;
+        const int c0 = D.own_lo * nsec + k * D.cfl_tile + tid;
         int i = c0 / nsec, j = c0 - i * nsec;
+        const int ncell = D.cfl_tile / kThreads;
         // kG cells at a time: their loads are issued together (cells past
         // the disk's end read cell 0 and are skipped); fewer with more bodies,
         // whose accumulators take the registers
         constexpr int kG = NB <= 2 ? 4 : (NB <= 4 ? 2 : 1);
-        for (int g = 0; g < kCflCells; g += kG) {
+        for (int g = 0; g < ncell; g += kG) {
           int ci[kG], cj[kG];
           bool ok[kG];
 #pragma unroll

@@ -99,9 +99,9 @@ def test_c5_stripes_bit_identical(gpu):
 
 
 def test_c2_unaligned_cuts_within_floor(gpu):
-    """Cuts at rings 100 and 171 (NSEC 768: whole tiles are 16 rings) split
-    CFL tiles: the FP64 force sums group differently, the planets move by
-    rounding, and the fields stay within the FP32 floor."""
+    """A cut at ring 171 (NSEC 768: C2's 1024-cell CFL tiles are 4 rings)
+    splits a CFL tile: the FP64 force sums group differently, the planets
+    move by rounding, and the fields stay within the FP32 floor."""
     P, nw, ns, a, b, pa, pb, _, _ = _run_pair(configs.c2(), "rad_c2u", 3, 3,
                                                parts=[(0, 100), (100, 171), (171, 256)])
     assert nw == ns
