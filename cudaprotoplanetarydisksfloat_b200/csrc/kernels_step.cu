@@ -34,8 +34,8 @@
 // (a float meeting a double literal is promoted and rounded back on
 // assignment); where the reference computes one IEEE operation in double on
 // two float operands and rounds to float, the float operation is used, which
-// gives the same bits.  Per-cell quotients by sums of densities (Substep1,
-// Substep2, the viscous update, the velocities) use div_refined
+// gives the same bits.  Per-cell quotients (Substep1, Substep2, the viscous
+// update, the viscous heating and energy update, the velocities) use div_refined
 // (fast_div.cuh): the IEEE quotient but within ~2^-22 ulp of a rounding
 // boundary, one ulp from it there.
 #include <cuda_runtime.h>
@@ -1758,17 +1758,60 @@ __device__ __forceinline__ float qplus_at(const DiskDev& D, int i, int j, int ns
   const float nu = D.visc[i];
   float q;
   if (nu != 0.0f) {
-    q = 0.5f / nu / D.dens[l] * (t.rr * t.rr + +t.rp * t.rp + t.pp * t.pp);
+    q = div_refined(div_refined(0.5f, nu), D.dens[l]) * (t.rr * t.rr + +t.rp * t.rp + t.pp * t.pp);
     q += (float)(2.0 / 9.0) * nu * D.dens[l] * t.divv * t.divv;
   } else
     q = 0.0f;
   return q;
 }
 
-__global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
+// qplus_at for the four cells of a quad in one ring i >= 1 (vector path):
+// the same expressions, the neighbours loaded as 16-byte rows and shifted
+// lanes instead of ten scalar loads per cell.
+template <bool V>
+__device__ __forceinline__ void qplus_quad(const DiskDev& D, const Quad<V>& q, int nsec, float (&qp)[4],
+                                           float (&dv)[4]) {
+  const int i = q.i[0];
+  float Vr0[4], Vrp[4], Vrj[4], Va0[4], Vap[4], Vam[4], Dn0[4], Dnm[4], Dnmj[4];
+  qld(Vr0, D.vrad, q);
+  qld(Vrp, D.vrad, q, nsec);
+  qld_jm(Vrj, Vr0, D.vrad, q, nsec);
+  qld(Va0, D.vtheta, q);
+  qld_jp(Vap, Va0, D.vtheta, q, nsec);
+  qld(Vam, D.vtheta, q, -nsec);
+  qld(Dn0, D.dens, q);
+  qld(Dnm, D.dens, q, -nsec);
+  qld_jm(Dnmj, Dnm, D.dens, q, nsec, -nsec);
+  const float Di = __ldg(D.dens + i * nsec);  // TAURP's third density sample (Kernels.cu:876)
+  const float nu = D.visc[i], iRm = D.invRmed[i], iRm1 = D.invRmed[i - 1], idRs = D.invdiffRsup[i];
+  const float Rs = D.Rsup[i], Ri = D.Rinf[i], idRm = D.invdiffRmed[i], iRi = D.invRinf[i];
+  const float invdphi = D.invdphi, onethird = D.onethird;
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    float DRR = (Vrp[u] - Vr0[u]) * idRs;
+    float DPP = (Vap[u] - Va0[u]) * invdphi * iRm + 0.5f * (Vrp[u] + Vr0[u]) * iRm;
+    float divV = (Vrp[u] * Rs - Vr0[u] * Ri) * idRs * iRm;
+    divV += (Vap[u] - Va0[u]) * invdphi * iRm;
+    const float rr = 2.0f * Dn0[u] * nu * (DRR - onethird * divV);
+    const float pp = 2.0f * Dn0[u] * nu * (DPP - onethird * divV);
+    float DRP = 0.5f * (Ri * (Va0[u] * iRm - Vam[u] * iRm1) * idRm + (Vr0[u] - Vrj[u]) * invdphi * iRi);
+    const float rp = 0.5f * (Dn0[u] + Dnm[u] + Di + Dnmj[u]) * nu * DRP;
+    dv[u] = divV;
+    if (nu != 0.0f) {
+      qp[u] = div_refined(div_refined(0.5f, nu), Dn0[u]) * (rr * rr + +rp * rp + pp * pp);
+      qp[u] += (float)(2.0 / 9.0) * nu * Dn0[u] * divV * divV;
+    } else {
+      qp[u] = 0.0f;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 3) k_energy(BatchDev B) {
   QUAD_BEGIN_T(1, -1)
   const float dt = C->dtf;
-  float qv[4], ev[4];
+  float qv[4], ev[4], dvq[4];
+  const bool quad = V && q.i[0] > 0;
+  if (quad) qplus_quad(D, q, nsec, qv, dvq);
 #pragma unroll
   for (int u = 0; u < 4; u++) {
     const int i = q.i[u], j = q.j[u], l = q.l[u];
@@ -1778,7 +1821,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
     }
     float divv;
     float qp = 0.0f;
-    if (i > 0) {
+    if (quad) {
+      qp = qv[u];
+      divv = dvq[u];
+    } else if (i > 0) {
       qp = qplus_at(D, i, j, nsec, &divv);
     } else {
       float dv1, dv2;
@@ -1803,7 +1849,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_energy(BatchDev B) {
       den = dt + D.CoolingTimeMed[i] + (D.ADIABATICINDEX - 1.0f) * dt * D.CoolingTimeMed[i] * divv;
     }
     qv[u] = qp;
-    ev[u] = num / den;
+    ev[u] = div_refined(num, den);
   }
   qst(D.qplus, q, qv);
   qst(D.energy, q, ev);
