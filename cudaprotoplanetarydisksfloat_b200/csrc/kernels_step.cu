@@ -156,63 +156,77 @@ __device__ double compute_smoothing(const DiskDev& D, double r, float PT, float 
 
 // ---------------------------------------------------------------- planets (FP64)
 
+// The planet integrator runs on the 32 lanes of one warp: lane l takes
+// planets l, l+32, ... in the derivative and elements l, l+32, ... of the
+// Runge-Kutta combinations, each with the reference's expression, so the
+// result is the one thread's result bit for bit (nothing is reassociated);
+// __syncwarp orders the phases.
+
 // DerivMotionRK5, RungeKutta.cu:9-46; the planet-planet term divides by the
 // cube of the perturber's distance to the star, as the reference does.
 __device__ void deriv_motion(const DiskDev& D, const DiskCtl* C, const double* q, double* deriv, int nb,
-                             float dt, double* Dist) {
+                             float dt, double* Dist, int lane) {
   const double *x = q, *y = q + nb, *vx = q + 2 * nb, *vy = q + 3 * nb;
   double *dx = deriv, *dy = deriv + nb, *dvx = deriv + 2 * nb, *dvy = deriv + 3 * nb;
   // m_j / d_j / d_j / d_j depends on j alone: formed once per perturber (the
   // same expression, so the same bits), not once per pair; Dist holds the
   // distances in [0, nb) and these quotients in [nb, 2 nb)
   double* mD3 = Dist + nb;
-  for (int i = 0; i < nb; i++) {
+  for (int i = lane; i < nb; i += 32) {
     Dist[i] = sqrt(x[i] * x[i] + y[i] * y[i]);
     mD3[i] = 1.0 * C->mass[i] / Dist[i] / Dist[i] / Dist[i];
   }
-  for (int i = 0; i < nb; i++) {
-    dx[i] = vx[i];
-    dy[i] = vy[i];
-    dvx[i] = -1.0 * 1.0 / Dist[i] / Dist[i] / Dist[i] * x[i];
-    dvy[i] = -1.0 * 1.0 / Dist[i] / Dist[i] / Dist[i] * y[i];
+  __syncwarp();
+  for (int i = lane; i < nb; i += 32) {
+    double ax = -1.0 * 1.0 / Dist[i] / Dist[i] / Dist[i] * x[i];
+    double ay = -1.0 * 1.0 / Dist[i] / Dist[i] / Dist[i] * y[i];
     for (int j = 0; j < nb; j++) {
       if (D.Indirect_Term) {
-        dvx[i] -= mD3[j] * x[j];
-        dvy[i] -= mD3[j] * y[j];
+        ax -= mD3[j] * x[j];
+        ay -= mD3[j] * y[j];
       }
       if ((j != i) && C->feelothers[i]) {
-        dvx[i] += mD3[j] * (x[j] - x[i]);
-        dvy[i] += mD3[j] * (y[j] - y[i]);
+        ax += mD3[j] * (x[j] - x[i]);
+        ay += mD3[j] * (y[j] - y[i]);
       }
     }
+    dx[i] = vx[i] * dt;
+    dy[i] = vy[i] * dt;
+    dvx[i] = ax * dt;
+    dvy[i] = ay * dt;
   }
-  for (int i = 0; i < 4 * nb; i++) deriv[i] *= dt;
+  __syncwarp();
 }
 
 // RungeKutta, RungeKutta.cu:55-74 (Cash-Karp coefficients of the reference)
 __device__ void runge_kutta(const DiskDev& D, const DiskCtl* C, const double* q0, float dt, double* q1,
-                            double* k, int nb, double* Dist) {
+                            double* k, int nb, double* Dist, int lane) {
   const double c[5][5] = {{0.2, 0.0, 0.0, 0.0, 0.0},
                           {0.075, 0.225, 0.0, 0.0, 0.0},
                           {0.3, -0.9, 1.2, 0.0, 0.0},
                           {-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0.0},
                           {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
   int n4 = 4 * nb;
-  for (int s = 0; s < 6 * n4; s++) k[s] = 0.0;
-  deriv_motion(D, C, q0, k, nb, dt, Dist);
+  for (int s = lane; s < 6 * n4; s += 32) k[s] = 0.0;
+  __syncwarp();
+  deriv_motion(D, C, q0, k, nb, dt, Dist, lane);
   for (int s = 0; s < 5; s++) {
-    for (int i = 0; i < n4; i++)
+    for (int i = lane; i < n4; i += 32)
       q1[i] = q0[i] + c[s][0] * k[i] + c[s][1] * k[n4 + i] + c[s][2] * k[2 * n4 + i] +
               c[s][3] * k[3 * n4 + i] + c[s][4] * k[4 * n4 + i];
-    deriv_motion(D, C, q1, k + (s + 1) * n4, nb, dt, Dist);
+    __syncwarp();
+    deriv_motion(D, C, q1, k + (s + 1) * n4, nb, dt, Dist, lane);
   }
-  for (int i = 0; i < n4; i++)
+  for (int i = lane; i < n4; i += 32)
     q1[i] = q0[i] + 37.0 / 378.0 * k[i] + 250.0 / 621.0 * k[2 * n4 + i] + 125.0 / 594.0 * k[3 * n4 + i] +
             512.0 / 1771.0 * k[5 * n4 + i];
+  __syncwarp();
 }
 
-// AdvanceSystemRK5, Pframeforce.cu:94-157; work holds FARGO_RK_WORK(nb) doubles
-__device__ void advance_system_rk5(const DiskDev& D, DiskCtl* C, float dt, float PT, double* work) {
+// AdvanceSystemRK5, Pframeforce.cu:94-157; work holds FARGO_RK_WORK(nb)
+// doubles.  Called by the 32 lanes of one warp (the Runge-Kutta step is
+// lane-parallel, the rest runs on lane 0).
+__device__ void advance_system_rk5(const DiskDev& D, DiskCtl* C, float dt, float PT, double* work, int lane) {
   int nb = C->nb;
   double dtheta, omega, rdot, x, y, r, new_r, vx, vy, theta, denom;
   double* q0 = work;
@@ -220,14 +234,16 @@ __device__ void advance_system_rk5(const DiskDev& D, DiskCtl* C, float dt, float
   double* k = work + 8 * nb;
   double* Dist = work + 32 * nb;
   if (!D.ForcedCircular && nb > 0) {
-    for (int i = 0; i < nb; i++) {
+    for (int i = lane; i < nb; i += 32) {
       q0[i] = C->x[i];
       q0[i + nb] = C->y[i];
       q0[i + 2 * nb] = C->vx[i];
       q0[i + 3 * nb] = C->vy[i];
     }
-    runge_kutta(D, C, q0, dt, q1, k, nb, Dist);
+    __syncwarp();
+    runge_kutta(D, C, q0, dt, q1, k, nb, Dist, lane);
   }
+  if (lane != 0) return;
   for (int i = 1 - (PT >= D.RELEASEDATE); i < nb; i++) {
     if (!D.ForcedCircular) {
       C->x[i] = q1[i];
@@ -669,7 +685,8 @@ __device__ float block_min_f(float v, float* sh) {
 // that completed a disk's last CFL tile (or, for a radial stripe, by
 // k_stripe_finish once every stripe's partials are gathered).
 constexpr int kRkShared = 16;  // planets whose RK5 scratch fits in shared memory
-__device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const double* s_sum, double* work);
+__device__ bool finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const double* s_sum);
+__device__ void finish_serial_tail(const DiskDev& D, DiskCtl* C);
 
 // ConditionCFL host part (SourceEuler.cu:513-535): the shear limit DT1D
 // (ConditionCFLKernel2D2, Kernels.cu:1425-1428) of the ring pairs (i, i+1),
@@ -783,7 +800,15 @@ __device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* Cg, DiskCtl* s
     for (int k = tid; k < (int)(sizeof(DiskCtl) / 4); k += blockDim.x) dst[k] = src[k];
   }
   __syncthreads();
-  if (tid == 0) finish_serial(D, sC, newdt, s_sum, sC->nb <= kRkShared ? s_work : D.rk_work);
+  // the serial part on thread 0, the planet integrator on warp 0, the rest
+  // on thread 0 again
+  __shared__ int s_go;
+  if (tid == 0) s_go = finish_serial(D, sC, newdt, s_sum) ? 1 : 0;
+  __syncthreads();
+  if (s_go && tid < 32)
+    advance_system_rk5(D, sC, sC->dtf, sC->PhysicalTime, sC->nb <= kRkShared ? s_work : D.rk_work, tid);
+  __syncthreads();
+  if (s_go && tid == 0) finish_serial_tail(D, sC);
   __syncthreads();
   {
     const int* src = reinterpret_cast<const int*>(sC);
@@ -792,7 +817,9 @@ __device__ void finish_cfl_and_planets(const DiskDev& D, DiskCtl* Cg, DiskCtl* s
   }
 }
 
-__device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const double* s_sum, double* work) {
+// ... through AdvanceSystemFromDisk; false: the DT stopped (non-finite or
+// non-positive CFL step), nothing more to do
+__device__ bool finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const double* s_sum) {
   const int nbody = C->nbody;
   const float PT = C->PhysicalTime;
   double DTd = (double)D.DT;
@@ -811,7 +838,7 @@ __device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const d
       C->more = 0;
       C->active = 0;
       C->counter = 0;
-      return;
+      return false;
     }
     int n = (int)ceilf(q);
     dt = (DTd - C->dtemp) / (double)n;
@@ -865,7 +892,13 @@ __device__ void finish_serial(const DiskDev& D, DiskCtl* C, float newdt, const d
       C->vy[k] += dtf * C->ity;
     }
   }
-  advance_system_rk5(D, C, dtf, PT, work);
+  return true;
+}
+
+// The rest of the substep's scalars, after the planet integrator.
+__device__ void finish_serial_tail(const DiskDev& D, DiskCtl* C) {
+  const double dt = C->dt, DTd = (double)D.DT;
+  const float PT = C->PhysicalTime;
   C->domega = 0.0f;
   if (D.Corotating) {
     double OmegaNew = get_psys_info(D, C, 0) / dt;
