@@ -86,3 +86,70 @@ def test_error_vs_fp64(gpu, name, mode):
     # mass and angular momentum: the FP32 run drifts as the FP64 run does
     assert abs(drift["mass_f32"] - drift["mass_f64"]) <= 1e-5
     assert abs(drift["am_f32"] - drift["am_f64"]) <= 1e-5
+
+
+# The configurations' own run lengths (C1: 200 DTs, C2: 500 DTs), reference
+# mode, against the FP64 run of the same algorithm from the same start.
+# Measured on the B200: after 10 DTs Sigma is 2.1e-5 (C1) and 7.3e-5 (C2);
+# C1 stays near 4e-5 to DT 100 and reaches 1.2e-3 by DT 200, C2 grows
+# steadily to 7.9e-4 at DT 500 (v_r 2.1e-3, v_theta 3.2e-5, energy 6.3e-4,
+# planet orbits 7.7e-4 of their radius).  The two runs take discrete
+# decisions from their own arithmetic -- the substep count of a DT (the CFL
+# minimum against DT) and every ring's FARGO shift floor(Ntilde + 0.5) --
+# and a different decision changes that DT's time integration at first
+# order; the test counts the DTs where they differ (measured: C1 a FARGO
+# shift first differs at DT 26, in 2 DTs of 200; C2 at DT 30, in 77 DTs of
+# 500, and one DT of C2 takes another substep count).  Bounds are ~5x the
+# measured errors: they catch a broken long run, not rounding.
+LONG = {"C1": (200, {"dens": 6e-3, "vrad": 3e-3, "vtheta": 2e-4}),
+        "C2": (500, {"dens": 4e-3, "vrad": 1e-2, "vtheta": 2e-4, "energy": 3e-3})}
+
+
+@pytest.mark.parametrize("name", ["C1", "C2"])
+def test_long_run_vs_fp64(gpu, name):
+    ndt, bound = LONG[name]
+    P, L, _ = _case(name)
+    d = Disk(P, L)
+    f0 = d.fields()
+    d.init_state(dens=noise.perturb_density(f0["dens"].reshape(-1), P.NRAD, P.NSEC, SEED))
+    g = d.fields()
+    set_threads(16, "f64")
+    o = Oracle(P, L, prec="f64")
+    o.set_fields(dens=g["dens"], vrad=g["vrad"], vtheta=g["vtheta"], energy=g["energy"])
+    s0, q0 = d.scalars(), o.scalars()
+    nrad = P.NRAD
+    diff_nsub = diff_shift = 0
+    first_diff = None
+    for n in range(1, ndt + 1):
+        d.advance_dt()
+        o.advance_dt()
+        na, nb = d.scalars()["nsub_last_dt"], o.scalars()["nsub_last_dt"]
+        if na != nb:
+            diff_nsub += 1
+        elif not np.array_equal(d.substep_log()[0], o.substep_log()[0]):
+            diff_shift += 1
+        if first_diff is None and (diff_nsub or diff_shift):
+            first_diff = n
+        if n in (10, 100, ndt):
+            a, b = d.fields(), o.fields(native=True)
+            err = {k: rel_l2(a[k][:nrad], b[k][:nrad]) for k in ("dens", "vrad", "vtheta")}
+            if P.Adiabatic:
+                err["energy"] = rel_l2(a["energy"][:nrad], b["energy"][:nrad])
+            pa, pb = planets_dict(d.planets()), planets_dict(o.planets())
+            orbit = float(np.max(np.hypot(pa["x"] - pb["x"], pa["y"] - pb["y"]) / np.hypot(pb["x"], pb["y"])))
+            print("\n%s DT %d: rel-L2 vs FP64 %s; planet orbit %.2e; DTs with another substep count %d, "
+                  "with another FARGO shift %d (first at DT %s)" % (
+                      name, n, {k: "%.2e" % v for k, v in err.items()}, orbit, diff_nsub, diff_shift, first_diff))
+    s1, q1 = d.scalars(), o.scalars()
+    drift = {"mass_f32": (s1["mass"] - s0["mass"]) / s0["mass"], "mass_f64": (q1["mass"] - q0["mass"]) / q0["mass"],
+             "am_f32": (s1["angular_momentum"] - s0["angular_momentum"]) / s0["angular_momentum"],
+             "am_f64": (q1["angular_momentum"] - q0["angular_momentum"]) / q0["angular_momentum"]}
+    print("%s after %d DTs: drift %s" % (name, ndt, {k: "%.3e" % v for k, v in drift.items()}))
+    o.close()
+    d.close()
+    for k, e in err.items():
+        assert e <= bound[k], (k, e)
+    assert orbit <= 5e-3
+    assert abs(drift["mass_f32"] - drift["mass_f64"]) <= 1e-6
+    # angular momentum: the FP32 run drifts as the FP64 run does (C2: 1.28e-3 against 1.24e-3)
+    assert abs(drift["am_f32"] - drift["am_f64"]) <= 0.1 * abs(drift["am_f64"]) + 1e-5
