@@ -23,8 +23,8 @@
 //   k_ring_mean<1>   ring means of v_theta for FARGO: Nshift, residual
 //   k_transport      a band of 8 rings x one segment of source sectors per
 //                    CTA: momenta + radial van Leer from staged rows, residual
-//                    and constant azimuthal van Leer sweeps in registers,
-//                    shift applied on the store
+//                    and constant azimuthal van Leer sweeps (quantities in
+//                    pairs of FP32 lanes), shift applied on the store
 //   k_velocities     velocities from the transported momenta
 //   k_substep_end    disks still inside their DT -> graph loop condition
 //
@@ -1921,9 +1921,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_energy(BatchDev B) {
 // van Leer slope of StarRadKernel (Kernels.cu:917-927)
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
 
-// Paired FP32 arithmetic (Blackwell's two-lane FADD2 / FMUL2): each lane
-// rounds to nearest as the scalar operation does, so a pair of quantities
-// goes through one instruction with the same results bit for bit.
+// Paired FP32 arithmetic (Blackwell's two-lane FADD2 / FMUL2, round to
+// nearest): a pair of quantities goes through one instruction.  The paired
+// transport agrees with the oracle within the same tolerances as the scalar
+// form; it is not bit-identical to a scalar build of the same expressions.
 __device__ __forceinline__ float2 bc2(float x) { return make_float2(x, x); }
 __device__ __forceinline__ float2 m2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 a2(float2 a, float2 b) { return __fadd2_rn(a, b); }
@@ -2255,6 +2256,172 @@ size_t fargo_transport_smem_bytes(int adiabatic) {
 }
 static_assert((kPad * 4) % 16 == 0 && (kRow * 4) % 16 == 0, "staged rows 16-byte aligned");
 
+#ifndef FARGO_NOFMA
+// One van Leer pass of OneWindTheta on the window (see sweep_ring).  kind 0:
+// every point's own velocity v[k] (the residual sweep); kind 1 / 2: one
+// velocity vu for the whole ring (the constant-residual sweep), whose
+// interfaces all take their upwind value from the left (1: vu dt > 0) or
+// from the right (2), at the same distance h: no per-point selects.
+// The quantities stay in the ring's shared-memory rows (each lane reads and
+// writes only its own 8 points there); they are processed two at a time as
+// the lanes of paired FP32 operations (each lane rounds as the scalar
+// operation), with an odd last quantity -- the density -- on its own.
+template <int nq, int kind>
+__device__ __forceinline__ void sweep_pass(float* sRr, int b0, const float (&v)[8], float vu, float dt,
+                                           float dxtheta, float invdxtheta, float invsurf, float dxrad) {
+  auto slope = [&](float wm, float w0, float wp) -> float {
+    float dqm = (w0 - wm);
+    float dqp = (wp - w0);
+    if (fm(dqp, dqm) > 0.0f) return fm(__fdividef(fm(dqp, dqm), dqp + dqm), invdxtheta);
+    return 0.0f;
+  };
+  auto slope2 = [&](float2 wm, float2 w0, float2 wp) -> float2 {
+    const float2 dqm = s2(w0, wm);
+    const float2 dqp = s2(wp, w0);
+    const float2 t = m2(dqp, dqm);
+    const float2 den = a2(dqp, dqm);
+    const float2 g = m2(make_float2(__fdividef(t.x, den.x), __fdividef(t.y, den.y)), bc2(invdxtheta));
+    return make_float2(t.x > 0.0f ? g.x : 0.0f, t.y > 0.0f ? g.y : 0.0f);
+  };
+  auto shup2 = [](float2 x) -> float2 {
+    return make_float2(__shfl_up_sync(0xffffffffu, x.x, 1), __shfl_up_sync(0xffffffffu, x.y, 1));
+  };
+  auto shdn2 = [](float2 x) -> float2 {
+    return make_float2(__shfl_down_sync(0xffffffffu, x.x, 1), __shfl_down_sync(0xffffffffu, x.y, 1));
+  };
+  // upwind side of each point's left interface and the distance to it:
+  // ksi > 0 takes point k-1 at dxtheta - ksi, else point k at -(dxtheta + ksi)
+  float vv[8], rr[8], S[8], GS[8], sD[8], h[8];
+  unsigned up = 0;
+  const float ksu = fm(vu, dt);
+  const float hu = (kind == 1) ? dxtheta - ksu : dxtheta + ksu;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    vv[k] = (kind == 0) ? v[k] : vu;
+    S[k] = sRr[(nq - 1) * kPad + b0 + k];
+    rr[k] = __fdividef(1.0f, S[k] + 1e-20f);
+    if (kind == 0) {
+      const float ksi = fm(vv[k], dt);
+      if (ksi > 0.0f) up |= 1u << k;
+      h[k] = (ksi > 0.0f) ? dxtheta - ksi : dxtheta + ksi;
+    } else {
+      h[k] = hu;
+    }
+  }
+  auto is_left = [&](int k) -> bool { return kind == 0 ? ((up >> k) & 1u) != 0 : kind == 1; };
+  const float Sl = __shfl_up_sync(0xffffffffu, S[7], 1);
+  const float Sr = __shfl_down_sync(0xffffffffu, S[0], 1);
+#pragma unroll
+  for (int k = 0; k < 8; k++) GS[k] = slope(k ? S[k - 1] : Sl, S[k], k < 7 ? S[k + 1] : Sr);
+  const float GSl = (kind == 2) ? 0.0f : __shfl_up_sync(0xffffffffu, GS[7], 1);
+  // DensStar (StarThetaKernel2 on the density); a - fm(h, g) = a + fm(h, -g)
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const bool u = is_left(k);
+    const float su = u ? (k ? S[k - 1] : Sl) : S[k];
+    const float gu = u ? (k ? GS[k - 1] : GSl) : -GS[k];
+    sD[k] = su + fm(h[k], gu);
+  }
+  // every quantity, density last; all quotients use the pre-sweep density
+  constexpr int npair = nq / 2;
+#pragma unroll
+  for (int c2 = 0; c2 < npair; c2++) {
+    float* r0 = sRr + (2 * c2) * kPad + b0;
+    float* r1 = r0 + kPad;
+    float2 W[8], G[8], F[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) W[k] = m2(make_float2(r0[k], r1[k]), bc2(rr[k]));
+    const float2 Wl = shup2(W[7]);
+    const float2 Wr = shdn2(W[0]);
+#pragma unroll
+    for (int k = 0; k < 8; k++) G[k] = slope2(k ? W[k - 1] : Wl, W[k], k < 7 ? W[k + 1] : Wr);
+    const float2 Gl = (kind == 2) ? bc2(0.0f) : shup2(G[7]);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const bool u = is_left(k);
+      const float2 wu = u ? (k ? W[k - 1] : Wl) : W[k];
+      const float2 gu = u ? (k ? G[k - 1] : Gl) : make_float2(-G[k].x, -G[k].y);
+      const float2 qr = a2(wu, m2(bc2(h[k]), gu));
+      F[k] = m2(m2(m2(bc2(dxrad), qr), bc2(sD[k])), bc2(vv[k]));  // flux through the left interface
+    }
+    const float2 Fr = shdn2(F[0]);
+    asm volatile("" ::: "memory");  // reread the rows rather than keep them in registers
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const float2 varq = s2(F[k], k < 7 ? F[k + 1] : Fr);
+      const float2 q = a2(make_float2(r0[k], r1[k]), m2(varq, bc2(invsurf)));  // unchanged rows: reread
+      r0[k] = q.x;
+      r1[k] = q.y;
+    }
+  }
+  if (nq & 1) {  // the density, on its own
+    asm volatile("" ::: "memory");  // reread the density rather than keep it in registers
+    float* r0 = sRr + (nq - 1) * kPad + b0;
+    float W[8], G[8], F[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) W[k] = fm(r0[k], rr[k]);  // the pre-sweep density S
+    const float Wl = __shfl_up_sync(0xffffffffu, W[7], 1);
+    const float Wr = __shfl_down_sync(0xffffffffu, W[0], 1);
+#pragma unroll
+    for (int k = 0; k < 8; k++) G[k] = slope(k ? W[k - 1] : Wl, W[k], k < 7 ? W[k + 1] : Wr);
+    const float Gl = (kind == 2) ? 0.0f : __shfl_up_sync(0xffffffffu, G[7], 1);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const bool u = is_left(k);
+      const float wu = u ? (k ? W[k - 1] : Wl) : W[k];
+      const float gu = u ? (k ? G[k - 1] : Gl) : -G[k];
+      const float qr = wu + fm(h[k], gu);
+      F[k] = fm(fm(fm(dxrad, qr), sD[k]), vv[k]);
+    }
+    const float Fr = __shfl_down_sync(0xffffffffu, F[0], 1);
+    asm volatile("" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      float varq = F[k];
+      varq -= (k < 7 ? F[k + 1] : Fr);
+      r0[k] = r0[k] + fm(varq, invsurf);
+    }
+  }
+}
+
+// The residual and constant-residual van Leer sweeps of OneWindTheta
+// (StarThetaKernel, StarThetaKernel2, VanLeerThetaKernel, Kernels.cu:1157-1273)
+// on one ring's window of 256 points, by one warp: lane l holds points
+// 8l .. 8l+7 and takes its neighbours' edge values by shuffle.
+// sRr: the ring's radial results [nq][kPad] and v_theta [kPad] (point x at
+// pidx(x)); the swept values go back to the same places.  The window's
+// points 0..3 and L-4.. (and any beyond L) are halo: each sweep's result at
+// a point depends on the points within two of it, so after the two sweeps
+// the values at 4 .. L-5 do not depend on anything outside the window and
+// the edges need no special case (their values are never stored).
+// The second sweep's velocity is the ring's constant residual: one upwind
+// side for the whole ring (a warp-uniform branch), and none of it when that
+// residual is exactly zero (every flux is then zero: the quantities are
+// unchanged, as the reference's q + 0 leaves them).
+template <int nq>
+__device__ __forceinline__ void sweep_ring(float* sRr, float VMed, float vconst, bool fast, float dt,
+                                           float dxtheta, float invdxtheta, float invsurf, float dxrad) {
+  const int lane = threadIdx.x & 31;
+  const int b0 = 9 * lane;  // pidx(8 * lane): points 8l .. 8l+7 are contiguous
+  float v[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    float vres = sRr[nq * kPad + b0 + k] - VMed;
+    if (!fast) vres = vconst + vres;
+    v[k] = vres;
+  }
+  if (!fast) vconst = 0.0f;
+  sweep_pass<nq, 0>(sRr, b0, v, 0.0f, dt, dxtheta, invdxtheta, invsurf, dxrad);
+  if (fm(vconst, dt) > 0.0f)
+    sweep_pass<nq, 1>(sRr, b0, v, vconst, dt, dxtheta, invdxtheta, invsurf, dxrad);
+  else if (vconst != 0.0f)
+    sweep_pass<nq, 2>(sRr, b0, v, vconst, dt, dxtheta, invdxtheta, invsurf, dxrad);
+  __syncwarp();  // the ring's swept values, lane by lane, before the shifted store
+}
+
+#else
+// The accurate mode's kernel set keeps the scalar sweeps with the
+// quantities in registers, the form its FP64 error was measured with.
 // One van Leer pass of OneWindTheta on the window (see sweep_ring).  kind 0:
 // every point's own velocity v[k] (the residual sweep); kind 1 / 2: one
 // velocity vu for the whole ring (the constant-residual sweep), whose
@@ -2372,6 +2539,8 @@ __device__ __forceinline__ void sweep_ring(float* sRr, float VMed, float vconst,
     for (int c = 0; c < nq; c++) sRr[c * kPad + b0 + k] = q[c][k];
   __syncwarp();
 }
+
+#endif
 
 // ---- TMA staging: mbarrier and bulk tensor copy (one CTA, no cluster) ----
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
