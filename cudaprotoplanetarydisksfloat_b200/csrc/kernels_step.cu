@@ -2267,7 +2267,8 @@ static_assert((kPad * 4) % 16 == 0 && (kRow * 4) % 16 == 0, "staged rows 16-byte
 // The quantities stay in the ring's shared-memory rows (each lane reads and
 // writes only its own 8 points there); they are processed two at a time as
 // the lanes of paired FP32 operations (each lane rounds as the scalar
-// operation), with an odd last quantity -- the density -- on its own.
+// operation); with an odd count the last quantity, the density, shares a
+// pair with its own star value.
 template <int nq, int kind>
 __device__ __forceinline__ void sweep_pass(float* sRr, int b0, const float (&v)[8], float vu, float dt,
                                            float dxtheta, float invdxtheta, float invsurf, float dxrad) {
@@ -2311,20 +2312,53 @@ __device__ __forceinline__ void sweep_pass(float* sRr, int b0, const float (&v)[
     }
   }
   auto is_left = [&](int k) -> bool { return kind == 0 ? ((up >> k) & 1u) != 0 : kind == 1; };
-  const float Sl = __shfl_up_sync(0xffffffffu, S[7], 1);
-  const float Sr = __shfl_down_sync(0xffffffffu, S[0], 1);
+  if constexpr ((nq & 1) == 0) {
+    const float Sl = __shfl_up_sync(0xffffffffu, S[7], 1);
+    const float Sr = __shfl_down_sync(0xffffffffu, S[0], 1);
 #pragma unroll
-  for (int k = 0; k < 8; k++) GS[k] = slope(k ? S[k - 1] : Sl, S[k], k < 7 ? S[k + 1] : Sr);
-  const float GSl = (kind == 2) ? 0.0f : __shfl_up_sync(0xffffffffu, GS[7], 1);
-  // DensStar (StarThetaKernel2 on the density); a - fm(h, g) = a + fm(h, -g)
+    for (int k = 0; k < 8; k++) GS[k] = slope(k ? S[k - 1] : Sl, S[k], k < 7 ? S[k + 1] : Sr);
+    const float GSl = (kind == 2) ? 0.0f : __shfl_up_sync(0xffffffffu, GS[7], 1);
+    // DensStar (StarThetaKernel2 on the density); a - fm(h, g) = a + fm(h, -g)
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const bool u = is_left(k);
-    const float su = u ? (k ? S[k - 1] : Sl) : S[k];
-    const float gu = u ? (k ? GS[k - 1] : GSl) : -GS[k];
-    sD[k] = su + fm(h[k], gu);
+    for (int k = 0; k < 8; k++) {
+      const bool u = is_left(k);
+      const float su = u ? (k ? S[k - 1] : Sl) : S[k];
+      const float gu = u ? (k ? GS[k - 1] : GSl) : -GS[k];
+      sD[k] = su + fm(h[k], gu);
+    }
+  } else {
+    // odd count (the isothermal density last): DensStar and the density's own
+    // interface value are the same slope and upwind expressions, on Sigma and
+    // on Sigma / (Sigma + 1e-20): the two lanes of one pair.  The density row
+    // is updated at once (the pairs below read only their own rows).
+    float2 X[8], GX[8], FX[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) X[k] = make_float2(S[k], fm(S[k], rr[k]));
+    const float2 Xl = shup2(X[7]);
+    const float2 Xr = shdn2(X[0]);
+#pragma unroll
+    for (int k = 0; k < 8; k++) GX[k] = slope2(k ? X[k - 1] : Xl, X[k], k < 7 ? X[k + 1] : Xr);
+    const float2 GXl = (kind == 2) ? bc2(0.0f) : shup2(GX[7]);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const bool u = is_left(k);
+      const float2 xu = u ? (k ? X[k - 1] : Xl) : X[k];
+      const float2 gu = u ? (k ? GX[k - 1] : GXl) : make_float2(-GX[k].x, -GX[k].y);
+      const float2 st = a2(xu, m2(bc2(h[k]), gu));  // (DensStar, the density's QRStar)
+      sD[k] = st.x;
+      FX[k].x = fm(fm(fm(dxrad, st.y), st.x), vv[k]);  // the density's flux, left interface
+    }
+    const float Fr = __shfl_down_sync(0xffffffffu, FX[0].x, 1);
+    float* rd = sRr + (nq - 1) * kPad + b0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      float varq = FX[k].x;
+      varq -= (k < 7 ? FX[k + 1].x : Fr);
+      rd[k] = S[k] + fm(varq, invsurf);
+    }
   }
-  // every quantity, density last; all quotients use the pre-sweep density
+  // the paired quantities (with an even count the last pair holds the
+  // density); all quotients use the pre-sweep density
   constexpr int npair = nq / 2;
 #pragma unroll
   for (int c2 = 0; c2 < npair; c2++) {
@@ -2354,34 +2388,6 @@ __device__ __forceinline__ void sweep_pass(float* sRr, int b0, const float (&v)[
       const float2 q = a2(make_float2(r0[k], r1[k]), m2(varq, bc2(invsurf)));  // unchanged rows: reread
       r0[k] = q.x;
       r1[k] = q.y;
-    }
-  }
-  if (nq & 1) {  // the density, on its own
-    asm volatile("" ::: "memory");  // reread the density rather than keep it in registers
-    float* r0 = sRr + (nq - 1) * kPad + b0;
-    float W[8], G[8], F[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) W[k] = fm(r0[k], rr[k]);  // the pre-sweep density S
-    const float Wl = __shfl_up_sync(0xffffffffu, W[7], 1);
-    const float Wr = __shfl_down_sync(0xffffffffu, W[0], 1);
-#pragma unroll
-    for (int k = 0; k < 8; k++) G[k] = slope(k ? W[k - 1] : Wl, W[k], k < 7 ? W[k + 1] : Wr);
-    const float Gl = (kind == 2) ? 0.0f : __shfl_up_sync(0xffffffffu, G[7], 1);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const bool u = is_left(k);
-      const float wu = u ? (k ? W[k - 1] : Wl) : W[k];
-      const float gu = u ? (k ? G[k - 1] : Gl) : -G[k];
-      const float qr = wu + fm(h[k], gu);
-      F[k] = fm(fm(fm(dxrad, qr), sD[k]), vv[k]);
-    }
-    const float Fr = __shfl_down_sync(0xffffffffu, F[0], 1);
-    asm volatile("" ::: "memory");
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      float varq = F[k];
-      varq -= (k < 7 ? F[k + 1] : Fr);
-      r0[k] = r0[k] + fm(varq, invsurf);
     }
   }
 }
